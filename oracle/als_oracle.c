@@ -1,0 +1,660 @@
+/*
+ * CPU restatement of alsfvm's cell-update hot path (test oracle).
+ *
+ * TEST INFRASTRUCTURE ONLY -- see als_oracle.h.  Compiled with
+ * -ffp-contract=off so that every a*b+c is two rounded operations, like the
+ * reference CPU build; every expression keeps the reference's evaluation
+ * order, which is cited beside it.
+ */
+#include "als_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define WENO_EPS 1e-8 /* WENOCoefficients.hpp:21 */
+
+/* ---------------------------------------------------------------- Euler */
+
+/* Conserved state plus the extra variables p and u of one cell
+ * (AllVariables, Euler.hpp:96-101,204-211, 279-284). */
+typedef struct {
+    double rho, m[3], E;
+    double p, u[3];
+} state_t;
+
+static void make_all(int nsd, double gamma, double rho, const double* m, double E,
+    state_t* s) {
+    double dot = 0.0;
+    int k;
+    s->rho = rho;
+    s->E = E;
+    for (k = 0; k < 3; ++k) {
+        s->m[k] = k < nsd ? m[k] : 0.0;
+    }
+    /* vec dot: x*x + y*y + z*z, left to right (vec1/2/3.hpp dot) */
+    dot = s->m[0] * s->m[0];
+    if (nsd > 1) {
+        dot = dot + s->m[1] * s->m[1];
+    }
+    if (nsd > 2) {
+        dot = dot + s->m[2] * s->m[2];
+    }
+    /* ie = E - 0.5 * m.m / rho  (Euler.hpp:207) */
+    {
+        double ie = E - 0.5 * dot / rho;
+        for (k = 0; k < 3; ++k) {
+            s->u[k] = k < nsd ? s->m[k] / rho : 0.0; /* Euler.hpp:208 */
+        }
+        s->p = (gamma - 1) * ie; /* Euler.hpp:209 */
+    }
+}
+
+/* Point flux in direction d (Euler.hpp:172-181). */
+static void point_flux(int nsd, int d, const state_t* s, double* F) {
+    int k;
+    F[0] = s->m[d];
+    for (k = 0; k < nsd; ++k) {
+        F[1 + k] = s->m[k] * s->u[d];
+    }
+    F[1 + d] = F[1 + d] + s->p;
+    F[1 + nsd] = (s->E + s->p) * s->u[d];
+}
+
+static void conserved_of(int nsd, const state_t* s, double* U) {
+    int k;
+    U[0] = s->rho;
+    for (k = 0; k < nsd; ++k) {
+        U[1 + k] = s->m[k];
+    }
+    U[1 + nsd] = s->E;
+}
+
+/* HLL, HLL.hpp:51-116. */
+static double flux_hll(int nsd, int d, double gamma, const state_t* L, const state_t* R,
+    double* F) {
+    const int nv = nsd + 2;
+    const double wl = sqrt(L->rho);
+    const double wr = sqrt(R->rho);
+    const double rho = (L->rho + R->rho) / 2;
+    const double ud = (wl * L->u[d] + wr * R->u[d]) / (wl + wr);
+    const double p = (L->p * wl + R->p * wr) / (wl + wr);
+    const double cs = sqrt(gamma * p / rho);
+    const double sL = fmin(L->u[d] - sqrt(gamma * L->p / L->rho), ud - cs);
+    const double sR = fmax(R->u[d] + sqrt(gamma * R->p / R->rho), ud + cs);
+    int k;
+    if (sL == 0) {
+        for (k = 0; k < nv; ++k) {
+            F[k] = 0;
+        }
+    } else if (sL > 0) {
+        point_flux(nsd, d, L, F);
+    } else if (sR < 0) {
+        point_flux(nsd, d, R, F);
+    } else {
+        double FL[5], FR[5], UL[5], UR[5];
+        point_flux(nsd, d, L, FL);
+        point_flux(nsd, d, R, FR);
+        conserved_of(nsd, L, UL);
+        conserved_of(nsd, R, UR);
+        for (k = 0; k < nv; ++k) {
+            F[k] = (sR * FL[k] - sL * FR[k] + sR * sL * (UR[k] - UL[k])) / (sR - sL);
+        }
+    }
+    return fmax(fabs(sL), fabs(sR));
+}
+
+/* HLL3, HLL3.hpp:52-149. */
+static double flux_hll3(int nsd, int d, double gamma, const state_t* L, const state_t* R,
+    double* F) {
+    const int nv = nsd + 2;
+    const double wl = sqrt(L->rho);
+    const double wr = sqrt(R->rho);
+    const double rho = (L->rho + R->rho) / 2;
+    const double ud = (wl * L->u[d] + wr * R->u[d]) / (wl + wr);
+    const double p = (wl * L->p + wr * R->p) / (wl + wr);
+    const double cfL = sqrt(gamma * L->p / L->rho);
+    const double cfR = sqrt(gamma * R->p / R->rho);
+    const double correct = 0.5 * fmax(0.0, L->u[d] - R->u[d]);
+    const double cs = sqrt(gamma * p / rho);
+    const double sL = fmin(L->u[d] + correct - cfL, ud - cs);
+    const double sR = fmax(R->u[d] - correct + cfR, ud + cs);
+    double FL[5], FR[5], us[3];
+    int k;
+    point_flux(nsd, d, L, FL);
+    point_flux(nsd, d, R, FR);
+    {
+        const double pL = L->p, pR = R->p;
+        const double udl = L->u[d] - sL;
+        const double udr = R->u[d] - sR;
+        const double aa = udr * R->rho - udl * L->rho;
+        const double sm = (R->m[d] * udr - L->m[d] * udl + pR - pL) / aa;
+        for (k = 0; k < nsd; ++k) {
+            us[k] = (FR[1 + k] - FL[1 + k] - sR * R->m[k] + sL * L->m[k]) / aa;
+        }
+        us[d] = sm;
+        if (sL == 0) {
+            for (k = 0; k < nv; ++k) {
+                F[k] = 0;
+            }
+        } else if (sL > 0) {
+            for (k = 0; k < nv; ++k) {
+                F[k] = FL[k];
+            }
+        } else if (sR < 0) {
+            for (k = 0; k < nv; ++k) {
+                F[k] = FR[k];
+            }
+        } else if (sm >= 0) {
+            double mid[5], U[5];
+            mid[0] = L->rho * udl / (sm - sL);
+            for (k = 0; k < nsd; ++k) {
+                mid[1 + k] = us[k] * mid[0];
+            }
+            {
+                const double ps = pL + L->rho * (L->u[d] - sm) * udl;
+                mid[1 + nsd] = (udl * L->E + pL * L->u[d] - ps * sm) / (sm - sL);
+            }
+            conserved_of(nsd, L, U);
+            for (k = 0; k < nv; ++k) {
+                F[k] = FL[k] + sL * (mid[k] - U[k]);
+            }
+        } else {
+            double mid[5], U[5];
+            mid[0] = R->rho * udr / (sm - sR);
+            for (k = 0; k < nsd; ++k) {
+                mid[1 + k] = us[k] * mid[0];
+            }
+            {
+                const double ps = pR + R->rho * (R->u[d] - sm) * udr;
+                mid[1 + nsd] = (udr * R->E + pR * R->u[d] - ps * sm) / (sm - sR);
+            }
+            conserved_of(nsd, R, U);
+            for (k = 0; k < nv; ++k) {
+                F[k] = FR[k] + sR * (mid[k] - U[k]);
+            }
+        }
+    }
+    return fmax(fabs(sL), fabs(sR));
+}
+
+/* Central, Central.hpp:39-56; wave speed Euler.hpp:251-258. */
+static double flux_central(int nsd, int d, double gamma, const state_t* L,
+    const state_t* R, double* F) {
+    const int nv = nsd + 2;
+    double FL[5], FR[5];
+    int k;
+    point_flux(nsd, d, L, FL);
+    point_flux(nsd, d, R, FR);
+    for (k = 0; k < nv; ++k) {
+        F[k] = 0.5 * (FL[k] + FR[k]);
+    }
+    return fmax(fabs(L->u[d]) + sqrt(gamma * L->p / L->rho),
+            fabs(R->u[d]) + sqrt(gamma * R->p / R->rho));
+}
+
+/* -------------------------------------------------------------- helpers */
+
+int orc_ghost_cells(int flux, int recon) {
+    int rg = 1;
+    (void)flux; /* every in-scope flux has the two-point stencil {0, 1} */
+    switch (recon) {
+    case ORC_RECON_NONE: rg = 1; break;
+    case ORC_RECON_WENO2: rg = 2; break;
+    case ORC_RECON_ENO2: rg = 2; break;
+    case ORC_RECON_ENO3: rg = 3; break;
+    case ORC_RECON_ENO4: rg = 4; break;
+    default: return -1;
+    }
+    return rg > 1 ? rg : 1;
+}
+
+int orc_configure(orc_config* cfg, int dim, const int* n, const double* lower,
+    const double* upper, int flux, int recon, int integrator, int bc, double gamma) {
+    int d;
+    if (dim < 1 || dim > 3) {
+        return -1;
+    }
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->dim = dim;
+    for (d = 0; d < 3; ++d) {
+        cfg->n[d] = d < dim ? n[d] : 1;
+    }
+    cfg->g = orc_ghost_cells(flux, recon);
+    if (cfg->g < 0) {
+        return -1;
+    }
+    cfg->gamma = gamma;
+    cfg->flux = flux;
+    cfg->recon = recon;
+    cfg->integrator = integrator;
+    cfg->bc = bc;
+    for (d = 0; d < 3; ++d) {
+        /* Grid.cpp:30-38: (top-origin)/n, and 1 for directions with one cell */
+        cfg->dx[d] = (upper[d] - lower[d]) / (double)cfg->n[d];
+        if (d > 0 && cfg->n[d] == 1) {
+            cfg->dx[d] = 1;
+        }
+    }
+    return 0;
+}
+
+static void padded(const orc_config* cfg, int* N) {
+    int d;
+    for (d = 0; d < 3; ++d) {
+        N[d] = cfg->n[d] + (d < cfg->dim ? 2 * cfg->g : 0);
+    }
+}
+
+long orc_plane_size(const orc_config* cfg) {
+    int N[3];
+    padded(cfg, N);
+    return (long)N[0] * N[1] * N[2];
+}
+
+static long idx3(const int* N, int x, int y, int z) {
+    return ((long)z * N[1] + y) * N[0] + x;
+}
+
+/* ------------------------------------------------------------- boundary */
+
+void orc_fill_ghosts(const orc_config* cfg, double* planes, int nvar) {
+    int N[3];
+    const int g = cfg->g;
+    const long plane = orc_plane_size(cfg);
+    int var, d, side;
+    padded(cfg, N);
+    for (var = 0; var < nvar; ++var) {
+        double* u = planes + var * plane;
+        for (d = 0; d < cfg->dim; ++d) {
+            for (side = 0; side < 2; ++side) {
+                /* the side loop covers the full transverse extent, ghosts included */
+                int x, y, z, k;
+                const int n = cfg->n[d];
+                const int first = side == 0 ? g : N[d] - g - 1;
+                for (z = 0; z < (d == 2 ? 1 : N[2]); ++z) {
+                    for (y = 0; y < (d == 1 ? 1 : N[1]); ++y) {
+                        for (x = 0; x < (d == 0 ? 1 : N[0]); ++x) {
+                            int c[3];
+                            c[0] = x;
+                            c[1] = y;
+                            c[2] = z;
+                            for (k = 1; k <= g; ++k) {
+                                int dst[3], src[3];
+                                memcpy(dst, c, sizeof(dst));
+                                memcpy(src, c, sizeof(src));
+                                if (cfg->bc == ORC_BC_NEUMANN) {
+                                    /* mirror: ghost[g-k] = U[g+k-1], ghost[N-g-1+k] = U[N-g-k] */
+                                    dst[d] = side == 0 ? first - k : first + k;
+                                    src[d] = side == 0 ? first + (k - 1) : first - (k - 1);
+                                } else {
+                                    /* periodic: ghost[g-k] = U[g-k+n], ghost[N-g-1+k] = U[N-g-1+k-n] */
+                                    dst[d] = side == 0 ? first - k : first + k;
+                                    src[d] = side == 0 ? first + (n - k) : first - (n - k);
+                                }
+                                u[idx3(N, dst[0], dst[1], dst[2])] =
+                                    u[idx3(N, src[0], src[1], src[2])];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------- reconstruction */
+
+static const double eno2c[3][2] = {
+    {3.0 / 2.0, -1.0 / 2.0},
+    {1.0 / 2.0, 1.0 / 2.0},
+    {-1.0 / 2.0, 3.0 / 2.0}
+};
+static const double eno3c[4][3] = {
+    {11.0 / 6.0, -7.0 / 6.0, 1.0 / 3.0},
+    {1.0 / 3.0, 5.0 / 6.0, -1.0 / 6.0},
+    {-1.0 / 6.0, 5.0 / 6.0, 1.0 / 3.0},
+    {1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0}
+};
+static const double eno4c[5][4] = {
+    {25.0 / 12.0, -23.0 / 12.0, 13.0 / 12.0, -1.0 / 4.0},
+    {1.0 / 4.0, 13.0 / 12.0, -5.0 / 12.0, 1.0 / 12.0},
+    {-1.0 / 12.0, 7.0 / 12.0, 7.0 / 12.0, -1.0 / 12.0},
+    {1.0 / 12.0, -5.0 / 12.0, 13.0 / 12.0, 1.0 / 4.0},
+    {-1.0 / 4.0, 13.0 / 12.0, -23.0 / 12.0, 25.0 / 12.0}
+};
+
+static double eno_coef(int order, int r, int j) {
+    switch (order) {
+    case 2: return eno2c[r][j];
+    case 3: return eno3c[r][j];
+    default: return eno4c[r][j];
+    }
+}
+
+/* Reconstructs cell c (index into the planes) along stride s.
+ * left/right receive nvar values. */
+static void reconstruct_cell(const orc_config* cfg, const double* in, long plane,
+    long c, long s, int nvar, double* left, double* right) {
+    int var;
+    if (cfg->recon == ORC_RECON_NONE) {
+        for (var = 0; var < nvar; ++var) {
+            left[var] = in[var * plane + c];
+            right[var] = in[var * plane + c];
+        }
+    } else if (cfg->recon == ORC_RECON_WENO2) {
+        /* WENO2.hpp:37-69; the indicator is rho (Euler.hpp:286-288) */
+        const double i0 = in[c];
+        const double b0 = (in[c + s] - i0) * (in[c + s] - i0);
+        const double b1 = (i0 - in[c - s]) * (i0 - in[c - s]);
+        const double a0Left = 1 / (3 * (WENO_EPS + b0) * (WENO_EPS + b0));
+        const double a1Left = 2 / (3 * (WENO_EPS + b1) * (WENO_EPS + b1));
+        const double w0Left = a0Left / (a0Left + a1Left);
+        const double w1Left = a1Left / (a0Left + a1Left);
+        const double a0Right = 2 / (3 * (WENO_EPS + b0) * (WENO_EPS + b0));
+        const double a1Right = 1 / (3 * (WENO_EPS + b1) * (WENO_EPS + b1));
+        const double w0Right = a0Right / (a0Right + a1Right);
+        const double w1Right = a1Right / (a0Right + a1Right);
+        for (var = 0; var < nvar; ++var) {
+            const double um = in[var * plane + c - s];
+            const double u0 = in[var * plane + c];
+            const double up = in[var * plane + c + s];
+            left[var] = 0.5 * (w1Left * um + (3 * w0Left + w1Left) * u0 - w0Left * up);
+            right[var] = 0.5 * (w0Right * up + (3 * w1Right + w0Right) * u0 - w1Right * um);
+        }
+    } else {
+        /* ENOCPU.cpp:140-180.  Level-l undivided differences of rho:
+         * DD0[i] = rho[i+1]-rho[i], DDl[i] = DD(l-1)[i+1]-DD(l-1)[i]
+         * (ENOCPU.cpp:205-267); compare |DD[i-1]| < |DD[i]| per level. */
+        const int order = cfg->recon == ORC_RECON_ENO2 ? 2 : (cfg->recon == ORC_RECON_ENO3 ? 3 : 4);
+        int shift = 0, level, j, k;
+        double dd[5]; /* dd[k+1] = level difference at offset k*s from c, k = -1..3 */
+        for (k = -1; k <= order - 2; ++k) {
+            dd[k + 1] = in[c + (k + 1) * s] - in[c + k * s];
+        }
+        for (level = 0; level < order - 1; ++level) {
+            if (level > 0) {
+                for (k = -1; k <= order - 2 - level; ++k) {
+                    dd[k + 1] = dd[k + 2] - dd[k + 1];
+                }
+            }
+            if (fabs(dd[0]) < fabs(dd[1])) {
+                shift++;
+            }
+        }
+        for (var = 0; var < nvar; ++var) {
+            double lv = 0.0, rv = 0.0;
+            for (j = 0; j < order; ++j) {
+                const double value = in[var * plane + c - (long)(shift - j) * s];
+                lv += eno_coef(order, shift, j) * value;
+                rv += eno_coef(order, shift + 1, j) * value;
+            }
+            left[var] = lv;
+            right[var] = rv;
+        }
+    }
+}
+
+void orc_reconstruct(const orc_config* cfg, int dir, const double* in, double* left,
+    double* right) {
+    int N[3];
+    const int g = cfg->g;
+    const int nvar = cfg->dim + 2;
+    const long plane = orc_plane_size(cfg);
+    long s;
+    int lo[3], hi[3], d, x, y, z, var;
+    padded(cfg, N);
+    s = dir == 0 ? 1 : (dir == 1 ? N[0] : (long)N[0] * N[1]);
+    for (d = 0; d < 3; ++d) {
+        const int gd = d < cfg->dim ? g : 0;
+        lo[d] = gd - (d == dir ? 1 : 0);
+        hi[d] = N[d] - gd + (d == dir ? 1 : 0);
+    }
+    for (z = lo[2]; z < hi[2]; ++z) {
+        for (y = lo[1]; y < hi[1]; ++y) {
+            for (x = lo[0]; x < hi[0]; ++x) {
+                double l[5], r[5];
+                const long c = idx3(N, x, y, z);
+                reconstruct_cell(cfg, in, plane, c, s, nvar, l, r);
+                for (var = 0; var < nvar; ++var) {
+                    left[var * plane + c] = l[var];
+                    right[var * plane + c] = r[var];
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------ net flux */
+
+static double face_flux(const orc_config* cfg, int d, const double* ul, const double* ur,
+    double* F) {
+    const int nsd = cfg->dim;
+    state_t L, R;
+    make_all(nsd, cfg->gamma, ul[0], ul + 1, ul[1 + nsd], &L);
+    make_all(nsd, cfg->gamma, ur[0], ur + 1, ur[1 + nsd], &R);
+    switch (cfg->flux) {
+    case ORC_FLUX_HLL: return flux_hll(nsd, d, cfg->gamma, &L, &R, F);
+    case ORC_FLUX_HLL3: return flux_hll3(nsd, d, cfg->gamma, &L, &R, F);
+    default: return flux_central(nsd, d, cfg->gamma, &L, &R, F);
+    }
+}
+
+void orc_net_flux(const orc_config* cfg, const double* in, double* out, double ws[3]) {
+    int N[3];
+    const int g = cfg->g;
+    const int nvar = cfg->dim + 2;
+    const long plane = orc_plane_size(cfg);
+    int d, x, y, z, var;
+    padded(cfg, N);
+    /* makeZero over interior cells (NumericalFluxCPU.cpp:122-146) */
+    for (z = (cfg->dim > 2 ? g : 0); z < N[2] - (cfg->dim > 2 ? g : 0); ++z) {
+        for (y = (cfg->dim > 1 ? g : 0); y < N[1] - (cfg->dim > 1 ? g : 0); ++y) {
+            for (x = g; x < N[0] - g; ++x) {
+                for (var = 0; var < nvar; ++var) {
+                    out[var * plane + idx3(N, x, y, z)] = 0;
+                }
+            }
+        }
+    }
+    ws[0] = ws[1] = ws[2] = 0;
+    for (d = 0; d < cfg->dim; ++d) {
+        const long s = d == 0 ? 1 : (d == 1 ? N[0] : (long)N[0] * N[1]);
+        const int len = N[d];
+        int lo[3], hi[3];
+        double wmax = 0;
+        double* rec = (double*)malloc(sizeof(double) * 2 * nvar * (size_t)len);
+        double* flux = (double*)malloc(sizeof(double) * nvar * (size_t)len);
+        for (x = 0; x < 3; ++x) {
+            const int gx = x < cfg->dim ? g : 0;
+            lo[x] = gx;
+            hi[x] = N[x] - gx;
+        }
+        lo[d] = 0;
+        hi[d] = 1;
+        for (z = lo[2]; z < hi[2]; ++z) {
+            for (y = lo[1]; y < hi[1]; ++y) {
+                for (x = lo[0]; x < hi[0]; ++x) {
+                    /* one line along d through (x,y,z) */
+                    const long base = idx3(N, x, y, z);
+                    int i;
+                    for (i = g - 1; i < len - g + 1; ++i) {
+                        reconstruct_cell(cfg, in, plane, base + i * s, s, nvar,
+                            rec + (size_t)i * 2 * nvar, rec + (size_t)i * 2 * nvar + nvar);
+                    }
+                    /* faces i|i+1 for i in [g-1, len-g): U- = right[i], U+ = left[i+1]
+                     * (numflux_util.hpp:62-92); temp = -F (NumericalFluxCPU.cpp:92) */
+                    for (i = g - 1; i < len - g; ++i) {
+                        const double* ul = rec + (size_t)i * 2 * nvar + nvar;
+                        const double* ur = rec + (size_t)(i + 1) * 2 * nvar;
+                        const double w = face_flux(cfg, d, ul, ur, flux + (size_t)i * nvar);
+                        if (wmax < w) { /* std::max(waveSpeedComputed, local) */
+                            wmax = w;
+                        }
+                    }
+                    /* out[i] += (-F_{i+1/2}) + (-(-F_{i-1/2})) (NumericalFluxCPU.cpp:100-117) */
+                    for (i = g; i < len - g; ++i) {
+                        for (var = 0; var < nvar; ++var) {
+                            const double tr = -flux[(size_t)i * nvar + var];
+                            const double tl = -flux[(size_t)(i - 1) * nvar + var];
+                            out[var * plane + base + i * s] += tr + (-tl);
+                        }
+                    }
+                }
+            }
+        }
+        ws[d] = wmax;
+        free(rec);
+        free(flux);
+    }
+}
+
+/* ---------------------------------------------------------- constraints */
+
+int orc_obeys_constraints(const orc_config* cfg, const double* planes) {
+    const int nsd = cfg->dim;
+    const int nvar = nsd + 2;
+    const long plane = orc_plane_size(cfg);
+    long c;
+    int var;
+    for (c = 0; c < plane; ++c) {
+        double U[5];
+        state_t s;
+        for (var = 0; var < nvar; ++var) {
+            U[var] = planes[var * plane + c];
+            if (isnan(U[var]) || isinf(U[var])) {
+                return 0;
+            }
+        }
+        make_all(nsd, cfg->gamma, U[0], U + 1, U[1 + nsd], &s);
+        for (var = 0; var < nsd; ++var) {
+            if (isnan(s.u[var]) || isinf(s.u[var])) {
+                return 0;
+            }
+        }
+        if (isnan(s.p) || isinf(s.p)) {
+            return 0;
+        }
+        if (!(s.rho > 0) || !(s.p > 0)) {
+            return 0;
+        }
+    }
+    return 1;
+}
+
+/* ------------------------------------------------------------ time loop */
+
+int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_steps,
+    double* planes, double* dts, long dts_capacity, long* steps_out, double* t_out) {
+    const int nvar = cfg->dim + 2;
+    const long plane = orc_plane_size(cfg);
+    const size_t bytes = sizeof(double) * (size_t)nvar * (size_t)plane;
+    const int substeps = cfg->integrator == ORC_INT_FE ? 1 : (cfg->integrator == ORC_INT_RK2 ? 2 : 3);
+    double* vol[4];
+    double t = 0;
+    long steps = 0, i;
+    int s, status = 0, d;
+    for (d = 0; d < cfg->dim; ++d) {
+        if (cfg->n[d] < 2 * cfg->g) {
+            return -1;
+        }
+    }
+    for (s = 0; s <= substeps; ++s) {
+        vol[s] = (double*)calloc(1, bytes);
+    }
+    memcpy(vol[0], planes, bytes);
+    orc_fill_ghosts(cfg, vol[0], nvar);
+    while (t < end_time && steps < max_steps) {
+        double dt = 0;
+        for (s = 0; s < substeps; ++s) {
+            double ws[3];
+            double* out = vol[s + 1];
+            const double* Us = vol[s];
+            const double* U0 = vol[0];
+            double c;
+            orc_net_flux(cfg, Us, out, ws);
+            if (s == 0) {
+                /* Integrator.cpp:20-46 then the end-time clamp */
+                double total = 0;
+                for (d = 0; d < 3; ++d) {
+                    if (cfg->dx[d] == 0) {
+                        continue;
+                    }
+                    total += ws[d] / cfg->dx[d];
+                }
+                dt = cfl / total;
+                dt = (end_time - t < dt) ? end_time - t : dt;
+            }
+            c = dt / cfg->dx[0];
+            /* the Volume operations run over every cell; ghosts are refilled below */
+            for (i = 0; i < nvar * plane; ++i) {
+                double v = out[i];
+                v *= c;
+                v += Us[i];
+                if (cfg->integrator == ORC_INT_RK3 && s == 1) {
+                    v *= 1. / 3.;
+                    v += U0[i];
+                    v *= 3. / 4.;
+                } else if (cfg->integrator == ORC_INT_RK3 && s == 2) {
+                    v *= 2;
+                    v += U0[i];
+                    v *= 1. / 3.;
+                } else if (cfg->integrator == ORC_INT_RK2 && s == 1) {
+                    v += U0[i];
+                    v *= 0.5;
+                }
+                out[i] = v;
+            }
+            orc_fill_ghosts(cfg, out, nvar);
+        }
+        {
+            double* tmp = vol[0];
+            vol[0] = vol[substeps];
+            vol[substeps] = tmp;
+        }
+        t += dt;
+        if (dts && steps < dts_capacity) {
+            dts[steps] = dt;
+        }
+        ++steps;
+        if (!orc_obeys_constraints(cfg, vol[0])) {
+            status = 1;
+            break;
+        }
+    }
+    memcpy(planes, vol[0], bytes);
+    for (s = 0; s <= substeps; ++s) {
+        free(vol[s]);
+    }
+    if (steps_out) {
+        *steps_out = steps;
+    }
+    if (t_out) {
+        *t_out = t;
+    }
+    return status;
+}
+
+/* ----------------------------------------------------------- statistics */
+
+void orc_meanvar(long count, long samples, const double* states, double* mean, double* var) {
+    /* a run-time exponent, as in HostMemory::addPower, so the call is not folded to u*u */
+    volatile double two = 2.0;
+    long i, k;
+    for (i = 0; i < count; ++i) {
+        mean[i] = 0;
+        var[i] = 0;
+    }
+    for (k = 0; k < samples; ++k) {
+        for (i = 0; i < count; ++i) {
+            const double u = states[k * count + i];
+            mean[i] += u;
+            var[i] += pow(u, two);
+        }
+    }
+    for (i = 0; i < count; ++i) {
+        mean[i] /= (double)samples;
+        var[i] /= (double)samples;
+        var[i] -= pow(mean[i], two);
+    }
+}

@@ -1,0 +1,78 @@
+/*
+ * CPU restatement of alsfvm's cell-update hot path, written in plain C.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the GPU path is compared
+ * against; it is never linked into, loaded by or called from the product
+ * library.  Only tests/, the smoke check and bench.py's CPU-baseline leg
+ * may use it.  It is pinned bit-for-bit against the reference's own CPU
+ * sources (oracle/_ref/libalsref.so, built by `make -C oracle ref`) by
+ * tests/test_oracle_pin.py and against committed fixtures in tests/golden/.
+ *
+ * Data layout (same as alsfvm::volume::Volume, alsfvm/src/volume/Volume.cpp:44-60):
+ * one contiguous plane of doubles per conserved variable, each plane
+ * (nx+2g)*(ny+2g)*(nz+2g) cells with x fastest, inactive dimensions have
+ * extent 1 and no ghost cells.  Variable order rho, mx, [my, [mz,]] E
+ * (alsfvm/src/equation/euler/Euler.cpp:20-75).
+ */
+#ifndef ALS_ORACLE_H
+#define ALS_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_FLUX_HLL = 0, ORC_FLUX_HLL3 = 1, ORC_FLUX_CENTRAL = 2 };
+enum { ORC_RECON_NONE = 0, ORC_RECON_WENO2 = 1, ORC_RECON_ENO2 = 2,
+       ORC_RECON_ENO3 = 3, ORC_RECON_ENO4 = 4 };
+enum { ORC_INT_FE = 0, ORC_INT_RK2 = 1, ORC_INT_RK3 = 2 };
+enum { ORC_BC_NEUMANN = 0, ORC_BC_PERIODIC = 1 };
+
+typedef struct {
+    int dim;          /* 1, 2 or 3 */
+    int n[3];         /* interior cells per direction (1 for inactive) */
+    int g;            /* ghost width */
+    double gamma;
+    int flux, recon, integrator, bc;
+    double dx[3];     /* cell lengths; 1 for inactive directions */
+} orc_config;
+
+/* Ghost width max(stencil-1, reconstruction ghosts), NumericalFluxCPU.cpp:227-231. */
+int orc_ghost_cells(int flux, int recon);
+
+/* Fills cfg->g, cell lengths from the domain [lower, upper], Grid.cpp:24-41. */
+int orc_configure(orc_config* cfg, int dim, const int* n, const double* lower,
+    const double* upper, int flux, int recon, int integrator, int bc, double gamma);
+
+long orc_plane_size(const orc_config* cfg);
+
+/* Ghost-cell fill, BoundaryCPU.cpp:30-106 with Neumann.hpp:24-35 / Periodic.hpp:24-42. */
+void orc_fill_ghosts(const orc_config* cfg, double* planes, int nvar);
+
+/* Reconstruction along direction `dir` for every cell the reference
+ * reconstructs (ReconstructionCPU.cpp:37-97, ENOCPU.cpp:41-187). */
+void orc_reconstruct(const orc_config* cfg, int dir, const double* in,
+    double* left, double* right);
+
+/* Net flux of every interior cell (ghost cells untouched) and the maximal
+ * face wave speed per direction (NumericalFluxCPU.cpp:32-221). */
+void orc_net_flux(const orc_config* cfg, const double* in, double* out, double ws[3]);
+
+/* The Simulator time loop with an end-time clamp (Simulator.cpp:191-214,
+ * Integrator.cpp:20-46, FixedIntervalWriter.cpp:45-53).  `planes` holds the
+ * initial state (ghosts are filled first) and receives the final state.
+ * Returns 0, 1 on a constraint violation, -1 on bad arguments. */
+int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_steps,
+    double* planes, double* dts, long dts_capacity, long* steps_out, double* t_out);
+
+/* MeanVariance with raw moments (MeanVariance.cpp:30-67): mean = S1/M,
+ * var = S2/M - mean^2, over `samples` states of `count` doubles each. */
+void orc_meanvar(long count, long samples, const double* states, double* mean, double* var);
+
+/* Constraint check of CPUCellComputer::obeysConstraints (CPUCellComputer.cpp:80-128)
+ * over all cells; returns 1 when every cell obeys. */
+int orc_obeys_constraints(const orc_config* cfg, const double* planes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,432 @@
+// Test oracle driver around the reference's own CPU implementation.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is compiled together with the
+// unmodified reference sources (see oracle/Makefile) into oracle/_ref/libalsref.so.
+// Only tests/, the smoke check and bench.py's CPU-baseline leg may load it,
+// and only as the checker or the timed CPU baseline, never as the product.
+//
+// What it reproduces (reference file:line):
+//  * Simulator::incrementSolution            alsfvm/src/simulator/Simulator.cpp:191-214
+//  * Simulator::atEnd / checkConstraints      alsfvm/src/simulator/Simulator.cpp:77-79,180-189
+//  * FixedIntervalWriter::adjustTimestep with one save at T
+//                                             alsfvm/src/io/FixedIntervalWriter.cpp:45-53
+//  * MeanVariance compute/combine/finalize    alsuq/src/stats/MeanVariance.cpp:30-67,
+//                                             alsuq/src/stats/StatisticsHelper.cpp:35-79
+//  * STLMersenne sample draws                 alsuq/src/generator/STLMersenne.cpp:38-85
+// All arithmetic is done by the reference's own classes; this file only wires
+// them together and copies planes in and out.
+#include "alsfvm/types.hpp"
+#include "alsfvm/grid/Grid.hpp"
+#include "alsfvm/boundary/BoundaryCPU.hpp"
+#include "alsfvm/boundary/Neumann.hpp"
+#include "alsfvm/boundary/Periodic.hpp"
+#include "alsfvm/numflux/NumericalFluxCPU.hpp"
+#include "alsfvm/numflux/euler/HLL.hpp"
+#include "alsfvm/numflux/euler/HLL3.hpp"
+#include "alsfvm/numflux/Central.hpp"
+#include "alsfvm/reconstruction/ReconstructionCPU.hpp"
+#include "alsfvm/reconstruction/WENO2.hpp"
+#include "alsfvm/reconstruction/ENOCPU.hpp"
+#include "alsfvm/reconstruction/NoReconstruction.hpp"
+#include "alsfvm/integrator/ForwardEuler.hpp"
+#include "alsfvm/integrator/RungeKutta2.hpp"
+#include "alsfvm/integrator/RungeKutta3.hpp"
+#include "alsfvm/integrator/TimestepAdjuster.hpp"
+#include "alsfvm/simulator/ConservedSystem.hpp"
+#include "alsfvm/simulator/SimulatorParameters.hpp"
+#include "alsfvm/simulator/TimestepInformation.hpp"
+#include "alsfvm/diffusion/NoDiffusion.hpp"
+#include "alsfvm/volume/VolumeFactory.hpp"
+#include "alsfvm/memory/MemoryFactory.hpp"
+#include "alsfvm/equation/euler/EulerParameters.hpp"
+#include "alsfvm/equation/CPUCellComputer.hpp"
+#include "alsfvm/DeviceConfiguration.hpp"
+#include "alsuq/generator/STLMersenne.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace alsfvm;
+
+namespace {
+
+std::string g_last_error;
+
+struct Setup {
+    int dim;
+    ivec3 n;
+    rvec3 lower, upper;
+    std::string flux, recon, integrator, bc;
+    double gamma, cfl;
+};
+
+// Stops the step that would pass the end time, like a FixedIntervalWriter
+// whose only save is at T (FixedIntervalWriter.cpp:45-53).
+class EndTimeClamp : public integrator::TimestepAdjuster {
+public:
+    explicit EndTimeClamp(real endTime) : endTime(endTime) {}
+    real adjustTimestep(real dt,
+        const simulator::TimestepInformation& info) const override {
+        return std::min(dt, endTime - info.getCurrentTime());
+    }
+private:
+    real endTime;
+};
+
+struct Objects {
+    std::shared_ptr<DeviceConfiguration> device;
+    std::shared_ptr<memory::MemoryFactory> memoryFactory;
+    std::shared_ptr<simulator::SimulatorParameters> params;
+    std::shared_ptr<grid::Grid> grid;
+    std::shared_ptr<reconstruction::Reconstruction> recon;
+    std::shared_ptr<numflux::NumericalFlux> flux;
+    std::shared_ptr<integrator::System> system;
+    std::shared_ptr<integrator::Integrator> integ;
+    std::shared_ptr<boundary::Boundary> boundary;
+    std::shared_ptr<volume::VolumeFactory> volumeFactory;
+    size_t ghosts = 0;
+    std::string eqName;
+};
+
+template<int d>
+std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Objects& o) {
+    typedef equation::euler::Euler<d> Eq;
+    if (s.recon == "weno2") {
+        return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::WENO2<Eq>, Eq>>(*o.params);
+    } else if (s.recon == "eno2") {
+        return std::make_shared<reconstruction::ENOCPU<2>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else if (s.recon == "eno3") {
+        return std::make_shared<reconstruction::ENOCPU<3>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else if (s.recon == "eno4") {
+        return std::make_shared<reconstruction::ENOCPU<4>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else if (s.recon == "none") {
+        return std::make_shared<reconstruction::NoReconstruction>();
+    }
+    THROW("unknown reconstruction " << s.recon);
+}
+
+template<int d>
+std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
+    typedef equation::euler::Euler<d> Eq;
+    if (s.flux == "hll") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::euler::HLL<d>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    } else if (s.flux == "hll3") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::euler::HLL3<d>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    } else if (s.flux == "central") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::Central<Eq>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    }
+    THROW("unknown flux " << s.flux);
+}
+
+Objects build(const Setup& s) {
+    Objects o;
+    o.device = std::make_shared<DeviceConfiguration>("cpu");
+    o.memoryFactory = std::make_shared<memory::MemoryFactory>(o.device);
+    o.eqName = "euler" + std::to_string(s.dim);
+    auto eulerParams = std::make_shared<equation::euler::EulerParameters>();
+    eulerParams->setGamma(s.gamma);
+    o.params = std::make_shared<simulator::SimulatorParameters>(o.eqName, "cpu");
+    o.params->setEquationParameters(eulerParams);
+    o.params->setCFLNumber(s.cfl);
+
+    boundary::Type t;
+    if (s.bc == "neumann") {
+        t = boundary::Type::NEUMANN;
+    } else if (s.bc == "periodic") {
+        t = boundary::Type::PERIODIC;
+    } else {
+        THROW("unknown boundary " << s.bc);
+    }
+    std::array<boundary::Type, 6> bcs = {t, t, t, t, t, t};
+    o.grid = std::make_shared<grid::Grid>(s.lower, s.upper, s.n, bcs);
+
+    switch (s.dim) {
+    case 1: o.recon = makeRecon<1>(s, o); o.flux = makeFlux<1>(s, o); break;
+    case 2: o.recon = makeRecon<2>(s, o); o.flux = makeFlux<2>(s, o); break;
+    case 3: o.recon = makeRecon<3>(s, o); o.flux = makeFlux<3>(s, o); break;
+    default: THROW("dimension must be 1, 2 or 3");
+    }
+    std::shared_ptr<diffusion::DiffusionOperator> diffusion =
+        std::make_shared<diffusion::NoDiffusion>();
+    o.system = std::make_shared<simulator::ConservedSystem>(o.flux, diffusion);
+    if (s.integrator == "forwardeuler") {
+        o.integ = std::make_shared<integrator::ForwardEuler>(o.system);
+    } else if (s.integrator == "rungekutta2") {
+        o.integ = std::make_shared<integrator::RungeKutta2>(o.system);
+    } else if (s.integrator == "rungekutta3") {
+        o.integ = std::make_shared<integrator::RungeKutta3>(o.system);
+    } else {
+        THROW("unknown integrator " << s.integrator);
+    }
+    o.ghosts = o.system->getNumberOfGhostCells();
+    if (t == boundary::Type::NEUMANN) {
+        o.boundary = std::make_shared<boundary::BoundaryCPU<boundary::Neumann>>(o.ghosts);
+    } else {
+        o.boundary = std::make_shared<boundary::BoundaryCPU<boundary::Periodic>>(o.ghosts);
+    }
+    o.volumeFactory = std::make_shared<volume::VolumeFactory>(o.eqName, o.memoryFactory);
+    return o;
+}
+
+Setup makeSetup(int dim, const int* n, const double* lower, const double* upper,
+    const char* flux, const char* recon, const char* integ, const char* bc,
+    double gamma, double cfl) {
+    Setup s;
+    s.dim = dim;
+    s.n = ivec3(n[0], dim > 1 ? n[1] : 1, dim > 2 ? n[2] : 1);
+    s.lower = rvec3(lower[0], lower[1], lower[2]);
+    s.upper = rvec3(upper[0], upper[1], upper[2]);
+    s.flux = flux ? flux : "";
+    s.recon = recon ? recon : "";
+    s.integrator = integ ? integ : "rungekutta3";
+    s.bc = bc ? bc : "";
+    s.gamma = gamma;
+    s.cfl = cfl;
+    return s;
+}
+
+size_t paddedCells(const volume::Volume& v) {
+    return v.getTotalNumberOfXCells() * v.getTotalNumberOfYCells() *
+        v.getTotalNumberOfZCells();
+}
+
+void copyIn(volume::Volume& v, const double* planes) {
+    const size_t cells = paddedCells(v);
+    for (size_t var = 0; var < v.getNumberOfVariables(); ++var) {
+        std::memcpy(v.getScalarMemoryArea(var)->getPointer(), planes + var * cells,
+            cells * sizeof(double));
+    }
+}
+
+void copyOut(const volume::Volume& v, double* planes) {
+    const size_t cells = paddedCells(v);
+    for (size_t var = 0; var < v.getNumberOfVariables(); ++var) {
+        std::memcpy(planes + var * cells, v.getScalarMemoryArea(var)->getPointer(),
+            cells * sizeof(double));
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+const char* alsref_last_error() {
+    return g_last_error.c_str();
+}
+
+// Ghost width the reference picks for a flux/reconstruction pair
+// (NumericalFluxCPU.cpp:227-231).
+int alsref_ghost_cells(int dim, const char* flux, const char* recon) {
+    try {
+        int n[3] = {16, 16, 16};
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, flux, recon, "forwardeuler", "neumann", 1.4, 0.5);
+        auto o = build(s);
+        return int(o.ghosts);
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// The reference time loop.  `planes` holds nvar padded planes of initial
+// conserved data (ghost cells are ignored on input and filled by the
+// boundary, Simulator.cpp:161).  On return it holds the final padded state.
+// dts[k] receives the dt of step k (up to dts_capacity entries).
+// Returns 0, or 1 when the constraint check failed, or -1 on error.
+int alsref_simulate(int dim, const int* n, const double* lower, const double* upper,
+    const char* flux, const char* recon, const char* integ, const char* bc,
+    double gamma, double cfl, double end_time, long max_steps,
+    double* planes, double* dts, long dts_capacity,
+    long* steps_out, double* t_out) {
+    try {
+        auto s = makeSetup(dim, n, lower, upper, flux, recon, integ, bc, gamma, cfl);
+        auto o = build(s);
+        std::shared_ptr<integrator::TimestepAdjuster> clamp =
+            std::make_shared<EndTimeClamp>(end_time);
+        o.integ->addTimestepAdjuster(clamp);
+
+        std::vector<std::shared_ptr<volume::Volume>> volumes;
+        for (size_t i = 0; i < o.integ->getNumberOfSubsteps() + 1; ++i) {
+            volumes.push_back(o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, o.ghosts));
+        }
+        copyIn(*volumes[0], planes);
+        o.boundary->applyBoundaryConditions(*volumes[0], *o.grid);
+
+        std::shared_ptr<equation::CellComputer> cellComputer;
+        switch (dim) {
+        case 1: cellComputer = std::make_shared<equation::CPUCellComputer<equation::euler::Euler<1>>>(*o.params); break;
+        case 2: cellComputer = std::make_shared<equation::CPUCellComputer<equation::euler::Euler<2>>>(*o.params); break;
+        default: cellComputer = std::make_shared<equation::CPUCellComputer<equation::euler::Euler<3>>>(*o.params); break;
+        }
+
+        simulator::TimestepInformation info;
+        int status = 0;
+        long steps = 0;
+        while (info.getCurrentTime() < end_time && steps < max_steps) {
+            real dt = 0;
+            for (size_t substep = 0; substep < o.integ->getNumberOfSubsteps(); ++substep) {
+                auto& next = volumes[substep + 1];
+                dt = o.integ->performSubstep(volumes, o.grid->getCellLengths(), dt,
+                        s.cfl, *next, substep, info);
+                o.boundary->applyBoundaryConditions(*next, *o.grid);
+            }
+            volumes[0].swap(volumes.back());
+            info.incrementTime(dt);
+            if (steps < dts_capacity && dts) {
+                dts[steps] = dt;
+            }
+            ++steps;
+            if (!cellComputer->obeysConstraints(*volumes[0])) {
+                status = 1;
+                break;
+            }
+        }
+        copyOut(*volumes[0], planes);
+        if (steps_out) {
+            *steps_out = steps;
+        }
+        if (t_out) {
+            *t_out = info.getCurrentTime();
+        }
+        return status;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// One spatial-operator evaluation: ConservedSystem::operator()
+// (ConservedSystem.cpp:31-103) on a state whose ghost cells are filled by the
+// boundary first.  out_planes receives the net flux (interior cells; ghost
+// cells are left zero), ws the per-direction maximal wave speeds.
+int alsref_compute_flux(int dim, const int* n, const double* lower, const double* upper,
+    const char* flux, const char* recon, const char* bc, double gamma,
+    double* in_planes, double* out_planes, double* ws) {
+    try {
+        auto s = makeSetup(dim, n, lower, upper, flux, recon, "forwardeuler", bc, gamma, 0.5);
+        auto o = build(s);
+        auto in = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, o.ghosts);
+        auto out = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, o.ghosts);
+        copyIn(*in, in_planes);
+        o.boundary->applyBoundaryConditions(*in, *o.grid);
+        out->makeZero();
+        rvec3 waveSpeed(0, 0, 0);
+        (*o.system)(*in, waveSpeed, true, *out);
+        copyOut(*in, in_planes);
+        copyOut(*out, out_planes);
+        ws[0] = waveSpeed.x;
+        ws[1] = waveSpeed.y;
+        ws[2] = waveSpeed.z;
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Reconstruction::performReconstruction along `direction` on a state whose
+// ghost cells are taken as given (no boundary applied).
+int alsref_reconstruct(int dim, const int* n, const char* recon, double gamma,
+    int direction, const double* in_planes, double* left, double* right) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", recon, "forwardeuler", "neumann", gamma, 0.5);
+        auto o = build(s);
+        const size_t g = o.recon->getNumberOfGhostCells();
+        auto in = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, g);
+        auto l = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, g);
+        auto r = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, g);
+        copyIn(*in, in_planes);
+        l->makeZero();
+        r->makeZero();
+        o.recon->performReconstruction(*in, direction, 0, *l, *r);
+        copyOut(*l, left);
+        copyOut(*r, right);
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Boundary::applyBoundaryConditions on nvar padded planes with ghost width g.
+int alsref_apply_boundary(int dim, const int* n, int ghosts, const char* bc,
+    double* planes) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", bc, 1.4, 0.5);
+        auto o = build(s);
+        auto v = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        copyIn(*v, planes);
+        std::shared_ptr<boundary::Boundary> b;
+        if (s.bc == "neumann") {
+            b = std::make_shared<boundary::BoundaryCPU<boundary::Neumann>>(ghosts);
+        } else {
+            b = std::make_shared<boundary::BoundaryCPU<boundary::Periodic>>(ghosts);
+        }
+        b->applyBoundaryConditions(*v, *o.grid);
+        copyOut(*v, planes);
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// MeanVariance over `samples` padded states of one volume shape
+// (MeanVariance.cpp:30-67 with StatisticsHelper.cpp:74 `/= samples`).
+int alsref_meanvar(int dim, const int* n, int ghosts, long samples,
+    const double* states, double* mean_out, double* var_out) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", "neumann", 1.4, 0.5);
+        auto o = build(s);
+        auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        auto mean = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        auto var = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        mean->makeZero();
+        var->makeZero();
+        const size_t stride = paddedCells(*u) * u->getNumberOfVariables();
+        for (long k = 0; k < samples; ++k) {
+            copyIn(*u, states + k * stride);
+            *mean += *u;
+            var->addPower(*u, 2);
+        }
+        for (size_t v = 0; v < u->getNumberOfVariables(); ++v) {
+            *mean->getScalarMemoryArea(v) /= real(samples);
+            *var->getScalarMemoryArea(v) /= real(samples);
+        }
+        var->subtractPower(*mean, 2.);
+        copyOut(*mean, mean_out);
+        copyOut(*var, var_out);
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Parameter draws of samples [first, first+count) for a parameter of length
+// `dimension` (STLMersenne.cpp:38-85): out[k*dimension + c].
+// The generator is a process-wide singleton in the reference, so this must
+// be called with increasing sample numbers within one process.
+int alsref_stlmersenne(long dimension, long first, long count, double* out) {
+    try {
+        alsuq::generator::STLMersenne gen(dimension);
+        for (long k = 0; k < count; ++k) {
+            for (long c = 0; c < dimension; ++c) {
+                out[k * dimension + c] = gen.generate(c, first + k);
+            }
+        }
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,20 @@
+// Plumbing shim: the reference's flux type list reduced to HLL, HLL3 and
+// Central for Euler 1/2/3 (the fluxes the oracle builds).
+#pragma once
+#include "alsfvm/equation/equation_list.hpp"
+#include "alsfvm/numflux/euler/HLL.hpp"
+#include "alsfvm/numflux/euler/HLL3.hpp"
+#include "alsfvm/numflux/Central.hpp"
+
+#define ALSFVM_FLUX_INSTANTIATE_ONE(X, F, E) \
+    template class X< F, E, 1>; template class X< F, E, 2>; template class X< F, E, 3>;
+#define ALSFVM_FLUX_INSTANTIATE(X) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL<1>, ::alsfvm::equation::euler::Euler<1>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL<2>, ::alsfvm::equation::euler::Euler<2>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL<3>, ::alsfvm::equation::euler::Euler<3>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL3<1>, ::alsfvm::equation::euler::Euler<1>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL3<2>, ::alsfvm::equation::euler::Euler<2>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::euler::HLL3<3>, ::alsfvm::equation::euler::Euler<3>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::Central< ::alsfvm::equation::euler::Euler<1> >, ::alsfvm::equation::euler::Euler<1>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::Central< ::alsfvm::equation::euler::Euler<2> >, ::alsfvm::equation::euler::Euler<2>) \
+    ALSFVM_FLUX_INSTANTIATE_ONE(X, ::alsfvm::numflux::Central< ::alsfvm::equation::euler::Euler<3> >, ::alsfvm::equation::euler::Euler<3>)

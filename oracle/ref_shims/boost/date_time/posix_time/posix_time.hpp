@@ -1,0 +1,2 @@
+// Plumbing shim: empty.
+#pragma once

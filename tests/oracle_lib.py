@@ -1,0 +1,228 @@
+"""ctypes bindings for the two test oracles.
+
+TEST INFRASTRUCTURE ONLY.
+
+* ``COracle`` wraps ``oracle/liboracle.so``: the plain-C restatement of the
+  reference's hot path (``oracle/als_oracle.c``).  It is built on demand with
+  ``make -C oracle`` (gcc only), so it is available on every machine.
+* ``RefOracle`` wraps ``oracle/_ref/libalsref.so``: the reference's own CPU
+  sources compiled by ``make -C oracle ref``.  It only exists where it was
+  built (it needs the reference source tree); tests that need it skip
+  otherwise, and the committed fixtures in ``tests/golden/`` carry its
+  outputs everywhere else.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+
+FLUX = {"hll": 0, "hll3": 1, "central": 2}
+RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4}
+INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
+BC = {"neumann": 0, "periodic": 1}
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _dptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+def ghost_cells(recon):
+    return {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4}[recon]
+
+
+def padded_shape(dim, n, g):
+    """(nvar, Nz, Ny, Nx) of a padded volume."""
+    nn = [n[d] if d < dim else 1 for d in range(3)]
+    N = [nn[d] + (2 * g if d < dim else 0) for d in range(3)]
+    return (dim + 2, N[2], N[1], N[0])
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("g", ctypes.c_int),
+        ("gamma", ctypes.c_double),
+        ("flux", ctypes.c_int),
+        ("recon", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("bc", ctypes.c_int),
+        ("dx", ctypes.c_double * 3),
+    ]
+
+
+def build_c_oracle():
+    path = os.path.join(ORACLE_DIR, "liboracle.so")
+    src = os.path.join(ORACLE_DIR, "als_oracle.c")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", ORACLE_DIR, "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return path
+
+
+class COracle:
+    def __init__(self):
+        self.lib = ctypes.CDLL(build_c_oracle())
+        L = self.lib
+        L.orc_configure.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, _I, _D, _D,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double]
+        L.orc_simulate.argtypes = [ctypes.POINTER(_Config), ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_long, _D, _D, ctypes.c_long,
+                                   ctypes.POINTER(ctypes.c_long), _D]
+        L.orc_net_flux.argtypes = [ctypes.POINTER(_Config), _D, _D, _D]
+        L.orc_reconstruct.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, _D, _D, _D]
+        L.orc_fill_ghosts.argtypes = [ctypes.POINTER(_Config), _D, ctypes.c_int]
+        L.orc_meanvar.argtypes = [ctypes.c_long, ctypes.c_long, _D, _D, _D]
+        L.orc_obeys_constraints.argtypes = [ctypes.POINTER(_Config), _D]
+
+    def config(self, dim, n, lower, upper, flux, recon, integrator, bc, gamma):
+        cfg = _Config()
+        nn = (ctypes.c_int * 3)(*[int(v) for v in (list(n) + [1, 1, 1])[:3]])
+        lo = (ctypes.c_double * 3)(*[float(v) for v in (list(lower) + [0, 0, 0])[:3]])
+        hi = (ctypes.c_double * 3)(*[float(v) for v in (list(upper) + [0, 0, 0])[:3]])
+        rc = self.lib.orc_configure(ctypes.byref(cfg), dim, nn, lo, hi, FLUX[flux],
+                                    RECON[recon], INTEGRATOR[integrator], BC[bc], gamma)
+        assert rc == 0
+        return cfg
+
+    def simulate(self, cfg, planes, cfl, end_time, max_steps=10 ** 9, dts_capacity=100000):
+        out = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        dts = np.zeros(dts_capacity)
+        steps = ctypes.c_long()
+        t = ctypes.c_double()
+        rc = self.lib.orc_simulate(ctypes.byref(cfg), cfl, end_time, max_steps, _dptr(out),
+                                   _dptr(dts), dts_capacity, ctypes.byref(steps),
+                                   ctypes.byref(t))
+        return rc, out, dts[:min(steps.value, dts_capacity)], steps.value, t.value
+
+    def net_flux(self, cfg, planes):
+        inp = np.ascontiguousarray(planes, dtype=np.float64)
+        out = np.zeros_like(inp)
+        ws = np.zeros(3)
+        self.lib.orc_net_flux(ctypes.byref(cfg), _dptr(inp), _dptr(out), _dptr(ws))
+        return out, ws
+
+    def reconstruct(self, cfg, direction, planes):
+        inp = np.ascontiguousarray(planes, dtype=np.float64)
+        left = np.zeros_like(inp)
+        right = np.zeros_like(inp)
+        self.lib.orc_reconstruct(ctypes.byref(cfg), direction, _dptr(inp), _dptr(left),
+                                 _dptr(right))
+        return left, right
+
+    def fill_ghosts(self, cfg, planes):
+        out = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        self.lib.orc_fill_ghosts(ctypes.byref(cfg), _dptr(out), out.shape[0])
+        return out
+
+    def meanvar(self, states):
+        st = np.ascontiguousarray(states, dtype=np.float64)
+        count = st[0].size
+        mean = np.zeros(count)
+        var = np.zeros(count)
+        self.lib.orc_meanvar(count, st.shape[0], _dptr(st), _dptr(mean), _dptr(var))
+        return mean.reshape(st.shape[1:]), var.reshape(st.shape[1:])
+
+    def obeys_constraints(self, cfg, planes):
+        p = np.ascontiguousarray(planes, dtype=np.float64)
+        return bool(self.lib.orc_obeys_constraints(ctypes.byref(cfg), _dptr(p)))
+
+
+def ref_library_path():
+    return os.path.join(ORACLE_DIR, "_ref", "libalsref.so")
+
+
+class RefOracle:
+    """The reference's own CPU code (only where ``make -C oracle ref`` ran)."""
+
+    def __init__(self):
+        path = ref_library_path()
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.alsref_last_error.restype = ctypes.c_char_p
+        L.alsref_simulate.argtypes = [ctypes.c_int, _I, _D, _D, ctypes.c_char_p,
+                                      ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_long, _D, _D, ctypes.c_long,
+                                      ctypes.POINTER(ctypes.c_long), _D]
+        L.alsref_compute_flux.argtypes = [ctypes.c_int, _I, _D, _D, ctypes.c_char_p,
+                                          ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                          _D, _D, _D]
+        L.alsref_reconstruct.argtypes = [ctypes.c_int, _I, ctypes.c_char_p, ctypes.c_double,
+                                         ctypes.c_int, _D, _D, _D]
+        L.alsref_apply_boundary.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_char_p, _D]
+        L.alsref_meanvar.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_long, _D, _D, _D]
+        L.alsref_stlmersenne.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, _D]
+        L.alsref_ghost_cells.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]
+
+    def _check(self, rc):
+        if rc < 0:
+            raise RuntimeError(self.lib.alsref_last_error().decode())
+        return rc
+
+    @staticmethod
+    def _vec(vals, ctype, fill):
+        vals = (list(vals) + [fill, fill, fill])[:3]
+        return (ctype * 3)(*vals)
+
+    def simulate(self, dim, n, lower, upper, flux, recon, integrator, bc, gamma, cfl,
+                 end_time, planes, max_steps=10 ** 9, dts_capacity=100000):
+        out = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        dts = np.zeros(dts_capacity)
+        steps = ctypes.c_long()
+        t = ctypes.c_double()
+        rc = self._check(self.lib.alsref_simulate(
+            dim, self._vec(n, ctypes.c_int, 1), self._vec(lower, ctypes.c_double, 0.0),
+            self._vec(upper, ctypes.c_double, 0.0), flux.encode(), recon.encode(),
+            integrator.encode(), bc.encode(), gamma, cfl, end_time, max_steps, _dptr(out),
+            _dptr(dts), dts_capacity, ctypes.byref(steps), ctypes.byref(t)))
+        return rc, out, dts[:min(steps.value, dts_capacity)], steps.value, t.value
+
+    def compute_flux(self, dim, n, lower, upper, flux, recon, bc, gamma, planes):
+        inp = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        out = np.zeros_like(inp)
+        ws = np.zeros(3)
+        self._check(self.lib.alsref_compute_flux(
+            dim, self._vec(n, ctypes.c_int, 1), self._vec(lower, ctypes.c_double, 0.0),
+            self._vec(upper, ctypes.c_double, 0.0), flux.encode(), recon.encode(),
+            bc.encode(), gamma, _dptr(inp), _dptr(out), _dptr(ws)))
+        return inp, out, ws
+
+    def reconstruct(self, dim, n, recon, gamma, direction, planes):
+        inp = np.ascontiguousarray(planes, dtype=np.float64)
+        left = np.zeros_like(inp)
+        right = np.zeros_like(inp)
+        self._check(self.lib.alsref_reconstruct(dim, self._vec(n, ctypes.c_int, 1),
+                                                recon.encode(), gamma, direction, _dptr(inp),
+                                                _dptr(left), _dptr(right)))
+        return left, right
+
+    def apply_boundary(self, dim, n, ghosts, bc, planes):
+        out = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        self._check(self.lib.alsref_apply_boundary(dim, self._vec(n, ctypes.c_int, 1), ghosts,
+                                                   bc.encode(), _dptr(out)))
+        return out
+
+    def meanvar(self, dim, n, ghosts, states):
+        st = np.ascontiguousarray(states, dtype=np.float64)
+        mean = np.zeros(st.shape[1:])
+        var = np.zeros(st.shape[1:])
+        self._check(self.lib.alsref_meanvar(dim, self._vec(n, ctypes.c_int, 1), ghosts,
+                                            st.shape[0], _dptr(st), _dptr(mean), _dptr(var)))
+        return mean, var
+
+    def stlmersenne(self, dimension, first, count):
+        out = np.zeros(dimension * count)
+        self._check(self.lib.alsref_stlmersenne(dimension, first, count, _dptr(out)))
+        return out.reshape(count, dimension)
