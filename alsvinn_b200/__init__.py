@@ -1,0 +1,18 @@
+"""B200-native cell-update hot path of alsvinn's finite-volume solver (alsfvm).
+
+The compute lives in ``libals_b200.so`` (hand-written sm_100a CUDA behind the
+C ABI in ``include/als_b200.h``); this package is the Python face of it.
+"""
+from . import _lib
+from .initial_data import (kelvin_helmholtz, kh_ensemble, padded_shape, sod, uniform_draws)
+from .simulator import (Boundary, Integrator, NumericalFlux, Reconstruction, Simulator,
+                        ghost_cells)
+
+__all__ = [
+    "Boundary", "Integrator", "NumericalFlux", "Reconstruction", "Simulator", "ghost_cells",
+    "kelvin_helmholtz", "kh_ensemble", "padded_shape", "sod", "uniform_draws",
+]
+
+
+def library_path():
+    return _lib.library_path()

@@ -1,0 +1,114 @@
+"""ctypes binding of ``libals_b200.so`` (declared in ``include/als_b200.h``).
+
+The library is the product: there is no fallback.  Loading fails loudly
+when it has not been built (``python -m alsvinn_b200.build``).
+"""
+import ctypes
+import os
+
+from . import build as _build
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_VP = ctypes.c_void_p
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("dimension", ctypes.c_int), ("n", ctypes.c_int * 3), ("ghosts", ctypes.c_int),
+                ("gamma", ctypes.c_double)]
+
+
+class SolverConfig(ctypes.Structure):
+    _fields_ = [
+        ("dimension", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("lower", ctypes.c_double * 3),
+        ("upper", ctypes.c_double * 3),
+        ("flux", ctypes.c_int),
+        ("reconstruction", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("boundary", ctypes.c_int),
+        ("gamma", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("end_time", ctypes.c_double),
+        ("max_steps", ctypes.c_longlong),
+        ("precision", ctypes.c_int),
+        ("members", ctypes.c_int),
+    ]
+
+
+class MemberInfo(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_longlong),
+                ("done", ctypes.c_int), ("status", ctypes.c_int),
+                ("bad_index", ctypes.c_longlong), ("bad_step", ctypes.c_longlong)]
+
+
+# name -> (restype, argtypes) for every function the header declares
+PROTOTYPES = {
+    "als_last_error": (ctypes.c_char_p, []),
+    "als_version": (ctypes.c_int, []),
+    "als_ghost_cells": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "als_fill_ghosts": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, _VP, ctypes.c_int,
+                                       ctypes.c_int, _VP]),
+    "als_compute_flux": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
+                                        _I, _I, _D, _VP]),
+    "als_reconstruct": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
+                                       _VP, _VP]),
+    "als_integrator_combine": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,
+                                              ctypes.c_size_t, ctypes.c_double, _VP]),
+    "als_compute_timestep": (ctypes.c_double, [_D, _D, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double]),
+    "als_solver_create": (ctypes.c_int, [ctypes.POINTER(SolverConfig), ctypes.c_int,
+                                         ctypes.POINTER(_VP)]),
+    "als_solver_destroy": (ctypes.c_int, [_VP]),
+    "als_solver_geometry": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong), _I]),
+    "als_solver_set_state": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.c_int]),
+    "als_solver_set_state_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int]),
+    "als_solver_get_state": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.c_int]),
+    "als_solver_state_pointer": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "als_solver_advance": (ctypes.c_int, [_VP, ctypes.c_longlong]),
+    "als_solver_run": (ctypes.c_int, [_VP]),
+    "als_solver_info": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(MemberInfo)]),
+    "als_solver_synchronize": (ctypes.c_int, [_VP]),
+    "als_solver_stream": (_VP, [_VP]),
+    "als_solver_launches_per_step": (ctypes.c_int, [_VP]),
+    "als_solver_profile_step": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "als_uniform_draws": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
+                                         ctypes.c_double, ctypes.c_double, _D]),
+}
+
+_lib = None
+
+
+class AlsError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("als error %d: %s" % (code, message))
+        self.code = code
+
+
+def library_path():
+    return _build.library_path()
+
+
+def load():
+    """Loads the shared library (once) and declares every prototype."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError("libals_b200.so is not built (%s); run `python -m alsvinn_b200.build`"
+                           % path)
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc < 0:
+        raise AlsError(rc, load().als_last_error().decode())
+    return rc

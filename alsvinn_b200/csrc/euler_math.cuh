@@ -1,0 +1,297 @@
+// Device-side Euler mathematics of the cell-update hot path.
+//
+// Every expression keeps the evaluation order of the reference so that,
+// compiled with -fmad=false and IEEE division/square root, FP64 results are
+// bit-identical to alsfvm's CPU path:
+//   state / extra variables  alsfvm/include/alsfvm/equation/euler/Euler.hpp:172-211
+//   HLL                      alsfvm/include/alsfvm/numflux/euler/HLL.hpp:51-116
+//   HLL3                     alsfvm/include/alsfvm/numflux/euler/HLL3.hpp:52-149
+//   Central                  alsfvm/include/alsfvm/numflux/Central.hpp:39-56
+//   WENO2                    alsfvm/include/alsfvm/reconstruction/WENO2.hpp:31-91
+//   ENO2/3/4                 alsfvm/src/reconstruction/ENOCPU.cpp:41-267,
+//                            alsfvm/src/reconstruction/ENOCoefficients.cpp:27-49
+// Only the velocity component along the face normal is formed: the
+// reference computes all components but uses only u[direction].
+#pragma once
+
+#include <cstdint>
+
+namespace als {
+
+enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4 };
+enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2 };
+
+__host__ __device__ constexpr int recon_ghosts(int recon) {
+    return recon == RECON_NONE ? 1 : (recon == RECON_WENO2 || recon == RECON_ENO2) ? 2
+        : (recon == RECON_ENO3 ? 3 : 4);
+}
+
+// Left/right face state of one cell along direction D.
+template<class R, int NSD>
+struct FaceState {
+    R c[NSD + 2];   // rho, m_0..m_{NSD-1}, E
+    R p;            // pressure
+    R ud;           // velocity along the face normal
+};
+
+// computeExtra (Euler.hpp:204-211): ie = E - 0.5*(m.m)/rho, u = m/rho, p = (gamma-1)*ie.
+template<class R, int NSD, int D>
+__device__ __forceinline__ void make_state(const R* U, R gamma, FaceState<R, NSD>& s) {
+#pragma unroll
+    for (int k = 0; k < NSD + 2; ++k) {
+        s.c[k] = U[k];
+    }
+    R dot = U[1] * U[1];
+    if (NSD > 1) {
+        dot = dot + U[2] * U[2];
+    }
+    if (NSD > 2) {
+        dot = dot + U[3] * U[3];
+    }
+    const R ie = U[NSD + 1] - R(0.5) * dot / U[0];
+    s.ud = U[1 + D] / U[0];
+    s.p = (gamma - R(1)) * ie;
+}
+
+// Point flux along D (Euler.hpp:172-181).
+template<class R, int NSD, int D>
+__device__ __forceinline__ void point_flux(const FaceState<R, NSD>& s, R* F) {
+    F[0] = s.c[1 + D];
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        F[1 + k] = s.c[1 + k] * s.ud;
+    }
+    F[1 + D] = F[1 + D] + s.p;
+    F[NSD + 1] = (s.c[NSD + 1] + s.p) * s.ud;
+}
+
+template<class R, int NSD, int D>
+__device__ __forceinline__ R flux_hll(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    const R wl = sqrt(L.c[0]);
+    const R wr = sqrt(Rt.c[0]);
+    const R rho = (L.c[0] + Rt.c[0]) / R(2);
+    const R ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
+    const R p = (L.p * wl + Rt.p * wr) / (wl + wr);
+    const R cs = sqrt(gamma * p / rho);
+    const R sL = fmin(L.ud - sqrt(gamma * L.p / L.c[0]), ud - cs);
+    const R sR = fmax(Rt.ud + sqrt(gamma * Rt.p / Rt.c[0]), ud + cs);
+    if (sL == R(0)) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = R(0);
+        }
+    } else if (sL > R(0)) {
+        point_flux<R, NSD, D>(L, F);
+    } else if (sR < R(0)) {
+        point_flux<R, NSD, D>(Rt, F);
+    } else {
+        R FL[NV], FR[NV];
+        point_flux<R, NSD, D>(L, FL);
+        point_flux<R, NSD, D>(Rt, FR);
+        const R srsl = sR * sL;
+        const R den = sR - sL;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = (sR * FL[k] - sL * FR[k] + srsl * (Rt.c[k] - L.c[k])) / den;
+        }
+    }
+    return fmax(fabs(sL), fabs(sR));
+}
+
+template<class R, int NSD, int D>
+__device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    const R wl = sqrt(L.c[0]);
+    const R wr = sqrt(Rt.c[0]);
+    const R rho = (L.c[0] + Rt.c[0]) / R(2);
+    const R ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
+    const R p = (wl * L.p + wr * Rt.p) / (wl + wr);
+    const R cfL = sqrt(gamma * L.p / L.c[0]);
+    const R cfR = sqrt(gamma * Rt.p / Rt.c[0]);
+    const R correct = R(0.5) * fmax(R(0), L.ud - Rt.ud);
+    const R cs = sqrt(gamma * p / rho);
+    const R sL = fmin(L.ud + correct - cfL, ud - cs);
+    const R sR = fmax(Rt.ud - correct + cfR, ud + cs);
+    if (sL == R(0)) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = R(0);
+        }
+    } else if (sL > R(0)) {
+        point_flux<R, NSD, D>(L, F);
+    } else if (sR < R(0)) {
+        point_flux<R, NSD, D>(Rt, F);
+    } else {
+        R FL[NV], FR[NV];
+        point_flux<R, NSD, D>(L, FL);
+        point_flux<R, NSD, D>(Rt, FR);
+        const R udl = L.ud - sL;
+        const R udr = Rt.ud - sR;
+        const R aa = udr * Rt.c[0] - udl * L.c[0];
+        const R sm = (Rt.c[1 + D] * udr - L.c[1 + D] * udl + Rt.p - L.p) / aa;
+        // us: transverse star velocities (the normal one is sm)
+        R us[NSD];
+#pragma unroll
+        for (int k = 0; k < NSD; ++k) {
+            if (k == D) {
+                us[k] = sm;
+            } else {
+                us[k] = (FR[1 + k] - FL[1 + k] - sR * Rt.c[1 + k] + sL * L.c[1 + k]) / aa;
+            }
+        }
+        const bool left = sm >= R(0);
+        const FaceState<R, NSD>& S = left ? L : Rt;
+        const R sK = left ? sL : sR;
+        const R udk = left ? udl : udr;
+        const R* FK = left ? FL : FR;
+        const R den = sm - sK;
+        R mid[NV];
+        mid[0] = S.c[0] * udk / den;
+#pragma unroll
+        for (int k = 0; k < NSD; ++k) {
+            mid[1 + k] = us[k] * mid[0];
+        }
+        const R ps = S.p + S.c[0] * (S.ud - sm) * udk;
+        mid[NSD + 1] = (udk * S.c[NSD + 1] + S.p * S.ud - ps * sm) / den;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = FK[k] + sK * (mid[k] - S.c[k]);
+        }
+    }
+    return fmax(fabs(sL), fabs(sR));
+}
+
+template<class R, int NSD, int D>
+__device__ __forceinline__ R flux_central(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    R FL[NV], FR[NV];
+    point_flux<R, NSD, D>(L, FL);
+    point_flux<R, NSD, D>(Rt, FR);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        F[k] = R(0.5) * (FL[k] + FR[k]);
+    }
+    return fmax(fabs(L.ud) + sqrt(gamma * L.p / L.c[0]),
+        fabs(Rt.ud) + sqrt(gamma * Rt.p / Rt.c[0]));
+}
+
+// F(U-, U+) at one face along D.  ul = right-reconstructed value of the cell
+// left of the face, ur = left-reconstructed value of the cell to its right
+// (numflux_util.hpp:62-92).  Returns the face wave speed.
+template<class R, int NSD, int FLUX, int D>
+__device__ __forceinline__ R face_flux(const R* ul, const R* ur, R gamma, R* F) {
+    FaceState<R, NSD> L, Rt;
+    make_state<R, NSD, D>(ul, gamma, L);
+    make_state<R, NSD, D>(ur, gamma, Rt);
+    if (FLUX == FLUX_HLL) {
+        return flux_hll<R, NSD, D>(L, Rt, gamma, F);
+    } else if (FLUX == FLUX_HLL3) {
+        return flux_hll3<R, NSD, D>(L, Rt, gamma, F);
+    } else {
+        return flux_central<R, NSD, D>(L, Rt, gamma, F);
+    }
+}
+
+// ENO coefficients c[r][j] (ENOCoefficients.cpp:27-49), each the correctly
+// rounded double quotient, converted to R on use.
+static __constant__ double kEno2[3][2] = {{3.0 / 2.0, -1.0 / 2.0}, {1.0 / 2.0, 1.0 / 2.0},
+    {-1.0 / 2.0, 3.0 / 2.0}};
+static __constant__ double kEno3[4][3] = {{11.0 / 6.0, -7.0 / 6.0, 1.0 / 3.0},
+    {1.0 / 3.0, 5.0 / 6.0, -1.0 / 6.0}, {-1.0 / 6.0, 5.0 / 6.0, 1.0 / 3.0},
+    {1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0}};
+static __constant__ double kEno4[5][4] = {{25.0 / 12.0, -23.0 / 12.0, 13.0 / 12.0, -1.0 / 4.0},
+    {1.0 / 4.0, 13.0 / 12.0, -5.0 / 12.0, 1.0 / 12.0},
+    {-1.0 / 12.0, 7.0 / 12.0, 7.0 / 12.0, -1.0 / 12.0},
+    {1.0 / 12.0, -5.0 / 12.0, 13.0 / 12.0, 1.0 / 4.0},
+    {-1.0 / 4.0, 13.0 / 12.0, -23.0 / 12.0, 25.0 / 12.0}};
+
+template<class R, int ORDER>
+__device__ __forceinline__ R eno_coef(int r, int j) {
+    if (ORDER == 2) {
+        return R(kEno2[r][j]);
+    } else if (ORDER == 3) {
+        return R(kEno3[r][j]);
+    } else {
+        return R(kEno4[r][j]);
+    }
+}
+
+// Reconstructs the cell at `src` (pointer to variable 0 of the cell; the
+// variables are `vstride` apart and neighbours along the direction `s` apart).
+// Writes NV left and NV right values.
+template<class R, int NV, int RECON>
+__device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R* left, R* right) {
+    if (RECON == RECON_NONE) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            left[v] = src[v * vstride];
+            right[v] = src[v * vstride];
+        }
+    } else if (RECON == RECON_WENO2) {
+        const R eps = R(1e-8);
+        const R i0 = src[0];
+        const R dp = src[s] - i0;
+        const R dm = i0 - src[-s];
+        const R b0 = dp * dp;
+        const R b1 = dm * dm;
+        const R d0 = R(3) * (eps + b0) * (eps + b0);
+        const R d1 = R(3) * (eps + b1) * (eps + b1);
+        const R a0Left = R(1) / d0;
+        const R a1Left = R(2) / d1;
+        const R w0Left = a0Left / (a0Left + a1Left);
+        const R w1Left = a1Left / (a0Left + a1Left);
+        const R a0Right = R(2) / d0;
+        const R a1Right = R(1) / d1;
+        const R w0Right = a0Right / (a0Right + a1Right);
+        const R w1Right = a1Right / (a0Right + a1Right);
+        const R cl = R(3) * w0Left + w1Left;
+        const R cr = R(3) * w1Right + w0Right;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const R um = src[v * vstride - s];
+            const R u0 = src[v * vstride];
+            const R up = src[v * vstride + s];
+            left[v] = R(0.5) * (w1Left * um + cl * u0 - w0Left * up);
+            right[v] = R(0.5) * (w0Right * up + cr * u0 - w1Right * um);
+        }
+    } else {
+        constexpr int ORDER = RECON == RECON_ENO2 ? 2 : (RECON == RECON_ENO3 ? 3 : 4);
+        // undivided differences of rho at offsets -1..ORDER-2, level by level
+        R dd[ORDER];
+#pragma unroll
+        for (int k = -1; k <= ORDER - 2; ++k) {
+            dd[k + 1] = src[(k + 1) * s] - src[k * s];
+        }
+        int shift = 0;
+#pragma unroll
+        for (int level = 0; level < ORDER - 1; ++level) {
+            if (level > 0) {
+#pragma unroll
+                for (int k = -1; k <= ORDER - 2 - level; ++k) {
+                    dd[k + 1] = dd[k + 2] - dd[k + 1];
+                }
+            }
+            if (fabs(dd[0]) < fabs(dd[1])) {
+                shift++;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R lv = R(0), rv = R(0);
+#pragma unroll
+            for (int j = 0; j < ORDER; ++j) {
+                const R value = src[v * vstride - (shift - j) * s];
+                lv += eno_coef<R, ORDER>(shift, j) * value;
+                rv += eno_coef<R, ORDER>(shift + 1, j) * value;
+            }
+            left[v] = lv;
+            right[v] = rv;
+        }
+    }
+}
+
+} // namespace als

@@ -1,0 +1,9 @@
+// Stage-kernel instantiations for double precision, 1-D Euler.
+#include "stage_dispatch.cuh"
+
+namespace als {
+cudaError_t launch_stage_f64_1d(int recon, int flux, int kind, const StageParams& P,
+    int members, cudaStream_t s) {
+    return launch_stage_dim<double, 1>(recon, flux, kind, P, members, s);
+}
+} // namespace als

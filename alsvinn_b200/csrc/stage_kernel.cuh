@@ -1,0 +1,459 @@
+// The fused cell-update stage kernel.
+//
+// One thread block owns a tile of interior cells.  It stages the tile plus a
+// halo of G cells (every variable) in shared memory, then, direction by
+// direction, reconstructs every cell the faces need, evaluates each face
+// flux exactly once, and accumulates the net flux of its cells in registers.
+// The epilogue applies the Runge-Kutta stage combination, writes the result
+// and (optionally) the boundary images of the updated cell, so no separate
+// ghost-fill pass is needed.
+//
+// This replaces, per stage, the reference's chain of kernels and host syncs
+// (alsfvm/src/numflux/NumericalFluxCUDA.cu:39-160,263-414,
+//  alsfvm/src/reconstruction/ReconstructionCUDA.cu:31-100,
+//  alsfvm/src/cuda/vector_operations.cu:24-95,233-335,
+//  alsfvm/src/boundary/BoundaryCUDA.cu:26-160) while keeping the arithmetic
+// of the CPU path (alsfvm/src/numflux/NumericalFluxCPU.cpp:32-221,
+// alsfvm/src/integrator/{ForwardEuler,RungeKutta2,RungeKutta3}.cpp).
+//
+// The first stage of a time step stores the unscaled net flux L(U^n) and
+// reduces the face wave speeds; the second stage rebuilds U1 = (dt/dx)L + U^n
+// while it loads its halo, so the CFL max never needs a separate pass over
+// the state and no stage waits on the host.
+#pragma once
+
+#include "euler_math.cuh"
+#include "stage_params.h"
+
+namespace als {
+
+constexpr int kStageThreads = 256;
+
+template<int DIM> struct TileShape;
+template<> struct TileShape<1> { static constexpr int X = 256, Y = 1, Z = 1; };
+template<> struct TileShape<2> { static constexpr int X = 32, Y = 16, Z = 1; };
+template<> struct TileShape<3> { static constexpr int X = 8, Y = 8, Z = 4; };
+
+template<class R, int DIM, int RECON>
+struct StageLayout {
+    static constexpr int NV = DIM + 2;
+    static constexpr int G = recon_ghosts(RECON);
+    static constexpr int TX = TileShape<DIM>::X;
+    static constexpr int TY = TileShape<DIM>::Y;
+    static constexpr int TZ = TileShape<DIM>::Z;
+    static constexpr int BX = TX + 2 * G;
+    static constexpr int BY = DIM > 1 ? TY + 2 * G : 1;
+    static constexpr int BZ = DIM > 2 ? TZ + 2 * G : 1;
+    static constexpr int BOX = BX * BY * BZ;
+    static constexpr int CELLS = TX * TY * TZ;
+    static constexpr int CPT = CELLS / kStageThreads;
+    // reconstructed cells / faces per direction: the tile extent grows by 2 / 1 along it
+    static constexpr int REC0 = (TX + 2) * TY * TZ;
+    static constexpr int REC1 = DIM > 1 ? TX * (TY + 2) * TZ : 0;
+    static constexpr int REC2 = DIM > 2 ? TX * TY * (TZ + 2) : 0;
+    static constexpr int REC = REC0 > REC1 ? (REC0 > REC2 ? REC0 : REC2) : (REC1 > REC2 ? REC1 : REC2);
+    static constexpr int FAC0 = (TX + 1) * TY * TZ;
+    static constexpr int FAC1 = DIM > 1 ? TX * (TY + 1) * TZ : 0;
+    static constexpr int FAC2 = DIM > 2 ? TX * TY * (TZ + 1) : 0;
+    static constexpr int FAC = FAC0 > FAC1 ? (FAC0 > FAC2 ? FAC0 : FAC2) : (FAC1 > FAC2 ? FAC1 : FAC2);
+    static constexpr size_t SMEM = sizeof(R) * (size_t(NV) * BOX + size_t(2 * NV) * REC + size_t(NV) * FAC);
+    static_assert(CELLS % kStageThreads == 0, "tile must be a multiple of the block");
+};
+
+// dt of the step (Integrator.cpp:20-46) followed by the end-time clamp
+// (FixedIntervalWriter.cpp:45-53): dt = min(cfl / sum_d ws_d/dx_d, T - t).
+__device__ __forceinline__ double step_dt(const StepState* st) {
+    double total = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (st->dx[d] == 0) {
+            continue;
+        }
+        total += __longlong_as_double((long long)st->ws[d]) / st->dx[d];
+    }
+    double dt = st->cfl / total;
+    const double rest = st->end_time - st->t;
+    return rest < dt ? rest : dt;
+}
+
+// Padded positions that hold a copy of interior cell i along one direction
+// (the cell itself first).  Neumann mirrors (Neumann.hpp:24-35), periodic
+// wraps (Periodic.hpp:24-42); valid for n >= G.
+__device__ __forceinline__ int boundary_images(int i, int n, int G, int bc, int* pos) {
+    int c = 0;
+    pos[c++] = i + G;
+    if (bc == BC_PERIODIC) {
+        if (i >= n - G) {
+            pos[c++] = i + G - n;
+        }
+        if (i < G) {
+            pos[c++] = i + G + n;
+        }
+    } else {
+        if (i < G) {
+            pos[c++] = G - 1 - i;
+        }
+        if (i >= n - G) {
+            pos[c++] = 2 * n + G - 1 - i;
+        }
+    }
+    return c;
+}
+
+// Simulator::checkConstraints (CPUCellComputer.cpp:80-128, Euler.hpp:269-277):
+// all conserved values and p, u finite, rho > 0, p > 0.
+template<class R, int NV>
+__device__ __forceinline__ bool obeys_constraints(const R* U, R gamma) {
+    bool ok = true;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        ok = ok && isfinite(U[v]);
+    }
+    R dot = U[1] * U[1];
+    if (NV > 3) {
+        dot = dot + U[2] * U[2];
+    }
+    if (NV > 4) {
+        dot = dot + U[3] * U[3];
+    }
+    const R ie = U[NV - 1] - R(0.5) * dot / U[0];
+    const R p = (gamma - R(1)) * ie;
+#pragma unroll
+    for (int k = 1; k < NV - 1; ++k) {
+        ok = ok && isfinite(U[k] / U[0]);
+    }
+    return ok && isfinite(p) && (U[0] > R(0)) && (p > R(0));
+}
+
+template<class R>
+__device__ __forceinline__ R warp_max(R v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+template<class R, int DIM, int RECON, int FLUX, int KIND, int D>
+__device__ __forceinline__ void stage_direction(const StageParams& P, const R* box, R* rec, R* flx,
+    R (&acc)[StageLayout<R, DIM, RECON>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
+    typedef StageLayout<R, DIM, RECON> Lay;
+    constexpr int NV = Lay::NV;
+    constexpr int G = Lay::G;
+    // extents of the reconstructed-cell index space (x fastest), offset -1 along D
+    constexpr int E0 = Lay::TX + (D == 0 ? 2 : 0);
+    constexpr int E1 = Lay::TY + (D == 1 ? 2 : 0);
+    constexpr int RC = E0 * E1 * (Lay::TZ + (D == 2 ? 2 : 0));
+    // extents of the face index space, offset -1 along D
+    constexpr int F0 = Lay::TX + (D == 0 ? 1 : 0);
+    constexpr int F1 = Lay::TY + (D == 1 ? 1 : 0);
+    constexpr int FC = F0 * F1 * (Lay::TZ + (D == 2 ? 1 : 0));
+    constexpr int S = D == 0 ? 1 : (D == 1 ? Lay::BX : Lay::BX * Lay::BY);
+    const int tid = threadIdx.x;
+    const R gamma = R(P.gamma);
+
+    for (int i = tid; i < RC; i += kStageThreads) {
+        const int ex = i % E0;
+        const int ey = (i / E0) % E1;
+        const int ez = i / (E0 * E1);
+        const int bx = ex - (D == 0 ? 1 : 0) + G;
+        const int by = DIM > 1 ? ey - (D == 1 ? 1 : 0) + G : 0;
+        const int bz = DIM > 2 ? ez - (D == 2 ? 1 : 0) + G : 0;
+        const R* src = box + (bz * Lay::BY + by) * Lay::BX + bx;
+        R l[NV], r[NV];
+        reconstruct<R, NV, RECON>(src, Lay::BOX, S, l, r);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            rec[v * RC + i] = l[v];
+            rec[(NV + v) * RC + i] = r[v];
+        }
+    }
+    __syncthreads();
+
+    const int hiD = D == 0 ? P.grid.hi[0] : (D == 1 ? P.grid.hi[1] : P.grid.hi[2]);
+    const int oD = D == 0 ? x0 : (D == 1 ? y0 : z0);
+    for (int i = tid; i < FC; i += kStageThreads) {
+        const int fx = i % F0;
+        const int fy = (i / F0) % F1;
+        const int fz = i / (F0 * F1);
+        // face between reconstructed cells (fx,fy,fz) and its +D neighbour in E space
+        const int rl = (fz * E1 + fy) * E0 + fx;
+        const int rr = rl + (D == 0 ? 1 : (D == 1 ? E0 : E0 * E1));
+        R ul[NV], ur[NV], F[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            ul[v] = rec[(NV + v) * RC + rl];
+            ur[v] = rec[v * RC + rr];
+        }
+        const R w = face_flux<R, DIM, FLUX, D>(ul, ur, gamma, F);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            flx[v * FC + i] = F[v];
+        }
+        if (KIND == KIND_FLUX0) {
+            // the face lies between cells oD+f-1 and oD+f of the update region
+            const int f = D == 0 ? fx : (D == 1 ? fy : fz);
+            bool valid = oD + f - 1 <= hiD - 1;
+            if (D != 0) {
+                valid = valid && (x0 + fx < P.grid.hi[0]);
+            }
+            if (D != 1 && DIM > 1) {
+                valid = valid && (y0 + fy < P.grid.hi[1]);
+            }
+            if (D != 2 && DIM > 2) {
+                valid = valid && (z0 + fz < P.grid.hi[2]);
+            }
+            if (valid && wmax < w) {
+                wmax = w;
+            }
+        }
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < Lay::CPT; ++k) {
+        const int ci = tid + k * kStageThreads;
+        const int cx = ci % Lay::TX;
+        const int cy = (ci / Lay::TX) % Lay::TY;
+        const int cz = ci / (Lay::TX * Lay::TY);
+        // left face of cell c has face coordinate c (faces are offset by -1)
+        const int fl = (cz * F1 + cy) * F0 + cx;
+        const int fr = fl + (D == 0 ? 1 : (D == 1 ? F0 : F0 * F1));
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            // out += temp[x+1] + (-temp[x]) with temp = -F (NumericalFluxCPU.cpp:92,113)
+            const R tr = -flx[v * FC + fr];
+            const R tl = -flx[v * FC + fl];
+            acc[k][v] = acc[k][v] + (tr + (-tl));
+        }
+    }
+    __syncthreads();
+}
+
+template<class R, int DIM, int RECON, int FLUX, int KIND>
+__device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int member,
+    unsigned char* smem) {
+    typedef StageLayout<R, DIM, RECON> Lay;
+    constexpr int NV = Lay::NV;
+    constexpr int G = Lay::G;
+    constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
+    const int tid = threadIdx.x;
+    const GridDesc& gd = P.grid;
+    StepState* st = P.state ? P.state + member : nullptr;
+
+    R* box = reinterpret_cast<R*>(smem);
+    R* rec = box + NV * Lay::BOX;
+    R* flx = rec + 2 * NV * Lay::REC;
+
+    const int tx = tile % gd.tiles[0];
+    const int ty = (tile / gd.tiles[0]) % gd.tiles[1];
+    const int tz = tile / (gd.tiles[0] * gd.tiles[1]);
+    const int x0 = gd.lo[0] + tx * Lay::TX;
+    const int y0 = gd.lo[1] + ty * Lay::TY;
+    const int z0 = gd.lo[2] + tz * Lay::TZ;
+    const long long base = (long long)member * P.sample_stride;
+    const R* in = static_cast<const R*>(P.in) + base;
+    const R* un = static_cast<const R*>(P.un) + base;
+    R* out = static_cast<R*>(P.out) + base;
+    const long long plane = gd.plane;
+
+    R c = R(0);
+    if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
+        if (st) {
+            const double dt = step_dt(st);
+            if (tile == 0 && tid == 0) {
+                st->dt = dt;
+            }
+            c = R(dt / st->dx[0]);
+        } else {
+            c = R(P.c_fixed);
+        }
+    } else if (KIND == KIND_RK3_2) {
+        c = st ? R(st->dt / st->dx[0]) : R(P.c_fixed);
+    }
+
+    // stage the tile and its halo; U1 = (dt/dx)*L + U^n is formed here for the
+    // second stage (RungeKutta{2,3}.cpp: output *= dt/dx; output += U)
+    for (int i = tid; i < NV * Lay::BOX; i += kStageThreads) {
+        const int v = i / Lay::BOX;
+        const int b = i - v * Lay::BOX;
+        const int bx = b % Lay::BX;
+        const int by = (b / Lay::BX) % Lay::BY;
+        const int bz = b / (Lay::BX * Lay::BY);
+        const int px = x0 + bx;
+        const int py = DIM > 1 ? y0 + by : 0;
+        const int pz = DIM > 2 ? z0 + bz : 0;
+        R val = R(0);
+        if (px < gd.N[0] && py < gd.N[1] && pz < gd.N[2]) {
+            const long long idx = v * plane + ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
+            if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
+                val = in[idx] * c;
+                val = val + un[idx];
+            } else {
+                val = in[idx];
+            }
+        }
+        box[i] = val;
+    }
+    __syncthreads();
+
+    R acc[Lay::CPT][NV];
+#pragma unroll
+    for (int k = 0; k < Lay::CPT; ++k) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            acc[k][v] = R(0);
+        }
+    }
+    R wmax[3] = {R(0), R(0), R(0)};
+    stage_direction<R, DIM, RECON, FLUX, KIND, 0>(P, box, rec, flx, acc, wmax[0], x0, y0, z0);
+    if (DIM > 1) {
+        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 1 ? 1 : 0)>(P, box, rec, flx, acc, wmax[1], x0, y0, z0);
+    }
+    if (DIM > 2) {
+        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 2 ? 2 : 0)>(P, box, rec, flx, acc, wmax[2], x0, y0, z0);
+    }
+
+    bool bad = false;
+    long long bad_idx = 0;
+#pragma unroll
+    for (int k = 0; k < Lay::CPT; ++k) {
+        const int ci = tid + k * kStageThreads;
+        const int cx = ci % Lay::TX;
+        const int cy = (ci / Lay::TX) % Lay::TY;
+        const int cz = ci / (Lay::TX * Lay::TY);
+        const int gx = x0 + cx, gy = y0 + cy, gz = z0 + cz;
+        if (gx >= gd.hi[0] || (DIM > 1 && gy >= gd.hi[1]) || (DIM > 2 && gz >= gd.hi[2])) {
+            continue;
+        }
+        const int px = gx + G;
+        const int py = DIM > 1 ? gy + G : 0;
+        const int pz = DIM > 2 ? gz + G : 0;
+        const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
+        const int bidx = ((DIM > 2 ? cz + G : 0) * Lay::BY + (DIM > 1 ? cy + G : 0)) * Lay::BX + cx + G;
+        R val[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R x = acc[k][v];
+            if (KIND == KIND_RK2_1) {
+                // RungeKutta2.cpp:57-63
+                x = x * c;
+                x = x + box[v * Lay::BOX + bidx];
+                x = x + un[v * plane + idx];
+                x = x * R(0.5);
+            } else if (KIND == KIND_RK3_1) {
+                // RungeKutta3.cpp:65-78
+                x = x * c;
+                x = x + box[v * Lay::BOX + bidx];
+                x = x * R(1. / 3.);
+                x = x + un[v * plane + idx];
+                x = x * R(3. / 4.);
+            } else if (KIND == KIND_RK3_2) {
+                // RungeKutta3.cpp:65-83
+                x = x * c;
+                x = x + box[v * Lay::BOX + bidx];
+                x = x * R(2);
+                x = x + un[v * plane + idx];
+                x = x * R(1. / 3.);
+            }
+            val[v] = x;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            out[v * plane + idx] = val[v];
+        }
+        if (P.write_ghosts) {
+            int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
+            const int nxi = boundary_images(gx, gd.n[0], G, P.bc, ix);
+            const int nyi = DIM > 1 ? boundary_images(gy, gd.n[1], G, P.bc, iy) : 1;
+            const int nzi = DIM > 2 ? boundary_images(gz, gd.n[2], G, P.bc, iz) : 1;
+            if (nxi * nyi * nzi > 1) {
+                for (int a = 0; a < nzi; ++a) {
+                    for (int b = 0; b < nyi; ++b) {
+                        for (int e = 0; e < nxi; ++e) {
+                            if (a == 0 && b == 0 && e == 0) {
+                                continue;
+                            }
+                            const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
+#pragma unroll
+                            for (int v = 0; v < NV; ++v) {
+                                out[v * plane + j] = val[v];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (LAST && st && !obeys_constraints<R, NV>(val, R(P.gamma))) {
+            bad = true;
+            bad_idx = idx;
+        }
+    }
+
+    if (KIND == KIND_FLUX0) {
+        __shared__ double wsh[3][kStageThreads / 32];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const R w = warp_max(wmax[d]);
+            if ((tid & 31) == 0) {
+                wsh[d][tid >> 5] = double(w);
+            }
+        }
+        __syncthreads();
+        if (tid < DIM) {
+            double m = 0;
+            for (int k = 0; k < kStageThreads / 32; ++k) {
+                m = fmax(m, wsh[tid][k]);
+            }
+            unsigned long long* dst = st ? &st->ws[tid] : (P.ws_out + 3 * member + tid);
+            atomicMax(dst, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+
+    if (LAST && st) {
+        if (bad) {
+            atomicOr(&st->status, 1);
+            atomicMin((unsigned long long*)&st->bad_index, (unsigned long long)bad_idx);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            const unsigned int prev = atomicAdd(&st->arrive, 1u);
+            const unsigned int total = gd.tiles[0] * gd.tiles[1] * gd.tiles[2];
+            if (prev == total - 1) {
+                // every tile of this member is done: advance time (Simulator.cpp:211-213)
+                __threadfence();
+                volatile StepState* vs = st;
+                const double t = vs->t + vs->dt;
+                vs->t = t;
+                vs->steps = vs->steps + 1;
+                vs->ws[0] = 0;
+                vs->ws[1] = 0;
+                vs->ws[2] = 0;
+                vs->arrive = 0;
+                if (vs->status != 0 && vs->bad_step < 0) {
+                    vs->bad_step = vs->steps;
+                }
+                if (t >= vs->end_time || vs->status != 0 || vs->steps >= vs->max_steps) {
+                    vs->done = 1;
+                }
+            }
+        }
+    }
+}
+
+template<class R, int DIM, int RECON, int FLUX, int KIND>
+__global__ void __launch_bounds__(kStageThreads)
+stage_kernel(const StageParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int member = P.member0 + blockIdx.y;
+    if (P.state) {
+        const volatile StepState* st = P.state + member;
+        if (st->done) {
+            return;
+        }
+    }
+    stage_tile<R, DIM, RECON, FLUX, KIND>(P, blockIdx.x, member, smem);
+}
+
+} // namespace als

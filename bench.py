@@ -1,0 +1,318 @@
+"""Benchmark of the cell-update hot path: cell-updates/s on B200.
+
+Default workload: 2-D Euler Kelvin-Helmholtz, 1024x1024 periodic unit
+square, FP64, WENO2 + HLL3, SSP-RK3, CFL 0.4 (the plain GPU drop-in
+configuration).  One bench step = one full time step (CFL reduction and
+three Runge-Kutta stages) over the whole grid.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank advances its own Kelvin-Helmholtz sample (sample
+index = rank): ensemble members are independent, so ranks share no data and
+no collective runs inside the timed region (weak scaling).  Timing: per-step
+CUDA events on the solver's stream with an L2 flush (a 512 MiB write)
+between timed steps, barrier + synchronize around the timed region, max over
+ranks.  `--impl reference` times the reference's own CPU implementation
+(oracle/_ref, the unmodified reference sources) on the host cores.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+N = 1024
+DIM = 2
+NVAR = 4
+GHOSTS = 2
+FLUX, RECON, INTEG, BC, CFL = "hll3", "weno2", "rungekutta3", "periodic", 0.4
+METRIC = "cell-updates/s (2-D Euler KH 1024^2, WENO2+HLL3, RK3, FP64)"
+WORKLOAD = {"workload": "kelvin-helmholtz 2-D Euler 1024x1024 periodic, FP64, weno2+hll3, "
+                        "rungekutta3, cfl 0.4; one step = one full time step",
+            "cells": N * N, "precision": "fp64", "l2": "flushed between timed steps (512 MiB write)"}
+# algorithmic bytes per interior cell and launch (FP64, 4 planes):
+#   stage 0 reads U^n, writes L                    -> 2 plane passes
+#   stage 1 reads L and U^n, writes U2             -> 3
+#   stage 2 reads U2 and U^n, writes U^{n+1}       -> 3
+ALG_BYTES_PER_CELL = {"flux0": 2 * NVAR * 8, "rk3_1": 3 * NVAR * 8, "rk3_2": 3 * NVAR * 8}
+KERNEL_NAMES = ["flux0", "rk3_1", "rk3_2"]
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def kh_state(sample):
+    import alsvinn_b200 as als
+    params = als.uniform_draws(40, sample, 1)[0]
+    return als.kelvin_helmholtz(N, params, GHOSTS)
+
+
+def cpu_baseline(state, target_seconds=12.0):
+    """The reference's own CPU path (oracle/_ref) on a bounded sample of the
+    same workload, all host threads; falls back to the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import COracle, RefOracle, ref_library_path
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if os.path.exists(ref_library_path()):
+        ref = RefOracle()
+        steps = 2
+        while True:
+            rc, _, _, done, _ = ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC,
+                                             1.4, CFL, 2.0, state, max_steps=steps)
+            secs = ref.lib.alsref_last_loop_seconds()
+            if secs * 2 > target_seconds or steps >= 64:
+                break
+            steps = max(steps + 1, int(steps * target_seconds / max(secs, 1e-3) * 0.6))
+            steps = min(steps, 64)
+        kind, sample = "reference", "%d time steps of the same KH 1024^2 state" % done
+        threads = int(os.environ.get("OMP_NUM_THREADS", cores))
+    else:
+        c = COracle()
+        cfg = c.config(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC, 1.4)
+        done = 2
+        t0 = time.perf_counter()
+        c.simulate(cfg, state, CFL, 2.0, max_steps=done)
+        secs = time.perf_counter() - t0
+        kind, sample, threads = "port", "%d time steps of the same KH 1024^2 state" % done, 1
+    return {"value": N * N * done / secs, "unit": "cell-updates/s", "cores": threads,
+            "kind": kind, "sample": sample, "seconds": secs}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    state = kh_state(0)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import RefOracle, ref_library_path
+    if not os.path.exists(ref_library_path()):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (reference CPU build) missing on this machine"}))
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    ref = RefOracle()
+    # each bench step: one full KH 1024^2 time step by the reference's CPU code
+    ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC, 1.4, CFL, 2.0, state,
+                 max_steps=args.warmup)
+    rc, _, _, steps, _ = ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC, 1.4,
+                                      CFL, 2.0, state, max_steps=args.steps)
+    secs = ref.lib.alsref_last_loop_seconds()
+    value = N * N * steps / secs
+    out = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": secs / steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": WORKLOAD, "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": "cell-updates/s",
+                            "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
+                            "sample": "%d time steps of KH 1024^2 (reference CPU sources, OpenMP)"
+                            % steps},
+           "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import alsvinn_b200 as als
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    state = kh_state(rank)
+    sim = als.Simulator(DIM, (N, N), (0, 0), (1, 1), flux=FLUX, reconstruction=RECON,
+                        integrator=INTEG, boundary=BC, cfl=CFL, end_time=1e9, device=local)
+    sim.set_state(state)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1.0)
+            sim.advance(1)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.3)
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            sim.advance(1)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        clock_info = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms = float(t.item())
+    info = sim.info()
+    if info["status"] != 0:
+        raise RuntimeError("constraint violation during the bench: %r" % info)
+
+    # per-kernel durations for the roofline (events around each kernel)
+    kms = np.array([sim.profile_step() for _ in range(5)])
+    avg_k = kms.mean(axis=0)
+    hbm_peak, peak_kind = peaks()
+    cells = N * N
+    roof = []
+    for name, ms in zip(KERNEL_NAMES, avg_k):
+        achieved = ALG_BYTES_PER_CELL[name] * cells / (ms * 1e-3) / 1e9
+        roof.append({"kernel": name, "ms": float(ms), "achieved_gbs": achieved})
+    dom = max(range(len(roof)), key=lambda i: roof[i]["ms"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_kh1024.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(KERNEL_NAMES[dom])
+
+    # end to end through the public API with host buffers: upload the state
+    # from pinned memory, advance the same number of steps, download it
+    pinned_in = torch.from_numpy(state).pin_memory()
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    sim.set_state(pinned_in.numpy())
+    sim.advance(args.warmup)
+    sim.synchronize()
+    e2e_steps = args.steps
+    t0 = time.perf_counter()
+    sim.set_state(pinned_in.numpy())
+    sim.advance(e2e_steps)
+    out = pinned_out.numpy()
+    sim._lib.als_solver_get_state(sim._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0, 1)
+    e2e_secs = time.perf_counter() - t0
+    tt = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_secs = float(tt.item())
+    state_bytes = state.nbytes
+
+    value = world * cells * args.steps / (total_ms * 1e-3)
+    result = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Kelvin-Helmholtz initial data, sample index = rank)",
+        "config": dict(WORKLOAD, parallelism="independent ensemble members per GPU (replicas)"),
+        "roofline": {"bound": "hbm", "achieved": roof[dom]["achieved_gbs"],
+                     "peak": hbm_peak, "unit": "GB/s",
+                     "frac": roof[dom]["achieved_gbs"] / hbm_peak, "traffic": traffic,
+                     "kernel": "stage kernel '%s' (%.4f ms)" % (roof[dom]["kernel"], roof[dom]["ms"]),
+                     "peak_source": peak_kind, "per_kernel": roof,
+                     "note": "FP64 divide/sqrt-bound; HBM fraction is of measured copy bandwidth"},
+        "e2e": {"value": world * cells * e2e_steps / e2e_secs, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": state_bytes / e2e_steps,
+                "d2h_bytes_per_step": state_bytes / e2e_steps,
+                "definition": "als_solver_set_state(pinned host) + %d steps + als_solver_get_state"
+                              "(pinned host), wall clock" % e2e_steps},
+        "gpu_launches": args.steps * sim.launches_per_step(),
+        "clocks": clock_info,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(state)
+    if rank == 0:
+        print(json.dumps(result))
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

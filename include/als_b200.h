@@ -1,0 +1,190 @@
+/*
+ * als_b200.h -- C ABI of the B200 cell-update hot path of alsfvm.
+ *
+ * Plain C types only: device pointers are `void*`/`double*` obtained from
+ * cudaMalloc (or any allocator of device memory), streams are passed as
+ * `void*` (a cudaStream_t; NULL = legacy default stream).  Every function
+ * returns ALS_OK (0) or a negative ALS_E* code; als_last_error() gives a
+ * readable message for the calling thread.  No C++ exception crosses the
+ * ABI.
+ *
+ * Data layout (alsfvm::volume::Volume, alsfvm/src/volume/Volume.cpp:44-60,
+ * alsfvm/include/alsfvm/memory/View.hpp): one contiguous plane per conserved
+ * variable, (nx+2g)(ny+2g)(nz+2g) cells each with x fastest, no pitch;
+ * inactive directions have extent 1 and no ghost cells.  Variable order
+ * rho, mx, [my, [mz,]] E (alsfvm/src/equation/euler/Euler.cpp:20-75).
+ * An ensemble of M members stores its members one after another.
+ */
+#ifndef ALS_B200_H
+#define ALS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ codes */
+#define ALS_OK 0
+#define ALS_E_INVALID (-1)          /* bad argument */
+#define ALS_E_CUDA (-2)             /* a CUDA call failed */
+#define ALS_E_CONSTRAINT (-3)       /* Simulator::checkConstraints would throw */
+#define ALS_E_UNSUPPORTED (-4)      /* combination not built */
+#define ALS_E_NOMEM (-5)
+
+/* names as in the reference's XML (<flux>, <reconstruction>, <integrator>, <boundary>) */
+#define ALS_FLUX_HLL 0              /* "hll",     numflux/euler/HLL.hpp */
+#define ALS_FLUX_HLL3 1             /* "hll3",    numflux/euler/HLL3.hpp */
+#define ALS_FLUX_CENTRAL 2          /* "central", numflux/Central.hpp */
+#define ALS_RECON_NONE 0            /* "none",  reconstruction/NoReconstruction.cpp */
+#define ALS_RECON_WENO2 1           /* "weno2", reconstruction/WENO2.hpp */
+#define ALS_RECON_ENO2 2            /* "eno2",  reconstruction/ENOCPU.cpp */
+#define ALS_RECON_ENO3 3            /* "eno3" */
+#define ALS_RECON_ENO4 4            /* "eno4" */
+#define ALS_INT_FORWARD_EULER 0     /* "forwardeuler", integrator/ForwardEuler.cpp */
+#define ALS_INT_RK2 1               /* "rungekutta2",  integrator/RungeKutta2.cpp */
+#define ALS_INT_RK3 2               /* "rungekutta3",  integrator/RungeKutta3.cpp */
+#define ALS_BC_NEUMANN 0            /* "neumann",  boundary/Neumann.hpp */
+#define ALS_BC_PERIODIC 1           /* "periodic", boundary/Periodic.hpp */
+#define ALS_FP64 0
+#define ALS_FP32 1
+
+const char* als_last_error(void);
+int als_version(void);
+
+/* Ghost width of a flux/reconstruction pair: max(stencil-1, reconstruction
+ * ghosts).  Replaces NumericalFlux::getNumberOfGhostCells,
+ * alsfvm/src/numflux/NumericalFluxCPU.cpp:227-231 (and
+ * Reconstruction::getNumberOfGhostCells, reconstruction/Reconstruction.hpp:56). */
+int als_ghost_cells(int flux, int reconstruction);
+
+/* ------------------------------------------------ plug-in level calls
+ * Each call works on caller-owned device planes, is stream ordered, and
+ * has the meaning of one virtual call of the reference interface it cites.
+ */
+typedef struct {
+    int dimension;      /* 1, 2 or 3 */
+    int n[3];           /* interior cells (1 for inactive directions) */
+    int ghosts;         /* ghost width of the planes */
+    double gamma;
+} als_grid;
+
+/* Boundary::applyBoundaryConditions(Volume&, const Grid&)
+ * (alsfvm/include/alsfvm/boundary/Boundary.hpp:30-31; BoundaryCPU.cpp:30-106).
+ * Fills the ghost cells of `nvar` planes of `members` consecutive states.
+ * Requires n >= ghosts in every active direction. */
+int als_fill_ghosts(const als_grid* grid, int boundary, double* planes, int nvar, int members,
+    void* stream);
+
+/* NumericalFlux::computeFlux(const Volume&, rvec3& waveSpeed, bool, Volume& out,
+ * const ivec3& start, const ivec3& end)
+ * (alsfvm/include/alsfvm/numflux/NumericalFlux.hpp:44-52; NumericalFluxCPU.cpp:171-221).
+ * `out` receives the net flux of the interior cells in the region
+ * [start, n+end) (start/end as in the reference: offsets from the interior
+ * bounds, end <= 0); other cells are left untouched.  `wave_speed` (host,
+ * 3 doubles) receives the maximal face wave speed per direction; the call
+ * synchronises `stream` to read it back, like the reference's CUDA path. */
+int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* in,
+    double* out, const int* start, const int* end, double* wave_speed, void* stream);
+
+/* Reconstruction::performReconstruction(const Volume& in, size_t direction,
+ * size_t indicatorVariable=0, Volume& left, Volume& right)
+ * (alsfvm/include/alsfvm/reconstruction/Reconstruction.hpp:46-58;
+ * ReconstructionCPU.cpp:37-97, ENOCPU.cpp:41-187).  The indicator is rho. */
+int als_reconstruct(const als_grid* grid, int reconstruction, int direction, const double* in,
+    double* left, double* right, void* stream);
+
+/* Stage combination of Integrator::performSubstep
+ * (alsfvm/include/alsfvm/integrator/Integrator.hpp:59-80; ForwardEuler.cpp:32-51,
+ * RungeKutta2.cpp:37-67, RungeKutta3.cpp:49-86) over `count` elements:
+ * on entry out = L(U_substep); us = U_substep, u0 = U_0; c = dt/dx. */
+int als_integrator_combine(int integrator, int substep, double* out, const double* us,
+    const double* u0, size_t count, double c, void* stream);
+
+/* Integrator::computeTimestep + adjustTimestep with an end-time clamp
+ * (alsfvm/src/integrator/Integrator.cpp:20-46, alsfvm/src/io/FixedIntervalWriter.cpp:45-53):
+ * dt = min(cfl / sum_d ws_d/dx_d, end_time - t).  Host-only arithmetic. */
+double als_compute_timestep(const double* wave_speed, const double* cell_lengths, double cfl,
+    double t, double end_time);
+
+/* ----------------------------------------------------- fused solver
+ * Owns the state of one simulation or of an ensemble of `members`
+ * simulations of the same grid, and advances whole time steps with no host
+ * round trip: the time step, the CFL dt and the end-time test live on the
+ * device.  Replaces Simulator::incrementSolution + checkConstraints
+ * (alsfvm/src/simulator/Simulator.cpp:180-214) and, for ensembles, the
+ * serial sample loop of alsuq::run::Runner::run (alsuq/src/run/Runner.cpp:42-78).
+ */
+typedef struct {
+    int dimension;
+    int n[3];
+    double lower[3];    /* domain corners; cell lengths as Grid.cpp:24-41 */
+    double upper[3];
+    int flux;
+    int reconstruction;
+    int integrator;
+    int boundary;
+    double gamma;
+    double cfl;
+    double end_time;
+    long long max_steps; /* <= 0: unlimited */
+    int precision;      /* ALS_FP64, or ALS_FP32 for ensemble members */
+    int members;        /* ensemble size, >= 1 */
+} als_solver_config;
+
+typedef struct {
+    double t;
+    double dt;          /* dt of the last completed step */
+    long long steps;
+    int done;
+    int status;         /* 0 ok, 1 constraint violation */
+    long long bad_index;  /* padded cell index of the first violation, or -1 */
+    long long bad_step;   /* step at which it was detected, or -1 */
+} als_member_info;
+
+typedef struct als_solver als_solver;
+
+int als_solver_create(const als_solver_config* cfg, int device, als_solver** out);
+int als_solver_destroy(als_solver* s);
+/* padded cells per plane and the ghost width the solver uses */
+int als_solver_geometry(const als_solver* s, long long* plane, int* ghosts);
+/* Uploads member states (host, FP64, padded planes; ghost cells are filled
+ * by the solver), resets time and step counters of those members. */
+int als_solver_set_state(als_solver* s, const double* host, int first_member, int count);
+/* Same from device memory already in the solver's precision. */
+int als_solver_set_state_device(als_solver* s, const void* dev, int first_member, int count);
+/* Downloads member states as FP64 into `host` (padded planes). */
+int als_solver_get_state(als_solver* s, double* host, int first_member, int count);
+/* Device pointer of the current state of member 0 (layout as above, members consecutive). */
+int als_solver_state_pointer(als_solver* s, void** dev);
+/* Enqueues `steps` time steps on the solver's stream (no synchronisation);
+ * members that are done skip them. */
+int als_solver_advance(als_solver* s, long long steps);
+/* Advances until every member is done (t >= end_time, max_steps, or a
+ * constraint violation); returns ALS_E_CONSTRAINT if any member failed. */
+int als_solver_run(als_solver* s);
+int als_solver_info(als_solver* s, int member, als_member_info* info);
+int als_solver_synchronize(als_solver* s);
+/* the stream the solver enqueues on (a cudaStream_t) */
+void* als_solver_stream(als_solver* s);
+/* Kernel launches a single time step issues (for launch accounting). */
+int als_solver_launches_per_step(const als_solver* s);
+/* Runs one time step with CUDA events around each kernel (the reference's
+ * ALSVINN_TIME_CUDA_BLOCK, alsutils/include/alsutils/timer/CudaTimer.hpp:42-47);
+ * kernel_ms[k] receives the duration of kernel k.  Synchronises; returns the
+ * number of kernels. */
+int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity);
+
+/* ------------------------------------------------------- UQ sampling
+ * Parameter draws of samples [first_sample, first_sample+count) for a
+ * parameter of length `dimension`: out[k*dimension + c].  Same numbers as
+ * alsuq's STLMersenne generator with a Uniform(lower, upper) distribution
+ * (alsuq/src/generator/STLMersenne.cpp:38-85, alsuq/src/distribution/Uniform.cpp:27-34,
+ * alsuq/src/samples/SampleGenerator.cpp:29-56).  Host-only. */
+int als_uniform_draws(long long dimension, long long first_sample, long long count,
+    double lower, double upper, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -404,6 +404,12 @@ void orc_reconstruct(const orc_config* cfg, int dir, const double* in, double* l
     long s;
     int lo[3], hi[3], d, x, y, z, var;
     padded(cfg, N);
+    if (cfg->recon == ORC_RECON_NONE) {
+        /* NoReconstruction copies every cell, ghosts included (NoReconstruction.cpp:51-61) */
+        memcpy(left, in, sizeof(double) * (size_t)nvar * (size_t)plane);
+        memcpy(right, in, sizeof(double) * (size_t)nvar * (size_t)plane);
+        return;
+    }
     s = dir == 0 ? 1 : (dir == 1 ? N[0] : (long)N[0] * N[1]);
     for (d = 0; d < 3; ++d) {
         const int gd = d < cfg->dim ? g : 0;

@@ -44,6 +44,7 @@
 #include "alsuq/generator/STLMersenne.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -54,6 +55,7 @@ using namespace alsfvm;
 namespace {
 
 std::string g_last_error;
+double g_last_loop_seconds = 0;
 
 struct Setup {
     int dim;
@@ -217,6 +219,12 @@ const char* alsref_last_error() {
     return g_last_error.c_str();
 }
 
+// Wall time of the step loop of the last alsref_simulate call (set-up,
+// initial boundary fill and copies excluded): the timed CPU baseline.
+double alsref_last_loop_seconds() {
+    return g_last_loop_seconds;
+}
+
 // Ghost width the reference picks for a flux/reconstruction pair
 // (NumericalFluxCPU.cpp:227-231).
 int alsref_ghost_cells(int dim, const char* flux, const char* recon) {
@@ -266,6 +274,7 @@ int alsref_simulate(int dim, const int* n, const double* lower, const double* up
         simulator::TimestepInformation info;
         int status = 0;
         long steps = 0;
+        const auto loop_start = std::chrono::steady_clock::now();
         while (info.getCurrentTime() < end_time && steps < max_steps) {
             real dt = 0;
             for (size_t substep = 0; substep < o.integ->getNumberOfSubsteps(); ++substep) {
@@ -285,6 +294,8 @@ int alsref_simulate(int dim, const int* n, const double* lower, const double* up
                 break;
             }
         }
+        g_last_loop_seconds = std::chrono::duration<double>(
+            std::chrono::steady_clock::now() - loop_start).count();
         copyOut(*volumes[0], planes);
         if (steps_out) {
             *steps_out = steps;

@@ -1,0 +1,114 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own CPU code.
+
+TEST INFRASTRUCTURE ONLY.  Run where the reference tree is available:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Every fixture is produced by oracle/_ref/libalsref.so, i.e. the reference's
+unmodified CPU sources (NumericalFluxCPU, ReconstructionCPU, ENOCPU,
+ForwardEuler/RungeKutta2/RungeKutta3, BoundaryCPU, ConservedSystem,
+MeanVariance arithmetic, STLMersenne), driven like Simulator::incrementSolution.
+Inputs are stored next to the outputs so the fixtures do not depend on the
+initial-data generators that made them.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle_lib import RefOracle, digest, ghost_cells, smooth_random_state  # noqa: E402
+
+# name: (dim, n, lower, upper, flux, recon, integrator, bc, cfl, end_time, init)
+SIMULATIONS = {
+    "sod1024_weno2_hll_rk3": (1, (1024,), (-1.0,), (1.0,), "hll", "weno2", "rungekutta3",
+                              "neumann", 0.45, 0.2, "sod"),
+    "sod256_eno3_hll3_rk2": (1, (256,), (-1.0,), (1.0,), "hll3", "eno3", "rungekutta2",
+                             "neumann", 0.45, 0.2, "sod"),
+    "sod128_none_hll_fe": (1, (128,), (-1.0,), (1.0,), "hll", "none", "forwardeuler",
+                           "neumann", 0.45, 0.2, "sod"),
+    "kh16_weno2_central_rk3": (2, (16, 16), (0.0, 0.0), (1.0, 1.0), "central", "weno2",
+                               "rungekutta3", "periodic", 0.4, 0.02, "kh"),
+    "kh32_weno2_hll3_rk3": (2, (32, 32), (0.0, 0.0), (1.0, 1.0), "hll3", "weno2", "rungekutta3",
+                            "periodic", 0.4, 0.3, "kh"),
+    "kh24_eno2_hll_rk2": (2, (24, 24), (0.0, 0.0), (1.0, 1.0), "hll", "eno2", "rungekutta2",
+                          "periodic", 0.4, 0.1, "kh"),
+    "kh20_eno4_hll3_fe_neumann": (2, (20, 20), (0.0, 0.0), (1.0, 1.0), "hll3", "eno4",
+                                  "forwardeuler", "neumann", 0.3, 0.05, "kh"),
+    "kh3d_12_weno2_hll3_rk3": (3, (12, 12, 12), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3", "weno2",
+                               "rungekutta3", "periodic", 0.4, 0.05, "kh3"),
+    # seeded smooth random states: variation along every direction
+    "rand2d_20x18_weno2_hll3_rk3": (2, (20, 18), (0.0, 0.0), (1.0, 1.0), "hll3", "weno2",
+                                    "rungekutta3", "periodic", 0.4, 0.05, "seed:11"),
+    "rand2d_16x17_eno3_hll_rk3_neumann": (2, (16, 17), (0.0, 0.0), (1.0, 1.0), "hll", "eno3",
+                                          "rungekutta3", "neumann", 0.4, 0.05, "seed:12"),
+    "rand3d_9x8x10_weno2_hll3_rk3": (3, (9, 8, 10), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3",
+                                     "weno2", "rungekutta3", "periodic", 0.4, 0.03, "seed:13"),
+    "rand3d_8x8x8_eno2_central_rk2": (3, (8, 8, 8), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "central",
+                                      "eno2", "rungekutta2", "neumann", 0.3, 0.02, "seed:14"),
+}
+
+
+def initial_state(kind, dim, n, g):
+    import alsvinn_b200.initial_data as init
+    if kind.startswith("seed:"):
+        return smooth_random_state(int(kind[5:]), dim, n, g)
+    if kind == "sod":
+        return init.sod(n[0], g)
+    params = np.asarray(RefOracle().stlmersenne(40, 0, 1)[0])
+    return init.kelvin_helmholtz(n[0], params, g, dimension=3 if kind == "kh3" else 2)
+
+
+def main():
+    ref = RefOracle()
+    out = {}
+    # the generator is a process-wide singleton: draw first, in sample order
+    draws = ref.stlmersenne(40, 0, 3)
+    np.savez_compressed(os.path.join(HERE, "stlmersenne_40x3.npz"), draws=draws)
+    for name, (dim, n, lo, hi, flux, recon, integ, bc, cfl, T, kind) in SIMULATIONS.items():
+        g = ghost_cells(recon)
+        U0 = initial_state(kind, dim, n, g)
+        rc, U, dts, steps, t = ref.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, cfl, T, U0)
+        assert rc == 0, name
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), initial=U0, final=U, dts=dts,
+                            steps=steps, t=t, dim=dim, n=np.array(n), lower=np.array(lo),
+                            upper=np.array(hi), flux=flux, recon=recon, integrator=integ, bc=bc,
+                            cfl=cfl, end_time=T, gamma=1.4)
+        out[name] = (steps, t)
+    # one spatial-operator evaluation per (dim, reconstruction, flux, boundary):
+    # seeded inputs, digest of the reference's net flux and wave speeds
+    cases = []
+    seed = 1000
+    for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
+        for recon in ("none", "weno2", "eno2", "eno3", "eno4"):
+            g = ghost_cells(recon)
+            if min(n) < 2 * g:
+                continue
+            for flux in ("hll", "hll3", "central"):
+                for bc in ("neumann", "periodic"):
+                    seed += 1
+                    st = smooth_random_state(seed, dim, n, g)
+                    lo = [0.0] * dim
+                    hi = [1.0] * dim
+                    filled, net, ws = ref.compute_flux(dim, n, lo, hi, flux, recon, bc, 1.4, st)
+                    cases.append((dim, ",".join(map(str, n)), recon, flux, bc, seed,
+                                  digest(filled), digest(net), digest(ws), float(ws.max())))
+    with open(os.path.join(HERE, "compute_flux_cases.txt"), "w") as f:
+        f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
+                "sha256(wave speeds) max_wave_speed\n")
+        for c in cases:
+            f.write("%d %s %s %s %s %d %s %s %s %.17g\n" % c)
+    states = np.stack([smooth_random_state(77 + k, 2, (6, 5), 2) for k in range(7)])
+    mean, var = ref.meanvar(2, (6, 5), 2, states)
+    np.savez_compressed(os.path.join(HERE, "meanvar_7.npz"), mean=mean, var=var,
+                        seeds=np.arange(77, 84))
+    for k, v in out.items():
+        print(k, "steps=%d t=%r" % v)
+
+
+if __name__ == "__main__":
+    main()

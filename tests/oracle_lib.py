@@ -151,6 +151,7 @@ class RefOracle:
         self.lib = ctypes.CDLL(path)
         L = self.lib
         L.alsref_last_error.restype = ctypes.c_char_p
+        L.alsref_last_loop_seconds.restype = ctypes.c_double
         L.alsref_simulate.argtypes = [ctypes.c_int, _I, _D, _D, ctypes.c_char_p,
                                       ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -226,3 +227,27 @@ class RefOracle:
         out = np.zeros(dimension * count)
         self._check(self.lib.alsref_stlmersenne(dimension, first, count, _dptr(out)))
         return out.reshape(count, dimension)
+
+
+def smooth_random_state(seed, dim, n, g, gamma=1.4, amplitude=0.1, velocity=0.2):
+    """A seeded random state near rho = p = 1 (padded planes, ghosts random too).
+
+    Uses numpy's PCG64, so the same seed gives the same state wherever the
+    same numpy runs (fixtures store a digest of the reference outputs for
+    such inputs)."""
+    rng = np.random.default_rng(seed)
+    shp = padded_shape(dim, n, g)
+    rho = rng.uniform(1 - amplitude, 1 + amplitude, shp[1:])
+    p = rng.uniform(1 - amplitude, 1 + amplitude, shp[1:])
+    u = [rng.uniform(-velocity, velocity, shp[1:]) for _ in range(dim)]
+    E = p / (gamma - 1) + 0.5 * rho * sum(x * x for x in u)
+    return np.ascontiguousarray(np.stack([rho] + [rho * x for x in u] + [E]))
+
+
+def digest(*arrays):
+    """sha256 of the exact bytes of float64 arrays (bit-exact comparison)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()

@@ -1,0 +1,246 @@
+"""Parity of the CUDA path with the oracle, through the C ABI.
+
+Every comparison of the FP64 path is bit-exact (assert_array_equal): the
+kernels keep the reference's operation order and are compiled with
+-fmad=false and IEEE division / square root.
+"""
+import zlib
+
+import numpy as np
+import pytest
+import torch
+
+import alsvinn_b200 as als
+from alsvinn_b200 import _lib
+from conftest import SIMULATION_FIXTURES, flux_cases, load_golden
+from oracle_lib import digest, ghost_cells, padded_shape, smooth_random_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def _sim(z, **kw):
+    return als.Simulator(z["dim"], tuple(z["n"]), tuple(z["lower"]), tuple(z["upper"]),
+                         flux=z["flux"], reconstruction=z["recon"], integrator=z["integrator"],
+                         boundary=z["bc"], gamma=z["gamma"], cfl=z["cfl"], end_time=z["end_time"],
+                         **kw)
+
+
+@pytest.mark.parametrize("name", SIMULATION_FIXTURES)
+def test_fused_solver_reproduces_reference_fixture(name):
+    z = load_golden(name)
+    with _sim(z) as sim:
+        sim.set_state(z["initial"])
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["steps"] == z["steps"]
+    assert info["t"] == z["t"]
+    assert info["dt"] == z["dts"][-1]
+    np.testing.assert_array_equal(U, z["final"])
+
+
+def test_sod_1024_reference_numbers():
+    z = load_golden("sod1024_weno2_hll_rk3")
+    with _sim(z) as sim:
+        sim.set_state(als.sod(1024))
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["steps"] == 498 and info["t"] == 0.2
+    assert U[0, 0, 0, 2 + 512] == 0.42568131167974621
+
+
+CASES = []
+for _dim, _n in ((1, (40,)), (2, (19, 21)), (3, (10, 9, 11))):
+    for _recon in ("none", "weno2", "eno2", "eno3", "eno4"):
+        if min(_n) < 2 * ghost_cells(_recon):
+            continue
+        for _flux in ("hll", "hll3", "central"):
+            for _integ in ("forwardeuler", "rungekutta2", "rungekutta3"):
+                for _bc in ("neumann", "periodic"):
+                    CASES.append((_dim, _n, _recon, _flux, _integ, _bc))
+
+
+@pytest.mark.parametrize("dim,n,recon,flux,integ,bc", CASES,
+                         ids=["d%d-%s-%s-%s-%s" % (c[0], c[2], c[3], c[4], c[5]) for c in CASES])
+def test_fused_solver_matches_oracle(c_oracle, dim, n, recon, flux, integ, bc):
+    g = ghost_cells(recon)
+    seed = zlib.crc32(("%d-%s-%s-%s-%s" % (dim, recon, flux, integ, bc)).encode()) % 100000
+    st = smooth_random_state(seed, dim, n, g)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    cfg = c_oracle.config(dim, n, lo, hi, flux, recon, integ, bc, 1.4)
+    rc, U_ref, dts, steps, t = c_oracle.simulate(cfg, st, 0.4, 0.04)
+    assert rc == 0 and steps >= 2
+    with als.Simulator(dim, n, lo, hi, flux=flux, reconstruction=recon, integrator=integ,
+                       boundary=bc, cfl=0.4, end_time=0.04) as sim:
+        sim.set_state(st)
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["steps"] == steps and info["t"] == t
+    np.testing.assert_array_equal(U, U_ref)
+
+
+@pytest.mark.parametrize("case", flux_cases(), ids=lambda c: "d%d_%s_%s_%s" % (
+    c["dim"], c["recon"], c["flux"], c["bc"]))
+def test_plugin_boundary_and_flux_match_reference(case):
+    """Boundary::applyBoundaryConditions then NumericalFlux::computeFlux, compared
+    with the digests of the reference's own outputs."""
+    dim, n = case["dim"], case["n"]
+    g = ghost_cells(case["recon"])
+    st = _dev(smooth_random_state(case["seed"], dim, n, g))
+    als.Boundary(dim, n, g, case["bc"]).applyBoundaryConditions(st)
+    torch.cuda.synchronize()
+    assert digest(st.cpu().numpy()) == case["filled"]
+    out = torch.zeros_like(st)
+    ws = als.NumericalFlux(dim, n, case["flux"], case["recon"]).computeFlux(st, out)
+    assert digest(ws) == case["ws"]
+    assert digest(out.cpu().numpy()) == case["net"]
+
+
+@pytest.mark.parametrize("dim,n", [(1, (20,)), (2, (11, 12)), (3, (8, 9, 10))])
+@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4"])
+def test_plugin_reconstruction_matches_oracle(c_oracle, dim, n, recon):
+    g = ghost_cells(recon)
+    if min(n) < 2 * g:
+        pytest.skip("grid smaller than two ghost widths")
+    st = smooth_random_state(99 + dim, dim, n, g)
+    cfg = c_oracle.config(dim, n, [0] * dim, [1] * dim, "hll", recon, "rungekutta3", "neumann", 1.4)
+    r = als.Reconstruction(dim, n, recon)
+    x = _dev(st)
+    for d in range(dim):
+        lref, rref = c_oracle.reconstruct(cfg, d, st)
+        left = torch.zeros_like(x)
+        right = torch.zeros_like(x)
+        r.performReconstruction(x, d, left, right)
+        np.testing.assert_array_equal(left.cpu().numpy(), lref)
+        np.testing.assert_array_equal(right.cpu().numpy(), rref)
+
+
+def test_plugin_weno2_known_answer():
+    """WenoTest.cpp:228-301 through the plug-in Reconstruction."""
+    n, g = 10, 2
+    st = np.zeros(padded_shape(1, (n,), g))
+    st[0] = 1.0
+    st[1] = 1.0
+    st[2] = 10.0
+    st[0, 0, 0, 1:4] = (2, 0, 1)
+    x = _dev(st)
+    left = torch.zeros_like(x)
+    right = torch.zeros_like(x)
+    als.Reconstruction(1, (n,), "weno2").performReconstruction(x, 0, left, right)
+    eps = 1e-8
+    a0, a1 = (2 / 3) / (1 + eps) ** 2, (1 / 3) / (4 + eps) ** 2
+    a0t, a1t = (1 / 3) / (1 + eps) ** 2, (2 / 3) / (4 + eps) ** 2
+    expect_r = a0 / (a0 + a1) * 0.5 - a1 / (a0 + a1)
+    expect_l = -0.5 * a0t / (a0t + a1t) + a1t / (a0t + a1t)
+    assert abs(right[0, 0, 0, 2].item() - expect_r) < 1e-8
+    assert abs(left[0, 0, 0, 2].item() - expect_l) < 1e-8
+
+
+@pytest.mark.parametrize("integ", ["forwardeuler", "rungekutta2", "rungekutta3"])
+def test_plugin_time_loop_matches_oracle(c_oracle, integ):
+    """Simulator::incrementSolution driven through the plug-in calls only."""
+    dim, n, recon, flux, bc = 2, (14, 13), "weno2", "hll3", "periodic"
+    g = ghost_cells(recon)
+    st = smooth_random_state(4242, dim, n, g)
+    cfg = c_oracle.config(dim, n, [0, 0], [1, 1], flux, recon, integ, bc, 1.4)
+    rc, U_ref, dts, steps, t_ref = c_oracle.simulate(cfg, st, 0.4, 0.03)
+    nf = als.NumericalFlux(dim, n, flux, recon)
+    bnd = als.Boundary(dim, n, g, bc)
+    it = als.Integrator(integ, nf, 0.4)
+    vols = [_dev(st)] + [torch.zeros_like(_dev(st)) for _ in range(it.getNumberOfSubsteps())]
+    bnd.applyBoundaryConditions(vols[0])
+    cell = [1 / 14, 1 / 13, 1.0]
+    t, k = 0.0, 0
+    while t < 0.03:
+        dt = 0.0
+        for s in range(it.getNumberOfSubsteps()):
+            dt = it.performSubstep(vols, cell, dt, vols[s + 1], s, t, 0.03)
+            bnd.applyBoundaryConditions(vols[s + 1])
+        vols[0], vols[-1] = vols[-1], vols[0]
+        assert dt == dts[k]
+        t += dt
+        k += 1
+    torch.cuda.synchronize()
+    assert k == steps and t == t_ref
+    np.testing.assert_array_equal(vols[0].cpu().numpy(), U_ref)
+
+
+def test_ensemble_members_match_independent_runs(c_oracle):
+    """Each member of a batched ensemble equals its own single simulation."""
+    n = 32
+    states, params = als.kh_ensemble(n, 0, 3)
+    states[1] = smooth_random_state(7, 2, (n, n), 2)
+    with als.Simulator(2, (n, n), (0, 0), (1, 1), flux="hll3", reconstruction="weno2",
+                       cfl=0.4, end_time=0.05, members=3) as sim:
+        sim.set_state(states)
+        sim.run()
+        U = sim.get_state()
+        infos = [sim.info(m) for m in range(3)]
+    cfg = c_oracle.config(2, (n, n), [0, 0], [1, 1], "hll3", "weno2", "rungekutta3", "periodic",
+                          1.4)
+    for m in range(3):
+        rc, U_ref, dts, steps, t = c_oracle.simulate(cfg, states[m], 0.4, 0.05)
+        assert infos[m]["steps"] == steps and infos[m]["t"] == t
+        np.testing.assert_array_equal(U[m], U_ref)
+
+
+def test_constraint_violation_flags_only_the_poisoned_member(c_oracle):
+    """Simulator::checkConstraints: a member with negative pressure fails
+    (status + first bad cell) while the others complete unaffected."""
+    n = 24
+    states = np.stack([smooth_random_state(300 + k, 2, (n, n), 2) for k in range(3)])
+    # E below the kinetic energy in one cell -> p < 0 after the first step
+    states[1, 3, 0, 10, 10] = -1.0
+    with als.Simulator(2, (n, n), (0, 0), (1, 1), flux="hll", reconstruction="weno2",
+                       cfl=0.4, end_time=0.02, members=3) as sim:
+        sim.set_state(states)
+        with pytest.raises(_lib.AlsError) as e:
+            sim.run()
+        assert e.value.code == -3
+        infos = [sim.info(m) for m in range(3)]
+        U = sim.get_state()
+    assert infos[1]["status"] == 1 and infos[1]["done"]
+    assert infos[1]["bad_step"] == 1 and infos[1]["bad_index"] >= 0
+    cfg = c_oracle.config(2, (n, n), [0, 0], [1, 1], "hll", "weno2", "rungekutta3", "periodic", 1.4)
+    for m in (0, 2):
+        assert infos[m]["status"] == 0
+        rc, U_ref, dts, steps, t = c_oracle.simulate(cfg, states[m], 0.4, 0.02)
+        np.testing.assert_array_equal(U[m], U_ref)
+    rc, _, _, steps, _ = c_oracle.simulate(cfg, states[1], 0.4, 0.02)
+    assert rc == 1 and steps == infos[1]["steps"]
+
+
+def test_max_steps_and_zero_end_time():
+    z = load_golden("kh32_weno2_hll3_rk3")
+    with _sim(z, max_steps=5) as sim:
+        sim.set_state(z["initial"])
+        sim.run()
+        assert sim.info()["steps"] == 5
+    z["end_time"] = 0.0
+    with _sim(z) as sim:
+        sim.set_state(z["initial"])
+        sim.run()
+        assert sim.info()["steps"] == 0
+
+
+def test_fp32_members_stay_close_to_fp64():
+    n = 64
+    states, _ = als.kh_ensemble(n, 0, 2)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        with als.Simulator(2, (n, n), (0, 0), (1, 1), flux="hll3", reconstruction="weno2",
+                           cfl=0.4, end_time=0.1, members=2, precision=prec) as sim:
+            sim.set_state(states)
+            sim.run()
+            out[prec] = sim.get_state()
+    g = 2
+    a = out["fp64"][:, :, :, g:-g, g:-g]
+    b = out["fp32"][:, :, :, g:-g, g:-g]
+    rel = np.abs(a - b).sum(axis=(2, 3, 4)) / np.abs(a).sum(axis=(2, 3, 4))
+    assert rel.max() < 1e-4, rel

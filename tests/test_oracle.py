@@ -1,0 +1,164 @@
+"""The oracle itself: pinned against the reference's own CPU code.
+
+CPU only.  The C restatement (oracle/als_oracle.c) must reproduce, bit for
+bit, every golden fixture produced by the reference's unmodified CPU
+sources (tests/golden/make_golden.py), and, where the reference build is
+present, fresh random cases.  The reference's own unit tests that pin this
+path (test/library_tests/src/fvm/...) are ported here against the oracle.
+"""
+import numpy as np
+import pytest
+
+from conftest import SIMULATION_FIXTURES, flux_cases, load_golden
+from oracle_lib import digest, ghost_cells, padded_shape, smooth_random_state
+
+
+@pytest.mark.parametrize("name", SIMULATION_FIXTURES)
+def test_c_oracle_reproduces_reference_simulation(c_oracle, name):
+    z = load_golden(name)
+    dim = z["dim"]
+    cfg = c_oracle.config(dim, z["n"], z["lower"], z["upper"], z["flux"], z["recon"],
+                          z["integrator"], z["bc"], z["gamma"])
+    rc, U, dts, steps, t = c_oracle.simulate(cfg, z["initial"], z["cfl"], z["end_time"])
+    assert rc == 0
+    assert steps == z["steps"]
+    assert t == z["t"]
+    np.testing.assert_array_equal(dts, z["dts"])
+    np.testing.assert_array_equal(U, z["final"])
+
+
+def test_sod_reference_numbers():
+    """Sod 1024, WENO2+HLL, RK3, CFL 0.45, T=0.2: 498 steps ending at T exactly."""
+    z = load_golden("sod1024_weno2_hll_rk3")
+    assert z["steps"] == 498
+    assert z["t"] == 0.2
+    g = 2
+    assert z["final"][0, 0, 0, g + 512] == 0.42568131167974621
+
+
+@pytest.mark.parametrize("case", flux_cases(), ids=lambda c: "d%d_%s_%s_%s" % (
+    c["dim"], c["recon"], c["flux"], c["bc"]))
+def test_c_oracle_net_flux_matches_reference(c_oracle, case):
+    dim, n = case["dim"], case["n"]
+    g = ghost_cells(case["recon"])
+    st = smooth_random_state(case["seed"], dim, n, g)
+    cfg = c_oracle.config(dim, n, [0] * dim, [1] * dim, case["flux"], case["recon"],
+                          "rungekutta3", case["bc"], 1.4)
+    filled = c_oracle.fill_ghosts(cfg, st)
+    assert digest(filled) == case["filled"]
+    net, ws = c_oracle.net_flux(cfg, filled)
+    assert digest(ws) == case["ws"]
+    assert digest(net) == case["net"]
+
+
+def test_c_oracle_meanvar_matches_reference(c_oracle):
+    z = load_golden("meanvar_7")
+    states = np.stack([smooth_random_state(int(s), 2, (6, 5), 2) for s in z["seeds"]])
+    mean, var = c_oracle.meanvar(states)
+    np.testing.assert_array_equal(mean, z["mean"])
+    np.testing.assert_array_equal(var, z["var"])
+
+
+@pytest.mark.parametrize("dim,n", [(1, (24,)), (2, (10, 11)), (3, (8, 9, 8))])
+@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4"])
+def test_c_oracle_matches_reference_build(c_oracle, ref_oracle, dim, n, recon):
+    """Fresh random cases against the reference build (skipped without it)."""
+    g = ghost_cells(recon)
+    if min(n) < 2 * g:
+        pytest.skip("grid smaller than two ghost widths")
+    seed = 5000 + 17 * dim + 3 * ["none", "weno2", "eno2", "eno3", "eno4"].index(recon)
+    for flux in ("hll", "hll3", "central"):
+        for bc in ("neumann", "periodic"):
+            st = smooth_random_state(seed, dim, n, g)
+            lo, hi = [0.0] * dim, [1.0] * dim
+            for integ in ("forwardeuler", "rungekutta2", "rungekutta3"):
+                cfg = c_oracle.config(dim, n, lo, hi, flux, recon, integ, bc, 1.4)
+                r = ref_oracle.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, 0.4, 0.03, st)
+                c = c_oracle.simulate(cfg, st, 0.4, 0.03)
+                assert r[0] == c[0] and r[3] == c[3] and r[4] == c[4]
+                np.testing.assert_array_equal(r[1], c[1])
+                np.testing.assert_array_equal(r[2], c[2])
+            for d in range(dim):
+                lr = ref_oracle.reconstruct(dim, n, recon, 1.4, d, st)
+                cfg = c_oracle.config(dim, n, lo, hi, flux, recon, "rungekutta3", bc, 1.4)
+                lc = c_oracle.reconstruct(cfg, d, st)
+                np.testing.assert_array_equal(lr[0], lc[0])
+                np.testing.assert_array_equal(lr[1], lc[1])
+
+
+# --------------------------------------------------------------------------
+# ports of the reference's unit tests for this path, against the oracle
+
+
+def test_weno2_known_answer(c_oracle):
+    """WenoTest.cpp:228-301: rho = (.., 2, 0, 1, ..) gives closed-form weights."""
+    n = 10
+    g = 2
+    st = np.zeros(padded_shape(1, (n,), g))
+    st[0] = 1.0
+    st[1] = 1.0
+    st[2] = 10.0
+    st[0, 0, 0, 1] = 2
+    st[0, 0, 0, 2] = 0
+    st[0, 0, 0, 3] = 1
+    cfg = c_oracle.config(1, (n,), (0,), (1,), "hll", "weno2", "rungekutta3", "neumann", 1.4)
+    left, right = c_oracle.reconstruct(cfg, 0, st)
+    eps = 1e-8
+    d0, d1 = 2.0 / 3.0, 1.0 / 3.0
+    b0, b1 = 1.0, 4.0
+    a0, a1 = d0 / (b0 + eps) ** 2, d1 / (b1 + eps) ** 2
+    a0t, a1t = d1 / (b0 + eps) ** 2, d0 / (b1 + eps) ** 2
+    w0, w1 = a0 / (a0 + a1), a1 / (a0 + a1)
+    w0t, w1t = a0t / (a0t + a1t), a1t / (a0t + a1t)
+    assert abs((w0 * 0.5 + w1 * -1) - right[0, 0, 0, 2]) < 1e-8
+    assert abs((w0t * -0.5 + w1t * 1) - left[0, 0, 0, 2]) < 1e-8
+
+
+@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4"])
+def test_reconstruction_of_constants_is_exact(c_oracle, recon):
+    """WenoTest.cpp:32-227: zero reconstructs exactly, one within 1e-8."""
+    g = ghost_cells(recon)
+    for value, tol in ((0.0, 0.0), (1.0, 1e-8)):
+        st = np.full(padded_shape(2, (10, 10), g), value)
+        cfg = c_oracle.config(2, (10, 10), (0, 0), (1, 1), "hll", recon, "rungekutta3",
+                              "neumann", 1.4)
+        for d in range(2):
+            left, right = c_oracle.reconstruct(cfg, d, st)
+            sl = (slice(None), slice(None), slice(g, -g), slice(g, -g))
+            assert np.all(np.abs(left[sl] - value) <= tol)
+            assert np.all(np.abs(right[sl] - value) <= tol)
+
+
+@pytest.mark.parametrize("flux", ["hll", "hll3", "central"])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_constant_state_has_zero_net_flux(c_oracle, flux, dim):
+    """numericalfluxtest.cpp:65-126: a constant state with Neumann gives net flux 0."""
+    n = (10,) * dim
+    g = 2
+    st = np.zeros(padded_shape(dim, n, g))
+    st[0] = 1.0
+    st[1] = 0.3
+    st[-1] = 3.0
+    cfg = c_oracle.config(dim, n, [0] * dim, [1] * dim, flux, "weno2", "rungekutta3", "neumann",
+                          1.4)
+    net, ws = c_oracle.net_flux(cfg, st)
+    assert np.all(net == 0.0)
+    assert ws[0] > 0
+
+
+def test_boundary_fills(c_oracle):
+    """BoundaryTest.cpp:52-334: Neumann mirrors, periodic wraps (2 ghost cells)."""
+    n = 6
+    g = 2
+    st = np.zeros(padded_shape(2, (n, n), g))
+    inner = np.arange(n * n, dtype=float).reshape(n, n) + 1
+    st[:, 0, g:-g, g:-g] = inner
+    cfgN = c_oracle.config(2, (n, n), (0, 0), (1, 1), "hll", "weno2", "rungekutta3", "neumann", 1.4)
+    cfgP = c_oracle.config(2, (n, n), (0, 0), (1, 1), "hll", "weno2", "rungekutta3", "periodic", 1.4)
+    N = c_oracle.fill_ghosts(cfgN, st)[0, 0]
+    P = c_oracle.fill_ghosts(cfgP, st)[0, 0]
+    for k in range(1, g + 1):
+        np.testing.assert_array_equal(N[g:-g, g - k], N[g:-g, g + k - 1])
+        np.testing.assert_array_equal(N[g:-g, -g - 1 + k], N[g:-g, -g - k])
+        np.testing.assert_array_equal(P[g:-g, g - k], P[g:-g, g - k + n])
+        np.testing.assert_array_equal(P[g - k, :], P[g - k + n, :])
