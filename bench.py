@@ -188,6 +188,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only run warmup+steps time steps (for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -214,6 +216,14 @@ def main():
     sim = als.Simulator(DIM, (N, N), (0, 0), (1, 1), flux=FLUX, reconstruction=RECON,
                         integrator=INTEG, boundary=BC, cfl=CFL, end_time=1e9, device=local)
     sim.set_state(state)
+    if args.kernels_only:
+        for _ in range(args.warmup + args.steps):
+            sim.advance(1)
+        sim.synchronize()
+        if sim.info()["status"] != 0:
+            raise RuntimeError("constraint violation")
+        sim.close()
+        return
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 

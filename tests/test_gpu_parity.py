@@ -74,14 +74,22 @@ def test_fused_solver_matches_oracle(c_oracle, dim, n, recon, flux, integ, bc):
     lo, hi = [0.0] * dim, [1.0] * dim
     cfg = c_oracle.config(dim, n, lo, hi, flux, recon, integ, bc, 1.4)
     rc, U_ref, dts, steps, t = c_oracle.simulate(cfg, st, 0.4, 0.04)
-    assert rc == 0 and steps >= 2
+    assert steps >= 1
     with als.Simulator(dim, n, lo, hi, flux=flux, reconstruction=recon, integrator=integ,
                        boundary=bc, cfl=0.4, end_time=0.04) as sim:
         sim.set_state(st)
-        sim.run()
+        if rc == 0:
+            sim.run()
+        else:
+            # some combinations (central flux, high-order ENO on noise) blow up:
+            # the reference stops with a constraint violation after `steps`
+            with pytest.raises(_lib.AlsError) as e:
+                sim.run()
+            assert e.value.code == -3
         info = sim.info()
         U = sim.get_state()[0]
     assert info["steps"] == steps and info["t"] == t
+    assert info["status"] == rc
     np.testing.assert_array_equal(U, U_ref)
 
 
@@ -242,5 +250,7 @@ def test_fp32_members_stay_close_to_fp64():
     g = 2
     a = out["fp64"][:, :, :, g:-g, g:-g]
     b = out["fp32"][:, :, :, g:-g, g:-g]
-    rel = np.abs(a - b).sum(axis=(2, 3, 4)) / np.abs(a).sum(axis=(2, 3, 4))
+    # L1 error per conserved variable relative to the L1 norm of the density
+    # (my starts at zero, so its own norm is no scale)
+    rel = np.abs(a - b).sum(axis=(2, 3, 4)) / np.abs(a[:, :1]).sum(axis=(2, 3, 4))
     assert rel.max() < 1e-4, rel
