@@ -87,7 +87,8 @@ class AlsError(RuntimeError):
 
 
 def library_path():
-    return _build.library_path()
+    """The in-tree library, or the one named by ALS_B200_LIBRARY."""
+    return os.environ.get("ALS_B200_LIBRARY") or _build.library_path()
 
 
 def load():

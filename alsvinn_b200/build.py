@@ -54,8 +54,8 @@ def _headers_mtime():
     return latest
 
 
-def _compile(nvcc, src, flags, force):
-    obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+def _compile(nvcc, src, flags, force, obj_dir=OBJ_DIR):
+    obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
     if (not force and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
             and os.path.getmtime(obj) > _headers_mtime()):
         return obj
@@ -70,16 +70,21 @@ def library_path():
     return os.path.join(OUT_DIR, LIB_NAME)
 
 
-def build(force=False, jobs=None, verbose=False):
-    """Compiles every unit (only what changed unless ``force``) and links the library."""
+def build(force=False, jobs=None, verbose=False, extra_flags=(), out=None, obj_dir=None):
+    """Compiles every unit (only what changed unless ``force``) and links the library.
+
+    ``extra_flags`` (e.g. tuning defines), ``out`` and ``obj_dir`` build a
+    variant elsewhere; the default is the in-tree library."""
     nvcc = nvcc_path()
-    os.makedirs(OBJ_DIR, exist_ok=True)
-    os.makedirs(OUT_DIR, exist_ok=True)
+    obj_dir = obj_dir or OBJ_DIR
+    lib = out or library_path()
+    os.makedirs(obj_dir, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     units = sources()
     jobs = jobs or min(len(units), os.cpu_count() or 4)
+    extra = list(extra_flags)
     with concurrent.futures.ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(lambda u: _compile(nvcc, u[0], u[1], force), units))
-    lib = library_path()
+        objs = list(ex.map(lambda u: _compile(nvcc, u[0], u[1] + extra, force, obj_dir), units))
     if force or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         res = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

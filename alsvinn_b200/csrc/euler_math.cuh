@@ -220,41 +220,59 @@ __device__ __forceinline__ R eno_coef(int r, int j) {
     }
 }
 
-// Reconstructs the cell at `src` (pointer to variable 0 of the cell; the
-// variables are `vstride` apart and neighbours along the direction `s` apart).
-// Writes NV left and NV right values.
-template<class R, int NV, int RECON>
-__device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R* left, R* right) {
+// Reconstruction of one cell along one direction.  The stencil values come
+// from a fetcher: f.at(v, o) is variable v at offset o along the direction
+// (o a compile-time constant after unrolling) and f.dyn(v, o) the same for
+// a run-time offset.  Writes NV left and NV right values.
+//
+// In WENO2, 2/d equals 2*(1/d) exactly whenever 1/d is a normal number (a
+// power-of-two scaling commutes with rounding), so the second division by
+// each d is replaced by a doubling; d above 2^1021 (never reached by a
+// physical state) takes the division.
+template<class R>
+__device__ __forceinline__ R twice_reciprocal(R d, R recip) {
+    const R big = sizeof(R) == 8 ? R(2.2471164185778949e307) : R(2.1267647932558654e37);
+    R out;
+    if (d < big) {
+        out = R(2) * recip;
+    } else {
+        out = R(2) / d;
+    }
+    return out;
+}
+
+template<class R, int NV, int RECON, class Fetch>
+__device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right) {
     if (RECON == RECON_NONE) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            left[v] = src[v * vstride];
-            right[v] = src[v * vstride];
+            left[v] = f.at(v, 0);
+            right[v] = left[v];
         }
     } else if (RECON == RECON_WENO2) {
         const R eps = R(1e-8);
-        const R i0 = src[0];
-        const R dp = src[s] - i0;
-        const R dm = i0 - src[-s];
+        const R i0 = f.at(0, 0);
+        const R dp = f.at(0, 1) - i0;
+        const R dm = i0 - f.at(0, -1);
         const R b0 = dp * dp;
         const R b1 = dm * dm;
         const R d0 = R(3) * (eps + b0) * (eps + b0);
         const R d1 = R(3) * (eps + b1) * (eps + b1);
         const R a0Left = R(1) / d0;
-        const R a1Left = R(2) / d1;
+        const R a1Right = R(1) / d1;
+        const R a1Left = twice_reciprocal(d1, a1Right);
+        const R a0Right = twice_reciprocal(d0, a0Left);
         const R w0Left = a0Left / (a0Left + a1Left);
         const R w1Left = a1Left / (a0Left + a1Left);
-        const R a0Right = R(2) / d0;
-        const R a1Right = R(1) / d1;
         const R w0Right = a0Right / (a0Right + a1Right);
         const R w1Right = a1Right / (a0Right + a1Right);
         const R cl = R(3) * w0Left + w1Left;
         const R cr = R(3) * w1Right + w0Right;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const R um = src[v * vstride - s];
-            const R u0 = src[v * vstride];
-            const R up = src[v * vstride + s];
+            const R um = f.at(v, -1);
+            const R u0 = f.at(v, 0);
+            const R up = f.at(v, 1);
             left[v] = R(0.5) * (w1Left * um + cl * u0 - w0Left * up);
             right[v] = R(0.5) * (w0Right * up + cr * u0 - w1Right * um);
         }
@@ -264,7 +282,7 @@ __device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R*
         R dd[ORDER];
 #pragma unroll
         for (int k = -1; k <= ORDER - 2; ++k) {
-            dd[k + 1] = src[(k + 1) * s] - src[k * s];
+            dd[k + 1] = f.at(0, k + 1) - f.at(0, k);
         }
         int shift = 0;
 #pragma unroll
@@ -284,7 +302,7 @@ __device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R*
             R lv = R(0), rv = R(0);
 #pragma unroll
             for (int j = 0; j < ORDER; ++j) {
-                const R value = src[v * vstride - (shift - j) * s];
+                const R value = f.dyn(v, j - shift);
                 lv += eno_coef<R, ORDER>(shift, j) * value;
                 rv += eno_coef<R, ORDER>(shift + 1, j) * value;
             }
@@ -292,6 +310,23 @@ __device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R*
             right[v] = rv;
         }
     }
+}
+
+// Stencil values from memory: variable v of the cell at `src` is v*vstride
+// away, neighbours along the direction s apart.
+template<class R, class I>
+struct StridedFetch {
+    const R* src;
+    I vstride;
+    I s;
+    __device__ __forceinline__ R at(int v, int o) const { return src[v * vstride + o * s]; }
+    __device__ __forceinline__ R dyn(int v, int o) const { return src[v * vstride + o * s]; }
+};
+
+template<class R, int NV, int RECON>
+__device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R* left, R* right) {
+    StridedFetch<R, int> f{src, vstride, s};
+    reconstruct_f<R, NV, RECON>(f, left, right);
 }
 
 } // namespace als
