@@ -27,11 +27,25 @@
 
 namespace als {
 
-constexpr int kStageThreads = 256;
+#ifndef ALS_STAGE_THREADS
+#define ALS_STAGE_THREADS 256
+#endif
+constexpr int kStageThreads = ALS_STAGE_THREADS;
 
 template<int DIM> struct TileShape;
 template<> struct TileShape<1> { static constexpr int X = 256, Y = 1, Z = 1; };
-template<> struct TileShape<2> { static constexpr int X = 32, Y = 16, Z = 1; };
+// The kernel is bound by the latency of dependent FP64 operations (the
+// divide and square-root sequences), so occupancy decides its speed: tiles
+// of 32x8 cells and at most 64 registers per thread keep four 256-thread
+// blocks (32 warps) on every SM, measured 2.2x faster on KH 1024^2 than
+// 32x16 tiles at 2 blocks per SM.  Both are build-time knobs.
+#ifndef ALS_TILE2_Y
+#define ALS_TILE2_Y 8
+#endif
+#ifndef ALS_STAGE_MAX_BLOCKS
+#define ALS_STAGE_MAX_BLOCKS 4
+#endif
+template<> struct TileShape<2> { static constexpr int X = 32, Y = ALS_TILE2_Y, Z = 1; };
 template<> struct TileShape<3> { static constexpr int X = 8, Y = 8, Z = 4; };
 
 template<class R, int DIM, int RECON>
@@ -58,6 +72,10 @@ struct StageLayout {
     static constexpr int FAC = FAC0 > FAC1 ? (FAC0 > FAC2 ? FAC0 : FAC2) : (FAC1 > FAC2 ? FAC1 : FAC2);
     static constexpr size_t SMEM = sizeof(R) * (size_t(NV) * BOX + size_t(2 * NV) * REC + size_t(NV) * FAC);
     static_assert(CELLS % kStageThreads == 0, "tile must be a multiple of the block");
+    // resident blocks per SM the shared memory allows (228 KB per SM, 1 KB
+    // reserved per block), capped; the register budget is sized to match
+    static constexpr int BY_SMEM = int((228 * 1024) / (SMEM + 1024));
+    static constexpr int BLOCKS = BY_SMEM < 1 ? 1 : (BY_SMEM > ALS_STAGE_MAX_BLOCKS ? ALS_STAGE_MAX_BLOCKS : BY_SMEM);
 };
 
 // dt of the step (Integrator.cpp:20-46) followed by the end-time clamp
@@ -443,7 +461,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
 }
 
 template<class R, int DIM, int RECON, int FLUX, int KIND>
-__global__ void __launch_bounds__(kStageThreads)
+__global__ void __launch_bounds__(kStageThreads, (StageLayout<R, DIM, RECON>::BLOCKS))
 stage_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int member = P.member0 + blockIdx.y;

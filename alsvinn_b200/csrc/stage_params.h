@@ -56,7 +56,6 @@ struct StageParams {
     StepState* state;        // per-member state (indexed by member), or null
     unsigned long long* ws_out; // FLUX0 without state: per-direction max face speed (3 per member)
     int member0;             // index of the first member this launch covers
-    int rows_per_warp;       // 1-D/2-D marching kernel: rows per warp (0 = automatic)
 };
 
 } // namespace als
