@@ -66,26 +66,31 @@ cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
     }
 }
 
-int tile_extent(int dim, int d) {
+// Tile extent along d of the kernels built for (precision, dim), as reported
+// by the unit that holds them.
+int tile_extent(int precision, int dim, int d) {
     if (d >= dim) {
         return 1;
     }
-    switch (dim) {
-    case 1: return als::TileShape<1>::X;
-    case 2: return d == 0 ? als::TileShape<2>::X : als::TileShape<2>::Y;
-    default: return d == 0 ? als::TileShape<3>::X : (d == 1 ? als::TileShape<3>::Y : als::TileShape<3>::Z);
+    int tile[3] = {1, 1, 1};
+    if (precision == ALS_FP64) {
+        dim == 1 ? als::stage_tile_f64_1d(tile) : (dim == 2 ? als::stage_tile_f64_2d(tile) : als::stage_tile_f64_3d(tile));
+    } else {
+        dim == 1 ? als::stage_tile_f32_1d(tile) : (dim == 2 ? als::stage_tile_f32_2d(tile) : als::stage_tile_f32_3d(tile));
     }
+    return tile[d];
 }
 
 // Geometry of a padded grid and the tiles covering the region [lo, hi).
-als::GridDesc make_grid(int dim, const int* n, int g, const int* lo, const int* hi) {
+als::GridDesc make_grid(int dim, const int* n, int g, const int* lo, const int* hi,
+    int precision = ALS_FP64) {
     als::GridDesc gd;
     for (int d = 0; d < 3; ++d) {
         gd.n[d] = d < dim ? n[d] : 1;
         gd.N[d] = gd.n[d] + (d < dim ? 2 * g : 0);
         gd.lo[d] = d < dim ? lo[d] : 0;
         gd.hi[d] = d < dim ? hi[d] : 1;
-        const int t = tile_extent(dim, d);
+        const int t = tile_extent(precision, dim, d);
         gd.tiles[d] = std::max(1, (gd.hi[d] - gd.lo[d] + t - 1) / t);
     }
     gd.plane = (long long)gd.N[0] * gd.N[1] * gd.N[2];
@@ -520,7 +525,7 @@ int als_solver_create(const als_solver_config* cfg, int device, als_solver** out
     for (int d = 0; d < 3; ++d) {
         n[d] = d < cfg->dimension ? cfg->n[d] : 1;
     }
-    s->grid = make_grid(cfg->dimension, n, g, lo, n);
+    s->grid = make_grid(cfg->dimension, n, g, lo, n, cfg->precision);
     s->member_elems = (long long)s->nv * s->grid.plane;
     for (int d = 0; d < 3; ++d) {
         // Grid.cpp:24-41: (top - origin) / n, and 1 for a direction with one cell

@@ -23,7 +23,7 @@ cudaError_t launch_stage_one(const StageParams& P, int members, cudaStream_t str
     }
     const unsigned int tiles = unsigned(P.grid.tiles[0]) * P.grid.tiles[1] * P.grid.tiles[2];
     dim3 grid(tiles, unsigned(members));
-    kernel<<<grid, kStageThreads, Lay::SMEM, stream>>>(P);
+    kernel<<<grid, Lay::THREADS, Lay::SMEM, stream>>>(P);
     return cudaGetLastError();
 }
 
@@ -72,7 +72,22 @@ size_t stage_smem_dim(int recon) {
     }
 }
 
+template<int DIM>
+void stage_tile_dim(int* tile) {
+    tile[0] = TileShape<DIM>::X;
+    tile[1] = TileShape<DIM>::Y;
+    tile[2] = TileShape<DIM>::Z;
+}
+
 // Entry points defined by the per-(precision, dimension) translation units.
+// stage_tile_* report the tile the kernels of that unit were built with, so
+// the host always covers the grid with the tiles the kernels expect.
+void stage_tile_f64_1d(int* tile);
+void stage_tile_f64_2d(int* tile);
+void stage_tile_f64_3d(int* tile);
+void stage_tile_f32_1d(int* tile);
+void stage_tile_f32_2d(int* tile);
+void stage_tile_f32_3d(int* tile);
 cudaError_t launch_stage_f64_1d(int recon, int flux, int kind, const StageParams& P, int members, cudaStream_t s);
 cudaError_t launch_stage_f64_2d(int recon, int flux, int kind, const StageParams& P, int members, cudaStream_t s);
 cudaError_t launch_stage_f64_3d(int recon, int flux, int kind, const StageParams& P, int members, cudaStream_t s);

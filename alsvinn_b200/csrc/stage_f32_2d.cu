@@ -6,4 +6,8 @@ cudaError_t launch_stage_f32_2d(int recon, int flux, int kind, const StageParams
     int members, cudaStream_t s) {
     return launch_stage_dim<float, 2>(recon, flux, kind, P, members, s);
 }
+
+void stage_tile_f32_2d(int* tile) {
+    stage_tile_dim<2>(tile);
+}
 } // namespace als

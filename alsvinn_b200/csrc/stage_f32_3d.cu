@@ -6,4 +6,8 @@ cudaError_t launch_stage_f32_3d(int recon, int flux, int kind, const StageParams
     int members, cudaStream_t s) {
     return launch_stage_dim<float, 3>(recon, flux, kind, P, members, s);
 }
+
+void stage_tile_f32_3d(int* tile) {
+    stage_tile_dim<3>(tile);
+}
 } // namespace als

@@ -6,4 +6,8 @@ cudaError_t launch_stage_f64_1d(int recon, int flux, int kind, const StageParams
     int members, cudaStream_t s) {
     return launch_stage_dim<double, 1>(recon, flux, kind, P, members, s);
 }
+
+void stage_tile_f64_1d(int* tile) {
+    stage_tile_dim<1>(tile);
+}
 } // namespace als

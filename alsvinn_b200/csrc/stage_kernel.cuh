@@ -27,26 +27,38 @@
 
 namespace als {
 
-#ifndef ALS_STAGE_THREADS
-#define ALS_STAGE_THREADS 256
+// Tile shape (X x Y x Z cells), threads per block T and the most blocks per
+// SM the register budget is sized for (B), per dimension.
+//
+// The kernel is bound by the issue of long dependent FP64 sequences (the
+// divide and square-root routines), so occupancy and lane utilisation
+// decide its speed.  In 2-D a 32x8 tile needs 272/320 reconstructions and
+// 264/288 face fluxes along x/y: with 320 threads every one of these phases
+// is a single round, where 256 threads would need two mostly idle rounds.
+// All of these are build-time knobs.
+#ifndef ALS_TILE2_X
+#define ALS_TILE2_X 32
 #endif
-constexpr int kStageThreads = ALS_STAGE_THREADS;
-
-template<int DIM> struct TileShape;
-template<> struct TileShape<1> { static constexpr int X = 256, Y = 1, Z = 1; };
-// The kernel is bound by the latency of dependent FP64 operations (the
-// divide and square-root sequences), so occupancy decides its speed: tiles
-// of 32x8 cells and at most 64 registers per thread keep four 256-thread
-// blocks (32 warps) on every SM, measured 2.2x faster on KH 1024^2 than
-// 32x16 tiles at 2 blocks per SM.  Both are build-time knobs.
 #ifndef ALS_TILE2_Y
 #define ALS_TILE2_Y 8
 #endif
-#ifndef ALS_STAGE_MAX_BLOCKS
-#define ALS_STAGE_MAX_BLOCKS 4
+#ifndef ALS_STAGE2_THREADS
+#define ALS_STAGE2_THREADS 320
 #endif
-template<> struct TileShape<2> { static constexpr int X = 32, Y = ALS_TILE2_Y, Z = 1; };
-template<> struct TileShape<3> { static constexpr int X = 8, Y = 8, Z = 4; };
+#ifndef ALS_STAGE2_BLOCKS
+#define ALS_STAGE2_BLOCKS 3
+#endif
+template<int DIM> struct TileShape;
+template<> struct TileShape<1> {
+    static constexpr int X = 256, Y = 1, Z = 1, T = 256, B = 4;
+};
+template<> struct TileShape<2> {
+    static constexpr int X = ALS_TILE2_X, Y = ALS_TILE2_Y, Z = 1, T = ALS_STAGE2_THREADS,
+        B = ALS_STAGE2_BLOCKS;
+};
+template<> struct TileShape<3> {
+    static constexpr int X = 8, Y = 8, Z = 4, T = 256, B = 4;
+};
 
 template<class R, int DIM, int RECON>
 struct StageLayout {
@@ -60,7 +72,8 @@ struct StageLayout {
     static constexpr int BZ = DIM > 2 ? TZ + 2 * G : 1;
     static constexpr int BOX = BX * BY * BZ;
     static constexpr int CELLS = TX * TY * TZ;
-    static constexpr int CPT = CELLS / kStageThreads;
+    static constexpr int THREADS = TileShape<DIM>::T;
+    static constexpr int CPT = (CELLS + THREADS - 1) / THREADS;  // cells per thread
     // reconstructed cells / faces per direction: the tile extent grows by 2 / 1 along it
     static constexpr int REC0 = (TX + 2) * TY * TZ;
     static constexpr int REC1 = DIM > 1 ? TX * (TY + 2) * TZ : 0;
@@ -71,11 +84,11 @@ struct StageLayout {
     static constexpr int FAC2 = DIM > 2 ? TX * TY * (TZ + 1) : 0;
     static constexpr int FAC = FAC0 > FAC1 ? (FAC0 > FAC2 ? FAC0 : FAC2) : (FAC1 > FAC2 ? FAC1 : FAC2);
     static constexpr size_t SMEM = sizeof(R) * (size_t(NV) * BOX + size_t(2 * NV) * REC + size_t(NV) * FAC);
-    static_assert(CELLS % kStageThreads == 0, "tile must be a multiple of the block");
+    static_assert(THREADS % 32 == 0, "whole warps");
     // resident blocks per SM the shared memory allows (228 KB per SM, 1 KB
     // reserved per block), capped; the register budget is sized to match
     static constexpr int BY_SMEM = int((228 * 1024) / (SMEM + 1024));
-    static constexpr int BLOCKS = BY_SMEM < 1 ? 1 : (BY_SMEM > ALS_STAGE_MAX_BLOCKS ? ALS_STAGE_MAX_BLOCKS : BY_SMEM);
+    static constexpr int BLOCKS = BY_SMEM < 1 ? 1 : (BY_SMEM > TileShape<DIM>::B ? TileShape<DIM>::B : BY_SMEM);
 };
 
 // dt of the step (Integrator.cpp:20-46) followed by the end-time clamp
@@ -170,7 +183,7 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
     const int tid = threadIdx.x;
     const R gamma = R(P.gamma);
 
-    for (int i = tid; i < RC; i += kStageThreads) {
+    for (int i = tid; i < RC; i += Lay::THREADS) {
         const int ex = i % E0;
         const int ey = (i / E0) % E1;
         const int ez = i / (E0 * E1);
@@ -190,7 +203,7 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
 
     const int hiD = D == 0 ? P.grid.hi[0] : (D == 1 ? P.grid.hi[1] : P.grid.hi[2]);
     const int oD = D == 0 ? x0 : (D == 1 ? y0 : z0);
-    for (int i = tid; i < FC; i += kStageThreads) {
+    for (int i = tid; i < FC; i += Lay::THREADS) {
         const int fx = i % F0;
         const int fy = (i / F0) % F1;
         const int fz = i / (F0 * F1);
@@ -230,7 +243,10 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
 
 #pragma unroll
     for (int k = 0; k < Lay::CPT; ++k) {
-        const int ci = tid + k * kStageThreads;
+        const int ci = tid + k * Lay::THREADS;
+        if (Lay::CELLS % Lay::THREADS != 0 && ci >= Lay::CELLS) {
+            continue;
+        }
         const int cx = ci % Lay::TX;
         const int cy = (ci / Lay::TX) % Lay::TY;
         const int cz = ci / (Lay::TX * Lay::TY);
@@ -292,7 +308,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
 
     // stage the tile and its halo; U1 = (dt/dx)*L + U^n is formed here for the
     // second stage (RungeKutta{2,3}.cpp: output *= dt/dx; output += U)
-    for (int i = tid; i < NV * Lay::BOX; i += kStageThreads) {
+    for (int i = tid; i < NV * Lay::BOX; i += Lay::THREADS) {
         const int v = i / Lay::BOX;
         const int b = i - v * Lay::BOX;
         const int bx = b % Lay::BX;
@@ -336,7 +352,10 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
     long long bad_idx = 0;
 #pragma unroll
     for (int k = 0; k < Lay::CPT; ++k) {
-        const int ci = tid + k * kStageThreads;
+        const int ci = tid + k * Lay::THREADS;
+        if (Lay::CELLS % Lay::THREADS != 0 && ci >= Lay::CELLS) {
+            continue;
+        }
         const int cx = ci % Lay::TX;
         const int cy = (ci / Lay::TX) % Lay::TY;
         const int cz = ci / (Lay::TX * Lay::TY);
@@ -409,7 +428,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
     }
 
     if (KIND == KIND_FLUX0) {
-        __shared__ double wsh[3][kStageThreads / 32];
+        __shared__ double wsh[3][Lay::THREADS / 32];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const R w = warp_max(wmax[d]);
@@ -420,7 +439,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
         __syncthreads();
         if (tid < DIM) {
             double m = 0;
-            for (int k = 0; k < kStageThreads / 32; ++k) {
+            for (int k = 0; k < Lay::THREADS / 32; ++k) {
                 m = fmax(m, wsh[tid][k]);
             }
             unsigned long long* dst = st ? &st->ws[tid] : (P.ws_out + 3 * member + tid);
@@ -461,7 +480,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
 }
 
 template<class R, int DIM, int RECON, int FLUX, int KIND>
-__global__ void __launch_bounds__(kStageThreads, (StageLayout<R, DIM, RECON>::BLOCKS))
+__global__ void __launch_bounds__((StageLayout<R, DIM, RECON>::THREADS), (StageLayout<R, DIM, RECON>::BLOCKS))
 stage_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int member = P.member0 + blockIdx.y;
