@@ -32,21 +32,27 @@ namespace als {
 //
 // The kernel is bound by the issue of long dependent FP64 sequences (the
 // divide and square-root routines), so occupancy and lane utilisation
-// decide its speed.  In 2-D a 32x8 tile needs 272/320 reconstructions and
-// 264/288 face fluxes along x/y: with 320 threads every one of these phases
-// is a single round, where 256 threads would need two mostly idle rounds.
+// decide its speed.  In 2-D a 32x16 tile needs 544/576 reconstructions and
+// 528/544 face fluxes along x/y: with 576 threads every one of these phases
+// is a single round (92-100% of the lanes busy), and two such blocks per SM
+// give 36 warps.  Measured on KH 1024^2 (ms per RK3 step, FP64, B200):
+//   32x16 / 576 threads / 2 blocks (56 regs)   0.420
+//   16x16 / 288 threads / 3 blocks (72 regs)   0.438
+//   32x8  / 320 threads / 3 blocks (64 regs)   0.454
+//   32x8  / 256 threads / 4 blocks (64 regs)   0.490
+//   32x16 / 256 threads / 2 blocks (~100 regs) 0.556
 // All of these are build-time knobs.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
 #endif
 #ifndef ALS_TILE2_Y
-#define ALS_TILE2_Y 8
+#define ALS_TILE2_Y 16
 #endif
 #ifndef ALS_STAGE2_THREADS
-#define ALS_STAGE2_THREADS 320
+#define ALS_STAGE2_THREADS 576
 #endif
 #ifndef ALS_STAGE2_BLOCKS
-#define ALS_STAGE2_BLOCKS 3
+#define ALS_STAGE2_BLOCKS 2
 #endif
 template<int DIM> struct TileShape;
 template<> struct TileShape<1> {
