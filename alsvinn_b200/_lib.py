@@ -52,6 +52,8 @@ PROTOTYPES = {
                                        ctypes.c_int, _VP]),
     "als_compute_flux": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
                                         _I, _I, _D, _VP]),
+    "als_compute_flux_static": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int,
+                                               _VP, _VP, ctypes.c_int, _D, _VP]),
     "als_reconstruct": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
                                        _VP, _VP]),
     "als_integrator_combine": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <string>
@@ -842,3 +843,93 @@ int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity) {
 }
 
 } // extern "C"
+
+// ------------------------------------------- allocation-free flux evaluation
+//
+// als_compute_flux reserves three wave-speed accumulators per call with
+// cudaMallocAsync.  Some hosts of NumericalFlux::computeFlux cannot let a
+// library allocate device memory: a runtime that plans every byte of device
+// memory up front (a memory pool owned by another framework, a fixed-budget
+// embedded or real-time deployment), or one that forbids allocation calls
+// while it drives the flux evaluation many times per time step.  For them,
+// als_compute_flux_static keeps those accumulators in the fixed array below
+// and allocates nothing.
+
+namespace {
+
+// at most this many states per call; 3 accumulators each: 24 KiB
+constexpr int kStaticFluxMembers = 1024;
+// every GPU that loads the library holds this array until the process exits
+static __device__ __align__(256) unsigned long long g_static_flux_wave_speeds[3 * kStaticFluxMembers];
+
+std::mutex g_static_flux_mutex;
+void* g_static_flux_address[256] = {};
+
+// Device address of the array on the current device, looked up once per
+// device (cudaGetSymbolAddress; the name itself is a host-side stand-in).
+int static_flux_scratch(void** address) {
+    int device = 0;
+    ALS_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= 256) {
+        return fail(ALS_E_UNSUPPORTED, "device ordinal out of range for the static scratch table");
+    }
+    std::lock_guard<std::mutex> lock(g_static_flux_mutex);
+    if (!g_static_flux_address[device]) {
+        void* p = nullptr;
+        ALS_CUDA(cudaGetSymbolAddress(&p, g_static_flux_wave_speeds));
+        g_static_flux_address[device] = p;
+    }
+    *address = g_static_flux_address[device];
+    return ALS_OK;
+}
+
+} // namespace
+
+extern "C" int als_compute_flux_static(const als_grid* grid, int flux, int reconstruction,
+    const double* in, double* out, int members, double* wave_speed, void* stream) {
+    int rc = check_grid(grid);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    if (!valid_choice(flux, reconstruction) || !in || !out || !wave_speed) {
+        return fail(ALS_E_INVALID, "invalid flux arguments");
+    }
+    if (members < 1 || members > kStaticFluxMembers) {
+        return fail(ALS_E_INVALID, "als_compute_flux_static takes 1 to 1024 states per call");
+    }
+    if (grid->ghosts != als_ghost_cells(flux, reconstruction)) {
+        return fail(ALS_E_UNSUPPORTED, "planes must have exactly the ghost width of the reconstruction");
+    }
+    void* scratch = nullptr;
+    rc = static_flux_scratch(&scratch);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    int lo[3] = {0, 0, 0};
+    int n[3];
+    for (int d = 0; d < 3; ++d) {
+        n[d] = d < grid->dimension ? grid->n[d] : 1;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    als::StageParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.in = in;
+    P.un = in;
+    P.out = out;
+    P.grid = make_grid(grid->dimension, n, grid->ghosts, lo, n);
+    P.sample_stride = (long long)(grid->dimension + 2) * P.grid.plane;
+    P.bc = ALS_BC_NEUMANN;
+    P.write_ghosts = 0;
+    P.gamma = grid->gamma;
+    P.ws_out = static_cast<unsigned long long*>(scratch);
+    // the array keeps the previous call's maxima: clear the slots used
+    const size_t bytes = sizeof(unsigned long long) * 3 * size_t(members);
+    ALS_CUDA(cudaMemsetAsync(scratch, 0, bytes, s));
+    ALS_CUDA(launch_stage(ALS_FP64, grid->dimension, reconstruction, flux, als::KIND_FLUX0, P,
+        members, s));
+    // a non-negative double and its bit pattern read as an unsigned integer
+    // are the same 8 bytes, so the maxima are copied straight into doubles
+    ALS_CUDA(cudaMemcpyAsync(wave_speed, scratch, bytes, cudaMemcpyDeviceToHost, s));
+    ALS_CUDA(cudaStreamSynchronize(s));
+    return ALS_OK;
+}

@@ -87,6 +87,25 @@ int als_fill_ghosts(const als_grid* grid, int boundary, double* planes, int nvar
 int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* in,
     double* out, const int* start, const int* end, double* wave_speed, void* stream);
 
+/* Allocation-free variant of als_compute_flux; it has no counterpart in the
+ * reference.  For callers that cannot let a library allocate device memory:
+ * a runtime that owns and pre-plans all device memory (another framework's
+ * pool, a fixed-budget deployment) or one that forbids allocation while it
+ * drives the flux evaluation many times per time step.  It evaluates the
+ * net flux of `members` (1..1024) consecutive states (each nvar padded
+ * planes, the whole interior, no region arguments) into `out`, and writes
+ * their maximal face wave speeds to `wave_speed` (host, 3 per state).  The
+ * wave-speed accumulators live in a fixed 24 KiB device array inside the
+ * library that every GPU loading it keeps until the process exits; no
+ * cudaMalloc, cudaFree or allocating routine is called.  The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  Calls share the array and the call
+ * clears what it uses, so calls that overlap on the GPU (from several
+ * threads or streams) race; the call synchronises `stream` before it
+ * returns.  More than 1024 states is rejected with ALS_E_INVALID. */
+int als_compute_flux_static(const als_grid* grid, int flux, int reconstruction, const double* in,
+    double* out, int members, double* wave_speed, void* stream);
+
 /* Reconstruction::performReconstruction(const Volume& in, size_t direction,
  * size_t indicatorVariable=0, Volume& left, Volume& right)
  * (alsfvm/include/alsfvm/reconstruction/Reconstruction.hpp:46-58;
