@@ -5,11 +5,12 @@ C ABI in ``include/als_b200.h``); this package is the Python face of it.
 """
 from . import _lib
 from .initial_data import (kelvin_helmholtz, kh_ensemble, padded_shape, sod, uniform_draws)
-from .simulator import (Boundary, Integrator, NumericalFlux, Reconstruction, Simulator,
-                        ghost_cells)
+from .simulator import (Boundary, Integrator, MeanVariance, NumericalFlux, Reconstruction,
+                        Simulator, ghost_cells)
 
 __all__ = [
-    "Boundary", "Integrator", "NumericalFlux", "Reconstruction", "Simulator", "ghost_cells",
+    "Boundary", "Integrator", "MeanVariance", "NumericalFlux", "Reconstruction", "Simulator",
+    "ghost_cells",
     "kelvin_helmholtz", "kh_ensemble", "padded_shape", "sod", "uniform_draws",
 ]
 

@@ -11,6 +11,8 @@ from . import build as _build
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
 _VP = ctypes.c_void_p
+_PP = ctypes.POINTER(ctypes.c_void_p)   # array of plane pointers
+_LL = ctypes.POINTER(ctypes.c_longlong)
 
 
 class Grid(ctypes.Structure):
@@ -48,20 +50,34 @@ PROTOTYPES = {
     "als_last_error": (ctypes.c_char_p, []),
     "als_version": (ctypes.c_int, []),
     "als_ghost_cells": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
-    "als_fill_ghosts": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, _VP, ctypes.c_int,
-                                       ctypes.c_int, _VP]),
-    "als_compute_flux": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
+    "als_fill_ghosts": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, _PP, ctypes.c_int,
+                                       _VP]),
+    "als_compute_flux": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _PP, _PP,
                                         _I, _I, _D, _VP]),
     "als_compute_flux_static": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int,
                                                _VP, _VP, ctypes.c_int, _D, _VP]),
-    "als_reconstruct": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _VP, _VP,
-                                       _VP, _VP]),
+    "als_reconstruct": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _PP, _PP,
+                                       _PP, _VP]),
     "als_integrator_combine": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,
                                               ctypes.c_size_t, ctypes.c_double, _VP]),
     "als_compute_timestep": (ctypes.c_double, [_D, _D, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double]),
     "als_solver_create": (ctypes.c_int, [ctypes.POINTER(SolverConfig), ctypes.c_int,
                                          ctypes.POINTER(_VP)]),
+    "als_solver_create_levels": (ctypes.c_int, [ctypes.POINTER(SolverConfig), ctypes.c_int,
+                                                ctypes.c_int, ctypes.POINTER(_VP)]),
+    "als_solver_level": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _LL]),
+    "als_solver_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, _I]),
+    "als_solver_get_schedule": (ctypes.c_int, [_VP, _I, _I]),
+    "als_solver_tune": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D]),
+    "als_solver_region_sums": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _I, _I, _D]),
+    "als_stats_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(_VP)]),
+    "als_stats_destroy": (ctypes.c_int, [_VP]),
+    "als_stats_add": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _VP]),
+    "als_stats_add_solver": (ctypes.c_int, [_VP, _VP, ctypes.c_int]),
+    "als_stats_merge": (ctypes.c_int, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
+    "als_stats_moments": (ctypes.c_int, [_VP, _LL, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+    "als_stats_result": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "als_solver_destroy": (ctypes.c_int, [_VP]),
     "als_solver_geometry": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong), _I]),
     "als_solver_set_state": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.c_int]),
@@ -109,6 +125,12 @@ def load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def plane_pointers(tensor):
+    """ctypes array of the per-variable plane pointers of a (nvar, ...) device tensor."""
+    nvar = tensor.shape[0]
+    return (ctypes.c_void_p * nvar)(*[tensor[v].data_ptr() for v in range(nvar)])
 
 
 def check(rc):

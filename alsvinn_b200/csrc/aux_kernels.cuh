@@ -6,19 +6,28 @@
 //   * fill_ghosts        Boundary::applyBoundaryConditions (BoundaryCPU.cpp:30-106)
 //   * reconstruct_dir    Reconstruction::performReconstruction (ReconstructionCPU.cpp:37-97,
 //                        ENOCPU.cpp:41-187) for the plug-in path
+//   * region_sums        FP64 sums of every variable over a box of cells, per
+//                        member (conservation check, observables)
+//   * welford_merge      FP64 mean / M2 of an ensemble, merged chunk by chunk
 #pragma once
 
 #include "stage_kernel.cuh"
 
 namespace als {
 
+// One pointer per conserved variable.
+template<class R>
+struct Planes {
+    R* p[kMaxVars];
+};
+
 // U^{n+1} = (dt/dx) L + U^n over every padded cell (ghost cells of L and U^n
 // are already images, so the result's ghosts are images too), then the
 // constraint check and the step bookkeeping of the last block.
 template<class R, int NV>
 __global__ void __launch_bounds__(256) fe_update(const R* L, R* un, long long plane,
-    long long sample_stride, StepState* state, int member0, double gamma) {
-    const int member = member0 + blockIdx.y;
+    long long sample_stride, StepState* state, double gamma) {
+    const int member = blockIdx.y;
     StepState* st = state + member;
     if (((volatile StepState*)st)->done) {
         return;
@@ -54,21 +63,8 @@ __global__ void __launch_bounds__(256) fe_update(const R* L, R* un, long long pl
         const unsigned int prev = atomicAdd(&st->arrive, 1u);
         if (prev == gridDim.x - 1) {
             __threadfence();
-            volatile StepState* vs = st;
-            vs->dt = dt;
-            const double t = vs->t + dt;
-            vs->t = t;
-            vs->steps = vs->steps + 1;
-            vs->ws[0] = 0;
-            vs->ws[1] = 0;
-            vs->ws[2] = 0;
-            vs->arrive = 0;
-            if (vs->status != 0 && vs->bad_step < 0) {
-                vs->bad_step = vs->steps;
-            }
-            if (t >= vs->end_time || vs->status != 0 || vs->steps >= vs->max_steps) {
-                vs->done = 1;
-            }
+            ((volatile StepState*)st)->dt = dt;
+            finish_step(st);
         }
     }
 }
@@ -116,14 +112,14 @@ __device__ __forceinline__ int ghost_source(int p, int n, int G, int bc) {
 
 // Every ghost cell takes the value of its source interior cell; sides are
 // independent once n >= G, so one pass reproduces the reference's
-// side-by-side sequential fill, corners included.
+// side-by-side sequential fill, corners included.  blockIdx.y = member.
 template<class R>
-__global__ void __launch_bounds__(256) fill_ghosts(R* planes, int nvar, long long plane,
-    long long sample_stride, int dim, int n0, int n1, int n2, int G, int bc) {
+__global__ void __launch_bounds__(256) fill_ghosts(Planes<R> planes, int nvar, long long plane,
+    long long member_stride, int dim, int n0, int n1, int n2, int G, int bc) {
     const int N0 = n0 + 2 * G;
     const int N1 = dim > 1 ? n1 + 2 * G : 1;
     const int N2 = dim > 2 ? n2 + 2 * G : 1;
-    planes += (long long)blockIdx.y * sample_stride;
+    const long long base = (long long)blockIdx.y * member_stride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane;
          i += (long long)gridDim.x * blockDim.x) {
         const int x = int(i % N0);
@@ -137,21 +133,32 @@ __global__ void __launch_bounds__(256) fill_ghosts(R* planes, int nvar, long lon
         }
         const long long s = ((long long)sz * N1 + sy) * N0 + sx;
         for (int v = 0; v < nvar; ++v) {
-            planes[v * plane + i] = planes[v * plane + s];
+            R* p = planes.p[v] + base;
+            p[i] = p[s];
         }
     }
 }
 
+// Stencil values from per-variable planes.
+template<class R, int NV>
+struct PlaneFetch {
+    const Planes<R>* planes;
+    long long idx;
+    long long s;
+    __device__ __forceinline__ R at(int v, int o) const { return planes->p[v][idx + o * s]; }
+    __device__ __forceinline__ R dyn(int v, int o) const { return planes->p[v][idx + o * s]; }
+};
+
 // Left/right values of every cell the reference reconstructs along `dir`:
 // cells [G-1, N-G] along dir, interior across (ReconstructionCPU.cpp:71-96).
 template<class R, int NV, int RECON>
-__global__ void __launch_bounds__(256) reconstruct_dir(const R* in, R* left, R* right,
-    long long plane, int dim, int N0, int N1, int N2, int G, int dir) {
+__global__ void __launch_bounds__(256) reconstruct_dir(Planes<R> in, Planes<R> left,
+    Planes<R> right, int dim, int N0, int N1, int N2, int G, int dir) {
     const int e0 = dir == 0 ? N0 - 2 * G + 2 : N0 - 2 * G;
     const int e1 = dim > 1 ? (dir == 1 ? N1 - 2 * G + 2 : N1 - 2 * G) : 1;
     const int e2 = dim > 2 ? (dir == 2 ? N2 - 2 * G + 2 : N2 - 2 * G) : 1;
     const long long count = (long long)e0 * e1 * e2;
-    const int s = dir == 0 ? 1 : (dir == 1 ? N0 : N0 * N1);
+    const long long s = dir == 0 ? 1 : (dir == 1 ? N0 : (long long)N0 * N1);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x) {
         const int a = int(i % e0);
@@ -161,12 +168,107 @@ __global__ void __launch_bounds__(256) reconstruct_dir(const R* in, R* left, R* 
         const int y = dim > 1 ? b + G - (dir == 1 ? 1 : 0) : 0;
         const int z = dim > 2 ? c + G - (dir == 2 ? 1 : 0) : 0;
         const long long idx = ((long long)z * N1 + y) * N0 + x;
+        PlaneFetch<R, NV> f{&in, idx, s};
         R l[NV], r[NV];
-        reconstruct<R, NV, RECON>(in + idx, (int)plane, s, l, r);
+        reconstruct_f<R, NV, RECON>(f, l, r);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            left[v * plane + idx] = l[v];
-            right[v * plane + idx] = r[v];
+            left.p[v][idx] = l[v];
+            right.p[v][idx] = r[v];
+        }
+    }
+}
+
+// FP64 sums of every variable over the padded-coordinate box [lo, hi) of
+// each member (one block per member, fixed summation order, so the result is
+// reproducible).  out[member * nvar + v].
+template<class R>
+__global__ void __launch_bounds__(256) region_sums(const R* states, long long plane,
+    long long member_stride, int nvar, int N0, int N1, int lo0, int lo1, int lo2, int hi0,
+    int hi1, int hi2, double* out) {
+    const int member = blockIdx.x;
+    const R* base = states + (long long)member * member_stride;
+    const int e0 = hi0 - lo0, e1 = hi1 - lo1, e2 = hi2 - lo2;
+    const long long count = (long long)e0 * e1 * e2;
+    __shared__ double part[kMaxVars][256 / 32];
+    double sum[kMaxVars] = {0, 0, 0, 0, 0};
+    for (long long i = threadIdx.x; i < count; i += blockDim.x) {
+        const int x = lo0 + int(i % e0);
+        const int y = lo1 + int((i / e0) % e1);
+        const int z = lo2 + int(i / ((long long)e0 * e1));
+        const long long idx = ((long long)z * N1 + y) * N0 + x;
+        for (int v = 0; v < nvar; ++v) {
+            sum[v] += double(base[v * plane + idx]);
+        }
+    }
+    for (int v = 0; v < nvar; ++v) {
+        double s = sum[v];
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            part[v][threadIdx.x >> 5] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nvar) {
+        double s = 0;
+        for (int k = 0; k < 256 / 32; ++k) {
+            s += part[threadIdx.x][k];
+        }
+        out[member * nvar + threadIdx.x] = s;
+    }
+}
+
+// Merges `members` states (member j at states + j*member_stride) into the
+// running FP64 (n_prev, mean, m2) of every element (Chan et al.'s pairwise
+// update): chunk mean and chunk M2 in FP64, then
+//   n = n_prev + k, d = mean_k - mean, mean += d*k/n, m2 += m2_k + d*d*n_prev*k/n.
+template<class R>
+__global__ void __launch_bounds__(256) welford_merge(const R* states, long long count,
+    int members, long long member_stride, double* mean, double* m2, long long n_prev) {
+    const double k = double(members);
+    const double n = double(n_prev) + k;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < members; ++j) {
+            s += double(states[(long long)j * member_stride + i]);
+        }
+        const double cm = s / k;
+        double cm2 = 0;
+        for (int j = 0; j < members; ++j) {
+            const double d = double(states[(long long)j * member_stride + i]) - cm;
+            cm2 += d * d;
+        }
+        const double d = cm - mean[i];
+        mean[i] = mean[i] + d * (k / n);
+        m2[i] = m2[i] + cm2 + d * d * (double(n_prev) * k / n);
+    }
+}
+
+// Chan's merge of another accumulator (n_b, mean_b, m2_b) into (n_a, mean, m2).
+__global__ void __launch_bounds__(256) welford_combine(double* mean, double* m2, long long n_a,
+    const double* mean_b, const double* m2_b, long long n_b, long long count) {
+    const double n = double(n_a) + double(n_b);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double d = mean_b[i] - mean[i];
+        mean[i] = mean[i] + d * (double(n_b) / n);
+        m2[i] = m2[i] + m2_b[i] + d * d * (double(n_a) * double(n_b) / n);
+    }
+}
+
+// variance = m2 / n (the biased estimator of MeanVariance, MeanVariance.cpp:55-67).
+__global__ void __launch_bounds__(256) welford_finish(const double* mean, const double* m2,
+    long long n, long long count, double* mean_out, double* var_out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (mean_out) {
+            mean_out[i] = mean[i];
+        }
+        if (var_out) {
+            var_out[i] = m2[i] / double(n);
         }
     }
 }

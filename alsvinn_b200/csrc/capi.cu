@@ -1,15 +1,18 @@
 // C ABI of the hot path (include/als_b200.h): plug-in level calls that
-// mirror one virtual call of the reference interfaces each, and the fused
-// solver that runs whole time steps on the device.
+// mirror one virtual call of the reference interfaces each, the fused
+// solver that runs whole time steps of one grid or of several grid levels
+// on the device, and the FP64 ensemble statistics.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <new>
+#include <numeric>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -52,18 +55,18 @@ bool valid_choice(int flux, int recon) {
 }
 
 cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
-    const als::StageParams& P, int members, cudaStream_t s) {
+    const als::StageParams& P, int blocks_per_sm, cudaStream_t s) {
     if (precision == ALS_FP64) {
         switch (dim) {
-        case 1: return als::launch_stage_f64_1d(recon, flux, kind, P, members, s);
-        case 2: return als::launch_stage_f64_2d(recon, flux, kind, P, members, s);
-        default: return als::launch_stage_f64_3d(recon, flux, kind, P, members, s);
+        case 1: return als::launch_stage_f64_1d(recon, flux, kind, P, blocks_per_sm, s);
+        case 2: return als::launch_stage_f64_2d(recon, flux, kind, P, blocks_per_sm, s);
+        default: return als::launch_stage_f64_3d(recon, flux, kind, P, blocks_per_sm, s);
         }
     }
     switch (dim) {
-    case 1: return als::launch_stage_f32_1d(recon, flux, kind, P, members, s);
-    case 2: return als::launch_stage_f32_2d(recon, flux, kind, P, members, s);
-    default: return als::launch_stage_f32_3d(recon, flux, kind, P, members, s);
+    case 1: return als::launch_stage_f32_1d(recon, flux, kind, P, blocks_per_sm, s);
+    case 2: return als::launch_stage_f32_2d(recon, flux, kind, P, blocks_per_sm, s);
+    default: return als::launch_stage_f32_3d(recon, flux, kind, P, blocks_per_sm, s);
     }
 }
 
@@ -110,6 +113,76 @@ int check_grid(const als_grid* g) {
     return ALS_OK;
 }
 
+int check_planes(const void* const* planes, int nvar) {
+    if (!planes) {
+        return fail(ALS_E_INVALID, "null plane array");
+    }
+    for (int v = 0; v < nvar; ++v) {
+        if (!planes[v]) {
+            return fail(ALS_E_INVALID, "null plane pointer");
+        }
+    }
+    return ALS_OK;
+}
+
+// A level of one state given as one pointer per variable.
+als::LevelDesc plane_level(const als::GridDesc& gd, int nvar, const void* const* in,
+    const void* const* un, void* const* out) {
+    als::LevelDesc L;
+    std::memset(&L, 0, sizeof(L));
+    L.grid = gd;
+    for (int v = 0; v < nvar; ++v) {
+        L.in[v] = in[v];
+        L.un[v] = un[v];
+        L.out[v] = out[v];
+    }
+    L.member_stride = 0;
+    L.members = 1;
+    L.tiles_per_member = gd.tiles[0] * gd.tiles[1] * gd.tiles[2];
+    return L;
+}
+
+// Fills work_begin of every level and the total work of the launch.
+void finish_params(als::StageParams& P) {
+    long long w = 0;
+    for (int l = 0; l < P.nlevels; ++l) {
+        P.level[l].work_begin = w;
+        w += (long long)P.level[l].members * P.level[l].tiles_per_member;
+    }
+    P.total_work = w;
+}
+
+template<class R>
+als::Planes<R> planes_of(void* const* p, int nvar) {
+    als::Planes<R> out;
+    std::memset(&out, 0, sizeof(out));
+    for (int v = 0; v < nvar; ++v) {
+        out.p[v] = static_cast<R*>(p[v]);
+    }
+    return out;
+}
+
+template<class R>
+als::Planes<R> contiguous_planes(void* base, int nvar, long long plane) {
+    als::Planes<R> out;
+    std::memset(&out, 0, sizeof(out));
+    for (int v = 0; v < nvar; ++v) {
+        out.p[v] = static_cast<R*>(base) + v * plane;
+    }
+    return out;
+}
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        cudaSetDevice(prev);
+    }
+};
+
 } // namespace
 
 extern "C" {
@@ -119,7 +192,7 @@ const char* als_last_error(void) {
 }
 
 int als_version(void) {
-    return 1;
+    return 2;
 }
 
 int als_ghost_cells(int flux, int reconstruction) {
@@ -130,33 +203,45 @@ int als_ghost_cells(int flux, int reconstruction) {
     return std::max(1, als::recon_ghosts(reconstruction));
 }
 
-int als_fill_ghosts(const als_grid* grid, int boundary, double* planes, int nvar, int members,
+int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, int nvar,
     void* stream) {
     int rc = check_grid(grid);
     if (rc != ALS_OK) {
         return rc;
     }
-    if (!planes || nvar < 1 || members < 1 || (boundary != ALS_BC_NEUMANN && boundary != ALS_BC_PERIODIC)) {
+    if (nvar < 1 || nvar > als::kMaxVars || (boundary != ALS_BC_NEUMANN && boundary != ALS_BC_PERIODIC)) {
         return fail(ALS_E_INVALID, "invalid ghost-fill arguments");
+    }
+    rc = check_planes((const void* const*)planes, nvar);
+    if (rc != ALS_OK) {
+        return rc;
     }
     int lo[3] = {0, 0, 0};
     als::GridDesc gd = make_grid(grid->dimension, grid->n, grid->ghosts, lo, grid->n);
-    dim3 blocks(grid_blocks(gd.plane, 256), members);
-    als::fill_ghosts<double><<<blocks, 256, 0, (cudaStream_t)stream>>>(planes, nvar, gd.plane,
-        (long long)nvar * gd.plane, grid->dimension, gd.n[0], gd.n[1], gd.n[2], grid->ghosts,
-        boundary);
+    dim3 blocks(grid_blocks(gd.plane, 256), 1);
+    als::fill_ghosts<double><<<blocks, 256, 0, (cudaStream_t)stream>>>(
+        planes_of<double>((void* const*)planes, nvar), nvar, gd.plane, 0, grid->dimension,
+        gd.n[0], gd.n[1], gd.n[2], grid->ghosts, boundary);
     ALS_CUDA(cudaGetLastError());
     return ALS_OK;
 }
 
-int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* in,
-    double* out, const int* start, const int* end, double* wave_speed, void* stream) {
+int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* const* in,
+    double* const* out, const int* start, const int* end, double* wave_speed, void* stream) {
     int rc = check_grid(grid);
     if (rc != ALS_OK) {
         return rc;
     }
-    if (!valid_choice(flux, reconstruction) || !in || !out || !wave_speed) {
+    if (!valid_choice(flux, reconstruction) || !wave_speed) {
         return fail(ALS_E_INVALID, "invalid flux arguments");
+    }
+    const int nvar = grid->dimension + 2;
+    rc = check_planes((const void* const*)in, nvar);
+    if (rc == ALS_OK) {
+        rc = check_planes((const void* const*)out, nvar);
+    }
+    if (rc != ALS_OK) {
+        return rc;
     }
     if (grid->ghosts < als_ghost_cells(flux, reconstruction)) {
         return fail(ALS_E_INVALID, "planes have fewer ghost cells than the reconstruction needs");
@@ -176,20 +261,20 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     cudaStream_t s = (cudaStream_t)stream;
     als::StageParams P;
     std::memset(&P, 0, sizeof(P));
-    P.in = in;
-    P.un = in;
-    P.out = out;
-    P.grid = make_grid(grid->dimension, grid->n, grid->ghosts, lo, hi);
-    P.sample_stride = 0;
+    als::GridDesc gd = make_grid(grid->dimension, grid->n, grid->ghosts, lo, hi);
+    P.level[0] = plane_level(gd, nvar, (const void* const*)in, (const void* const*)in,
+        (void* const*)out);
+    P.nlevels = 1;
     P.bc = ALS_BC_NEUMANN;
     P.write_ghosts = 0;
     P.gamma = grid->gamma;
     unsigned long long* ws_dev = nullptr;
     ALS_CUDA(cudaMallocAsync((void**)&ws_dev, 3 * sizeof(unsigned long long), s));
     ALS_CUDA(cudaMemsetAsync(ws_dev, 0, 3 * sizeof(unsigned long long), s));
-    P.ws_out = ws_dev;
+    P.level[0].ws_out = ws_dev;
+    finish_params(P);
     cudaError_t err = launch_stage(ALS_FP64, grid->dimension, reconstruction, flux,
-        als::KIND_FLUX0, P, 1, s);
+        als::KIND_FLUX0, P, 0, s);
     unsigned long long host[3] = {0, 0, 0};
     if (err == cudaSuccess) {
         err = cudaMemcpyAsync(host, ws_dev, sizeof(host), cudaMemcpyDeviceToHost, s);
@@ -209,15 +294,26 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     return ALS_OK;
 }
 
-int als_reconstruct(const als_grid* grid, int reconstruction, int direction, const double* in,
-    double* left, double* right, void* stream) {
+int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
+    const double* const* in, double* const* left, double* const* right, void* stream) {
     int rc = check_grid(grid);
     if (rc != ALS_OK) {
         return rc;
     }
-    if (direction < 0 || direction >= grid->dimension || !in || !left || !right ||
-        reconstruction < ALS_RECON_NONE || reconstruction > ALS_RECON_ENO4) {
+    const int nvar = grid->dimension + 2;
+    if (direction < 0 || direction >= grid->dimension || reconstruction < ALS_RECON_NONE ||
+        reconstruction > ALS_RECON_ENO4) {
         return fail(ALS_E_INVALID, "invalid reconstruction arguments");
+    }
+    rc = check_planes((const void* const*)in, nvar);
+    if (rc == ALS_OK) {
+        rc = check_planes((const void* const*)left, nvar);
+    }
+    if (rc == ALS_OK) {
+        rc = check_planes((const void* const*)right, nvar);
+    }
+    if (rc != ALS_OK) {
+        return rc;
     }
     const int G = grid->ghosts;
     if (G != std::max(1, als::recon_ghosts(reconstruction))) {
@@ -229,25 +325,25 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction, con
         N[d] = d < grid->dimension ? grid->n[d] + 2 * G : 1;
         plane *= N[d];
     }
-    if (plane > INT_MAX) {
-        return fail(ALS_E_UNSUPPORTED, "plane too large for the plug-in reconstruction");
-    }
-    const int blocks = grid_blocks(plane, 256);
     cudaStream_t s = (cudaStream_t)stream;
     const int dim = grid->dimension;
     if (reconstruction == ALS_RECON_NONE) {
         // NoReconstruction copies every cell, ghosts included (NoReconstruction.cpp:51-61)
-        const size_t bytes = sizeof(double) * size_t(dim + 2) * size_t(plane);
-        ALS_CUDA(cudaMemcpyAsync(left, in, bytes, cudaMemcpyDeviceToDevice, s));
-        ALS_CUDA(cudaMemcpyAsync(right, in, bytes, cudaMemcpyDeviceToDevice, s));
+        for (int v = 0; v < nvar; ++v) {
+            ALS_CUDA(cudaMemcpyAsync(left[v], in[v], sizeof(double) * plane, cudaMemcpyDeviceToDevice, s));
+            ALS_CUDA(cudaMemcpyAsync(right[v], in[v], sizeof(double) * plane, cudaMemcpyDeviceToDevice, s));
+        }
         return ALS_OK;
     }
+    const int blocks = grid_blocks(plane, 256);
+    const als::Planes<double> pin = planes_of<double>((void* const*)in, nvar);
+    const als::Planes<double> pl = planes_of<double>((void* const*)left, nvar);
+    const als::Planes<double> pr = planes_of<double>((void* const*)right, nvar);
 #define ALS_RECON_CASE(NV, RC)                                                               \
-    als::reconstruct_dir<double, NV, RC><<<blocks, 256, 0, s>>>(in, left, right, plane, dim,  \
-        N[0], N[1], N[2], G, direction)
+    als::reconstruct_dir<double, NV, RC><<<blocks, 256, 0, s>>>(pin, pl, pr, dim, N[0], N[1], \
+        N[2], G, direction)
 #define ALS_RECON_NV(NV)                                                                     \
     switch (reconstruction) {                                                                \
-    case ALS_RECON_NONE: ALS_RECON_CASE(NV, als::RECON_NONE); break;                         \
     case ALS_RECON_WENO2: ALS_RECON_CASE(NV, als::RECON_WENO2); break;                       \
     case ALS_RECON_ENO2: ALS_RECON_CASE(NV, als::RECON_ENO2); break;                         \
     case ALS_RECON_ENO3: ALS_RECON_CASE(NV, als::RECON_ENO3); break;                         \
@@ -297,23 +393,38 @@ double als_compute_timestep(const double* wave_speed, const double* cell_lengths
 
 // ------------------------------------------------------------------ solver
 
+namespace {
+
+// One grid level of a solver: its geometry, its members and its buffers.
+struct SolverLevel {
+    als_solver_config cfg;        // this level's n, lower, upper, members
+    als::GridDesc grid;
+    int first = 0;                // global index of its first member
+    long long member_elems = 0;   // nvar * plane
+    double dx[3];
+    void* buf[3] = {nullptr, nullptr, nullptr};  // state A, flux L, state B
+};
+
+} // namespace
+
 struct als_solver {
-    als_solver_config cfg;
+    als_solver_config cfg;        // shared settings (level 0's config)
     int device = 0;
     int g = 0;
     int nv = 0;
     size_t elem = 8;
-    als::GridDesc grid;
-    long long member_elems = 0;   // nv * plane
-    void* buf[3] = {nullptr, nullptr, nullptr};  // state A, flux L, state B
-    int cur = 0;                  // RK2 ping-pong: index (0 -> buf[0], 1 -> buf[2]) of U^n
+    std::vector<SolverLevel> levels;
+    std::vector<int> order;       // order of the levels in the work list
+    int blocks_per_sm = 0;        // 0: one block per work item; > 0: persistent, blocks per SM
+    unsigned long long* counter = nullptr;  // work counter of the persistent launches
+    int members = 0;              // over all levels
+    int cur = 0;                  // RK2 ping-pong: 1 when U^n of active members sits in B
     als::StepState* state = nullptr;
     als::StepState* host_state = nullptr;  // pinned mirror
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
-    int graph_cur = 0;            // ping-pong position the graph was captured at
-    double dx[3];
+    int graph_cur = 0;
 
     ~als_solver() {
         int prev = 0;
@@ -322,13 +433,18 @@ struct als_solver {
         if (graph) {
             cudaGraphExecDestroy(graph);
         }
-        for (void* p : buf) {
-            if (p) {
-                cudaFree(p);
+        for (SolverLevel& L : levels) {
+            for (void* p : L.buf) {
+                if (p) {
+                    cudaFree(p);
+                }
             }
         }
         if (state) {
             cudaFree(state);
+        }
+        if (counter) {
+            cudaFree(counter);
         }
         if (host_state) {
             cudaFreeHost(host_state);
@@ -339,106 +455,140 @@ struct als_solver {
         cudaSetDevice(prev);
     }
 
-    void* current() const {
-        return cfg.integrator == ALS_INT_RK2 && cur == 1 ? buf[2] : buf[0];
+    void* current(const SolverLevel& L) const {
+        return cfg.integrator == ALS_INT_RK2 && cur == 1 ? L.buf[2] : L.buf[0];
     }
-    void* other() const {
-        return cfg.integrator == ALS_INT_RK2 && cur == 1 ? buf[0] : buf[2];
+    void* other(const SolverLevel& L) const {
+        return cfg.integrator == ALS_INT_RK2 && cur == 1 ? L.buf[0] : L.buf[2];
+    }
+    int level_of(int member) const {
+        for (size_t l = 0; l < levels.size(); ++l) {
+            if (member >= levels[l].first && member < levels[l].first + levels[l].cfg.members) {
+                return int(l);
+            }
+        }
+        return -1;
     }
 };
 
 namespace {
 
-struct DeviceGuard {
-    int prev = 0;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        cudaSetDevice(dev);
+als::LevelDesc solver_level(const als_solver* s, const SolverLevel& L, const void* in,
+    const void* un, void* out) {
+    als::LevelDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.grid = L.grid;
+    const long long plane = L.grid.plane;
+    for (int v = 0; v < s->nv; ++v) {
+        D.in[v] = static_cast<const char*>(in) + size_t(v) * plane * s->elem;
+        D.un[v] = static_cast<const char*>(un) + size_t(v) * plane * s->elem;
+        D.out[v] = static_cast<char*>(out) + size_t(v) * plane * s->elem;
     }
-    ~DeviceGuard() {
-        cudaSetDevice(prev);
-    }
-};
+    D.member_stride = L.member_elems;
+    D.state = s->state + L.first;
+    D.members = L.cfg.members;
+    D.tiles_per_member = L.grid.tiles[0] * L.grid.tiles[1] * L.grid.tiles[2];
+    return D;
+}
 
-als::StageParams solver_params(const als_solver* s) {
+// Parameters of one stage over every level; `pick` chooses (in, un, out)
+// per level.
+template<class Pick>
+als::StageParams solver_params(const als_solver* s, Pick pick) {
     als::StageParams P;
     std::memset(&P, 0, sizeof(P));
-    P.grid = s->grid;
-    P.sample_stride = s->member_elems;
+    P.nlevels = int(s->levels.size());
+    for (int k = 0; k < P.nlevels; ++k) {
+        const SolverLevel& L = s->levels[s->order[k]];
+        const void* in;
+        const void* un;
+        void* out;
+        pick(L, in, un, out);
+        P.level[k] = solver_level(s, L, in, un, out);
+    }
     P.bc = s->cfg.boundary;
     P.write_ghosts = 1;
     P.gamma = s->cfg.gamma;
-    P.state = s->state;
-    P.member0 = 0;
+    P.counter = s->blocks_per_sm > 0 ? s->counter : nullptr;
+    finish_params(P);
     return P;
 }
 
-// Enqueues one time step.  FE: FLUX0 + fe_update.  RK2: FLUX0 + RK2_1 into the
-// other buffer (ping-pong).  RK3: FLUX0 + RK3_1 + RK3_2 in place.
-// With `ev` (launches+1 events), records ev[0] before the first kernel and
-// ev[k] after kernel k.
+template<class R, int NV>
+cudaError_t launch_fe_update(als_solver* s, const SolverLevel& L) {
+    dim3 blocks(grid_blocks(L.grid.plane, 256), L.cfg.members);
+    als::fe_update<R, NV><<<blocks, 256, 0, s->stream>>>(static_cast<const R*>(L.buf[1]),
+        static_cast<R*>(s->current(L)), L.grid.plane, L.member_elems, s->state + L.first,
+        s->cfg.gamma);
+    return cudaGetLastError();
+}
+
+// Enqueues one time step of every level, each stage as one launch over all
+// levels.  FE: FLUX0 + fe_update.  RK2: FLUX0 + RK2_1 into the other buffer
+// (ping-pong).  RK3: FLUX0 + RK3_1 + RK3_2 in place.  With `ev`
+// (launches+1 events), records ev[0] before the first kernel and ev[k]
+// after kernel k.
 int enqueue_step(als_solver* s, cudaEvent_t* ev = nullptr) {
     const int prec = s->cfg.precision;
     const int dim = s->cfg.dimension;
     const int recon = s->cfg.reconstruction;
     const int flux = s->cfg.flux;
-    const int members = s->cfg.members;
-    als::StageParams P = solver_params(s);
-    void* un = s->current();
-    P.in = un;
-    P.un = un;
-    P.out = s->buf[1];
+    const int bps = s->blocks_per_sm;
     if (ev) {
         ALS_CUDA(cudaEventRecord(ev[0], s->stream));
     }
-    ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_FLUX0, P, members, s->stream));
+    als::StageParams P = solver_params(s, [s](const SolverLevel& L, const void*& in,
+                                              const void*& un, void*& out) {
+        in = s->current(L);
+        un = in;
+        out = L.buf[1];
+    });
+    ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_FLUX0, P, bps, s->stream));
     if (ev) {
         ALS_CUDA(cudaEventRecord(ev[1], s->stream));
     }
     if (s->cfg.integrator == ALS_INT_FORWARD_EULER) {
-        dim3 blocks(grid_blocks(s->grid.plane, 256), members);
-        if (prec == ALS_FP64) {
-            if (dim == 1) {
-                als::fe_update<double, 3><<<blocks, 256, 0, s->stream>>>((const double*)s->buf[1], (double*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
-            } else if (dim == 2) {
-                als::fe_update<double, 4><<<blocks, 256, 0, s->stream>>>((const double*)s->buf[1], (double*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
+        for (const SolverLevel& L : s->levels) {
+            cudaError_t err;
+            if (prec == ALS_FP64) {
+                err = dim == 1 ? launch_fe_update<double, 3>(s, L)
+                    : (dim == 2 ? launch_fe_update<double, 4>(s, L) : launch_fe_update<double, 5>(s, L));
             } else {
-                als::fe_update<double, 5><<<blocks, 256, 0, s->stream>>>((const double*)s->buf[1], (double*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
+                err = dim == 1 ? launch_fe_update<float, 3>(s, L)
+                    : (dim == 2 ? launch_fe_update<float, 4>(s, L) : launch_fe_update<float, 5>(s, L));
             }
-        } else {
-            if (dim == 1) {
-                als::fe_update<float, 3><<<blocks, 256, 0, s->stream>>>((const float*)s->buf[1], (float*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
-            } else if (dim == 2) {
-                als::fe_update<float, 4><<<blocks, 256, 0, s->stream>>>((const float*)s->buf[1], (float*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
-            } else {
-                als::fe_update<float, 5><<<blocks, 256, 0, s->stream>>>((const float*)s->buf[1], (float*)un, s->grid.plane, s->member_elems, s->state, 0, s->cfg.gamma);
-            }
+            ALS_CUDA(err);
         }
-        ALS_CUDA(cudaGetLastError());
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
     } else if (s->cfg.integrator == ALS_INT_RK2) {
-        P.in = s->buf[1];
-        P.un = un;
-        P.out = s->other();
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK2_1, P, members, s->stream));
+        P = solver_params(s, [s](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+            in = L.buf[1];
+            un = s->current(L);
+            out = s->other(L);
+        });
+        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK2_1, P, bps, s->stream));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
         s->cur ^= 1;
     } else {
-        P.in = s->buf[1];
-        P.un = un;
-        P.out = s->buf[2];
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_1, P, members, s->stream));
+        P = solver_params(s, [](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+            in = L.buf[1];
+            un = L.buf[0];
+            out = L.buf[2];
+        });
+        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_1, P, bps, s->stream));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
-        P.in = s->buf[2];
-        P.un = un;
-        P.out = un;
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_2, P, members, s->stream));
+        P = solver_params(s, [](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+            in = L.buf[2];
+            un = L.buf[0];
+            out = L.buf[0];
+        });
+        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_2, P, bps, s->stream));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[3], s->stream));
         }
@@ -447,22 +597,22 @@ int enqueue_step(als_solver* s, cudaEvent_t* ev = nullptr) {
 }
 
 template<class R>
-int fill_member_ghosts(als_solver* s, void* base, int first, int count) {
-    dim3 blocks(grid_blocks(s->grid.plane, 256), count);
-    als::fill_ghosts<R><<<blocks, 256, 0, s->stream>>>(
-        static_cast<R*>(base) + (long long)first * s->member_elems, s->nv, s->grid.plane,
-        s->member_elems, s->cfg.dimension, s->grid.n[0], s->grid.n[1], s->grid.n[2], s->g,
-        s->cfg.boundary);
+int fill_member_ghosts(als_solver* s, const SolverLevel& L, void* base, int first_local,
+    int count) {
+    dim3 blocks(grid_blocks(L.grid.plane, 256), count);
+    void* start = static_cast<char*>(base) + size_t(first_local) * L.member_elems * s->elem;
+    als::fill_ghosts<R><<<blocks, 256, 0, s->stream>>>(contiguous_planes<R>(start, s->nv, L.grid.plane),
+        s->nv, L.grid.plane, L.member_elems, s->cfg.dimension, L.grid.n[0], L.grid.n[1],
+        L.grid.n[2], s->g, s->cfg.boundary);
     ALS_CUDA(cudaGetLastError());
     return ALS_OK;
 }
 
 int reset_members(als_solver* s, int first, int count) {
     for (int m = first; m < first + count; ++m) {
+        const SolverLevel& L = s->levels[s->level_of(m)];
         als::StepState& st = s->host_state[m];
         std::memset(&st, 0, sizeof(st));
-        st.t = 0;
-        st.dt = 0;
         st.end_time = s->cfg.end_time;
         st.cfl = s->cfg.cfl;
         st.max_steps = s->cfg.max_steps > 0 ? s->cfg.max_steps : LLONG_MAX;
@@ -470,7 +620,7 @@ int reset_members(als_solver* s, int first, int count) {
         st.bad_index = -1;  // as unsigned: the largest value, lowered by atomicMin
         st.bad_step = -1;
         for (int d = 0; d < 3; ++d) {
-            st.dx[d] = s->dx[d];
+            st.dx[d] = L.dx[d];
         }
     }
     ALS_CUDA(cudaMemcpyAsync(s->state + first, s->host_state + first,
@@ -480,21 +630,30 @@ int reset_members(als_solver* s, int first, int count) {
 }
 
 int refresh_host_state(als_solver* s) {
-    ALS_CUDA(cudaMemcpyAsync(s->host_state, s->state, sizeof(als::StepState) * s->cfg.members,
+    ALS_CUDA(cudaMemcpyAsync(s->host_state, s->state, sizeof(als::StepState) * s->members,
         cudaMemcpyDeviceToHost, s->stream));
     ALS_CUDA(cudaStreamSynchronize(s->stream));
     return ALS_OK;
 }
 
-} // namespace
-
-extern "C" {
-
-int als_solver_create(const als_solver_config* cfg, int device, als_solver** out) {
-    if (!cfg || !out) {
-        return fail(ALS_E_INVALID, "null argument");
+void drop_graph(als_solver* s) {
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
     }
-    *out = nullptr;
+}
+
+// members [first, first+count) must lie in one level; returns it or -1
+int range_level(const als_solver* s, int first, int count) {
+    if (first < 0 || count < 1 || first + count > s->members) {
+        return -1;
+    }
+    const int l = s->level_of(first);
+    const SolverLevel& L = s->levels[l];
+    return first + count <= L.first + L.cfg.members ? l : -1;
+}
+
+int check_config(const als_solver_config* cfg) {
     if (cfg->dimension < 1 || cfg->dimension > 3 || !valid_choice(cfg->flux, cfg->reconstruction) ||
         cfg->integrator < ALS_INT_FORWARD_EULER || cfg->integrator > ALS_INT_RK3 ||
         (cfg->boundary != ALS_BC_NEUMANN && cfg->boundary != ALS_BC_PERIODIC) ||
@@ -512,47 +671,95 @@ int als_solver_create(const als_solver_config* cfg, int device, als_solver** out
             return fail(ALS_E_INVALID, "every active direction needs at least 2*ghosts interior cells");
         }
     }
+    return ALS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int als_solver_create_levels(const als_solver_config* cfgs, int nlevels, int device,
+    als_solver** out) {
+    if (!cfgs || !out) {
+        return fail(ALS_E_INVALID, "null argument");
+    }
+    *out = nullptr;
+    if (nlevels < 1 || nlevels > als::kMaxLevels) {
+        return fail(ALS_E_INVALID, "1 to 4 grid levels");
+    }
+    for (int l = 0; l < nlevels; ++l) {
+        int rc = check_config(&cfgs[l]);
+        if (rc != ALS_OK) {
+            return rc;
+        }
+        const als_solver_config& a = cfgs[0];
+        const als_solver_config& b = cfgs[l];
+        if (b.dimension != a.dimension || b.flux != a.flux || b.reconstruction != a.reconstruction ||
+            b.integrator != a.integrator || b.boundary != a.boundary || b.precision != a.precision ||
+            b.gamma != a.gamma || b.cfl != a.cfl || b.end_time != a.end_time ||
+            b.max_steps != a.max_steps) {
+            return fail(ALS_E_INVALID, "levels may differ only in grid size, domain and members");
+        }
+    }
     std::unique_ptr<als_solver> s(new (std::nothrow) als_solver());
     if (!s) {
         return fail(ALS_E_NOMEM, "out of host memory");
     }
-    s->cfg = *cfg;
+    const als_solver_config& cfg = cfgs[0];
+    s->cfg = cfg;
     s->device = device;
-    s->g = g;
-    s->nv = cfg->dimension + 2;
-    s->elem = cfg->precision == ALS_FP64 ? 8 : 4;
-    int lo[3] = {0, 0, 0};
-    int n[3];
-    for (int d = 0; d < 3; ++d) {
-        n[d] = d < cfg->dimension ? cfg->n[d] : 1;
-    }
-    s->grid = make_grid(cfg->dimension, n, g, lo, n, cfg->precision);
-    s->member_elems = (long long)s->nv * s->grid.plane;
-    for (int d = 0; d < 3; ++d) {
-        // Grid.cpp:24-41: (top - origin) / n, and 1 for a direction with one cell
-        s->dx[d] = (cfg->upper[d] - cfg->lower[d]) / double(n[d]);
-        if (d > 0 && n[d] == 1) {
-            s->dx[d] = 1;
-        }
-    }
+    s->g = als_ghost_cells(cfg.flux, cfg.reconstruction);
+    s->nv = cfg.dimension + 2;
+    s->elem = cfg.precision == ALS_FP64 ? 8 : 4;
     DeviceGuard guard(device);
     ALS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    const size_t bytes = size_t(s->member_elems) * cfg->members * s->elem;
-    for (int b = 0; b < 3; ++b) {
-        if (b == 2 && cfg->integrator == ALS_INT_FORWARD_EULER) {
-            continue;
+    int first = 0;
+    for (int l = 0; l < nlevels; ++l) {
+        SolverLevel L;
+        L.cfg = cfgs[l];
+        int lo[3] = {0, 0, 0};
+        int n[3];
+        for (int d = 0; d < 3; ++d) {
+            n[d] = d < cfg.dimension ? cfgs[l].n[d] : 1;
         }
-        ALS_CUDA(cudaMalloc(&s->buf[b], bytes));
-        ALS_CUDA(cudaMemset(s->buf[b], 0, bytes));
+        L.grid = make_grid(cfg.dimension, n, s->g, lo, n, cfg.precision);
+        L.member_elems = (long long)s->nv * L.grid.plane;
+        L.first = first;
+        first += cfgs[l].members;
+        for (int d = 0; d < 3; ++d) {
+            // Grid.cpp:24-41: (top - origin) / n, and 1 for a direction with one cell
+            L.dx[d] = (cfgs[l].upper[d] - cfgs[l].lower[d]) / double(n[d]);
+            if (d > 0 && n[d] == 1) {
+                L.dx[d] = 1;
+            }
+        }
+        const size_t bytes = size_t(L.member_elems) * cfgs[l].members * s->elem;
+        for (int b = 0; b < 3; ++b) {
+            if (b == 2 && cfg.integrator == ALS_INT_FORWARD_EULER) {
+                continue;
+            }
+            ALS_CUDA(cudaMalloc(&L.buf[b], bytes));
+            ALS_CUDA(cudaMemset(L.buf[b], 0, bytes));
+        }
+        s->levels.push_back(L);
     }
-    ALS_CUDA(cudaMalloc((void**)&s->state, sizeof(als::StepState) * cfg->members));
-    ALS_CUDA(cudaMallocHost((void**)&s->host_state, sizeof(als::StepState) * cfg->members));
-    int rc = reset_members(s.get(), 0, cfg->members);
+    s->members = first;
+    s->order.resize(nlevels);
+    std::iota(s->order.begin(), s->order.end(), 0);
+    ALS_CUDA(cudaMalloc((void**)&s->state, sizeof(als::StepState) * s->members));
+    ALS_CUDA(cudaMalloc((void**)&s->counter, 2 * sizeof(unsigned long long)));
+    ALS_CUDA(cudaMemset(s->counter, 0, 2 * sizeof(unsigned long long)));
+    ALS_CUDA(cudaMallocHost((void**)&s->host_state, sizeof(als::StepState) * s->members));
+    int rc = reset_members(s.get(), 0, s->members);
     if (rc != ALS_OK) {
         return rc;
     }
     *out = s.release();
     return ALS_OK;
+}
+
+int als_solver_create(const als_solver_config* cfg, int device, als_solver** out) {
+    return als_solver_create_levels(cfg, 1, device, out);
 }
 
 int als_solver_destroy(als_solver* s) {
@@ -565,7 +772,7 @@ int als_solver_geometry(const als_solver* s, long long* plane, int* ghosts) {
         return fail(ALS_E_INVALID, "null solver");
     }
     if (plane) {
-        *plane = s->grid.plane;
+        *plane = s->levels[0].grid.plane;
     }
     if (ghosts) {
         *ghosts = s->g;
@@ -573,17 +780,38 @@ int als_solver_geometry(const als_solver* s, long long* plane, int* ghosts) {
     return ALS_OK;
 }
 
+int als_solver_level(const als_solver* s, int level, int* first_member, int* members,
+    long long* plane) {
+    if (!s || level < 0 || level >= int(s->levels.size())) {
+        return fail(ALS_E_INVALID, "invalid level");
+    }
+    const SolverLevel& L = s->levels[level];
+    if (first_member) {
+        *first_member = L.first;
+    }
+    if (members) {
+        *members = L.cfg.members;
+    }
+    if (plane) {
+        *plane = L.grid.plane;
+    }
+    return ALS_OK;
+}
+
 int als_solver_set_state(als_solver* s, const double* host, int first_member, int count) {
-    if (!s || !host || first_member < 0 || count < 1 || first_member + count > s->cfg.members) {
-        return fail(ALS_E_INVALID, "invalid set_state arguments");
+    const int l = s ? range_level(s, first_member, count) : -1;
+    if (!s || !host || l < 0) {
+        return fail(ALS_E_INVALID, "invalid set_state arguments (members must lie in one level)");
     }
     DeviceGuard guard(s->device);
-    const size_t n = size_t(s->member_elems) * count;
+    const SolverLevel& L = s->levels[l];
+    const int local = first_member - L.first;
+    const size_t n = size_t(L.member_elems) * count;
     s->cur = 0;
     if (s->cfg.precision == ALS_FP64) {
-        ALS_CUDA(cudaMemcpyAsync(static_cast<double*>(s->buf[0]) + (long long)first_member * s->member_elems,
+        ALS_CUDA(cudaMemcpyAsync(static_cast<double*>(L.buf[0]) + (long long)local * L.member_elems,
             host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-        int rc = fill_member_ghosts<double>(s, s->buf[0], first_member, count);
+        int rc = fill_member_ghosts<double>(s, L, L.buf[0], local, count);
         if (rc != ALS_OK) {
             return rc;
         }
@@ -592,9 +820,9 @@ int als_solver_set_state(als_solver* s, const double* host, int first_member, in
         for (size_t i = 0; i < n; ++i) {
             tmp[i] = float(host[i]);
         }
-        ALS_CUDA(cudaMemcpyAsync(static_cast<float*>(s->buf[0]) + (long long)first_member * s->member_elems,
+        ALS_CUDA(cudaMemcpyAsync(static_cast<float*>(L.buf[0]) + (long long)local * L.member_elems,
             tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        int rc = fill_member_ghosts<float>(s, s->buf[0], first_member, count);
+        int rc = fill_member_ghosts<float>(s, L, L.buf[0], local, count);
         if (rc != ALS_OK) {
             return rc;
         }
@@ -604,43 +832,49 @@ int als_solver_set_state(als_solver* s, const double* host, int first_member, in
 }
 
 int als_solver_set_state_device(als_solver* s, const void* dev, int first_member, int count) {
-    if (!s || !dev || first_member < 0 || count < 1 || first_member + count > s->cfg.members) {
-        return fail(ALS_E_INVALID, "invalid set_state_device arguments");
+    const int l = s ? range_level(s, first_member, count) : -1;
+    if (!s || !dev || l < 0) {
+        return fail(ALS_E_INVALID, "invalid set_state_device arguments (members must lie in one level)");
     }
     DeviceGuard guard(s->device);
+    const SolverLevel& L = s->levels[l];
+    const int local = first_member - L.first;
     s->cur = 0;
-    const size_t bytes = size_t(s->member_elems) * count * s->elem;
-    ALS_CUDA(cudaMemcpyAsync(static_cast<char*>(s->buf[0]) + size_t(first_member) * s->member_elems * s->elem,
+    const size_t bytes = size_t(L.member_elems) * count * s->elem;
+    ALS_CUDA(cudaMemcpyAsync(static_cast<char*>(L.buf[0]) + size_t(local) * L.member_elems * s->elem,
         dev, bytes, cudaMemcpyDeviceToDevice, s->stream));
-    int rc = s->cfg.precision == ALS_FP64 ? fill_member_ghosts<double>(s, s->buf[0], first_member, count)
-                                          : fill_member_ghosts<float>(s, s->buf[0], first_member, count);
+    int rc = s->cfg.precision == ALS_FP64 ? fill_member_ghosts<double>(s, L, L.buf[0], local, count)
+                                          : fill_member_ghosts<float>(s, L, L.buf[0], local, count);
     if (rc != ALS_OK) {
         return rc;
     }
     return reset_members(s, first_member, count);
 }
 
+// Device address of member m's current state (RK2: by its own step parity).
+static const char* member_state_address(als_solver* s, int m) {
+    const SolverLevel& L = s->levels[s->level_of(m)];
+    const void* base = L.buf[0];
+    if (s->cfg.integrator == ALS_INT_RK2 && (s->host_state[m].steps & 1)) {
+        base = L.buf[2];
+    }
+    return static_cast<const char*>(base) + size_t(m - L.first) * L.member_elems * s->elem;
+}
+
 int als_solver_get_state(als_solver* s, double* host, int first_member, int count) {
-    if (!s || !host || first_member < 0 || count < 1 || first_member + count > s->cfg.members) {
-        return fail(ALS_E_INVALID, "invalid get_state arguments");
+    const int l = s ? range_level(s, first_member, count) : -1;
+    if (!s || !host || l < 0) {
+        return fail(ALS_E_INVALID, "invalid get_state arguments (members must lie in one level)");
     }
     DeviceGuard guard(s->device);
-    if (s->cfg.integrator == ALS_INT_RK2) {
-        // RK2 alternates between two buffers; a member's state sits in the
-        // buffer given by the parity of its own completed steps
-        int rc = refresh_host_state(s);
-        if (rc != ALS_OK) {
-            return rc;
-        }
+    int rc = refresh_host_state(s);
+    if (rc != ALS_OK) {
+        return rc;
     }
-    const size_t n = size_t(s->member_elems);
+    const size_t n = size_t(s->levels[l].member_elems);
     std::vector<float> tmp(s->cfg.precision == ALS_FP64 ? 0 : n);
     for (int m = first_member; m < first_member + count; ++m) {
-        const void* base = s->buf[0];
-        if (s->cfg.integrator == ALS_INT_RK2 && (s->host_state[m].steps & 1)) {
-            base = s->buf[2];
-        }
-        const char* src = static_cast<const char*>(base) + size_t(m) * n * s->elem;
+        const char* src = member_state_address(s, m);
         double* dst = host + size_t(m - first_member) * n;
         if (s->cfg.precision == ALS_FP64) {
             ALS_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -660,7 +894,7 @@ int als_solver_state_pointer(als_solver* s, void** dev) {
     if (!s || !dev) {
         return fail(ALS_E_INVALID, "null argument");
     }
-    *dev = s->current();
+    *dev = s->current(s->levels[0]);
     return ALS_OK;
 }
 
@@ -742,12 +976,9 @@ int als_solver_run(als_solver* s) {
         bool failed = false;
         double remaining_steps = 0;
         double progress = 0.0;  // sum of member times: must grow while any member is running
-        for (int m = 0; m < s->cfg.members; ++m) {
+        for (int m = 0; m < s->members; ++m) {
             const als::StepState& st = s->host_state[m];
             progress += st.t;
-        }
-        for (int m = 0; m < s->cfg.members; ++m) {
-            const als::StepState& st = s->host_state[m];
             failed = failed || st.status != 0;
             if (!st.done) {
                 all_done = false;
@@ -777,7 +1008,7 @@ int als_solver_run(als_solver* s) {
 }
 
 int als_solver_info(als_solver* s, int member, als_member_info* info) {
-    if (!s || !info || member < 0 || member >= s->cfg.members) {
+    if (!s || !info || member < 0 || member >= s->members) {
         return fail(ALS_E_INVALID, "invalid info arguments");
     }
     DeviceGuard guard(s->device);
@@ -804,21 +1035,28 @@ int als_solver_launches_per_step(const als_solver* s) {
     if (!s) {
         return fail(ALS_E_INVALID, "null solver");
     }
-    return s->cfg.integrator == ALS_INT_RK3 ? 3 : 2;
+    if (s->cfg.integrator == ALS_INT_RK3) {
+        return 3;
+    }
+    if (s->cfg.integrator == ALS_INT_RK2) {
+        return 2;
+    }
+    return 1 + int(s->levels.size());
 }
 
 int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity) {
     if (!s || !kernel_ms) {
         return fail(ALS_E_INVALID, "null argument");
     }
-    const int k = als_solver_launches_per_step(s);
+    // events sit between the stages: FE counts its per-level updates as one
+    const int k = s->cfg.integrator == ALS_INT_RK3 ? 3 : 2;
     if (capacity < k) {
-        return fail(ALS_E_INVALID, "capacity below the launches per step");
+        return fail(ALS_E_INVALID, "capacity below the stages per step");
     }
     DeviceGuard guard(s->device);
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int rc = ALS_OK;
-    for (int i = 0; i <= k && rc == ALS_OK; ++i) {
+    for (int i = 0; i <= 3 && rc == ALS_OK; ++i) {
         if (cudaEventCreate(&ev[i]) != cudaSuccess) {
             rc = fail(ALS_E_CUDA, "cudaEventCreate failed");
         }
@@ -834,12 +1072,402 @@ int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity) {
             rc = fail(ALS_E_CUDA, "cudaEventElapsedTime failed");
         }
     }
-    for (int i = 0; i <= k; ++i) {
+    for (int i = 0; i <= 3; ++i) {
         if (ev[i]) {
             cudaEventDestroy(ev[i]);
         }
     }
     return rc == ALS_OK ? k : rc;
+}
+
+int als_solver_set_schedule(als_solver* s, int blocks_per_sm, const int* level_order) {
+    if (!s || blocks_per_sm < 0) {
+        return fail(ALS_E_INVALID, "invalid schedule");
+    }
+    std::vector<int> order(s->levels.size());
+    if (level_order) {
+        std::vector<int> seen(s->levels.size(), 0);
+        for (size_t k = 0; k < order.size(); ++k) {
+            const int l = level_order[k];
+            if (l < 0 || l >= int(order.size()) || seen[l]) {
+                return fail(ALS_E_INVALID, "level order must be a permutation of the levels");
+            }
+            seen[l] = 1;
+            order[k] = l;
+        }
+    } else {
+        std::iota(order.begin(), order.end(), 0);
+    }
+    DeviceGuard guard(s->device);
+    ALS_CUDA(cudaStreamSynchronize(s->stream));
+    s->blocks_per_sm = blocks_per_sm;
+    s->order = order;
+    drop_graph(s);
+    return ALS_OK;
+}
+
+int als_solver_get_schedule(const als_solver* s, int* blocks_per_sm, int* level_order) {
+    if (!s) {
+        return fail(ALS_E_INVALID, "null solver");
+    }
+    if (blocks_per_sm) {
+        *blocks_per_sm = s->blocks_per_sm;
+    }
+    if (level_order) {
+        for (size_t k = 0; k < s->order.size(); ++k) {
+            level_order[k] = s->order[k];
+        }
+    }
+    return ALS_OK;
+}
+
+// The schedule autotuner: times `steps` time steps under every candidate
+// (persistent blocks per SM x level order) from the same saved state, keeps
+// the fastest, and restores the state and member clocks, so tuning changes
+// no result.
+int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_order,
+    double* best_ms_per_step) {
+    if (!s || steps < 1) {
+        return fail(ALS_E_INVALID, "invalid tune arguments");
+    }
+    DeviceGuard guard(s->device);
+    ALS_CUDA(cudaStreamSynchronize(s->stream));
+    // save every buffer that holds state, and the member clocks
+    std::vector<void*> saved;
+    size_t total = 0;
+    for (SolverLevel& L : s->levels) {
+        const size_t bytes = size_t(L.member_elems) * L.cfg.members * s->elem;
+        for (int b = 0; b < 3; ++b) {
+            if (!L.buf[b]) {
+                continue;
+            }
+            void* p = nullptr;
+            ALS_CUDA(cudaMalloc(&p, bytes));
+            ALS_CUDA(cudaMemcpyAsync(p, L.buf[b], bytes, cudaMemcpyDeviceToDevice, s->stream));
+            saved.push_back(p);
+            total += bytes;
+        }
+    }
+    als::StepState* saved_state = nullptr;
+    ALS_CUDA(cudaMalloc((void**)&saved_state, sizeof(als::StepState) * s->members));
+    ALS_CUDA(cudaMemcpyAsync(saved_state, s->state, sizeof(als::StepState) * s->members,
+        cudaMemcpyDeviceToDevice, s->stream));
+    const int cur0 = s->cur;
+    const int bps0 = s->blocks_per_sm;
+    const std::vector<int> order0 = s->order;
+
+    auto restore = [&]() -> int {
+        size_t k = 0;
+        for (SolverLevel& L : s->levels) {
+            const size_t bytes = size_t(L.member_elems) * L.cfg.members * s->elem;
+            for (int b = 0; b < 3; ++b) {
+                if (!L.buf[b]) {
+                    continue;
+                }
+                ALS_CUDA(cudaMemcpyAsync(L.buf[b], saved[k++], bytes, cudaMemcpyDeviceToDevice, s->stream));
+            }
+        }
+        ALS_CUDA(cudaMemcpyAsync(s->state, saved_state, sizeof(als::StepState) * s->members,
+            cudaMemcpyDeviceToDevice, s->stream));
+        s->cur = cur0;
+        return ALS_OK;
+    };
+
+    // candidate level orders: as given, finest first, coarsest first
+    std::vector<std::vector<int>> orders;
+    orders.push_back(order0);
+    std::vector<int> by_cells(s->levels.size());
+    std::iota(by_cells.begin(), by_cells.end(), 0);
+    std::stable_sort(by_cells.begin(), by_cells.end(), [s](int a, int b) {
+        return s->levels[a].grid.plane > s->levels[b].grid.plane;
+    });
+    orders.push_back(by_cells);
+    std::reverse(by_cells.begin(), by_cells.end());
+    orders.push_back(by_cells);
+    std::sort(orders.begin(), orders.end());
+    orders.erase(std::unique(orders.begin(), orders.end()), orders.end());
+    // 0: one block per work item; k > 0: persistent, k resident blocks per SM
+    const int bps_candidates[] = {0, 1, 2, 3, 4};
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ALS_CUDA(cudaEventCreate(&e0));
+    ALS_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    int best_bps = bps0;
+    std::vector<int> best_order = order0;
+    int rc = ALS_OK;
+    for (const std::vector<int>& ord : orders) {
+        for (int bps : bps_candidates) {
+            if (rc != ALS_OK) {
+                break;
+            }
+            s->order = ord;
+            s->blocks_per_sm = bps;
+            rc = restore();
+            // one untimed step, then the timed ones
+            for (int k = 0; k < 1 + steps && rc == ALS_OK; ++k) {
+                if (k == 1 && cudaEventRecord(e0, s->stream) != cudaSuccess) {
+                    rc = fail(ALS_E_CUDA, "cudaEventRecord failed");
+                }
+                if (rc == ALS_OK) {
+                    rc = enqueue_step(s);
+                }
+            }
+            if (rc == ALS_OK && (cudaEventRecord(e1, s->stream) != cudaSuccess ||
+                                    cudaEventSynchronize(e1) != cudaSuccess)) {
+                rc = fail(ALS_E_CUDA, "timing failed");
+            }
+            float ms = 0;
+            if (rc == ALS_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = fail(ALS_E_CUDA, "cudaEventElapsedTime failed");
+            }
+            if (rc == ALS_OK && ms / steps < best) {
+                best = ms / steps;
+                best_bps = bps;
+                best_order = ord;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc2 = restore();
+    cudaStreamSynchronize(s->stream);
+    for (void* p : saved) {
+        cudaFree(p);
+    }
+    cudaFree(saved_state);
+    s->blocks_per_sm = best_bps;
+    s->order = best_order;
+    drop_graph(s);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    if (rc2 != ALS_OK) {
+        return rc2;
+    }
+    if (blocks_per_sm) {
+        *blocks_per_sm = best_bps;
+    }
+    if (level_order) {
+        for (size_t k = 0; k < best_order.size(); ++k) {
+            level_order[k] = best_order[k];
+        }
+    }
+    if (best_ms_per_step) {
+        *best_ms_per_step = best;
+    }
+    (void)total;
+    return ALS_OK;
+}
+
+// FP64 sums of every conserved variable over the interior box [lo, hi)
+// (interior cell coordinates, NULL = whole interior) of members
+// [first, first+count) of one level: out[k*nvar + v].
+int als_solver_region_sums(als_solver* s, int first_member, int count, const int* lo,
+    const int* hi, double* out) {
+    const int l = s ? range_level(s, first_member, count) : -1;
+    if (!s || !out || l < 0) {
+        return fail(ALS_E_INVALID, "invalid region_sums arguments (members must lie in one level)");
+    }
+    const SolverLevel& L = s->levels[l];
+    int plo[3], phi[3];
+    for (int d = 0; d < 3; ++d) {
+        const bool active = d < s->cfg.dimension;
+        const int n = L.grid.n[d];
+        const int a = lo && active ? lo[d] : 0;
+        const int b = hi && active ? hi[d] : n;
+        if (active && (a < 0 || b > n || a >= b)) {
+            return fail(ALS_E_INVALID, "region must lie inside the interior");
+        }
+        plo[d] = active ? a + s->g : 0;
+        phi[d] = active ? b + s->g : 1;
+    }
+    DeviceGuard guard(s->device);
+    int rc = refresh_host_state(s);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    double* dev = nullptr;
+    ALS_CUDA(cudaMallocAsync((void**)&dev, sizeof(double) * s->nv * count, s->stream));
+    for (int m = first_member; m < first_member + count; ++m) {
+        const void* base = member_state_address(s, m);
+        cudaError_t err;
+        if (s->cfg.precision == ALS_FP64) {
+            als::region_sums<double><<<1, 256, 0, s->stream>>>(static_cast<const double*>(base),
+                L.grid.plane, 0, s->nv, L.grid.N[0], L.grid.N[1], plo[0], plo[1], plo[2], phi[0],
+                phi[1], phi[2], dev + (m - first_member) * s->nv);
+        } else {
+            als::region_sums<float><<<1, 256, 0, s->stream>>>(static_cast<const float*>(base),
+                L.grid.plane, 0, s->nv, L.grid.N[0], L.grid.N[1], plo[0], plo[1], plo[2], phi[0],
+                phi[1], phi[2], dev + (m - first_member) * s->nv);
+        }
+        err = cudaGetLastError();
+        if (err != cudaSuccess) {
+            cudaFreeAsync(dev, s->stream);
+            return fail(ALS_E_CUDA, std::string("region_sums: ") + cudaGetErrorString(err));
+        }
+    }
+    ALS_CUDA(cudaMemcpyAsync(out, dev, sizeof(double) * s->nv * count, cudaMemcpyDeviceToHost, s->stream));
+    ALS_CUDA(cudaFreeAsync(dev, s->stream));
+    ALS_CUDA(cudaStreamSynchronize(s->stream));
+    return ALS_OK;
+}
+
+} // extern "C"
+
+// -------------------------------------------------------------- statistics
+
+struct als_stats {
+    int device = 0;
+    long long count = 0;          // elements per state
+    long long n = 0;              // states accumulated
+    double* mean = nullptr;
+    double* m2 = nullptr;
+    ~als_stats() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        if (mean) {
+            cudaFree(mean);
+        }
+        if (m2) {
+            cudaFree(m2);
+        }
+        cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+template<class R>
+int stats_merge_states(als_stats* st, const R* states, int members, long long member_stride,
+    cudaStream_t s) {
+    // chunks of at most 64 states keep each chunk's two passes in L2
+    for (int first = 0; first < members; first += 64) {
+        const int k = std::min(64, members - first);
+        als::welford_merge<R><<<grid_blocks(st->count, 256), 256, 0, s>>>(
+            states + (long long)first * member_stride, st->count, k, member_stride, st->mean, st->m2,
+            st->n);
+        ALS_CUDA(cudaGetLastError());
+        st->n += k;
+    }
+    return ALS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int als_stats_create(long long count, int device, als_stats** out) {
+    if (!out || count < 1) {
+        return fail(ALS_E_INVALID, "invalid stats arguments");
+    }
+    *out = nullptr;
+    std::unique_ptr<als_stats> st(new (std::nothrow) als_stats());
+    if (!st) {
+        return fail(ALS_E_NOMEM, "out of host memory");
+    }
+    st->device = device;
+    st->count = count;
+    DeviceGuard guard(device);
+    ALS_CUDA(cudaMalloc((void**)&st->mean, sizeof(double) * count));
+    ALS_CUDA(cudaMalloc((void**)&st->m2, sizeof(double) * count));
+    ALS_CUDA(cudaMemset(st->mean, 0, sizeof(double) * count));
+    ALS_CUDA(cudaMemset(st->m2, 0, sizeof(double) * count));
+    *out = st.release();
+    return ALS_OK;
+}
+
+int als_stats_destroy(als_stats* st) {
+    delete st;
+    return ALS_OK;
+}
+
+int als_stats_add(als_stats* st, const void* states, int precision, int members,
+    long long member_stride, void* stream) {
+    if (!st || !states || members < 1 || member_stride < st->count ||
+        (precision != ALS_FP64 && precision != ALS_FP32)) {
+        return fail(ALS_E_INVALID, "invalid stats_add arguments");
+    }
+    DeviceGuard guard(st->device);
+    return precision == ALS_FP64
+        ? stats_merge_states(st, static_cast<const double*>(states), members, member_stride, (cudaStream_t)stream)
+        : stats_merge_states(st, static_cast<const float*>(states), members, member_stride, (cudaStream_t)stream);
+}
+
+int als_stats_add_solver(als_stats* st, als_solver* s, int level) {
+    if (!st || !s || level < 0 || level >= int(s->levels.size())) {
+        return fail(ALS_E_INVALID, "invalid stats_add_solver arguments");
+    }
+    const SolverLevel& L = s->levels[level];
+    if (L.member_elems != st->count) {
+        return fail(ALS_E_INVALID, "statistics size differs from the level's state size");
+    }
+    DeviceGuard guard(s->device);
+    int rc = refresh_host_state(s);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    // RK2 members may sit in either buffer: add them one by one then
+    if (s->cfg.integrator == ALS_INT_RK2) {
+        for (int m = L.first; m < L.first + L.cfg.members; ++m) {
+            rc = als_stats_add(st, member_state_address(s, m), s->cfg.precision, 1, L.member_elems,
+                s->stream);
+            if (rc != ALS_OK) {
+                return rc;
+            }
+        }
+    } else {
+        rc = als_stats_add(st, L.buf[0], s->cfg.precision, L.cfg.members, L.member_elems, s->stream);
+        if (rc != ALS_OK) {
+            return rc;
+        }
+    }
+    ALS_CUDA(cudaStreamSynchronize(s->stream));
+    return ALS_OK;
+}
+
+int als_stats_merge(als_stats* st, long long n, const double* mean, const double* m2, void* stream) {
+    if (!st || n < 0 || (n > 0 && (!mean || !m2))) {
+        return fail(ALS_E_INVALID, "invalid stats_merge arguments");
+    }
+    if (n == 0) {
+        return ALS_OK;
+    }
+    DeviceGuard guard(st->device);
+    als::welford_combine<<<grid_blocks(st->count, 256), 256, 0, (cudaStream_t)stream>>>(
+        st->mean, st->m2, st->n, mean, m2, n, st->count);
+    ALS_CUDA(cudaGetLastError());
+    st->n += n;
+    return ALS_OK;
+}
+
+int als_stats_moments(als_stats* st, long long* n, double** mean, double** m2) {
+    if (!st) {
+        return fail(ALS_E_INVALID, "null stats");
+    }
+    if (n) {
+        *n = st->n;
+    }
+    if (mean) {
+        *mean = st->mean;
+    }
+    if (m2) {
+        *m2 = st->m2;
+    }
+    return ALS_OK;
+}
+
+int als_stats_result(als_stats* st, double* mean, double* variance, void* stream) {
+    if (!st || st->n < 1) {
+        return fail(ALS_E_INVALID, "no states accumulated");
+    }
+    DeviceGuard guard(st->device);
+    als::welford_finish<<<grid_blocks(st->count, 256), 256, 0, (cudaStream_t)stream>>>(
+        st->mean, st->m2, st->n, st->count, mean, variance);
+    ALS_CUDA(cudaGetLastError());
+    ALS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return ALS_OK;
 }
 
 } // extern "C"
@@ -911,22 +1539,30 @@ extern "C" int als_compute_flux_static(const als_grid* grid, int flux, int recon
         n[d] = d < grid->dimension ? grid->n[d] : 1;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    const int nvar = grid->dimension + 2;
     als::StageParams P;
     std::memset(&P, 0, sizeof(P));
-    P.in = in;
-    P.un = in;
-    P.out = out;
-    P.grid = make_grid(grid->dimension, n, grid->ghosts, lo, n);
-    P.sample_stride = (long long)(grid->dimension + 2) * P.grid.plane;
+    als::GridDesc gd = make_grid(grid->dimension, n, grid->ghosts, lo, n);
+    const void* planes_in[als::kMaxVars];
+    void* planes_out[als::kMaxVars];
+    for (int v = 0; v < nvar; ++v) {
+        planes_in[v] = in + v * gd.plane;
+        planes_out[v] = out + v * gd.plane;
+    }
+    P.level[0] = plane_level(gd, nvar, planes_in, planes_in, planes_out);
+    P.level[0].member_stride = (long long)nvar * gd.plane;
+    P.level[0].members = members;
+    P.level[0].ws_out = static_cast<unsigned long long*>(scratch);
+    P.nlevels = 1;
     P.bc = ALS_BC_NEUMANN;
     P.write_ghosts = 0;
     P.gamma = grid->gamma;
-    P.ws_out = static_cast<unsigned long long*>(scratch);
+    finish_params(P);
     // the array keeps the previous call's maxima: clear the slots used
     const size_t bytes = sizeof(unsigned long long) * 3 * size_t(members);
     ALS_CUDA(cudaMemsetAsync(scratch, 0, bytes, s));
     ALS_CUDA(launch_stage(ALS_FP64, grid->dimension, reconstruction, flux, als::KIND_FLUX0, P,
-        members, s));
+        0, s));
     // a non-negative double and its bit pattern read as an unsigned integer
     // are the same 8 bytes, so the maxima are copied straight into doubles
     ALS_CUDA(cudaMemcpyAsync(wave_speed, scratch, bytes, cudaMemcpyDeviceToHost, s));

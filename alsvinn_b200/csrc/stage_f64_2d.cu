@@ -3,8 +3,8 @@
 
 namespace als {
 cudaError_t launch_stage_f64_2d(int recon, int flux, int kind, const StageParams& P,
-    int members, cudaStream_t s) {
-    return launch_stage_dim<double, 2>(recon, flux, kind, P, members, s);
+    int blocks_per_sm, cudaStream_t s) {
+    return launch_stage_dim<double, 2>(recon, flux, kind, P, blocks_per_sm, s);
 }
 
 void stage_tile_f64_2d(int* tile) {

@@ -172,8 +172,8 @@ __device__ __forceinline__ R warp_max(R v) {
 }
 
 template<class R, int DIM, int RECON, int FLUX, int KIND, int D>
-__device__ __forceinline__ void stage_direction(const StageParams& P, const R* box, R* rec, R* flx,
-    R (&acc)[StageLayout<R, DIM, RECON>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
+__device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, const R* box, R* rec,
+    R* flx, R (&acc)[StageLayout<R, DIM, RECON>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
     typedef StageLayout<R, DIM, RECON> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
@@ -187,7 +187,6 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
     constexpr int FC = F0 * F1 * (Lay::TZ + (D == 2 ? 1 : 0));
     constexpr int S = D == 0 ? 1 : (D == 1 ? Lay::BX : Lay::BX * Lay::BY);
     const int tid = threadIdx.x;
-    const R gamma = R(P.gamma);
 
     for (int i = tid; i < RC; i += Lay::THREADS) {
         const int ex = i % E0;
@@ -207,7 +206,7 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
     }
     __syncthreads();
 
-    const int hiD = D == 0 ? P.grid.hi[0] : (D == 1 ? P.grid.hi[1] : P.grid.hi[2]);
+    const int hiD = D == 0 ? gd.hi[0] : (D == 1 ? gd.hi[1] : gd.hi[2]);
     const int oD = D == 0 ? x0 : (D == 1 ? y0 : z0);
     for (int i = tid; i < FC; i += Lay::THREADS) {
         const int fx = i % F0;
@@ -232,13 +231,13 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
             const int f = D == 0 ? fx : (D == 1 ? fy : fz);
             bool valid = oD + f - 1 <= hiD - 1;
             if (D != 0) {
-                valid = valid && (x0 + fx < P.grid.hi[0]);
+                valid = valid && (x0 + fx < gd.hi[0]);
             }
             if (D != 1 && DIM > 1) {
-                valid = valid && (y0 + fy < P.grid.hi[1]);
+                valid = valid && (y0 + fy < gd.hi[1]);
             }
             if (D != 2 && DIM > 2) {
-                valid = valid && (z0 + fz < P.grid.hi[2]);
+                valid = valid && (z0 + fz < gd.hi[2]);
             }
             if (valid && wmax < w) {
                 wmax = w;
@@ -270,16 +269,36 @@ __device__ __forceinline__ void stage_direction(const StageParams& P, const R* b
     __syncthreads();
 }
 
+// Advances the time bookkeeping of a member once its last tile of the last
+// stage is done (Simulator.cpp:211-213 and checkConstraints).
+__device__ __forceinline__ void finish_step(StepState* st) {
+    volatile StepState* vs = st;
+    const double t = vs->t + vs->dt;
+    vs->t = t;
+    vs->steps = vs->steps + 1;
+    vs->ws[0] = 0;
+    vs->ws[1] = 0;
+    vs->ws[2] = 0;
+    vs->arrive = 0;
+    if (vs->status != 0 && vs->bad_step < 0) {
+        vs->bad_step = vs->steps;
+    }
+    if (t >= vs->end_time || vs->status != 0 || vs->steps >= vs->max_steps) {
+        vs->done = 1;
+    }
+}
+
+// One work item: tile `tile` of member `member` of level L.
 template<class R, int DIM, int RECON, int FLUX, int KIND>
-__device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int member,
-    unsigned char* smem) {
+__device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc& L, int tile,
+    int member, unsigned char* smem) {
     typedef StageLayout<R, DIM, RECON> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
     constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
     const int tid = threadIdx.x;
-    const GridDesc& gd = P.grid;
-    StepState* st = P.state ? P.state + member : nullptr;
+    const GridDesc& gd = L.grid;
+    StepState* st = L.state ? L.state + member : nullptr;
 
     R* box = reinterpret_cast<R*>(smem);
     R* rec = box + NV * Lay::BOX;
@@ -291,11 +310,17 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
     const int x0 = gd.lo[0] + tx * Lay::TX;
     const int y0 = gd.lo[1] + ty * Lay::TY;
     const int z0 = gd.lo[2] + tz * Lay::TZ;
-    const long long base = (long long)member * P.sample_stride;
-    const R* in = static_cast<const R*>(P.in) + base;
-    const R* un = static_cast<const R*>(P.un) + base;
-    R* out = static_cast<R*>(P.out) + base;
-    const long long plane = gd.plane;
+    const long long base = (long long)member * L.member_stride;
+    const R* in[NV];
+    const R* un[NV];
+    R* out[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        in[v] = static_cast<const R*>(L.in[v]) + base;
+        un[v] = static_cast<const R*>(L.un[v]) + base;
+        out[v] = static_cast<R*>(L.out[v]) + base;
+    }
+    const R gamma = R(P.gamma);
 
     R c = R(0);
     if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
@@ -325,12 +350,22 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
         const int pz = DIM > 2 ? z0 + bz : 0;
         R val = R(0);
         if (px < gd.N[0] && py < gd.N[1] && pz < gd.N[2]) {
-            const long long idx = v * plane + ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
+            const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
+            // v is warp-uniform except at variable boundaries; select the plane
+            const R* src = in[0];
+            const R* usrc = un[0];
+#pragma unroll
+            for (int k = 1; k < NV; ++k) {
+                if (v == k) {
+                    src = in[k];
+                    usrc = un[k];
+                }
+            }
             if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
-                val = in[idx] * c;
-                val = val + un[idx];
+                val = src[idx] * c;
+                val = val + usrc[idx];
             } else {
-                val = in[idx];
+                val = src[idx];
             }
         }
         box[i] = val;
@@ -346,12 +381,12 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
         }
     }
     R wmax[3] = {R(0), R(0), R(0)};
-    stage_direction<R, DIM, RECON, FLUX, KIND, 0>(P, box, rec, flx, acc, wmax[0], x0, y0, z0);
+    stage_direction<R, DIM, RECON, FLUX, KIND, 0>(gd, gamma, box, rec, flx, acc, wmax[0], x0, y0, z0);
     if (DIM > 1) {
-        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 1 ? 1 : 0)>(P, box, rec, flx, acc, wmax[1], x0, y0, z0);
+        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 1 ? 1 : 0)>(gd, gamma, box, rec, flx, acc, wmax[1], x0, y0, z0);
     }
     if (DIM > 2) {
-        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 2 ? 2 : 0)>(P, box, rec, flx, acc, wmax[2], x0, y0, z0);
+        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 2 ? 2 : 0)>(gd, gamma, box, rec, flx, acc, wmax[2], x0, y0, z0);
     }
 
     bool bad = false;
@@ -382,28 +417,28 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
                 // RungeKutta2.cpp:57-63
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
-                x = x + un[v * plane + idx];
+                x = x + un[v][idx];
                 x = x * R(0.5);
             } else if (KIND == KIND_RK3_1) {
                 // RungeKutta3.cpp:65-78
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
                 x = x * R(1. / 3.);
-                x = x + un[v * plane + idx];
+                x = x + un[v][idx];
                 x = x * R(3. / 4.);
             } else if (KIND == KIND_RK3_2) {
                 // RungeKutta3.cpp:65-83
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
                 x = x * R(2);
-                x = x + un[v * plane + idx];
+                x = x + un[v][idx];
                 x = x * R(1. / 3.);
             }
             val[v] = x;
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            out[v * plane + idx] = val[v];
+            out[v][idx] = val[v];
         }
         if (P.write_ghosts) {
             int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
@@ -420,14 +455,14 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
                             const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
 #pragma unroll
                             for (int v = 0; v < NV; ++v) {
-                                out[v * plane + j] = val[v];
+                                out[v][j] = val[v];
                             }
                         }
                     }
                 }
             }
         }
-        if (LAST && st && !obeys_constraints<R, NV>(val, R(P.gamma))) {
+        if (LAST && st && !obeys_constraints<R, NV>(val, gamma)) {
             bad = true;
             bad_idx = idx;
         }
@@ -448,7 +483,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
             for (int k = 0; k < Lay::THREADS / 32; ++k) {
                 m = fmax(m, wsh[tid][k]);
             }
-            unsigned long long* dst = st ? &st->ws[tid] : (P.ws_out + 3 * member + tid);
+            unsigned long long* dst = st ? &st->ws[tid] : (L.ws_out + 3 * member + tid);
             atomicMax(dst, (unsigned long long)__double_as_longlong(m));
         }
     }
@@ -462,41 +497,74 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, int tile, int m
         if (tid == 0) {
             __threadfence();
             const unsigned int prev = atomicAdd(&st->arrive, 1u);
-            const unsigned int total = gd.tiles[0] * gd.tiles[1] * gd.tiles[2];
-            if (prev == total - 1) {
-                // every tile of this member is done: advance time (Simulator.cpp:211-213)
+            if (prev == unsigned(L.tiles_per_member) - 1) {
                 __threadfence();
-                volatile StepState* vs = st;
-                const double t = vs->t + vs->dt;
-                vs->t = t;
-                vs->steps = vs->steps + 1;
-                vs->ws[0] = 0;
-                vs->ws[1] = 0;
-                vs->ws[2] = 0;
-                vs->arrive = 0;
-                if (vs->status != 0 && vs->bad_step < 0) {
-                    vs->bad_step = vs->steps;
-                }
-                if (t >= vs->end_time || vs->status != 0 || vs->steps >= vs->max_steps) {
-                    vs->done = 1;
-                }
+                finish_step(st);
             }
         }
     }
 }
 
+// Work item w of the launch: its level, member and tile, skipping members
+// that are done.
 template<class R, int DIM, int RECON, int FLUX, int KIND>
-__global__ void __launch_bounds__((StageLayout<R, DIM, RECON>::THREADS), (StageLayout<R, DIM, RECON>::BLOCKS))
-stage_kernel(const StageParams P) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int member = P.member0 + blockIdx.y;
-    if (P.state) {
-        const volatile StepState* st = P.state + member;
+__device__ __forceinline__ void stage_item(const StageParams& P, long long w, unsigned char* smem) {
+    int l = 0;
+#pragma unroll
+    for (int k = 1; k < kMaxLevels; ++k) {
+        if (k < P.nlevels && w >= P.level[k].work_begin) {
+            l = k;
+        }
+    }
+    const LevelDesc& L = P.level[l];
+    const long long local = w - L.work_begin;
+    const int member = int(local / L.tiles_per_member);
+    const int tile = int(local - (long long)member * L.tiles_per_member);
+    if (L.state) {
+        const volatile StepState* st = L.state + member;
         if (st->done) {
             return;
         }
     }
-    stage_tile<R, DIM, RECON, FLUX, KIND>(P, blockIdx.x, member, smem);
+    stage_tile<R, DIM, RECON, FLUX, KIND>(P, L, tile, member, smem);
+}
+
+// Two launch modes.  Without a work counter every block takes the work item
+// of its index (the hardware hands out blocks as SMs free up).  With one,
+// the launch is persistent: a fixed number of resident blocks take items
+// from the counter until the list is exhausted, and the last block to
+// leave resets the counter for the next launch.
+template<class R, int DIM, int RECON, int FLUX, int KIND>
+__global__ void __launch_bounds__((StageLayout<R, DIM, RECON>::THREADS), (StageLayout<R, DIM, RECON>::BLOCKS))
+stage_kernel(const StageParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (!P.counter) {
+        stage_item<R, DIM, RECON, FLUX, KIND>(P, blockIdx.x, smem);
+        return;
+    }
+    __shared__ long long item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item = (long long)atomicAdd(&P.counter[0], 1ull);
+        }
+        __syncthreads();
+        const long long w = item;
+        if (w >= P.total_work) {
+            break;
+        }
+        stage_item<R, DIM, RECON, FLUX, KIND>(P, w, smem);
+        // the next item reuses the shared memory and `item`
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long prev = atomicAdd(&P.counter[1], 1ull);
+        if (prev == gridDim.x - 1) {
+            P.counter[0] = 0;
+            P.counter[1] = 0;
+            __threadfence();
+        }
+    }
 }
 
 } // namespace als

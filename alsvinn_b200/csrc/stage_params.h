@@ -14,6 +14,9 @@ enum Kind {
 
 enum Boundary { BC_NEUMANN = 0, BC_PERIODIC = 1 };
 
+constexpr int kMaxVars = 5;
+constexpr int kMaxLevels = 4;
+
 // Per-simulation time-stepping state kept on the device, so a whole time
 // step runs without a host round trip.  One per ensemble member.
 struct alignas(64) StepState {
@@ -26,7 +29,7 @@ struct alignas(64) StepState {
     long long max_steps;
     int done;                       // 1 once t >= T, max_steps reached or a constraint failed
     int status;                     // 0 ok, 1 constraint violation
-    unsigned int arrive;            // blocks of the last stage that finished (last-block bookkeeping)
+    unsigned int arrive;            // tiles of the last stage that finished (last-tile bookkeeping)
     unsigned int pad0;
     long long bad_index;            // first padded cell index that violated a constraint
     long long bad_step;             // step number at which it happened
@@ -43,19 +46,33 @@ struct GridDesc {
     long long plane;   // padded cells per plane
 };
 
-struct StageParams {
-    const void* in;          // stencil input: U^n (FLUX0), L (RK*_1), U2 (RK3_2)
-    const void* un;          // U^n (RK*_1 and RK3_2); may alias `out` for RK3_2
-    void* out;
-    long long sample_stride; // elements between consecutive ensemble members
+// One grid level of a launch: its geometry, its planes (one pointer per
+// conserved variable, member 0; member m is m*member_stride elements
+// further), its members and their states.
+struct LevelDesc {
     GridDesc grid;
+    const void* in[kMaxVars];   // stencil input: U^n (FLUX0), L (RK*_1), U2 (RK3_2)
+    const void* un[kMaxVars];   // U^n (RK*_1 and RK3_2); may alias `out` for RK3_2
+    void* out[kMaxVars];
+    long long member_stride;
+    StepState* state;           // member 0's state, or null for plug-in calls
+    unsigned long long* ws_out; // FLUX0 without state: 3 maxima per member
+    int members;
+    int tiles_per_member;
+    long long work_begin;       // first work item of this level in the launch
+};
+
+// A launch walks a list of work items (level, member, tile): levels one
+// after another, members one after another, tiles of a member together.
+struct StageParams {
+    LevelDesc level[kMaxLevels];
+    int nlevels;
+    long long total_work;
     int bc;                  // BC_NEUMANN / BC_PERIODIC
     int write_ghosts;        // 1: also write the boundary images of every updated cell
     double gamma;
-    double c_fixed;          // dt/dx for stages when `state` is null
-    StepState* state;        // per-member state (indexed by member), or null
-    unsigned long long* ws_out; // FLUX0 without state: per-direction max face speed (3 per member)
-    int member0;             // index of the first member this launch covers
+    double c_fixed;          // dt/dx for stages when a level has no state
+    unsigned long long* counter; // persistent mode: [next item, blocks done], zero between launches; null: one item per block
 };
 
 } // namespace als

@@ -2,10 +2,12 @@
 
 ``Simulator`` wraps the fused device solver (``als_solver_*``): it is what
 ``alsvinncli``'s time loop (Simulator::performStep, Simulator.cpp:81-85,
-191-214) and, with ``members > 1``, ``alsuqcli``'s sample loop
-(alsuq/src/run/Runner.cpp:42-78) become.  The plug-in level calls
-(``NumericalFlux``, ``Reconstruction``, ``Boundary``, ``Integrator``) take
-device tensors and mirror one virtual call of the reference each.
+191-214) and, with ``members > 1`` or several ``levels``, ``alsuqcli``'s
+sample loop (alsuq/src/run/Runner.cpp:42-78) become.  ``MeanVariance``
+wraps the FP64 ensemble statistics (alsuq/src/stats/MeanVariance.cpp).  The
+plug-in level calls (``NumericalFlux``, ``Reconstruction``, ``Boundary``,
+``Integrator``) take device tensors of shape (nvar, ...) and mirror one
+virtual call of the reference each.
 """
 import ctypes
 
@@ -22,6 +24,7 @@ PRECISION = {"fp64": 0, "fp32": 1}
 EQUATION = {"euler1": 1, "euler2": 2, "euler3": 3}
 
 _D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
 
 
 def _choice(table, value, what):
@@ -40,46 +43,64 @@ def ghost_cells(flux, reconstruction):
 
 
 class Simulator:
-    """Advances one simulation, or an ensemble of ``members`` simulations of
-    the same grid, by whole time steps on the GPU."""
+    """Advances one simulation, an ensemble of ``members`` simulations of the
+    same grid, or several grid ``levels`` (list of dicts with ``n``,
+    ``members`` and optionally ``lower``/``upper``) by whole time steps on
+    the GPU.  Members are numbered level after level."""
 
-    def __init__(self, dimension, n, lower, upper, flux="hll3", reconstruction="weno2",
-                 integrator="rungekutta3", boundary="periodic", gamma=1.4, cfl=0.4,
-                 end_time=1.0, max_steps=0, precision="fp64", members=1, device=0):
+    def __init__(self, dimension, n=None, lower=None, upper=None, flux="hll3",
+                 reconstruction="weno2", integrator="rungekutta3", boundary="periodic", gamma=1.4,
+                 cfl=0.4, end_time=1.0, max_steps=0, precision="fp64", members=1, device=0,
+                 levels=None):
         lib = _lib.load()
         self._lib = lib
-        cfg = _lib.SolverConfig()
-        cfg.dimension = dimension
-        nn = list(n) + [1] * (3 - len(n))
-        lo = list(lower) + [0.0] * (3 - len(lower))
-        hi = list(upper) + [0.0] * (3 - len(upper))
-        for d in range(3):
-            cfg.n[d] = int(nn[d])
-            cfg.lower[d] = float(lo[d])
-            cfg.upper[d] = float(hi[d])
-        cfg.flux = _choice(FLUX, flux, "flux")
-        cfg.reconstruction = _choice(RECONSTRUCTION, reconstruction, "reconstruction")
-        cfg.integrator = _choice(INTEGRATOR, integrator, "integrator")
-        cfg.boundary = _choice(BOUNDARY, boundary, "boundary")
-        cfg.gamma = gamma
-        cfg.cfl = cfl
-        cfg.end_time = end_time
-        cfg.max_steps = int(max_steps)
-        cfg.precision = _choice(PRECISION, precision, "precision")
-        cfg.members = int(members)
-        self.config = cfg
+        if levels is None:
+            levels = [{"n": n, "members": members, "lower": lower, "upper": upper}]
+        cfgs = (_lib.SolverConfig * len(levels))()
+        for k, lev in enumerate(levels):
+            cfg = cfgs[k]
+            cfg.dimension = dimension
+            nn = list(lev["n"]) + [1] * (3 - len(lev["n"]))
+            lo = list(lev.get("lower") or [0.0] * dimension) + [0.0] * 3
+            hi = list(lev.get("upper") or [1.0] * dimension) + [0.0] * 3
+            for d in range(3):
+                cfg.n[d] = int(nn[d])
+                cfg.lower[d] = float(lo[d])
+                cfg.upper[d] = float(hi[d])
+            cfg.flux = _choice(FLUX, flux, "flux")
+            cfg.reconstruction = _choice(RECONSTRUCTION, reconstruction, "reconstruction")
+            cfg.integrator = _choice(INTEGRATOR, integrator, "integrator")
+            cfg.boundary = _choice(BOUNDARY, boundary, "boundary")
+            cfg.gamma = gamma
+            cfg.cfl = cfl
+            cfg.end_time = end_time
+            cfg.max_steps = int(max_steps)
+            cfg.precision = _choice(PRECISION, precision, "precision")
+            cfg.members = int(lev.get("members", 1))
+        self.config = cfgs[0]
         self.dimension = dimension
-        self.n = tuple(int(v) for v in nn[:dimension])
-        self.members = int(members)
+        self.precision = precision
         handle = ctypes.c_void_p()
-        _lib.check(lib.als_solver_create(ctypes.byref(cfg), device, ctypes.byref(handle)))
+        _lib.check(lib.als_solver_create_levels(cfgs, len(levels), device, ctypes.byref(handle)))
         self._h = handle
-        plane = ctypes.c_longlong()
         g = ctypes.c_int()
-        _lib.check(lib.als_solver_geometry(self._h, ctypes.byref(plane), ctypes.byref(g)))
-        self.plane = plane.value
+        _lib.check(lib.als_solver_geometry(self._h, None, ctypes.byref(g)))
         self.ghosts = g.value
-        self.shape = padded_shape(dimension, self.n, self.ghosts)
+        self.levels = []
+        for k, lev in enumerate(levels):
+            first = ctypes.c_int()
+            count = ctypes.c_int()
+            plane = ctypes.c_longlong()
+            _lib.check(lib.als_solver_level(self._h, k, ctypes.byref(first), ctypes.byref(count),
+                                            ctypes.byref(plane)))
+            nn = tuple(int(v) for v in lev["n"][:dimension])
+            self.levels.append({"first": first.value, "members": count.value,
+                                "plane": plane.value, "n": nn,
+                                "shape": padded_shape(dimension, nn, self.ghosts)})
+        self.members = sum(lev["members"] for lev in self.levels)
+        self.n = self.levels[0]["n"]
+        self.plane = self.levels[0]["plane"]
+        self.shape = self.levels[0]["shape"]
 
     def close(self):
         if getattr(self, "_h", None):
@@ -98,13 +119,20 @@ class Simulator:
     def __exit__(self, *exc):
         self.close()
 
+    def _level_of(self, member):
+        for k, lev in enumerate(self.levels):
+            if lev["first"] <= member < lev["first"] + lev["members"]:
+                return k
+        raise ValueError("member %d out of range" % member)
+
     def set_state(self, states, first_member=0):
-        """Uploads FP64 host states of shape (members, nvar, Nz, Ny, Nx) or (nvar, Nz, Ny, Nx)."""
+        """Uploads FP64 host states, shape (count, nvar, Nz, Ny, Nx) or (nvar, Nz, Ny, Nx)."""
+        shape = self.levels[self._level_of(first_member)]["shape"]
         a = np.ascontiguousarray(states, dtype=np.float64)
-        if a.shape == self.shape:
+        if a.shape == shape:
             a = a[None]
-        if a.shape[1:] != self.shape:
-            raise ValueError("state shape %s does not match %s" % (a.shape, self.shape))
+        if a.shape[1:] != shape:
+            raise ValueError("state shape %s does not match %s" % (a.shape, shape))
         _lib.check(self._lib.als_solver_set_state(self._h, a.ctypes.data_as(_D), first_member,
                                                   a.shape[0]))
 
@@ -114,8 +142,10 @@ class Simulator:
                                                          first_member, count))
 
     def get_state(self, first_member=0, count=None):
-        count = self.members - first_member if count is None else count
-        out = np.zeros((count,) + self.shape)
+        lev = self.levels[self._level_of(first_member)]
+        if count is None:
+            count = lev["first"] + lev["members"] - first_member
+        out = np.zeros((count,) + lev["shape"])
         _lib.check(self._lib.als_solver_get_state(self._h, out.ctypes.data_as(_D), first_member,
                                                   count))
         return out
@@ -149,10 +179,100 @@ class Simulator:
         return _lib.check(self._lib.als_solver_launches_per_step(self._h))
 
     def profile_step(self):
-        """Runs one step with events around each kernel; returns their durations in ms."""
+        """Runs one step with events between the stages; returns their durations in ms."""
         buf = (ctypes.c_float * 8)()
         k = _lib.check(self._lib.als_solver_profile_step(self._h, buf, 8))
         return [buf[i] for i in range(k)]
+
+    def set_schedule(self, blocks_per_sm=0, level_order=None):
+        order = None
+        if level_order is not None:
+            order = (ctypes.c_int * len(self.levels))(*level_order)
+        _lib.check(self._lib.als_solver_set_schedule(self._h, int(blocks_per_sm), order))
+
+    def schedule(self):
+        bps = ctypes.c_int()
+        order = (ctypes.c_int * len(self.levels))()
+        _lib.check(self._lib.als_solver_get_schedule(self._h, ctypes.byref(bps), order))
+        return {"blocks_per_sm": bps.value, "level_order": list(order)}
+
+    def tune(self, steps=3):
+        """Runs the schedule autotuner (state and clocks are restored)."""
+        bps = ctypes.c_int()
+        order = (ctypes.c_int * len(self.levels))()
+        ms = ctypes.c_double()
+        _lib.check(self._lib.als_solver_tune(self._h, int(steps), ctypes.byref(bps), order,
+                                             ctypes.byref(ms)))
+        return {"blocks_per_sm": bps.value, "level_order": list(order), "ms_per_step": ms.value}
+
+    def region_sums(self, first_member=0, count=None, lo=None, hi=None):
+        """FP64 sums of each conserved variable over the interior box [lo, hi)
+        (interior cell coordinates, default the whole interior): (count, nvar)."""
+        lev = self.levels[self._level_of(first_member)]
+        if count is None:
+            count = lev["first"] + lev["members"] - first_member
+        nvar = self.dimension + 2
+        out = np.zeros((count, nvar))
+        clo = (ctypes.c_int * 3)(*(list(lo) + [0, 0, 0])[:3]) if lo is not None else None
+        chi = (ctypes.c_int * 3)(*(list(hi) + [1, 1, 1])[:3]) if hi is not None else None
+        _lib.check(self._lib.als_solver_region_sums(self._h, first_member, count, clo, chi,
+                                                    out.ctypes.data_as(_D)))
+        return out
+
+
+class MeanVariance:
+    """alsuq::stats::MeanVariance (MeanVariance.cpp:30-67) in FP64 Welford
+    form: add ensemble states (any precision) and read mean and the biased
+    variance as device tensors."""
+
+    def __init__(self, count, device=0):
+        self._lib = _lib.load()
+        self.count = int(count)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.als_stats_create(self.count, device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.als_stats_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_solver(self, simulator, level=0):
+        _lib.check(self._lib.als_stats_add_solver(self._h, simulator._h, level))
+
+    def add(self, states, precision="fp64", stream=0):
+        """Adds a (members, ...) device tensor of states."""
+        members = states.shape[0]
+        stride = states[0].numel()
+        _lib.check(self._lib.als_stats_add(self._h, ctypes.c_void_p(states.data_ptr()),
+                                           _choice(PRECISION, precision, "precision"), members,
+                                           stride, ctypes.c_void_p(stream) if stream else None))
+
+    def merge(self, n, mean, m2, stream=0):
+        _lib.check(self._lib.als_stats_merge(self._h, int(n), ctypes.c_void_p(mean.data_ptr()),
+                                             ctypes.c_void_p(m2.data_ptr()),
+                                             ctypes.c_void_p(stream) if stream else None))
+
+    def moments(self):
+        """(n, mean device pointer, M2 device pointer)."""
+        n = ctypes.c_longlong()
+        mean = ctypes.c_void_p()
+        m2 = ctypes.c_void_p()
+        _lib.check(self._lib.als_stats_moments(self._h, ctypes.byref(n), ctypes.byref(mean),
+                                               ctypes.byref(m2)))
+        return n.value, mean.value, m2.value
+
+    def result(self, mean, variance, stream=0):
+        """Writes mean and variance into FP64 device tensors of `count` elements."""
+        _lib.check(self._lib.als_stats_result(self._h, ctypes.c_void_p(mean.data_ptr()),
+                                              ctypes.c_void_p(variance.data_ptr()),
+                                              ctypes.c_void_p(stream) if stream else None))
 
 
 def _grid(dimension, n, ghosts, gamma):
@@ -189,15 +309,16 @@ class NumericalFlux:
         return self.ghosts
 
     def computeFlux(self, conserved, out, start=(0, 0, 0), end=(0, 0, 0), stream=0):
-        """Net flux of the region into ``out`` (device FP64 tensors); returns the wave speeds."""
+        """Net flux of the region into ``out`` ((nvar, ...) FP64 device tensors);
+        returns the per-direction wave speeds."""
         lib = _lib.load()
         g = _grid(self.dimension, self.n, self.ghosts, self.gamma)
         ws = np.zeros(3)
         s = (ctypes.c_int * 3)(*start)
         e = (ctypes.c_int * 3)(*end)
         _lib.check(lib.als_compute_flux(ctypes.byref(g), self.flux, self.reconstruction,
-                                        _ptr(conserved), _ptr(out), s, e, ws.ctypes.data_as(_D),
-                                        _stream(stream)))
+                                        _lib.plane_pointers(conserved), _lib.plane_pointers(out),
+                                        s, e, ws.ctypes.data_as(_D), _stream(stream)))
         return ws
 
 
@@ -218,7 +339,8 @@ class Reconstruction:
         lib = _lib.load()
         g = _grid(self.dimension, self.n, self.ghosts, self.gamma)
         _lib.check(lib.als_reconstruct(ctypes.byref(g), self.reconstruction, direction,
-                                       _ptr(conserved), _ptr(left), _ptr(right), _stream(stream)))
+                                       _lib.plane_pointers(conserved), _lib.plane_pointers(left),
+                                       _lib.plane_pointers(right), _stream(stream)))
 
 
 class Boundary:
@@ -230,12 +352,11 @@ class Boundary:
         self.ghosts = ghosts
         self.boundary = _choice(BOUNDARY, boundary, "boundary")
 
-    def applyBoundaryConditions(self, planes, nvar=None, members=1, stream=0):
+    def applyBoundaryConditions(self, planes, stream=0):
         lib = _lib.load()
-        nvar = self.dimension + 2 if nvar is None else nvar
         g = _grid(self.dimension, self.n, self.ghosts, 1.4)
-        _lib.check(lib.als_fill_ghosts(ctypes.byref(g), self.boundary, _ptr(planes), nvar, members,
-                                       _stream(stream)))
+        _lib.check(lib.als_fill_ghosts(ctypes.byref(g), self.boundary, _lib.plane_pointers(planes),
+                                       planes.shape[0], _stream(stream)))
 
 
 class Integrator:

@@ -216,6 +216,8 @@ def main():
     sim = als.Simulator(DIM, (N, N), (0, 0), (1, 1), flux=FLUX, reconstruction=RECON,
                         integrator=INTEG, boundary=BC, cfl=CFL, end_time=1e9, device=local)
     sim.set_state(state)
+    # the schedule autotuner (state and clocks are restored afterwards)
+    schedule = sim.tune(steps=3)
     if args.kernels_only:
         for _ in range(args.warmup + args.steps):
             sim.advance(1)
@@ -313,6 +315,7 @@ def main():
                 "definition": "als_solver_set_state(pinned host) + %d steps + als_solver_get_state"
                               "(pinned host), wall clock" % e2e_steps},
         "gpu_launches": args.steps * sim.launches_per_step(),
+        "schedule": schedule,
         "clocks": clock_info,
     }
     if rank == 0 and not args.no_cpu_baseline:

@@ -69,11 +69,15 @@ typedef struct {
     double gamma;
 } als_grid;
 
+/* Planes are passed as arrays of `nvar` device pointers, one per conserved
+ * variable, like the reference Volume's one Memory per variable
+ * (alsfvm/src/volume/Volume.cpp:44-60); the planes need not be adjacent. */
+
 /* Boundary::applyBoundaryConditions(Volume&, const Grid&)
  * (alsfvm/include/alsfvm/boundary/Boundary.hpp:30-31; BoundaryCPU.cpp:30-106).
- * Fills the ghost cells of `nvar` planes of `members` consecutive states.
- * Requires n >= ghosts in every active direction. */
-int als_fill_ghosts(const als_grid* grid, int boundary, double* planes, int nvar, int members,
+ * Fills the ghost cells of `nvar` planes.  Requires n >= ghosts in every
+ * active direction. */
+int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, int nvar,
     void* stream);
 
 /* NumericalFlux::computeFlux(const Volume&, rvec3& waveSpeed, bool, Volume& out,
@@ -84,16 +88,16 @@ int als_fill_ghosts(const als_grid* grid, int boundary, double* planes, int nvar
  * bounds, end <= 0); other cells are left untouched.  `wave_speed` (host,
  * 3 doubles) receives the maximal face wave speed per direction; the call
  * synchronises `stream` to read it back, like the reference's CUDA path. */
-int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* in,
-    double* out, const int* start, const int* end, double* wave_speed, void* stream);
+int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* const* in,
+    double* const* out, const int* start, const int* end, double* wave_speed, void* stream);
 
 /* Allocation-free variant of als_compute_flux; it has no counterpart in the
  * reference.  For callers that cannot let a library allocate device memory:
  * a runtime that owns and pre-plans all device memory (another framework's
  * pool, a fixed-budget deployment) or one that forbids allocation while it
  * drives the flux evaluation many times per time step.  It evaluates the
- * net flux of `members` (1..1024) consecutive states (each nvar padded
- * planes, the whole interior, no region arguments) into `out`, and writes
+ * net flux of `members` (1..1024) consecutive states (each nvar adjacent
+ * padded planes, the whole interior, no region arguments) into `out`, and writes
  * their maximal face wave speeds to `wave_speed` (host, 3 per state).  The
  * wave-speed accumulators live in a fixed 24 KiB device array inside the
  * library that every GPU loading it keeps until the process exits; no
@@ -110,8 +114,8 @@ int als_compute_flux_static(const als_grid* grid, int flux, int reconstruction, 
  * size_t indicatorVariable=0, Volume& left, Volume& right)
  * (alsfvm/include/alsfvm/reconstruction/Reconstruction.hpp:46-58;
  * ReconstructionCPU.cpp:37-97, ENOCPU.cpp:41-187).  The indicator is rho. */
-int als_reconstruct(const als_grid* grid, int reconstruction, int direction, const double* in,
-    double* left, double* right, void* stream);
+int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
+    const double* const* in, double* const* left, double* const* right, void* stream);
 
 /* Stage combination of Integrator::performSubstep
  * (alsfvm/include/alsfvm/integrator/Integrator.hpp:59-80; ForwardEuler.cpp:32-51,
@@ -164,11 +168,22 @@ typedef struct {
 typedef struct als_solver als_solver;
 
 int als_solver_create(const als_solver_config* cfg, int device, als_solver** out);
+/* A solver over 1..4 grid levels (e.g. the levels of a multilevel Monte
+ * Carlo batch) advanced together: every stage is one persistent launch over
+ * the tiles of every member of every level.  Levels may differ only in n,
+ * lower, upper and members; members are numbered level after level. */
+int als_solver_create_levels(const als_solver_config* levels, int nlevels, int device,
+    als_solver** out);
+/* First member index, member count and padded plane size of a level. */
+int als_solver_level(const als_solver* s, int level, int* first_member, int* members,
+    long long* plane);
 int als_solver_destroy(als_solver* s);
-/* padded cells per plane and the ghost width the solver uses */
+/* padded cells per plane (level 0) and the ghost width the solver uses */
 int als_solver_geometry(const als_solver* s, long long* plane, int* ghosts);
 /* Uploads member states (host, FP64, padded planes; ghost cells are filled
- * by the solver), resets time and step counters of those members. */
+ * by the solver), resets time and step counters of those members.  The
+ * members of one call must belong to one level.  Set every member before
+ * advancing (RK2 keeps one ping-pong parity for all members). */
 int als_solver_set_state(als_solver* s, const double* host, int first_member, int count);
 /* Same from device memory already in the solver's precision. */
 int als_solver_set_state_device(als_solver* s, const void* dev, int first_member, int count);
@@ -193,6 +208,51 @@ int als_solver_launches_per_step(const als_solver* s);
  * kernel_ms[k] receives the duration of kernel k.  Synchronises; returns the
  * number of kernels. */
 int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity);
+/* Schedule of the stage launches: blocks_per_sm = 0 launches one block per
+ * work item (level, member, tile); k > 0 makes every stage one persistent
+ * launch of k resident blocks per SM (capped by what fits) that take work
+ * items from a counter.  level_order is the order of the levels in the
+ * work list (a permutation, NULL = as created). */
+int als_solver_set_schedule(als_solver* s, int blocks_per_sm, const int* level_order);
+int als_solver_get_schedule(const als_solver* s, int* blocks_per_sm, int* level_order);
+/* Autotuner: times `steps` steps under every candidate schedule (blocks per
+ * SM in {0 (one per item), 1, 2, 3, 4} x level order in {as created, finest
+ * first, coarsest first}) from the same saved state, keeps the fastest and
+ * restores the state and member clocks, so results are unchanged.  Returns
+ * the choice and its ms per step. */
+int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_order,
+    double* best_ms_per_step);
+/* FP64 sums of every conserved variable over the interior box [lo, hi)
+ * (interior cell coordinates; NULL = whole interior) of members
+ * [first_member, first_member+count) of one level: out[k*nvar + v].  The
+ * conservation check of FP32 members and the observables use it. */
+int als_solver_region_sums(als_solver* s, int first_member, int count, const int* lo,
+    const int* hi, double* out);
+
+/* ------------------------------------------------ ensemble statistics
+ * FP64 mean and variance of an ensemble, accumulated with Welford/Chan
+ * updates (mean and M2 per element, merged chunk by chunk), whatever the
+ * members' precision.  Replaces alsuq::stats::MeanVariance
+ * (alsuq/src/stats/MeanVariance.cpp:30-67, raw sums S1, S2 and
+ * var = S2/M - (S1/M)^2) and StatisticsHelper::combineStatistics
+ * (alsuq/src/stats/StatisticsHelper.cpp:35-79).  The variance is the biased
+ * one (divided by M), like the reference. */
+typedef struct als_stats als_stats;
+int als_stats_create(long long count, int device, als_stats** out);
+int als_stats_destroy(als_stats* st);
+/* Adds `members` states (each `count` elements, `member_stride` apart) in
+ * ALS_FP64 or ALS_FP32 from device memory. */
+int als_stats_add(als_stats* st, const void* states, int precision, int members,
+    long long member_stride, void* stream);
+/* Adds the current state of every member of a solver level. */
+int als_stats_add_solver(als_stats* st, als_solver* s, int level);
+/* Chan merge of another accumulator's (n, mean, M2) (device arrays), e.g.
+ * from another GPU. */
+int als_stats_merge(als_stats* st, long long n, const double* mean, const double* m2, void* stream);
+/* n and device pointers of the running mean and M2. */
+int als_stats_moments(als_stats* st, long long* n, double** mean, double** m2);
+/* Writes mean and variance (device arrays of `count` doubles; either may be NULL). */
+int als_stats_result(als_stats* st, double* mean, double* variance, void* stream);
 
 /* ------------------------------------------------------- UQ sampling
  * Parameter draws of samples [first_sample, first_sample+count) for a

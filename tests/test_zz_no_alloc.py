@@ -44,8 +44,9 @@ def _states(seed, members, dim, n, g):
     x = torch.from_numpy(np.stack([smooth_random_state(seed + k, dim, n, g)
                                    for k in range(members)])).cuda()
     grid = _grid(dim, n, g)
-    assert lib.als_fill_ghosts(ctypes.byref(grid), 1, ctypes.c_void_p(x.data_ptr()), dim + 2,
-                               members, None) == 0
+    for m in range(members):
+        assert lib.als_fill_ghosts(ctypes.byref(grid), 1, _lib.plane_pointers(x[m]), dim + 2,
+                                   None) == 0
     torch.cuda.synchronize()
     return x
 
@@ -59,7 +60,7 @@ def _allocating(x, dim, n, g, flux, recon):
     for m in range(x.shape[0]):
         w = np.zeros(3)
         rc = lib.als_compute_flux(ctypes.byref(grid), FLUX[flux], RECON[recon],
-                                  ctypes.c_void_p(x[m].data_ptr()), ctypes.c_void_p(out[m].data_ptr()),
+                                  _lib.plane_pointers(x[m]), _lib.plane_pointers(out[m]),
                                   None, None, w.ctypes.data_as(_D), None)
         assert rc == 0, lib.als_last_error()
         ws[m] = w
