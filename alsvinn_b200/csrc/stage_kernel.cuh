@@ -311,15 +311,11 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     const int y0 = gd.lo[1] + ty * Lay::TY;
     const int z0 = gd.lo[2] + tz * Lay::TZ;
     const long long base = (long long)member * L.member_stride;
-    const R* in[NV];
-    const R* un[NV];
-    R* out[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        in[v] = static_cast<const R*>(L.in[v]) + base;
-        un[v] = static_cast<const R*>(L.un[v]) + base;
-        out[v] = static_cast<R*>(L.out[v]) + base;
-    }
+    // plane pointers are read from the launch parameters where they are
+    // used; arrays of them would be held (and spilled) across the kernel
+    auto inp = [&](int v) { return static_cast<const R*>(L.in[v]) + base; };
+    auto unp = [&](int v) { return static_cast<const R*>(L.un[v]) + base; };
+    auto outp = [&](int v) { return static_cast<R*>(L.out[v]) + base; };
     const R gamma = R(P.gamma);
 
     R c = R(0);
@@ -351,21 +347,11 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         R val = R(0);
         if (px < gd.N[0] && py < gd.N[1] && pz < gd.N[2]) {
             const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
-            // v is warp-uniform except at variable boundaries; select the plane
-            const R* src = in[0];
-            const R* usrc = un[0];
-#pragma unroll
-            for (int k = 1; k < NV; ++k) {
-                if (v == k) {
-                    src = in[k];
-                    usrc = un[k];
-                }
-            }
             if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
-                val = src[idx] * c;
-                val = val + usrc[idx];
+                val = inp(v)[idx] * c;
+                val = val + unp(v)[idx];
             } else {
-                val = src[idx];
+                val = inp(v)[idx];
             }
         }
         box[i] = val;
@@ -417,28 +403,28 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
                 // RungeKutta2.cpp:57-63
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
-                x = x + un[v][idx];
+                x = x + unp(v)[idx];
                 x = x * R(0.5);
             } else if (KIND == KIND_RK3_1) {
                 // RungeKutta3.cpp:65-78
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
                 x = x * R(1. / 3.);
-                x = x + un[v][idx];
+                x = x + unp(v)[idx];
                 x = x * R(3. / 4.);
             } else if (KIND == KIND_RK3_2) {
                 // RungeKutta3.cpp:65-83
                 x = x * c;
                 x = x + box[v * Lay::BOX + bidx];
                 x = x * R(2);
-                x = x + un[v][idx];
+                x = x + unp(v)[idx];
                 x = x * R(1. / 3.);
             }
             val[v] = x;
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            out[v][idx] = val[v];
+            outp(v)[idx] = val[v];
         }
         if (P.write_ghosts) {
             int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
@@ -455,7 +441,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
                             const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
 #pragma unroll
                             for (int v = 0; v < NV; ++v) {
-                                out[v][j] = val[v];
+                                outp(v)[j] = val[v];
                             }
                         }
                     }
@@ -538,25 +524,26 @@ template<class R, int DIM, int RECON, int FLUX, int KIND>
 __global__ void __launch_bounds__((StageLayout<R, DIM, RECON>::THREADS), (StageLayout<R, DIM, RECON>::BLOCKS))
 stage_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (!P.counter) {
-        stage_item<R, DIM, RECON, FLUX, KIND>(P, blockIdx.x, smem);
-        return;
-    }
     __shared__ long long item;
-    for (;;) {
+    if (threadIdx.x == 0) {
+        item = P.counter ? (long long)atomicAdd(&P.counter[0], 1ull) : (long long)blockIdx.x;
+    }
+    __syncthreads();
+    // one call site, so the tile code is inlined once
+    for (long long w = item; w < P.total_work;) {
+        stage_item<R, DIM, RECON, FLUX, KIND>(P, w, smem);
+        if (!P.counter) {
+            break;
+        }
+        // the next item reuses the shared memory and `item`
+        __syncthreads();
         if (threadIdx.x == 0) {
             item = (long long)atomicAdd(&P.counter[0], 1ull);
         }
         __syncthreads();
-        const long long w = item;
-        if (w >= P.total_work) {
-            break;
-        }
-        stage_item<R, DIM, RECON, FLUX, KIND>(P, w, smem);
-        // the next item reuses the shared memory and `item`
-        __syncthreads();
+        w = item;
     }
-    if (threadIdx.x == 0) {
+    if (P.counter && threadIdx.x == 0) {
         __threadfence();
         const unsigned long long prev = atomicAdd(&P.counter[1], 1ull);
         if (prev == gridDim.x - 1) {
