@@ -181,6 +181,93 @@ def run_reference_arm(args, rank):
     print(json.dumps(out))
 
 
+# Ensemble workloads: (dimension, [(n, members), ...]).  "ensemble": 512 KH
+# samples at 256^2; "multilevel": four KH levels (2048x128^2, 512x256^2,
+# 128x512^2, 32x1024^2) in one launch per stage; "kh3d": 8 3-D KH samples
+# at 128^3 (FP64 spot check).
+BATCHES = {
+    "ensemble": (2, [(256, 512)]),
+    "multilevel": (2, [(128, 2048), (256, 512), (512, 128), (1024, 32)]),
+    "kh3d": (3, [(128, 8)]),
+}
+
+
+def run_batch(args, rank, world, local):
+    """Times `steps` time steps of every member of every level (one launch
+    per stage over all of them); value = member cell-updates / s."""
+    import torch
+    import alsvinn_b200 as als
+    torch.cuda.set_device(local)
+    dim, levels = BATCHES[args.workload]
+    precision = "fp64" if args.workload == "kh3d" else args.precision
+    nvar = dim + 2
+    elem = 8 if precision == "fp64" else 4
+    lv = [{"n": (n,) * dim, "members": m} for n, m in levels]
+    sim = als.Simulator(dim, levels=lv, flux=FLUX, reconstruction=RECON, integrator=INTEG,
+                        boundary=BC, cfl=CFL, end_time=1e9, precision=precision, device=local)
+    first = 0
+    for lev in sim.levels:
+        n = lev["n"][0]
+        for a in range(0, lev["members"], 64):
+            k = min(64, lev["members"] - a)
+            params = als.uniform_draws(40, rank * sim.members + first + a, k)
+            states = np.stack([als.kelvin_helmholtz(n, params[j], GHOSTS, dimension=dim)
+                               for j in range(k)])
+            sim.set_state(states, first_member=lev["first"] + a)
+        first += lev["members"]
+    schedule = sim.tune(steps=2)
+    sim.advance(args.warmup)
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    sim.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    bad = [m for m in range(sim.members) if sim.info(m)["status"] != 0]
+    if bad:
+        raise RuntimeError("constraint violation in members %r" % bad[:8])
+    cells = sum((lev["n"][0] ** dim) * lev["members"] for lev in sim.levels)
+    value = cells * args.steps / (ms * 1e-3)
+    kms = np.array([sim.profile_step() for _ in range(3)]).mean(axis=0)
+    hbm_peak, peak_kind = peaks()
+    per_cell = {"flux0": 2 * nvar * elem, "rk3_1": 3 * nvar * elem, "rk3_2": 3 * nvar * elem}
+    roof = [{"kernel": k, "ms": float(t), "achieved_gbs": per_cell[k] * cells / (t * 1e-3) / 1e9}
+            for k, t in zip(KERNEL_NAMES, kms)]
+    dom = max(range(3), key=lambda i: roof[i]["ms"])
+    # FP64 statistics of the final states (every level) and the FP64 conservation sums
+    t0 = time.perf_counter()
+    for k, lev in enumerate(sim.levels):
+        mv = als.MeanVariance(nvar * lev["plane"], device=local)
+        mv.add_solver(sim, k)
+        mv.close()
+    stats_s = time.perf_counter() - t0
+    result = {
+        "metric": "member cell-updates/s (%s, KH, WENO2+HLL3, RK3, %s)" % (args.workload, precision),
+        "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32",
+        "data": "synthetic (Kelvin-Helmholtz samples from the reference's generator)",
+        "config": {"workload": args.workload, "levels": levels, "dimension": dim,
+                   "precision": precision, "member_cells": cells,
+                   "l2": "inputs larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": roof[dom]["achieved_gbs"], "peak": hbm_peak,
+                     "unit": "GB/s", "frac": roof[dom]["achieved_gbs"] / hbm_peak,
+                     "traffic": None, "kernel": roof[dom]["kernel"], "peak_source": peak_kind,
+                     "per_kernel": roof},
+        "schedule": schedule, "statistics_seconds": stats_s,
+        "gpu_launches": args.steps * sim.launches_per_step(), "clocks": clock_info,
+    }
+    print(json.dumps(result))
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -190,6 +277,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only run warmup+steps time steps (for profiler captures)")
+    ap.add_argument("--workload", default="kh1024", choices=sorted(["kh1024"] + list(BATCHES)),
+                    help="kh1024 (default, the plain FP64 drop-in), or an ensemble workload")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="member precision of the ensemble workloads")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -200,6 +291,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload != "kh1024":
+        run_batch(args, rank, world, local)
         return
 
     import torch
@@ -216,8 +310,6 @@ def main():
     sim = als.Simulator(DIM, (N, N), (0, 0), (1, 1), flux=FLUX, reconstruction=RECON,
                         integrator=INTEG, boundary=BC, cfl=CFL, end_time=1e9, device=local)
     sim.set_state(state)
-    # the schedule autotuner (state and clocks are restored afterwards)
-    schedule = sim.tune(steps=3)
     if args.kernels_only:
         for _ in range(args.warmup + args.steps):
             sim.advance(1)
@@ -226,6 +318,8 @@ def main():
             raise RuntimeError("constraint violation")
         sim.close()
         return
+    # the schedule autotuner (state and clocks are restored afterwards)
+    schedule = sim.tune(steps=3)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
