@@ -7,10 +7,12 @@ from . import _lib
 from .initial_data import (kelvin_helmholtz, kh_ensemble, padded_shape, sod, uniform_draws)
 from .simulator import (Boundary, Integrator, MeanVariance, NumericalFlux, Reconstruction,
                         Simulator, ghost_cells)
+from .surrogate import Surrogate
+from . import uq
 
 __all__ = [
     "Boundary", "Integrator", "MeanVariance", "NumericalFlux", "Reconstruction", "Simulator",
-    "ghost_cells",
+    "Surrogate", "ghost_cells", "uq",
     "kelvin_helmholtz", "kh_ensemble", "padded_shape", "sod", "uniform_draws",
 ]
 

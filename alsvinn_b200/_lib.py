@@ -39,6 +39,11 @@ class SolverConfig(ctypes.Structure):
     ]
 
 
+class MlpConfig(ctypes.Structure):
+    _fields_ = [("inputs", ctypes.c_int), ("width", ctypes.c_int), ("hidden", ctypes.c_int),
+                ("max_batch", ctypes.c_int)]
+
+
 class MemberInfo(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_longlong),
                 ("done", ctypes.c_int), ("status", ctypes.c_int),
@@ -93,6 +98,19 @@ PROTOTYPES = {
     "als_solver_profile_step": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "als_uniform_draws": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
                                          ctypes.c_double, ctypes.c_double, _D]),
+    # include/als_surrogate.h
+    "als_mlp_create": (ctypes.c_int, [ctypes.POINTER(MlpConfig), ctypes.c_int, _PP]),
+    "als_mlp_destroy": (ctypes.c_int, [_VP]),
+    "als_mlp_param_count": (ctypes.c_int, [_VP, _LL]),
+    "als_mlp_init": (ctypes.c_int, [_VP, ctypes.c_ulonglong]),
+    "als_mlp_set_params": (ctypes.c_int, [_VP, _VP]),
+    "als_mlp_get_params": (ctypes.c_int, [_VP, _VP]),
+    "als_mlp_forward": (ctypes.c_int, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
+    "als_mlp_gradients": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _VP,
+                                         ctypes.POINTER(ctypes.c_float), _VP]),
+    "als_mlp_train": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                     _VP, _VP]),
+    "als_mlp_sample_uniform": (ctypes.c_int, [_VP, ctypes.c_longlong, ctypes.c_ulonglong, _VP]),
 }
 
 _lib = None

@@ -40,7 +40,7 @@ def sources():
     for name in sorted(os.listdir(CSRC)):
         if not name.endswith(".cu"):
             continue
-        flags = FAST32 if "_f32_" in name else EXACT
+        flags = FAST32 if ("_f32_" in name or name.startswith("mlp")) else EXACT
         units.append((os.path.join(CSRC, name), flags))
     return units
 

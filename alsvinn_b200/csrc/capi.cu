@@ -185,6 +185,14 @@ struct DeviceGuard {
 
 } // namespace
 
+namespace als {
+// Error text for the other translation units of the library (one message
+// per host thread, read by als_last_error).
+int report_error(int code, const char* msg) {
+    return fail(code, msg);
+}
+} // namespace als
+
 extern "C" {
 
 const char* als_last_error(void) {

@@ -1,0 +1,571 @@
+// C ABI of the MLP surrogate (include/als_surrogate.h): parameter layout,
+// workspaces, the training step as one captured CUDA graph, inference in
+// row chunks.  The kernels are in mlp_kernels.cuh / mlp_tc.cuh.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "als_surrogate.h"
+#include "mlp_kernels.cuh"
+
+namespace als {
+int report_error(int code, const char* msg);
+}
+
+using namespace mlpk;
+
+namespace {
+
+constexpr long long kInferChunk = 32768;   // rows per inference chunk (multiple of 128)
+
+int mlp_fail(int code, const std::string& msg) {
+    return als::report_error(code, msg.c_str());
+}
+
+#define MLP_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t err_ = (call);                                                      \
+        if (err_ != cudaSuccess) {                                                      \
+            std::ostringstream os_;                                                     \
+            os_ << #call << ": " << cudaGetErrorString(err_);                           \
+            return mlp_fail(ALS_E_CUDA, os_.str());                                     \
+        }                                                                               \
+    } while (0)
+
+struct Layer {
+    int in, out, kpad;      // kpad: K of the BF16 copy (multiple of 64)
+    long long w_off, b_off; // offsets in the flat vector
+    __nv_bfloat16* wb;      // BF16 weights (out x kpad), null for the head
+};
+
+int round_up(int v, int m) {
+    return (v + m - 1) / m * m;
+}
+
+} // namespace
+
+struct als_mlp {
+    als_mlp_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    std::vector<Layer> layers;      // hidden layers then the head
+    long long nparams = 0;
+    float* p = nullptr;             // master parameters
+    float* g = nullptr;             // gradients
+    float* m = nullptr;             // Adam moments
+    float* v = nullptr;
+    long long* step = nullptr;      // Adam step counter (device)
+    int* error = nullptr;           // set by a GEMM whose wait gave up
+    // training workspace (max_batch rows)
+    __nv_bfloat16* xb = nullptr;    // packed inputs (rows x kpad0)
+    std::vector<float*> z;          // pre-activations per hidden layer
+    std::vector<__nv_bfloat16*> h;  // activations per hidden layer
+    __nv_bfloat16* dz[2] = {nullptr, nullptr};
+    float* y = nullptr;
+    float* dy = nullptr;
+    float* loss1 = nullptr;         // loss of a gradient evaluation
+    // inference workspace (kInferChunk rows)
+    __nv_bfloat16* xi = nullptr;
+    __nv_bfloat16* hi[2] = {nullptr, nullptr};
+    std::vector<void*> allocations;
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(als_mlp* s, T** p, size_t count) {
+    MLP_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+    MLP_CUDA(cudaMemset(*p, 0, count * sizeof(T)));
+    s->allocations.push_back(*p);
+    return ALS_OK;
+}
+
+#define MLP_TRY(expr)             \
+    do {                          \
+        int rc_ = (expr);         \
+        if (rc_ != ALS_OK) {      \
+            return rc_;           \
+        }                         \
+    } while (0)
+
+int grid_for(long long work, int threads) {
+    long long b = (work + threads - 1) / threads;
+    return int(b < 1 ? 1 : (b > 148LL * 16 ? 148LL * 16 : b));
+}
+
+template <int BN, int EPI>
+int launch_gemm(const GemmArgs& a, int n_valid, cudaStream_t s) {
+    if (a.M % kTileM || a.N % BN || a.K % kChunkK || a.K <= 0) {
+        return mlp_fail(ALS_E_INVALID, "GEMM shape is not a multiple of the tile");
+    }
+    constexpr int smem = gemm_smem_bytes<BN>();   // limit set by configure_kernels()
+    dim3 grid(a.M / kTileM, a.N / BN);
+    gemm_kernel<BN, EPI><<<grid, kThreads, smem, s>>>(a, n_valid);
+    MLP_CUDA(cudaGetLastError());
+    return ALS_OK;
+}
+
+Operand rows_of(const __nv_bfloat16* p, long long ld) {
+    return Operand{p, ld, 1};
+}
+
+Operand columns_of(const __nv_bfloat16* p, long long ld) {
+    return Operand{p, 1, ld};
+}
+
+// Forward pass of `rows_pad` rows (multiple of 128) from packed inputs `x`
+// through the hidden layers into `hout` (the last activation), storing
+// pre-activations when `zs` is given (training), ping-ponging `hbuf`
+// otherwise (inference).
+int forward_hidden(als_mlp* s, const __nv_bfloat16* x, long long rows_pad,
+                   const std::vector<float*>* zs, const std::vector<__nv_bfloat16*>* hs,
+                   __nv_bfloat16* const* hbuf, const __nv_bfloat16** hout, cudaStream_t st) {
+    const int nh = s->cfg.hidden;
+    const __nv_bfloat16* in = x;
+    long long ld_in = s->layers[0].kpad;
+    for (int l = 0; l < nh; ++l) {
+        const Layer& L = s->layers[l];
+        GemmArgs a = {};
+        a.a = rows_of(in, ld_in);
+        a.b = rows_of(L.wb, L.kpad);
+        a.M = int(rows_pad);
+        a.N = L.out;
+        a.K = L.kpad;
+        a.bias = s->p + L.b_off;
+        a.z = zs ? (*zs)[l] : nullptr;
+        a.h = hs ? (*hs)[l] : hbuf[l & 1];
+        a.ldz = L.out;
+        a.ldh = L.out;
+        a.error = s->error;
+        // training batches: narrow N tiles for more CTAs; inference: the
+        // whole layer width per CTA, so each activation tile is read once
+        if (zs || L.out % 128 != 0) {
+            MLP_TRY((launch_gemm<64, EPI_FORWARD>(a, L.out, st)));
+        } else if (L.out % 256 != 0) {
+            MLP_TRY((launch_gemm<128, EPI_FORWARD>(a, L.out, st)));
+        } else {
+            MLP_TRY((launch_gemm<256, EPI_FORWARD>(a, L.out, st)));
+        }
+        in = a.h;
+        ld_in = L.out;
+    }
+    *hout = in;
+    return ALS_OK;
+}
+
+int check_error_flag(als_mlp* s) {
+    int e = 0;
+    MLP_CUDA(cudaMemcpyAsync(&e, s->error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    MLP_CUDA(cudaStreamSynchronize(s->stream));
+    if (e) {
+        cudaMemsetAsync(s->error, 0, sizeof(int), s->stream);
+        return mlp_fail(ALS_E_CUDA, "tensor-core GEMM wait timed out");
+    }
+    return ALS_OK;
+}
+
+// The caller's stream waits for nothing of ours and we wait for the caller's
+// prior work: work is ordered caller -> ours via an event.
+int join_caller(als_mlp* s, void* stream) {
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    MLP_CUDA(cudaEventRecord(s->ev, cs));
+    MLP_CUDA(cudaStreamWaitEvent(s->stream, s->ev, 0));
+    return ALS_OK;
+}
+
+} // namespace
+
+namespace {
+
+// Forward + MSE backward of one batch (rows <= max_batch), gradients into
+// s->g.  `loss`/`base` select where the loss goes (see head_backward).
+int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, float* loss,
+                      long long base, cudaStream_t st) {
+    const int nh = s->cfg.hidden;
+    const int W = s->cfg.width;
+    const long long rp = round_up(rows, kTileM);
+    const Layer& L0 = s->layers[0];
+    const Layer& head = s->layers[nh];
+    pack_inputs<<<grid_for(rp * L0.kpad, 256), 256, 0, st>>>(x, rows, s->cfg.inputs, s->xb, rp,
+                                                             L0.kpad);
+    MLP_CUDA(cudaGetLastError());
+    const __nv_bfloat16* last = nullptr;
+    MLP_TRY(forward_hidden(s, s->xb, rp, &s->z, &s->h, nullptr, &last, st));
+    head_forward<<<grid_for(rows * 32LL, 256), 256, 0, st>>>(last, W, s->p + head.w_off,
+                                                              s->p + head.b_off, rows, s->y);
+    MLP_CUDA(cudaGetLastError());
+    // rows beyond `rows` in the padded batch must not contribute: their
+    // dZ rows are zeroed once here (the GEMMs read full 128-row tiles)
+    if (rp > rows) {
+        for (int k = 0; k < 2; ++k) {
+            MLP_CUDA(cudaMemsetAsync(s->dz[k] + (long long)rows * W, 0,
+                                     sizeof(__nv_bfloat16) * (rp - rows) * W, st));
+        }
+    }
+    head_backward<<<(rows + 7) / 8, 256, 0, st>>>(s->y, t, rows, s->p + head.w_off, s->z[nh - 1], W,
+                                                  s->dy, s->dz[(nh - 1) & 1], s->step, loss, base);
+    MLP_CUDA(cudaGetLastError());
+    // head gradients: dw = sum_r dy_r h_r, db = sum_r dy_r
+    column_sums<__nv_bfloat16><<<(W + 31) / 32, 256, 0, st>>>(last, rows, W, W, s->dy,
+                                                              s->g + head.w_off);
+    column_sums<float><<<1, 256, 0, st>>>(s->dy, rows, 1, 1, nullptr, s->g + head.b_off);
+    MLP_CUDA(cudaGetLastError());
+    for (int l = nh - 1; l >= 0; --l) {
+        const Layer& L = s->layers[l];
+        const __nv_bfloat16* dzl = s->dz[l & 1];
+        const __nv_bfloat16* hin = l > 0 ? s->h[l - 1] : s->xb;
+        const long long ld_in = l > 0 ? s->layers[l - 1].out : L0.kpad;
+        // dW = dZ^T H_in : M = out, N = kpad(in), K = rows (padded rows are zero in dZ)
+        GemmArgs a = {};
+        a.a = columns_of(dzl, L.out);
+        a.b = columns_of(hin, ld_in);
+        a.M = L.out;
+        a.N = L.kpad;
+        a.K = int(rp);
+        a.g = s->g + L.w_off;
+        a.ldg = L.in;
+        a.error = s->error;
+        MLP_TRY((launch_gemm<64, EPI_WGRAD>(a, L.in, st)));
+        column_sums<__nv_bfloat16><<<(L.out + 31) / 32, 256, 0, st>>>(dzl, rows, L.out, L.out,
+                                                                       nullptr, s->g + L.b_off);
+        MLP_CUDA(cudaGetLastError());
+        if (l > 0) {
+            // dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}) : M = rows, N = in, K = out
+            GemmArgs b = {};
+            b.a = rows_of(dzl, L.out);
+            b.b = columns_of(L.wb, L.kpad);
+            b.M = int(rp);
+            b.N = L.in;
+            b.K = L.out;
+            b.zin = s->z[l - 1];
+            b.h = s->dz[(l - 1) & 1];
+            b.ldz = L.in;
+            b.ldh = L.in;
+            b.error = s->error;
+            MLP_TRY((launch_gemm<64, EPI_BACKWARD>(b, L.in, st)));
+        }
+    }
+    return ALS_OK;
+}
+
+int refresh_bf16(als_mlp* s, cudaStream_t st) {
+    for (int l = 0; l < s->cfg.hidden; ++l) {
+        const Layer& L = s->layers[l];
+        Segment sg = {L.w_off, L.out, L.in, L.kpad, L.wb};
+        cast_weights<<<grid_for((long long)L.out * L.kpad, 256), 256, 0, st>>>(s->p, sg);
+        MLP_CUDA(cudaGetLastError());
+    }
+    return ALS_OK;
+}
+
+template <int BN, int EPI>
+int configure_one() {
+    MLP_CUDA(cudaFuncSetAttribute(gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  gemm_smem_bytes<BN>()));
+    return ALS_OK;
+}
+
+// Dynamic shared memory limits of every GEMM instantiation, set on the
+// current device before any launch (and before any graph capture).
+int configure_kernels() {
+    MLP_TRY((configure_one<64, EPI_FORWARD>()));
+    MLP_TRY((configure_one<128, EPI_FORWARD>()));
+    MLP_TRY((configure_one<256, EPI_FORWARD>()));
+    MLP_TRY((configure_one<64, EPI_BACKWARD>()));
+    MLP_TRY((configure_one<64, EPI_WGRAD>()));
+    return ALS_OK;
+}
+
+int reset_adam(als_mlp* s, cudaStream_t st) {
+    MLP_CUDA(cudaMemsetAsync(s->m, 0, sizeof(float) * s->nparams, st));
+    MLP_CUDA(cudaMemsetAsync(s->v, 0, sizeof(float) * s->nparams, st));
+    MLP_CUDA(cudaMemsetAsync(s->step, 0, sizeof(long long), st));
+    return ALS_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int als_mlp_create(const als_mlp_config* cfg, int device, als_mlp** out) {
+    if (!cfg || !out) {
+        return mlp_fail(ALS_E_INVALID, "null argument");
+    }
+    *out = nullptr;
+    const als_mlp_config c = *cfg;
+    if (c.inputs < 1 || c.inputs > 64 || !(c.width == 64 || c.width == 128 || c.width == 256) ||
+        c.hidden < 1 || c.hidden > 6 || c.max_batch < kTileM || c.max_batch % kTileM) {
+        return mlp_fail(ALS_E_INVALID, "invalid MLP configuration (inputs 1..64, width 64/128/256, "
+                                       "hidden 1..6, max_batch a positive multiple of 128)");
+    }
+    MLP_CUDA(cudaSetDevice(device));
+    als_mlp* s = new als_mlp();
+    s->cfg = c;
+    s->device = device;
+    auto cleanup = [&](int rc) {
+        als_mlp_destroy(s);
+        return rc;
+    };
+    long long off = 0;
+    for (int l = 0; l <= c.hidden; ++l) {
+        Layer L = {};
+        L.in = l == 0 ? c.inputs : c.width;
+        L.out = l == c.hidden ? 1 : c.width;
+        L.kpad = round_up(L.in, kChunkK);
+        L.w_off = off;
+        off += (long long)L.in * L.out;
+        L.b_off = off;
+        off += L.out;
+        s->layers.push_back(L);
+    }
+    s->nparams = off;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming) != cudaSuccess) {
+        return cleanup(mlp_fail(ALS_E_CUDA, "stream/event creation failed"));
+    }
+    int rc = ALS_OK;
+    const size_t B = size_t(c.max_batch);
+    const size_t Wd = size_t(c.width);
+    rc = rc ? rc : dev_alloc(s, &s->p, s->nparams);
+    rc = rc ? rc : dev_alloc(s, &s->g, s->nparams);
+    rc = rc ? rc : dev_alloc(s, &s->m, s->nparams);
+    rc = rc ? rc : dev_alloc(s, &s->v, s->nparams);
+    rc = rc ? rc : dev_alloc(s, &s->step, 1);
+    rc = rc ? rc : dev_alloc(s, &s->error, 1);
+    rc = rc ? rc : dev_alloc(s, &s->loss1, 1);
+    for (int l = 0; l < c.hidden && !rc; ++l) {
+        rc = dev_alloc(s, &s->layers[l].wb, size_t(s->layers[l].out) * s->layers[l].kpad);
+    }
+    rc = rc ? rc : dev_alloc(s, &s->xb, B * s->layers[0].kpad);
+    s->z.assign(c.hidden, nullptr);
+    s->h.assign(c.hidden, nullptr);
+    for (int l = 0; l < c.hidden && !rc; ++l) {
+        rc = dev_alloc(s, &s->z[l], B * Wd);
+        rc = rc ? rc : dev_alloc(s, &s->h[l], B * Wd);
+    }
+    rc = rc ? rc : dev_alloc(s, &s->dz[0], B * Wd);
+    rc = rc ? rc : dev_alloc(s, &s->dz[1], B * Wd);
+    rc = rc ? rc : dev_alloc(s, &s->y, B);
+    rc = rc ? rc : dev_alloc(s, &s->dy, B);
+    rc = rc ? rc : dev_alloc(s, &s->xi, size_t(kInferChunk) * s->layers[0].kpad);
+    rc = rc ? rc : dev_alloc(s, &s->hi[0], size_t(kInferChunk) * Wd);
+    rc = rc ? rc : dev_alloc(s, &s->hi[1], size_t(kInferChunk) * Wd);
+    if (rc) {
+        return cleanup(rc);
+    }
+    rc = configure_kernels();
+    if (rc) {
+        return cleanup(rc);
+    }
+    *out = s;
+    return als_mlp_init(s, 0);
+}
+
+int als_mlp_destroy(als_mlp* s) {
+    if (!s) {
+        return ALS_OK;
+    }
+    cudaSetDevice(s->device);
+    if (s->stream) {
+        cudaStreamSynchronize(s->stream);
+    }
+    for (void* p : s->allocations) {
+        cudaFree(p);
+    }
+    if (s->ev) {
+        cudaEventDestroy(s->ev);
+    }
+    if (s->stream) {
+        cudaStreamDestroy(s->stream);
+    }
+    delete s;
+    return ALS_OK;
+}
+
+int als_mlp_param_count(const als_mlp* s, long long* count) {
+    if (!s || !count) {
+        return mlp_fail(ALS_E_INVALID, "null argument");
+    }
+    *count = s->nparams;
+    return ALS_OK;
+}
+
+int als_mlp_init(als_mlp* s, unsigned long long seed) {
+    if (!s) {
+        return mlp_fail(ALS_E_INVALID, "null handle");
+    }
+    std::vector<float> host(size_t(s->nparams));
+    std::mt19937_64 engine(seed);
+    for (const Layer& L : s->layers) {
+        const float bound = 1.0f / std::sqrt(float(L.in));
+        std::uniform_real_distribution<float> u(-bound, bound);
+        for (long long i = 0; i < (long long)L.in * L.out; ++i) {
+            host[size_t(L.w_off + i)] = u(engine);
+        }
+        for (int i = 0; i < L.out; ++i) {
+            host[size_t(L.b_off + i)] = u(engine);
+        }
+    }
+    return als_mlp_set_params(s, host.data());
+}
+
+int als_mlp_set_params(als_mlp* s, const float* params) {
+    if (!s || !params) {
+        return mlp_fail(ALS_E_INVALID, "null argument");
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_CUDA(cudaMemcpyAsync(s->p, params, sizeof(float) * s->nparams, cudaMemcpyHostToDevice,
+                             s->stream));
+    MLP_TRY(refresh_bf16(s, s->stream));
+    MLP_TRY(reset_adam(s, s->stream));
+    MLP_CUDA(cudaStreamSynchronize(s->stream));
+    return ALS_OK;
+}
+
+int als_mlp_get_params(const als_mlp* s, float* params) {
+    if (!s || !params) {
+        return mlp_fail(ALS_E_INVALID, "null argument");
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_CUDA(cudaMemcpyAsync(params, s->p, sizeof(float) * s->nparams, cudaMemcpyDeviceToHost,
+                             s->stream));
+    MLP_CUDA(cudaStreamSynchronize(s->stream));
+    return ALS_OK;
+}
+
+int als_mlp_forward(als_mlp* s, const float* x_dev, long long rows, float* y_dev, void* stream) {
+    if (!s || rows < 0 || (rows > 0 && (!x_dev || !y_dev))) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument");
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_TRY(join_caller(s, stream));
+    const cudaStream_t st = s->stream;
+    const Layer& L0 = s->layers[0];
+    const Layer& head = s->layers[s->cfg.hidden];
+    for (long long r0 = 0; r0 < rows; r0 += kInferChunk) {
+        const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
+        const long long rp = (n + kTileM - 1) / kTileM * kTileM;
+        pack_inputs<<<grid_for(rp * L0.kpad, 256), 256, 0, st>>>(
+            x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, s->xi, rp, L0.kpad);
+        MLP_CUDA(cudaGetLastError());
+        const __nv_bfloat16* last = nullptr;
+        MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st));
+        head_forward<<<grid_for(n * 32, 256), 256, 0, st>>>(last, s->cfg.width, s->p + head.w_off,
+                                                            s->p + head.b_off, n, y_dev + r0);
+        MLP_CUDA(cudaGetLastError());
+    }
+    return check_error_flag(s);
+}
+
+int als_mlp_gradients(als_mlp* s, const float* x_dev, const float* t_dev, int rows,
+                      float* grad_dev, float* loss, void* stream) {
+    if (!s || !x_dev || !t_dev || !grad_dev || rows < 1 || rows > s->cfg.max_batch) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument (1 <= rows <= max_batch)");
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_TRY(join_caller(s, stream));
+    const cudaStream_t st = s->stream;
+    // the loss slot is loss1[step - base - 1] with base = step - 1
+    long long stepv = 0;
+    MLP_CUDA(cudaMemcpyAsync(&stepv, s->step, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    MLP_CUDA(cudaStreamSynchronize(st));
+    MLP_CUDA(cudaMemsetAsync(s->loss1, 0, sizeof(float), st));
+    MLP_TRY(enqueue_gradients(s, x_dev, t_dev, rows, s->loss1, stepv - 1, st));
+    MLP_CUDA(cudaMemcpyAsync(grad_dev, s->g, sizeof(float) * s->nparams, cudaMemcpyDeviceToDevice,
+                             st));
+    float l = 0.0f;
+    MLP_CUDA(cudaMemcpyAsync(&l, s->loss1, sizeof(float), cudaMemcpyDeviceToHost, st));
+    MLP_TRY(check_error_flag(s));
+    if (loss) {
+        *loss = l;
+    }
+    return ALS_OK;
+}
+
+int als_mlp_train(als_mlp* s, const float* x_dev, const float* t_dev, int rows, int steps,
+                  float lr, float* loss_dev, void* stream) {
+    if (!s || !x_dev || !t_dev || rows < 1 || rows > s->cfg.max_batch || steps < 0 ||
+        !(lr > 0.0f)) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument (1 <= rows <= max_batch, lr > 0)");
+    }
+    if (steps == 0) {
+        return ALS_OK;
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_TRY(join_caller(s, stream));
+    const cudaStream_t st = s->stream;
+    long long base = 0;
+    MLP_CUDA(cudaMemcpyAsync(&base, s->step, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    MLP_CUDA(cudaStreamSynchronize(st));
+
+    AdamArgs a = {};
+    a.p = s->p;
+    a.g = s->g;
+    a.m = s->m;
+    a.v = s->v;
+    a.n = s->nparams;
+    a.lr = lr;
+    a.beta1 = 0.9f;
+    a.beta2 = 0.999f;
+    a.eps = 1e-8f;
+    a.step = s->step;
+    a.nseg = 0;
+    for (int l = 0; l < s->cfg.hidden; ++l) {
+        const Layer& L = s->layers[l];
+        a.seg[a.nseg++] = Segment{L.w_off, L.out, L.in, L.kpad, L.wb};
+    }
+
+    // one training step, captured once and replayed
+    cudaGraph_t graph = nullptr;
+    MLP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    begin_step<<<1, 1, 0, st>>>(s->step, loss_dev, base);
+    int rc = enqueue_gradients(s, x_dev, t_dev, rows, loss_dev, base, st);
+    if (rc == ALS_OK) {
+        adam_update<<<grid_for(s->nparams, 256), 256, 0, st>>>(a);
+    }
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc != ALS_OK || ce != cudaSuccess) {
+        if (graph) {
+            cudaGraphDestroy(graph);
+        }
+        return rc != ALS_OK ? rc : mlp_fail(ALS_E_CUDA, "graph capture of the training step failed");
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return mlp_fail(ALS_E_CUDA, "graph instantiation of the training step failed");
+    }
+    cudaError_t le = cudaSuccess;
+    for (int k = 0; k < steps && le == cudaSuccess; ++k) {
+        le = cudaGraphLaunch(exec, st);
+    }
+    const cudaError_t se = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (le != cudaSuccess || se != cudaSuccess) {
+        return mlp_fail(ALS_E_CUDA, std::string("training step: ") +
+                                        cudaGetErrorString(le != cudaSuccess ? le : se));
+    }
+    return check_error_flag(s);
+}
+
+int als_mlp_sample_uniform(float* x_dev, long long count, unsigned long long seed, void* stream) {
+    if (count < 0 || (count > 0 && !x_dev)) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument");
+    }
+    if (count == 0) {
+        return ALS_OK;
+    }
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    sample_uniform<<<grid_for(count, 256), 256, 0, st>>>(x_dev, count, seed);
+    MLP_CUDA(cudaGetLastError());
+    MLP_CUDA(cudaStreamSynchronize(st));
+    return ALS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,340 @@
+// Kernels of the MLP surrogate: the tcgen05 GEMM with its fused epilogues
+// and the small CUDA-core kernels around it (input packing, the 256 -> 1
+// output head, its loss and backward, column sums for bias gradients, Adam).
+#pragma once
+
+#include "mlp_tc.cuh"
+
+namespace mlpk {
+
+template <int BN>
+constexpr int gemm_smem_bytes() {
+    return 2 * (kTileM * kChunkK * 2 + BN * kChunkK * 2) + 1024;
+}
+
+template <int BN, int EPI>
+__device__ __forceinline__ void epilogue16(const GemmArgs& g, long long m, int n, const float* v,
+                                           int n_valid) {
+    if (EPI == EPI_FORWARD) {
+        __align__(16) __nv_bfloat16 hb[16];
+        __align__(16) float z[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            z[i] = v[i] + g.bias[n + i];
+            hb[i] = __float2bfloat16_rn(gelu(z[i]));
+        }
+        if (g.z) {
+            float4* dz = reinterpret_cast<float4*>(g.z + m * g.ldz + n);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                dz[i] = reinterpret_cast<const float4*>(z)[i];
+            }
+        }
+        uint4* dh = reinterpret_cast<uint4*>(g.h + m * g.ldh + n);
+        dh[0] = reinterpret_cast<const uint4*>(hb)[0];
+        dh[1] = reinterpret_cast<const uint4*>(hb)[1];
+    } else if (EPI == EPI_BACKWARD) {
+        __align__(16) float zin[16];
+        const float4* sz = reinterpret_cast<const float4*>(g.zin + m * g.ldz + n);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            reinterpret_cast<float4*>(zin)[i] = sz[i];
+        }
+        __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            hb[i] = __float2bfloat16_rn(v[i] * gelu_grad(zin[i]));
+        }
+        uint4* dh = reinterpret_cast<uint4*>(g.h + m * g.ldh + n);
+        dh[0] = reinterpret_cast<const uint4*>(hb)[0];
+        dh[1] = reinterpret_cast<const uint4*>(hb)[1];
+    } else {
+        float* dst = g.g + m * g.ldg + n;
+        if (n + 16 <= n_valid && (g.ldg & 3) == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                reinterpret_cast<float4*>(dst)[i] = make_float4(v[4 * i], v[4 * i + 1],
+                                                                v[4 * i + 2], v[4 * i + 3]);
+            }
+        } else {
+            for (int i = 0; i < 16; ++i) {
+                if (n + i < n_valid) {
+                    dst[i] = v[i];
+                }
+            }
+        }
+    }
+}
+
+// D[128 x BN tile] = A * B^T over K, then the epilogue.  Grid: (M/128, N/BN).
+// `n_valid` limits the stored columns of EPI_WGRAD (padded inputs).
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid) {
+    static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM columns: power of two");
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_base;
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    constexpr int kABytes = kTileM * kChunkK * 2;
+    constexpr int kBBytes = BN * kChunkK * 2;
+    unsigned char* sa[2] = {base, base + kABytes + kBBytes};
+    unsigned char* sb[2] = {base + kABytes, base + 2 * kABytes + kBBytes};
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long m0 = (long long)blockIdx.x * kTileM;
+    const long long n0 = (long long)blockIdx.y * BN;
+
+    if (warp == 0) {
+        tmem_alloc(&tmem_base, BN);
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = instr_desc_bf16(kTileM, BN);
+    const int nk = g.K / kChunkK;
+
+    int last = -1;          // last chunk whose MMAs were committed
+    bool failed = false;
+    for (int c = 0; c < nk; ++c) {
+        const int s = c & 1;
+        bool ok = true;
+        if (c >= 2) {
+            ok = mbar_wait(&bars[s], unsigned((c - 2) >> 1) & 1u);
+        }
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        stage_operand<kTileM>(sa[s], g.a, m0, c * kChunkK);
+        stage_operand<BN>(sb[s], g.b, n0, c * kChunkK);
+        fence_async_shared();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sa[s]);
+            const uint32_t b0 = smem_u32(sb[s]);
+#pragma unroll
+            for (int j = 0; j < kChunkK / 16; ++j) {
+                mma_bf16(tmem, smem_desc(a0 + j * 256, 128, 1024),
+                         smem_desc(b0 + j * 256, 128, 1024), idesc, (c > 0 || j > 0) ? 1u : 0u);
+            }
+            mma_commit(&bars[s]);
+        }
+        last = c;
+    }
+    bool done = false;
+    if (last >= 0) {
+        done = mbar_wait(&bars[last & 1], unsigned(last >> 1) & 1u);
+    }
+    if (__syncthreads_or(!done) || failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(g.error, 1);
+        }
+    } else {
+        tc_fence_after();
+        const long long m = m0 + warp * 32 + lane;
+        const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tmem_load16(lane_base + uint32_t(c0), v);
+            epilogue16<BN, EPI>(g, m, int(n0) + c0, v, n_valid);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free(tmem, BN);
+    }
+}
+
+// x (rows x nin, FP32) -> xb (rows_pad x kpad, BF16), zero padded.
+__global__ void pack_inputs(const float* __restrict__ x, long long rows, int nin,
+                            __nv_bfloat16* __restrict__ xb, long long rows_pad, int kpad) {
+    const long long total = rows_pad * kpad;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / kpad;
+        const int k = int(i - r * kpad);
+        const float v = (r < rows && k < nin) ? x[r * nin + k] : 0.0f;
+        xb[i] = __float2bfloat16_rn(v);
+    }
+}
+
+// y[r] = sum_i h[r][i] * w[i] + b (one warp per row, FP32).
+__global__ void head_forward(const __nv_bfloat16* __restrict__ h, int width,
+                             const float* __restrict__ w, const float* __restrict__ b,
+                             long long rows, float* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+         r += warps) {
+        float acc = 0.0f;
+        for (int i = lane; i < width; i += 32) {
+            acc += __bfloat162float(h[r * width + i]) * w[i];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        }
+        if (lane == 0) {
+            y[r] = acc + b[0];
+        }
+    }
+}
+
+// One training step begins: Adam step counter + 1, loss slot cleared.
+__global__ void begin_step(long long* step, float* loss, long long base) {
+    const long long t = ++step[0];
+    if (loss) {
+        loss[t - base - 1] = 0.0f;
+    }
+}
+
+// MSE head backward: dy = 2 (y - t) / B; dZ = bf16(dy * w * gelu'(Z)); loss
+// accumulated into loss[step - base - 1] (block partial sums, atomics).
+__global__ void head_backward(const float* __restrict__ y, const float* __restrict__ t, int rows,
+                              const float* __restrict__ w, const float* __restrict__ z, int width,
+                              float* __restrict__ dy, __nv_bfloat16* __restrict__ dz,
+                              const long long* step, float* loss, long long base) {
+    __shared__ float part[8];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int r = blockIdx.x * (blockDim.x >> 5) + wib;
+    float sq = 0.0f;
+    if (r < rows) {
+        const float res = y[r] - t[r];
+        const float d = 2.0f * res / float(rows);
+        sq = res * res;
+        if (lane == 0) {
+            dy[r] = d;
+        }
+        for (int i = lane; i < width; i += 32) {
+            dz[(long long)r * width + i] =
+                __float2bfloat16_rn(d * w[i] * gelu_grad(z[(long long)r * width + i]));
+        }
+    }
+    if (lane == 0) {
+        part[wib] = sq;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && loss) {
+        float s = 0.0f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            s += part[i];
+        }
+        atomicAdd(&loss[step[0] - base - 1], s / float(rows));
+    }
+}
+
+// out[n] = sum_r wt[r] * X[r][n] (wt null: weights 1), deterministic order.
+// Block: 32 columns x 8 row groups.
+template <typename T>
+__global__ void column_sums(const T* __restrict__ x, int rows, int cols, long long ld,
+                            const float* __restrict__ wt, float* __restrict__ out) {
+    __shared__ float part[8][33];
+    const int cx = threadIdx.x & 31;
+    const int gy = threadIdx.x >> 5;
+    const int n = blockIdx.x * 32 + cx;
+    float acc = 0.0f;
+    if (n < cols) {
+        for (int r = gy; r < rows; r += 8) {
+            float v;
+            if constexpr (sizeof(T) == 2) {
+                v = __bfloat162float(x[(long long)r * ld + n]);
+            } else {
+                v = x[(long long)r * ld + n];
+            }
+            acc += wt ? wt[r] * v : v;
+        }
+    }
+    part[gy][cx] = acc;
+    __syncthreads();
+    if (gy == 0 && n < cols) {
+        float s = 0.0f;
+        for (int i = 0; i < 8; ++i) {
+            s += part[i][cx];
+        }
+        out[n] = s;
+    }
+}
+
+// One weight matrix of the network in the flat parameter vector and its
+// BF16 copy for the tensor cores.
+struct Segment {
+    long long w_off;    // W (out x in) in the flat vector
+    int out, in, kpad;  // kpad: padded K of the BF16 copy
+    __nv_bfloat16* wb;  // null for the FP32 head
+};
+
+struct AdamArgs {
+    float* p;
+    const float* g;
+    float* m;
+    float* v;
+    long long n;
+    float lr, beta1, beta2, eps;
+    const long long* step;
+    Segment seg[8];
+    int nseg;
+};
+
+__global__ void adam_update(AdamArgs a) {
+    const long long t = a.step[0];
+    const float c1 = 1.0f - powf(a.beta1, float(t));
+    const float c2 = 1.0f - powf(a.beta2, float(t));
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float gi = a.g[i];
+        const float mi = a.beta1 * a.m[i] + (1.0f - a.beta1) * gi;
+        const float vi = a.beta2 * a.v[i] + (1.0f - a.beta2) * gi * gi;
+        a.m[i] = mi;
+        a.v[i] = vi;
+        const float pi = a.p[i] - a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+        a.p[i] = pi;
+        for (int s = 0; s < a.nseg; ++s) {
+            const Segment& sg = a.seg[s];
+            const long long rel = i - sg.w_off;
+            if (sg.wb && rel >= 0 && rel < (long long)sg.out * sg.in) {
+                const long long o = rel / sg.in;
+                const int k = int(rel - o * sg.in);
+                sg.wb[o * sg.kpad + k] = __float2bfloat16_rn(pi);
+            }
+        }
+    }
+}
+
+// BF16 copies of every weight matrix from the flat FP32 vector.
+__global__ void cast_weights(const float* __restrict__ p, Segment sg) {
+    const long long total = (long long)sg.out * sg.kpad;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long o = i / sg.kpad;
+        const int k = int(i - o * sg.kpad);
+        sg.wb[i] = __float2bfloat16_rn(k < sg.in ? p[sg.w_off + o * sg.in + k] : 0.0f);
+    }
+}
+
+// Counter-based U[0,1) draws (splitmix64 finaliser of (seed, index)),
+// 24-bit mantissa so every value is exact in FP32.
+__global__ void sample_uniform(float* __restrict__ x, long long count, unsigned long long seed) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        x[i] = float(z >> 40) * (1.0f / 16777216.0f);
+    }
+}
+
+} // namespace mlpk

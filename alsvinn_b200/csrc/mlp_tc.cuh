@@ -1,0 +1,198 @@
+// BF16 tensor-core GEMM tile for the MLP surrogate (sm_100a, tcgen05).
+//
+// One CTA of 128 threads computes a 128 x BN tile of D = A * B^T, where
+// A is M x K and B is N x K (both read as "K-major" rows of K elements),
+// accumulating in FP32 in tensor memory (TMEM).  Operands go from global
+// memory through registers into shared memory in the canonical no-swizzle
+// K-major UMMA layout: core matrices of 8 rows x 16 bytes (8 BF16 along K),
+// the 8 core matrices of a 64-wide K chunk of one 8-row group contiguous
+// (1024 bytes), so the descriptor's leading byte offset (next core matrix
+// along K) is 128 bytes and its stride byte offset (next 8-row group) is
+// 1024 bytes.  Strided staging lets the same kernel read transposed
+// operands (dZ^T, H^T, W^T) for the backward pass without extra copies.
+//
+// Two shared-memory stages: while the tensor core works on chunk c, the
+// threads stage chunk c+1; an mbarrier per stage, arrived on by
+// tcgen05.commit, says when a stage may be refilled.  Every wait is
+// bounded: on timeout the kernel records an error code, waits once more
+// (bounded) for its own MMAs, frees its TMEM and returns.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace mlpk {
+
+constexpr int kTileM = 128;
+constexpr int kChunkK = 64;
+constexpr int kThreads = 128;
+constexpr unsigned kWaitLimit = 1u << 22;   // try_wait polls before giving up
+
+enum Epilogue {
+    EPI_FORWARD = 0,    // z = acc + bias; Z = z (optional); H = bf16(gelu(z))
+    EPI_BACKWARD = 1,   // dZ = bf16(acc * gelu'(Zin))
+    EPI_WGRAD = 2,      // G = acc (FP32)
+};
+
+struct Operand {
+    const __nv_bfloat16* p;
+    long long rs;   // element stride between rows (M or N index)
+    long long ks;   // element stride along K
+};
+
+struct GemmArgs {
+    Operand a, b;
+    int M, N, K;                // M % 128 == 0, N % BN == 0, K % 64 == 0
+    const float* bias;          // EPI_FORWARD
+    float* z;                   // EPI_FORWARD (may be null); ld = ldz
+    __nv_bfloat16* h;           // EPI_FORWARD / EPI_BACKWARD output; ld = ldh
+    const float* zin;           // EPI_BACKWARD: pre-activations; ld = ldz
+    float* g;                   // EPI_WGRAD output; ld = ldg
+    long long ldz, ldh, ldg;
+    int* error;                 // set to 1 when a wait gave up
+};
+
+__device__ __forceinline__ float gelu(float z) {
+    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+
+__device__ __forceinline__ float gelu_grad(float z) {
+    // d/dz [z Phi(z)] = Phi(z) + z phi(z)
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (sm100 format): start address, leading
+// and stride byte offsets in 16-byte units, descriptor version 1 at bit 46,
+// base offset 0, layout type 0 = no swizzle (bits 61-63).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+        (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1),
+// A and B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) |
+        (uint32_t(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the completion of phase `parity` of `bar`.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (unsigned i = 0; i < kWaitLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) {
+            return true;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(dst)), "r"(cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols));
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 32 lanes x 32 bits, 16 consecutive columns per thread.
+__device__ __forceinline__ void tmem_load16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r[i]);
+    }
+}
+
+// Byte offset of element (r, k) of a staged rows x 64 chunk.
+__device__ __forceinline__ uint32_t staged_offset(int r, int kc) {
+    return uint32_t((r >> 3) * 1024 + kc * 128 + (r & 7) * 16);
+}
+
+// Stages rows [row0, row0+ROWS) x K [k0, k0+64) of an operand into `dst`.
+template <int ROWS>
+__device__ __forceinline__ void stage_operand(unsigned char* dst, const Operand& op, long long row0,
+                                              int k0) {
+    if (op.ks == 1) {
+        // rows of contiguous K: one 16-byte vector per (row, 8-wide K group)
+        for (int idx = threadIdx.x; idx < ROWS * 8; idx += kThreads) {
+            const int r = idx >> 3;
+            const int kc = idx & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(op.p + (row0 + r) * op.rs + k0 + kc * 8);
+            *reinterpret_cast<uint4*>(dst + staged_offset(r, kc)) = v;
+        }
+    } else {
+        // transposed operand: consecutive rows are contiguous in memory
+        for (int idx = threadIdx.x; idx < ROWS * 8; idx += kThreads) {
+            const int r = idx % ROWS;
+            const int kc = idx / ROWS;
+            const __nv_bfloat16* src = op.p + (row0 + r) * op.rs + (long long)(k0 + kc * 8) * op.ks;
+            __align__(16) __nv_bfloat16 e[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                e[j] = src[(long long)j * op.ks];
+            }
+            *reinterpret_cast<uint4*>(dst + staged_offset(r, kc)) = *reinterpret_cast<uint4*>(e);
+        }
+    }
+}
+
+} // namespace mlpk

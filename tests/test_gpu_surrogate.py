@@ -1,0 +1,152 @@
+"""The BF16 tensor-core MLP surrogate on the GPU, against the CPU oracle.
+
+Forward outputs and MSE gradients of the tcgen05 kernels are compared with
+oracle/mlp_oracle.py, which rounds to BF16 at the same points; what is left
+is FP32 accumulation order and the odd BF16 rounding flip, hence relative
+tolerances of 1e-2 (stated per test).  Training, Adam and inference in
+chunks are checked for their own invariants, and the control variate built
+from a trained network is shown to cut the variance of the Monte Carlo
+estimator on solver-generated Kelvin-Helmholtz samples.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+import alsvinn_b200 as als
+from conftest import ROOT
+
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import mlp_oracle as mo  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _blocks(flat, inputs, width, hidden):
+    out = []
+    off = 0
+    for o, i in mo.layer_shapes(inputs, width, hidden):
+        out.append(("W%d" % len(out), flat[off:off + o * i]))
+        off += o * i
+        out.append(("b%d" % (len(out) // 2), flat[off:off + o]))
+        off += o
+    return out
+
+
+@pytest.mark.parametrize("inputs,width,hidden,rows", [(40, 256, 4, 300), (7, 64, 2, 128),
+                                                      (40, 128, 3, 1000)])
+def test_forward_matches_oracle(inputs, width, hidden, rows):
+    rng = np.random.default_rng(rows + width)
+    x = rng.uniform(0, 1, (rows, inputs)).astype(np.float32)
+    with als.Surrogate(inputs, width, hidden, max_batch=1024, seed=11) as s:
+        y = s.forward_raw(x).cpu().numpy().astype(np.float64)
+        p = s.params()
+    ref, _ = mo.forward(p, x, inputs, width, hidden, bf16_path=True)
+    scale = np.abs(ref).max() + 1e-3
+    # FP32 accumulation vs FP64, occasional BF16 rounding flips: 1e-2 of the output scale
+    assert np.abs(y - ref).max() <= 1e-2 * scale, np.abs(y - ref).max()
+    # and a close match on average
+    assert np.abs(y - ref).mean() <= 1e-3 * scale
+
+
+@pytest.mark.parametrize("rows", [256, 200])
+def test_gradients_match_oracle(rows):
+    inputs, width, hidden = 40, 256, 4
+    rng = np.random.default_rng(rows)
+    x = rng.uniform(0, 1, (rows, inputs)).astype(np.float32)
+    t = rng.normal(0, 1, rows).astype(np.float32)
+    with als.Surrogate(inputs, width, hidden, max_batch=1024, seed=5) as s:
+        g, loss = s.gradients(x, t)
+        g = g.cpu().numpy().astype(np.float64)
+        p = s.params()
+    ref, ref_loss = mo.gradients(p, x, t, inputs, width, hidden, bf16_path=True)
+    assert loss == pytest.approx(ref_loss, rel=1e-3)
+    for (name, a), (_, b) in zip(_blocks(g, inputs, width, hidden),
+                                 _blocks(ref, inputs, width, hidden)):
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        # relative error of each parameter block's gradient: 1e-2
+        assert rel < 1e-2, (name, rel)
+    cos = np.dot(g, ref) / (np.linalg.norm(g) * np.linalg.norm(ref))
+    assert cos > 0.9999
+
+
+def test_first_adam_step_moves_every_parameter_by_lr():
+    inputs, width, hidden, rows = 40, 256, 4, 512
+    rng = np.random.default_rng(9)
+    x = rng.uniform(0, 1, (rows, inputs)).astype(np.float32)
+    t = rng.normal(0, 1, rows).astype(np.float32)
+    lr = 1e-3
+    with als.Surrogate(inputs, width, hidden, max_batch=1024, seed=2) as s:
+        p0 = s.params()
+        g, _ = s.gradients(x, t)
+        g = g.cpu().numpy()
+        s.train_raw(x, t, 1, lr)
+        p1 = s.params()
+    # first Adam step: m_hat = g, v_hat = g^2 -> p - lr * g / (|g| + eps)
+    expected = p0.astype(np.float64) - lr * g / (np.abs(g) + 1e-8)
+    assert np.abs(p1 - expected).max() <= 1e-6
+
+
+def test_training_reduces_the_loss():
+    inputs, width, hidden, rows = 40, 256, 4, 1024
+    rng = np.random.default_rng(4)
+    x = rng.uniform(0, 1, (rows, inputs))
+    a = rng.normal(0, 1, inputs)
+    y = np.sin(x @ a / 3.0) + 0.5 * x[:, 0] * x[:, 1]
+    with als.Surrogate(inputs, width, hidden, max_batch=1024, seed=1) as s:
+        losses = s.fit(x, y, steps=400, lr=1e-3)
+        pred = s(x).cpu().numpy()
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.02 * losses[0]
+    resid = (y - pred).var() / y.var()
+    assert resid < 0.02
+
+
+def test_inference_in_chunks_is_row_independent():
+    inputs = 40
+    rng = np.random.default_rng(8)
+    x = rng.uniform(0, 1, (70000, inputs)).astype(np.float32)
+    with als.Surrogate(seed=3) as s:
+        full = s.forward_raw(x).cpu().numpy()
+        part = s.forward_raw(x[65500:65700]).cpu().numpy()
+    np.testing.assert_array_equal(full[65500:65700], part)
+
+
+def test_device_uniform_draws_and_moments():
+    with als.Surrogate(seed=3) as s:
+        x = torch.empty(40 * 4096, dtype=torch.float32, device="cuda")
+        from alsvinn_b200 import _lib
+        _lib.check(s._lib.als_mlp_sample_uniform(x.data_ptr(), x.numel(), 7, 0))
+        torch.cuda.synchronize()
+        xs = x.cpu().numpy()
+        assert xs.min() >= 0.0 and xs.max() < 1.0
+        assert abs(xs.mean() - 0.5) < 5e-3
+        m1, m2 = s.moments(1 << 18, seed=1)
+        f = s(x.view(4096, 40)).double().cpu().numpy()
+    assert abs(m1 - f.mean()) < 5 * f.std() / np.sqrt(4096)
+    assert m2 >= m1 * m1
+
+
+def test_control_variate_gain_on_kelvin_helmholtz_samples():
+    """Solver-generated samples (KH 128^2 to T = 0.2): a surrogate trained on
+    1024 of them removes most of the variance of the observable on 512 held
+    out samples, i.e. the control-variate estimator needs several times
+    fewer solver samples for the same mean-square error as plain MC."""
+    params, y, info = als.uq.kh_observable_ensemble(128, 0, 1536, precision="fp32",
+                                                    end_time=0.2)
+    assert np.all(np.isfinite(y)) and y.std() > 0
+    with als.Surrogate(seed=0) as s:
+        s.fit(params[:1024], y[:1024], steps=1000, lr=1e-3)
+        f = s(params[1024:]).double().cpu().numpy()
+        m1, m2 = s.moments(1 << 20, seed=2)
+    yh = y[1024:]
+    fc = f - f.mean()
+    beta = np.dot(fc, yh - yh.mean()) / np.dot(fc, fc)
+    reduction = np.var(yh - beta * f) / np.var(yh)
+    assert reduction < 0.25, reduction
+    # the estimator itself, on the held-out samples
+    mean_cv, var_cv, _, _ = als.uq.control_variate(yh, f, m1, m2)
+    mean_pl, var_pl = als.uq.plain_mc(yh)
+    assert abs(mean_cv - mean_pl) < 4 * np.sqrt(var_pl / yh.size)
