@@ -1,0 +1,113 @@
+"""Ensembles sharded over GPUs, one process per GPU (torch.distributed).
+
+Samples are independent, so the only exchange is the statistics at the end:
+
+* ``samples_for_rank``: contiguous blocks of total/world samples per rank, the
+  reference's SimpleLoadBalancer (alsuq/src/mpi/SimpleLoadBalancer.cpp:35-97),
+  including its requirement that the world size divides the sample count;
+* ``gather_moments``: every rank's Welford (n, mean, M2) gathered on every
+  rank with one all_gather per array (NCCL over NVLink for device tensors,
+  gloo for host tensors);
+* ``merge_statistics``: a fresh FP64 accumulator into which all ranks'
+  moments are Chan-merged in rank order on the device, so every rank holds
+  the same bits.  The reference instead MPI_Reduces raw sums S1, S2 to rank 0
+  (alsuq/src/stats/StatisticsHelper.cpp:35-79).
+
+No step of the solve itself communicates.
+"""
+
+
+def samples_for_rank(total, world, rank):
+    """Sample indices [first, first + count) of `rank` (contiguous blocks)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank %d outside a world of %d" % (rank, world))
+    if total % world != 0:
+        raise ValueError("the number of processes (%d) must divide the number of samples (%d)"
+                         % (world, total))
+    per = total // world
+    return rank * per, per
+
+
+def gather_moments(n, mean, m2, group=None):
+    """All ranks' (n, mean, M2), in rank order, on every rank.
+
+    ``mean`` and ``m2`` are FP64 tensors of the same length on every rank
+    (device tensors with NCCL, host tensors with gloo)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    ns = torch.tensor([int(n)], dtype=torch.int64, device=mean.device)
+    n_all = [torch.zeros_like(ns) for _ in range(world)]
+    dist.all_gather(n_all, ns, group=group)
+    mean_all = [torch.empty_like(mean) for _ in range(world)]
+    dist.all_gather(mean_all, mean.contiguous(), group=group)
+    m2_all = [torch.empty_like(m2) for _ in range(world)]
+    dist.all_gather(m2_all, m2.contiguous(), group=group)
+    return [int(v.item()) for v in n_all], mean_all, m2_all
+
+
+def merge_statistics(local, group=None):
+    """Chan merge of every rank's MeanVariance ``local`` into a new
+    accumulator, identical on all ranks.  Returns the new MeanVariance."""
+    import torch
+    from .simulator import MeanVariance
+    torch.cuda.synchronize()
+    n, mean_ptr, m2_ptr = local.moments()
+    device = torch.cuda.current_device()
+    mean = _device_view(mean_ptr, local.count, device).clone()
+    m2 = _device_view(m2_ptr, local.count, device).clone()
+    ns, means, m2s = gather_moments(n, mean, m2, group)
+    merged = MeanVariance(local.count, device=device)
+    for k in range(len(ns)):
+        if ns[k] > 0:
+            merged.merge(ns[k], means[k], m2s[k])
+    torch.cuda.synchronize()
+    return merged
+
+
+class _DeviceArray:
+    """Zero-copy view of library-owned device memory (CUDA array interface)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def _device_view(ptr, count, device):
+    """FP64 tensor aliasing `count` doubles at a library device pointer."""
+    import torch
+    return torch.as_tensor(_DeviceArray(ptr, count), device="cuda:%d" % device)
+
+
+def kh_observable_ensemble(n, total_samples, precision="fp64", end_time=2.0, group=None, **kw):
+    """The UQ ensemble of uq.kh_observable_ensemble sharded over the ranks of
+    `group`: each rank solves its block of samples on its own GPU; the
+    observables are all-gathered (sample order) and the FP64 field
+    statistics merged.  Returns (params, y, info) on every rank, info with
+    the merged "field_mean" / "field_var" and this rank's "solve_seconds"."""
+    import torch
+    import torch.distributed as dist
+    from . import uq
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    first, count = samples_for_rank(total_samples, world, rank)
+    params, y, info = uq.kh_observable_ensemble(n, first, count, precision=precision,
+                                                end_time=end_time, keep_statistics=True, **kw)
+    local = info.pop("statistics")
+    merged = merge_statistics(local, group)
+    local.close()
+    count_all = merged.count
+    mean = torch.zeros(count_all, dtype=torch.float64, device="cuda")
+    var = torch.zeros_like(mean)
+    merged.result(mean, var)
+    merged.close()
+    yt = torch.as_tensor(y, dtype=torch.float64, device="cuda")
+    ys = [torch.empty_like(yt) for _ in range(world)]
+    dist.all_gather(ys, yt, group=group)
+    pt = torch.as_tensor(params, dtype=torch.float64, device="cuda")
+    ps = [torch.empty_like(pt) for _ in range(world)]
+    dist.all_gather(ps, pt, group=group)
+    shape = info["shape"]
+    info["field_mean"] = mean.cpu().numpy().reshape(shape)
+    info["field_var"] = var.cpu().numpy().reshape(shape)
+    return torch.cat(ps).cpu().numpy(), torch.cat(ys).cpu().numpy(), info

@@ -107,12 +107,36 @@ class Surrogate:
                                            int(steps), float(lr), loss.data_ptr(), stream))
         return loss[:steps].cpu().numpy()
 
-    def fit(self, params, y, steps=2000, lr=1e-3):
-        """Trains on (parameters, observables) with the target standardised."""
+    def fit(self, params, y, steps=2000, lr=1e-3, validation=None, check_every=100):
+        """Trains on (parameters, observables) with the target standardised.
+
+        With ``validation = (params_v, y_v)`` the validation error is checked
+        every ``check_every`` steps and the parameters with the lowest one are
+        kept (early stopping); ``self.best_step`` records which.  Returns the
+        training loss of every step."""
         y = np.asarray(y, dtype=np.float64)
         self.y_shift = float(y.mean())
         self.y_scale = float(y.std()) or 1.0
-        return self.train_raw(params, (y - self.y_shift) / self.y_scale, steps, lr)
+        t = (y - self.y_shift) / self.y_scale
+        if validation is None:
+            self.best_step = steps
+            return self.train_raw(params, t, steps, lr)
+        pv = self._dev(validation[0])
+        yv = np.asarray(validation[1], dtype=np.float64)
+        best = (np.mean((self(pv).double().cpu().numpy() - yv) ** 2), 0, self.params())
+        losses = []
+        done = 0
+        while done < steps:
+            k = min(check_every, steps - done)
+            losses.append(self.train_raw(params, t, k, lr))
+            done += k
+            err = np.mean((self(pv).double().cpu().numpy() - yv) ** 2)
+            if err < best[0]:
+                best = (err, done, self.params())
+        # restore the best parameters; their Adam state is not needed afterwards
+        self.set_params(best[2])
+        self.best_step = best[1]
+        return np.concatenate(losses)
 
     def moments(self, samples, seed=1, chunk=1 << 20):
         """E[f] and E[f^2] over U[0,1)^inputs from `samples` device draws (FP64 sums)."""

@@ -31,7 +31,8 @@ def _box_cells(n, box):
 
 
 def kh_observable_ensemble(n, first_sample, count, precision="fp64", end_time=2.0, cfl=0.4,
-                           box=KH_BOX, device=0, field_statistics=False, upload_chunk=256):
+                           box=KH_BOX, device=0, field_statistics=False, keep_statistics=False,
+                           upload_chunk=256):
     """Solves the 2-D KH samples [first_sample, first_sample + count) at n x n
     to ``end_time`` (WENO2 + HLL3, RK3, periodic) as one batched ensemble.
 
@@ -41,6 +42,8 @@ def kh_observable_ensemble(n, first_sample, count, precision="fp64", end_time=2.
     solve's wall-clock seconds (states resident on the device), the steps of
     every member and, with ``field_statistics``, the FP64 Welford mean and
     variance of every conserved variable over the ensemble (padded planes).
+    With ``keep_statistics`` the FP64 accumulator itself is returned open in
+    info["statistics"] (for merging across GPUs; the caller closes it).
     """
     params = uniform_draws(KH_PARAMETERS, first_sample, count)
     with Simulator(2, (n, n), (0.0, 0.0), (1.0, 1.0), flux="hll3", reconstruction="weno2",
@@ -61,8 +64,12 @@ def kh_observable_ensemble(n, first_sample, count, precision="fp64", end_time=2.
         y = sums[:, 0] / float((hi - lo) ** 2)
         steps = np.array([sim.info(m)["steps"] for m in range(count)])
         info = {"solve_seconds": seconds, "steps": steps, "n": n, "precision": precision,
-                "end_time": end_time, "box_cells": (lo, hi)}
-        if field_statistics:
+                "end_time": end_time, "box_cells": (lo, hi), "shape": sim.shape}
+        if keep_statistics:
+            mv = MeanVariance(4 * sim.plane, device=device)
+            mv.add_solver(sim, 0)
+            info["statistics"] = mv
+        elif field_statistics:
             mv = MeanVariance(4 * sim.plane, device=device)
             mv.add_solver(sim, 0)
             import torch

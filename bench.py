@@ -196,8 +196,14 @@ def run_batch(args, rank, world, local):
     """Times `steps` time steps of every member of every level (one launch
     per stage over all of them); value = member cell-updates / s."""
     import torch
+    import torch.distributed as dist
     import alsvinn_b200 as als
+    from alsvinn_b200 import distributed
     torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     dim, levels = BATCHES[args.workload]
     precision = "fp64" if args.workload == "kh3d" else args.precision
     nvar = dim + 2
@@ -224,17 +230,30 @@ def run_batch(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
     e0.record(stream)
     sim.advance(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
     bad = [m for m in range(sim.members) if sim.info(m)["status"] != 0]
-    if bad:
-        raise RuntimeError("constraint violation in members %r" % bad[:8])
+    nbad = len(bad)
+    if world > 1:
+        tb = torch.tensor([nbad], dtype=torch.int64, device="cuda")
+        dist.all_reduce(tb, op=dist.ReduceOp.MAX)
+        nbad = int(tb.item())
+    if nbad:
+        raise RuntimeError("constraint violation in members %r (this rank)" % bad[:8])
     cells = sum((lev["n"][0] ** dim) * lev["members"] for lev in sim.levels)
-    value = cells * args.steps / (ms * 1e-3)
+    value = world * cells * args.steps / (ms * 1e-3)
     kms = np.array([sim.profile_step() for _ in range(3)]).mean(axis=0)
     hbm_peak, peak_kind = peaks()
     per_cell = {"flux0": 2 * nvar * elem, "rk3_1": 3 * nvar * elem, "rk3_2": 3 * nvar * elem}
@@ -242,15 +261,20 @@ def run_batch(args, rank, world, local):
             for k, t in zip(KERNEL_NAMES, kms)]
     dom = max(range(3), key=lambda i: roof[i]["ms"])
     # FP64 statistics of the final states (every level) and the FP64 conservation sums
+    # (one all_gather of (n, mean, M2) per level and a rank-ordered merge across GPUs)
     t0 = time.perf_counter()
     for k, lev in enumerate(sim.levels):
         mv = als.MeanVariance(nvar * lev["plane"], device=local)
         mv.add_solver(sim, k)
+        if world > 1:
+            merged = distributed.merge_statistics(mv)
+            merged.close()
         mv.close()
+    torch.cuda.synchronize()
     stats_s = time.perf_counter() - t0
     result = {
         "metric": "member cell-updates/s (%s, KH, WENO2+HLL3, RK3, %s)" % (args.workload, precision),
-        "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
+        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32",
         "data": "synthetic (Kelvin-Helmholtz samples from the reference's generator)",
@@ -264,9 +288,127 @@ def run_batch(args, rank, world, local):
         "schedule": schedule, "statistics_seconds": stats_s,
         "gpu_launches": args.steps * sim.launches_per_step(), "clocks": clock_info,
     }
-    print(json.dumps(result))
+    if rank == 0:
+        print(json.dumps(result))
     sim.close()
+    if world > 1:
+        dist.destroy_process_group()
 
+
+UQ_ORACLE = os.path.join(ROOT, "tests", "golden", "uq_kh256_fp64_4096.npz")
+
+
+def run_uq(args, rank, world, local):
+    """UQ time-to-error: plain batched Monte Carlo against the surrogate
+    control variate, KH 256^2 to T = 2, observable = mean density over
+    [0.25, 0.75]^2, both judged by the 4096-sample FP64 ensemble.
+
+    The surrogate (40 -> 256 x4 -> 1, BF16 tensor cores) is trained on the
+    FP64 ensemble's samples 0..1023 (Adam, lr 1e-3, up to 2000 steps, early
+    stopping on samples 1024..2047) and judged on samples 2048..4095: there
+    the residual variance Var(Y - b f) / Var(Y) (and the same for Y^2) says
+    how many fewer solver samples the control-variate estimator needs for
+    the RMS error of plain MC with M samples.  Both arms are then run for
+    real on fresh samples (FP32 members, FP64 statistics): plain MC with M
+    samples, the control variate with the reduced count plus the surrogate's
+    E[f], E[f^2] from 2^22 evaluations.  value = plain wall-clock / control
+    variate wall-clock (training included, training data reused from the
+    oracle ensemble; the ratio with the training data's solves counted too
+    is reported beside it)."""
+    import torch
+    import alsvinn_b200 as als
+    from alsvinn_b200 import uq
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    if not os.path.exists(UQ_ORACLE):
+        raise RuntimeError("missing %s (python tests/golden/make_uq_oracle.py)" % UQ_ORACLE)
+    z = np.load(UQ_ORACLE)
+    y_or = np.asarray(z["y"], dtype=np.float64)
+    n_or = y_or.size
+    n = int(z["n"])
+    T = float(z["end_time"])
+    p_or = als.uniform_draws(40, 0, n_or)
+    mu_or, var_or = uq.plain_mc(y_or)
+    M = args.samples
+    prec = args.precision
+
+    def now():
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = now()
+    sur = als.Surrogate(seed=0, device=local)
+    losses = sur.fit(p_or[:1024], y_or[:1024], steps=2000, lr=1e-3,
+                     validation=(p_or[1024:2048], y_or[1024:2048]))
+    t_train = now() - t0
+    fj = sur(p_or[2048:]).double().cpu().numpy()
+    yj = y_or[2048:]
+    fc = fj - fj.mean()
+    beta = np.dot(fc, yj - yj.mean()) / np.dot(fc, fc)
+    r_mean = float(np.var(yj - beta * fj) / np.var(yj))
+    g2 = fj * fj
+    y2 = yj * yj
+    gc = g2 - g2.mean()
+    beta2 = np.dot(gc, y2 - y2.mean()) / np.dot(gc, gc)
+    r_var = float(np.var(y2 - beta2 * g2) / np.var(y2))
+    rho2 = float(np.corrcoef(yj, fj)[0, 1] ** 2)
+    t0 = now()
+    m1, m2 = sur.moments(1 << 22, seed=3)
+    t_moments = now() - t0
+
+    # plain batched MC, M fresh samples
+    p_pl, y_pl, info_pl = uq.kh_observable_ensemble(n, n_or, M, precision=prec, end_time=T,
+                                                    device=local)
+    t_plain = info_pl["solve_seconds"]
+    mean_pl, var_pl = uq.plain_mc(y_pl)
+    # control variate: the sample count that matches plain MC's RMS errors
+    m_cv = int(np.ceil(M * max(r_mean, r_var))) + 1
+    m_cv = min(max(m_cv, 8), M)
+    p_cv, y_cv, info_cv = uq.kh_observable_ensemble(n, n_or + M, m_cv, precision=prec,
+                                                    end_time=T, device=local)
+    t0 = now()
+    f_cv = sur(p_cv).double().cpu().numpy()
+    mean_cv, var_cv, _, _ = uq.control_variate(y_cv, f_cv, m1, m2)
+    t_eval = now() - t0
+    clock_info = clocks.stop()
+    sur.close()
+    t_cv = info_cv["solve_seconds"] + t_train + t_moments + t_eval
+    per_sample = t_plain / M
+    t_cv_with_data = t_cv + 1024 * per_sample
+    result = {
+        "metric": "UQ time-to-error, plain batched MC / surrogate control variate "
+                  "(KH %d^2, T=%g, mean and variance of mean rho over [0.25,0.75]^2)" % (n, T),
+        "value": t_plain / t_cv, "unit": "x (plain wall-clock / control-variate wall-clock)",
+        "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * t_cv,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 members, f64 statistics, bf16 surrogate",
+        "data": "synthetic (Kelvin-Helmholtz samples from the reference's generator)",
+        "config": {"workload": "uq", "n": n, "end_time": T, "plain_samples": M,
+                   "cv_samples": m_cv, "member_precision": prec,
+                   "oracle": "%d-sample FP64 ensemble (tests/golden)" % n_or,
+                   "surrogate": "40-256x4-1 GELU, Adam lr 1e-3, <=2000 steps, early stop"},
+        "uq": {
+            "oracle_mean": mu_or, "oracle_var": var_or,
+            "heldout_rho2": rho2, "residual_ratio_mean": r_mean, "residual_ratio_var": r_var,
+            "surrogate_best_step": int(sur.best_step), "final_train_loss": float(losses[-1]),
+            "plain": {"mean": mean_pl, "var": var_pl, "err_mean": mean_pl - mu_or,
+                      "err_var": var_pl - var_or, "rms_err_mean_expected": np.sqrt(var_or / M),
+                      "seconds": t_plain},
+            "cv": {"mean": mean_cv, "var": var_cv, "err_mean": mean_cv - mu_or,
+                   "err_var": var_cv - var_or,
+                   "rms_err_mean_expected": np.sqrt(r_mean * var_or / m_cv),
+                   "seconds_solve": info_cv["solve_seconds"], "seconds_train": t_train,
+                   "seconds_moments": t_moments, "seconds_eval": t_eval},
+            "ratio_including_training_data": t_plain / t_cv_with_data,
+            "per_sample_seconds": per_sample,
+        },
+        "gpu_launches": None,
+        "clocks": clock_info,
+    }
+    print(json.dumps(result, default=float))
 
 def main():
     ap = argparse.ArgumentParser()
@@ -277,8 +419,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only run warmup+steps time steps (for profiler captures)")
-    ap.add_argument("--workload", default="kh1024", choices=sorted(["kh1024"] + list(BATCHES)),
-                    help="kh1024 (default, the plain FP64 drop-in), or an ensemble workload")
+    ap.add_argument("--workload", default="kh1024",
+                    choices=sorted(["kh1024", "uq"] + list(BATCHES)),
+                    help="kh1024 (default, the plain FP64 drop-in), an ensemble workload, or "
+                         "uq (time-to-error of the surrogate control variate)")
+    ap.add_argument("--samples", type=int, default=1024, help="plain MC samples of --workload uq")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="member precision of the ensemble workloads")
     args = ap.parse_args()
@@ -291,6 +436,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload == "uq":
+        run_uq(args, rank, world, local)
         return
     if args.workload != "kh1024":
         run_batch(args, rank, world, local)
