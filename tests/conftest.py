@@ -36,14 +36,15 @@ def ref_oracle():
 def load_golden(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     out = {k: z[k] for k in z.files}
+    # scalars stored as 0-d arrays become Python values
     for k in ("flux", "recon", "integrator", "bc"):
-        if k in out:
+        if k in out and np.ndim(out[k]) == 0:
             out[k] = str(out[k])
     for k in ("cfl", "end_time", "gamma", "t"):
-        if k in out:
+        if k in out and np.ndim(out[k]) == 0:
             out[k] = float(out[k])
-    for k in ("dim", "steps"):
-        if k in out:
+    for k in ("dim", "steps", "n", "samples", "first_sample"):
+        if k in out and np.ndim(out[k]) == 0:
             out[k] = int(out[k])
     return out
 

@@ -150,3 +150,14 @@ def test_region_sums_and_conservation():
     np.testing.assert_allclose(s1, s0, rtol=1e-12, atol=1e-10)
     np.testing.assert_allclose(box, U[:, :, 0, g + 12:g + 36, g + 12:g + 36].sum(axis=(2, 3)),
                                rtol=1e-13, atol=1e-12)
+
+
+@pytest.mark.parametrize("sample", [7, 4095])
+def test_uq_oracle_members_equal_single_runs_at_full_size(sample):
+    """Members of the 4096-sample FP64 ensemble (256^2 to T = 2, committed
+    observables) re-solved alone: identical observable and step count."""
+    z = load_golden("uq_kh256_fp64_4096")
+    params, y, info = als.uq.kh_observable_ensemble(256, sample, 1, precision="fp64",
+                                                    end_time=2.0)
+    assert info["steps"][0] == z["steps"][sample]
+    assert y[0] == z["y"][sample]

@@ -81,3 +81,20 @@ def test_control_variate_reduces_the_error_of_plain_mc():
     rms_plain = np.sqrt(np.mean(np.square(err_plain)))
     rms_cv = np.sqrt(np.mean(np.square(err_cv)))
     assert rms_cv < 0.2 * rms_plain
+
+
+def test_uq_oracle_ensemble_fixture():
+    """The committed FP64 ensemble that judges the UQ estimators."""
+    from conftest import load_golden
+    z = load_golden("uq_kh256_fp64_4096")
+    y = z["y"]
+    assert z["samples"] == 4096 and y.shape == (4096,) and z["n"] == 256
+    assert z["end_time"] == 2.0 and z["first_sample"] == 0
+    assert np.all(np.isfinite(y))
+    # mean density over [0.25,0.75]^2 starts near 2 (heavy band) and mixes towards 1.5
+    assert 1.5 < y.mean() < 2.0 and 0 < y.std() < 0.2
+    assert z["steps"].min() > 5000
+    m, v = uq.plain_mc(y)
+    assert m == pytest.approx(y.mean(), rel=1e-15) and v == pytest.approx(y.var(), rel=1e-12)
+    # the FP64 Welford density statistics cover the padded plane
+    assert z["rho_mean"].shape == (1, 260, 260) and np.all(z["rho_var"] >= 0)
