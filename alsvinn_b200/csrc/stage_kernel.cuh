@@ -62,8 +62,33 @@ template<> struct TileShape<2> {
     static constexpr int X = ALS_TILE2_X, Y = ALS_TILE2_Y, Z = 1, T = ALS_STAGE2_THREADS,
         B = ALS_STAGE2_BLOCKS;
 };
+#ifndef ALS_TILE3_X
+#define ALS_TILE3_X 8
+#endif
+#ifndef ALS_TILE3_Y
+#define ALS_TILE3_Y 8
+#endif
+#ifndef ALS_TILE3_Z
+#define ALS_TILE3_Z 4
+#endif
+// 3-D: an 8x8x4 tile needs 320/320/384 reconstructions and 288/288/320
+// face fluxes along x/y/z; its FP64 shared memory (90 KB) allows two blocks
+// per SM.  Measured on KH 128^3 x 8 members (FP64, ms per RK3 step):
+//   8x8x4 / 320 threads / 2 blocks (96 regs)   15.9
+//   8x4x4 / 192 threads / 4 blocks             17.2
+//   8x8x4 / 384 threads / 2 blocks (80 regs)   17.2
+//   8x8x2 / 256 threads / 3 blocks             19.8
+//   8x8x4 / 256 threads / 2 blocks             20.1
+//   8x8x2 / 192 threads / 4 blocks             21.3
+#ifndef ALS_STAGE3_THREADS
+#define ALS_STAGE3_THREADS 320
+#endif
+#ifndef ALS_STAGE3_BLOCKS
+#define ALS_STAGE3_BLOCKS 2
+#endif
 template<> struct TileShape<3> {
-    static constexpr int X = 8, Y = 8, Z = 4, T = 256, B = 4;
+    static constexpr int X = ALS_TILE3_X, Y = ALS_TILE3_Y, Z = ALS_TILE3_Z, T = ALS_STAGE3_THREADS,
+        B = ALS_STAGE3_BLOCKS;
 };
 
 template<class R, int DIM, int RECON>

@@ -64,7 +64,8 @@ def kh_observable_ensemble(n, first_sample, count, precision="fp64", end_time=2.
         y = sums[:, 0] / float((hi - lo) ** 2)
         steps = np.array([sim.info(m)["steps"] for m in range(count)])
         info = {"solve_seconds": seconds, "steps": steps, "n": n, "precision": precision,
-                "end_time": end_time, "box_cells": (lo, hi), "shape": sim.shape}
+                "end_time": end_time, "box_cells": (lo, hi), "shape": sim.shape,
+                "stage_launches": int(steps.max()) * sim.launches_per_step()}
         if keep_statistics:
             mv = MeanVariance(4 * sim.plane, device=device)
             mv.add_solver(sim, 0)

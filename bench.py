@@ -56,6 +56,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def tensor_peak():
+    """(burst, sustained, source) dense BF16 TFLOP/s."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p.get("bf16_tflops", 1590.0), p.get("bf16_tflops", 1590.0), "measured (burst)"
+    return 1590.0, 1590.0, "fallback (burst)"
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -405,10 +415,74 @@ def run_uq(args, rank, world, local):
             "ratio_including_training_data": t_plain / t_cv_with_data,
             "per_sample_seconds": per_sample,
         },
-        "gpu_launches": None,
+        # stage launches of both solves, plus the surrogate's (about 20 per
+        # training step, 6 per inference chunk of 32768 rows)
+        "gpu_launches": int(info_pl["stage_launches"] + info_cv["stage_launches"]
+                            + 20 * 2000 + 6 * (((1 << 22) + 32767) // 32768)),
         "clocks": clock_info,
     }
     print(json.dumps(result, default=float))
+
+
+def run_surrogate(args, rank, world, local):
+    """The surrogate's tensor-core kernels: inference over 2^20 parameter
+    rows (the E[f], E[f^2] pass of the control variate) and full-batch
+    training steps on 1024 rows.  Rates are taken around whole library
+    calls (each call ends synchronised); FLOPs are algorithmic (2 per
+    multiply-add of the 40 -> 256 x4 -> 1 network, K unpadded)."""
+    import torch
+    import alsvinn_b200 as als
+    from alsvinn_b200 import _lib
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    rows = 1 << 20
+    flop_row = 2 * (40 * 256 + 3 * 256 * 256 + 256)
+    sur = als.Surrogate(seed=0, device=local)
+    x = torch.empty(rows * 40, dtype=torch.float32, device="cuda")
+    _lib.check(sur._lib.als_mlp_sample_uniform(x.data_ptr(), x.numel(), 5, 0))
+    x = x.view(rows, 40)
+    for _ in range(max(args.warmup, 3)):
+        sur.forward_raw(x)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sur.forward_raw(x)
+    torch.cuda.synchronize()
+    infer_s = (time.perf_counter() - t0) / args.steps
+    xt = x[:1024].clone()
+    tt = torch.sin(xt.sum(dim=1))
+    sur.train_raw(xt, tt, 5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    train_steps = 200
+    sur.train_raw(xt, tt, train_steps)
+    torch.cuda.synchronize()
+    train_s = (time.perf_counter() - t0) / train_steps
+    clock_info = clocks.stop()
+    sur.close()
+    _, bf16_peak, kind = tensor_peak()
+    achieved = rows * flop_row / infer_s / 1e12
+    result = {
+        "metric": "surrogate inference rows/s (40-256x4-1 MLP, BF16 tcgen05, FP32 accumulate)",
+        "value": rows / infer_s, "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * infer_s, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic (U[0,1) parameter draws)",
+        "config": {"workload": "surrogate", "rows": rows, "train_batch": 1024},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_peak,
+                     "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
+                     "kernel": "whole forward call (4 tcgen05 GEMMs + head)",
+                     "peak_source": kind},
+        "train_step_ms": 1e3 * train_s,
+        "train_tflops": 3 * 1024 * flop_row / train_s / 1e12,
+        "gpu_launches": args.steps * 6,
+        "clocks": clock_info,
+    }
+    print(json.dumps(result))
 
 def main():
     ap = argparse.ArgumentParser()
@@ -420,7 +494,7 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only run warmup+steps time steps (for profiler captures)")
     ap.add_argument("--workload", default="kh1024",
-                    choices=sorted(["kh1024", "uq"] + list(BATCHES)),
+                    choices=sorted(["kh1024", "uq", "surrogate"] + list(BATCHES)),
                     help="kh1024 (default, the plain FP64 drop-in), an ensemble workload, or "
                          "uq (time-to-error of the surrogate control variate)")
     ap.add_argument("--samples", type=int, default=1024, help="plain MC samples of --workload uq")
@@ -439,6 +513,9 @@ def main():
         return
     if args.workload == "uq":
         run_uq(args, rank, world, local)
+        return
+    if args.workload == "surrogate":
+        run_surrogate(args, rank, world, local)
         return
     if args.workload != "kh1024":
         run_batch(args, rank, world, local)
