@@ -98,6 +98,10 @@ PROTOTYPES = {
     "als_solver_profile_step": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "als_uniform_draws": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
                                          ctypes.c_double, ctypes.c_double, _D]),
+    "als_structure_functions": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_double, _VP,
+                                                ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
+                                                _VP, _VP]),
     # include/als_surrogate.h
     "als_mlp_create": (ctypes.c_int, [ctypes.POINTER(MlpConfig), ctypes.c_int, _PP]),
     "als_mlp_destroy": (ctypes.c_int, [_VP]),

@@ -254,6 +254,27 @@ int als_stats_moments(als_stats* st, long long* n, double** mean, double** m2);
 /* Writes mean and variance (device arrays of `count` doubles; either may be NULL). */
 int als_stats_result(als_stats* st, double* mean, double* variance, void* stream);
 
+/* ------------------------------------------------- structure functions
+ * Structure-function statistics of `members` states (device memory, FP64
+ * or FP32, `member_stride` elements apart, dimension+2 padded planes each)
+ * into out (device, FP64): out[(member*nvar + var)*H + h].
+ *   ALS_STRUCTURE_CUBE  - alsuq/src/stats/StructureCube.cpp:39-75 and
+ *     alsfvm/src/functional/StructureCube.cpp via
+ *     alsfvm/include/alsfvm/functional/structure_common.hpp:39-160:
+ *     sum over cells and over the cube surface at distance h = 1..H-1 of
+ *     |u - u_h|^p / (nx*ny*nz); out[.., 0] = 0.
+ *   ALS_STRUCTURE_BASIC - alsuq/src/stats/StructureBasic.cpp:74-118: the
+ *     point h cells along `direction`, h = 0..H-1.
+ * Points outside the interior wrap (ALS_BC_PERIODIC) or clamp
+ * (ALS_BC_NEUMANN) as in ValueAtBoundary.hpp:20-110.  H <= 512.  Sums are
+ * FP64 in a fixed order; they equal the reference's sequential sums to
+ * rounding.  Stream-ordered. */
+#define ALS_STRUCTURE_CUBE 0
+#define ALS_STRUCTURE_BASIC 1
+int als_structure_functions(const als_grid* grid, int boundary, int kind, int direction, int H,
+    double p, const void* states, int precision, long long member_stride, int members,
+    double* out, void* stream);
+
 /* ------------------------------------------------------- UQ sampling
  * Parameter draws of samples [first_sample, first_sample+count) for a
  * parameter of length `dimension`: out[k*dimension + c].  Same numbers as

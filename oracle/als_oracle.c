@@ -664,3 +664,134 @@ void orc_meanvar(long count, long samples, const double* states, double* mean, d
         var[i] -= pow(mean[i], two);
     }
 }
+
+/* ------------------------------------------------------ structure functions */
+
+/* ValueAtBoundary<PERIODIC/NEUMANN>::getValueAtBoundary, ValueAtBoundary.hpp:20-110 */
+static double value_at(const double* plane, const int* n, const int* gh, const int* N, int bc,
+    int x, int y, int z) {
+    int pos[3] = {x, y, z};
+    int d;
+    for (d = 0; d < 3; ++d) {
+        if (bc == ORC_BC_PERIODIC) {
+            while (pos[d] < 0) {
+                pos[d] += n[d];
+            }
+            pos[d] = pos[d] % n[d];
+        } else {
+            if (pos[d] > n[d] - 1) {
+                pos[d] = n[d] - 1;
+            }
+            if (pos[d] < 0) {
+                pos[d] = 0;
+            }
+        }
+        pos[d] += gh[d];
+    }
+    return plane[((long)pos[2] * N[1] + pos[1]) * N[0] + pos[0]];
+}
+
+/* FastPower<p> (alsutils/math/FastPower.hpp): x * FastPower<p-1>(x); PowPower: pow */
+static double structure_power(double x, double p) {
+    if (p == 1.0) {
+        return x;
+    } else if (p == 2.0) {
+        return x * x;
+    } else if (p == 3.0) {
+        return x * (x * x);
+    } else if (p == 4.0) {
+        return x * (x * (x * x));
+    } else if (p == 5.0) {
+        return x * (x * (x * (x * x)));
+    }
+    return pow(x, p);
+}
+
+static void structure_geometry(int dim, const int* n, int g, int* nn, int* gh, int* N) {
+    int d;
+    for (d = 0; d < 3; ++d) {
+        nn[d] = d < dim ? n[d] : 1;
+        gh[d] = d < dim ? g : 0;
+        N[d] = nn[d] + 2 * gh[d];
+    }
+}
+
+void orc_structure_cube(int dim, const int* n, int g, int bc, int nvar, int H, double p,
+    const double* planes, double* out) {
+    int nn[3], gh[3], N[3];
+    long plane;
+    int v, i, j, k, h, d, side, x, y, z;
+    structure_geometry(dim, n, g, nn, gh, N);
+    plane = (long)N[0] * N[1] * N[2];
+    for (v = 0; v < nvar * H; ++v) {
+        out[v] = 0;
+    }
+    for (v = 0; v < nvar; ++v) {
+        const double* u_plane = planes + v * plane;
+        double* o = out + (long)v * H;
+        for (k = 0; k < nn[2]; ++k) {
+            for (j = 0; j < nn[1]; ++j) {
+                for (i = 0; i < nn[0]; ++i) {
+                    const double u = u_plane[((long)(k + gh[2]) * N[1] + j + gh[1]) * N[0] + i + gh[0]];
+                    for (h = 1; h < H; ++h) {
+                        /* forEachPointInComputeStructureCube, structure_common.hpp:39-104 */
+                        for (d = 0; d < dim; ++d) {
+                            for (side = 0; side < 2; ++side) {
+                                const int zDir = d == 2, yDir = d == 1, xDir = d == 0;
+                                const int zStart = zDir ? (side == 0 ? k - h : k + h) : (dim > 2 ? k - h : 0);
+                                const int zEnd = zDir ? zStart + 1 : (dim > 2 ? k + h + 1 : 1);
+                                const int yStart = yDir ? (side == 0 ? j - h : j + h)
+                                                        : (dim >= 2 ? j - h + 1 : 0);
+                                const int yEnd = yDir ? yStart + 1 : (dim >= 2 ? j + h : 1);
+                                int xStart = xDir ? (side == 0 ? i - h : i + h) : i - h;
+                                int xEnd = xDir ? xStart + 1 : i + h + 1;
+                                if (zDir) {
+                                    xStart += 1;
+                                    xEnd -= 1;
+                                }
+                                for (z = zStart; z < zEnd; ++z) {
+                                    for (y = yStart; y < yEnd; ++y) {
+                                        for (x = xStart; x < xEnd; ++x) {
+                                            const double uh = value_at(u_plane, nn, gh, N, bc, x, y, z);
+                                            o[h] += structure_power(fabs(u - uh), p) /
+                                                (double)(nn[0] * nn[1] * nn[2]);
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+void orc_structure_basic(int dim, const int* n, int g, int bc, int nvar, int direction, int H,
+    double p, const double* planes, double* out) {
+    int nn[3], gh[3], N[3];
+    long plane;
+    int v, i, j, k, h;
+    const int dv[3] = {direction == 0, direction == 1, direction == 2};
+    structure_geometry(dim, n, g, nn, gh, N);
+    plane = (long)N[0] * N[1] * N[2];
+    for (v = 0; v < nvar * H; ++v) {
+        out[v] = 0;
+    }
+    for (v = 0; v < nvar; ++v) {
+        const double* u_plane = planes + v * plane;
+        double* o = out + (long)v * H;
+        for (k = 0; k < nn[2]; ++k) {
+            for (j = 0; j < nn[1]; ++j) {
+                for (i = 0; i < nn[0]; ++i) {
+                    for (h = 0; h < H; ++h) {
+                        const double u = u_plane[((long)(k + gh[2]) * N[1] + j + gh[1]) * N[0] + i + gh[0]];
+                        const double uh = value_at(u_plane, nn, gh, N, bc, i + h * dv[0],
+                            j + h * dv[1], k + h * dv[2]);
+                        o[h] += pow(fabs(u - uh), p) / (double)(nn[0] * nn[1] * nn[2]);
+                    }
+                }
+            }
+        }
+    }
+}

@@ -68,6 +68,20 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
  * var = S2/M - mean^2, over `samples` states of `count` doubles each. */
 void orc_meanvar(long count, long samples, const double* states, double* mean, double* var);
 
+/* Structure functions of each of `nvar` padded planes (ghost width g on the
+ * active sides).  Cube (alsfvm/include/alsfvm/functional/structure_common.hpp:39-160,
+ * used by alsuq/src/stats/StructureCube.cpp:39-75 and
+ * alsfvm/src/functional/StructureCube.cpp): out[v*H + h] = sum over cells and
+ * over the points of the cube surface at distance h (h = 1..H-1) of
+ * |u - u_h|^p / (nx*ny*nz), FastPower for p = 1..5, pow otherwise.
+ * Basic (alsuq/src/stats/StructureBasic.cpp:74-118): the single point
+ * h steps along `direction`, h = 0..H-1, pow always.  Points outside the
+ * interior wrap (periodic) or clamp (Neumann), ValueAtBoundary.hpp:20-110. */
+void orc_structure_cube(int dim, const int* n, int g, int bc, int nvar, int H, double p,
+    const double* planes, double* out);
+void orc_structure_basic(int dim, const int* n, int g, int bc, int nvar, int direction, int H,
+    double p, const double* planes, double* out);
+
 /* Constraint check of CPUCellComputer::obeysConstraints (CPUCellComputer.cpp:80-128)
  * over all cells; returns 1 when every cell obeys. */
 int orc_obeys_constraints(const orc_config* cfg, const double* planes);

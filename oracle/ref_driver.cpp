@@ -42,6 +42,7 @@
 #include "alsfvm/equation/CPUCellComputer.hpp"
 #include "alsfvm/DeviceConfiguration.hpp"
 #include "alsuq/generator/STLMersenne.hpp"
+#include "alsfvm/functional/structure_common.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -432,6 +433,36 @@ int alsref_stlmersenne(long dimension, long first, long count, double* out) {
             for (long c = 0; c < dimension; ++c) {
                 out[k * dimension + c] = gen.generate(c, first + k);
             }
+        }
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Structure-function cube of every variable of one padded state, through the
+// reference's own dispatchComputeStructureCubeCPU (structure_common.hpp:122-160)
+// into a (numberOfH x 1 x 1) volume made as StatisticsHelper::findOrCreateSnapshot
+// makes it (StatisticsHelper.cpp:127-160): out[var*numberOfH + h].
+int alsref_structure_cube(int dim, const int* n, int ghosts, const char* bc, int numberOfH,
+    double p, const double* planes, double* out) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", bc, 1.4, 0.5);
+        auto o = build(s);
+        auto in = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        copyIn(*in, planes);
+        auto res = in->makeInstance(size_t(numberOfH), 1, 1, "default");
+        res->makeZero();
+        if (s.bc == "periodic") {
+            functional::dispatchComputeStructureCubeCPU<boundary::PERIODIC>(*res, *in, numberOfH, p);
+        } else {
+            functional::dispatchComputeStructureCubeCPU<boundary::NEUMANN>(*res, *in, numberOfH, p);
+        }
+        for (size_t var = 0; var < res->getNumberOfVariables(); ++var) {
+            std::memcpy(out + var * numberOfH, res->getScalarMemoryArea(var)->getPointer(),
+                size_t(numberOfH) * sizeof(double));
         }
         return 0;
     } catch (std::exception& e) {

@@ -102,6 +102,21 @@ def main():
                 "sha256(wave speeds) max_wave_speed\n")
         for c in cases:
             f.write("%d %s %s %s %s %d %s %s %s %.17g\n" % c)
+    # structure-function cubes through the reference's dispatchComputeStructureCubeCPU
+    rows = []
+    seed = 3000
+    for dim, n in ((1, (32,)), (2, (12, 10)), (3, (7, 6, 8))):
+        for bc in ("periodic", "neumann"):
+            for H, p in ((6, 1.0), (5, 2.0), (4, 3.0), (5, 2.5)):
+                seed += 1
+                st = smooth_random_state(seed, dim, n, 2)
+                out = ref.structure_cube(dim, n, 2, bc, H, p, st)
+                rows.append((dim, ",".join(map(str, n)), bc, H, p, seed, digest(out),
+                             float(out.max())))
+    with open(os.path.join(HERE, "structure_cube_cases.txt"), "w") as f:
+        f.write("# dim n bc H p seed sha256(out, nvar x H) max\n")
+        for r in rows:
+            f.write("%d %s %s %d %.17g %d %s %.17g\n" % r)
     states = np.stack([smooth_random_state(77 + k, 2, (6, 5), 2) for k in range(7)])
     mean, var = ref.meanvar(2, (6, 5), 2, states)
     np.savez_compressed(os.path.join(HERE, "meanvar_7.npz"), mean=mean, var=var,

@@ -83,6 +83,11 @@ class COracle:
         L.orc_fill_ghosts.argtypes = [ctypes.POINTER(_Config), _D, ctypes.c_int]
         L.orc_meanvar.argtypes = [ctypes.c_long, ctypes.c_long, _D, _D, _D]
         L.orc_obeys_constraints.argtypes = [ctypes.POINTER(_Config), _D]
+        L.orc_structure_cube.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D]
+        L.orc_structure_basic.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, _D, _D]
 
     def config(self, dim, n, lower, upper, flux, recon, integrator, bc, gamma):
         cfg = _Config()
@@ -136,6 +141,22 @@ class COracle:
         p = np.ascontiguousarray(planes, dtype=np.float64)
         return bool(self.lib.orc_obeys_constraints(ctypes.byref(cfg), _dptr(p)))
 
+    def structure_cube(self, dim, n, g, bc, H, p, planes):
+        st = np.ascontiguousarray(planes, dtype=np.float64)
+        out = np.zeros((st.shape[0], H))
+        nn = (ctypes.c_int * 3)(*(list(n) + [1, 1, 1])[:3])
+        self.lib.orc_structure_cube(dim, nn, g, 1 if bc == "periodic" else 0, st.shape[0], H,
+                                    float(p), _dptr(st), _dptr(out))
+        return out
+
+    def structure_basic(self, dim, n, g, bc, direction, H, p, planes):
+        st = np.ascontiguousarray(planes, dtype=np.float64)
+        out = np.zeros((st.shape[0], H))
+        nn = (ctypes.c_int * 3)(*(list(n) + [1, 1, 1])[:3])
+        self.lib.orc_structure_basic(dim, nn, g, 1 if bc == "periodic" else 0, st.shape[0],
+                                     direction, H, float(p), _dptr(st), _dptr(out))
+        return out
+
 
 def ref_library_path():
     return os.path.join(ORACLE_DIR, "_ref", "libalsref.so")
@@ -166,6 +187,8 @@ class RefOracle:
         L.alsref_meanvar.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_long, _D, _D, _D]
         L.alsref_stlmersenne.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, _D]
         L.alsref_ghost_cells.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]
+        L.alsref_structure_cube.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_char_p,
+                                            ctypes.c_int, ctypes.c_double, _D, _D]
 
     def _check(self, rc):
         if rc < 0:
@@ -222,6 +245,14 @@ class RefOracle:
         self._check(self.lib.alsref_meanvar(dim, self._vec(n, ctypes.c_int, 1), ghosts,
                                             st.shape[0], _dptr(st), _dptr(mean), _dptr(var)))
         return mean, var
+
+    def structure_cube(self, dim, n, ghosts, bc, H, p, planes):
+        st = np.ascontiguousarray(planes, dtype=np.float64)
+        out = np.zeros((st.shape[0], H))
+        self._check(self.lib.alsref_structure_cube(dim, self._vec(n, ctypes.c_int, 1), ghosts,
+                                                   bc.encode(), H, float(p), _dptr(st),
+                                                   _dptr(out)))
+        return out
 
     def stlmersenne(self, dimension, first, count):
         out = np.zeros(dimension * count)

@@ -6,10 +6,12 @@ sources (tests/golden/make_golden.py), and, where the reference build is
 present, fresh random cases.  The reference's own unit tests that pin this
 path (test/library_tests/src/fvm/...) are ported here against the oracle.
 """
+import os
+
 import numpy as np
 import pytest
 
-from conftest import SIMULATION_FIXTURES, flux_cases, load_golden
+from conftest import GOLDEN, SIMULATION_FIXTURES, flux_cases, load_golden
 from oracle_lib import digest, ghost_cells, padded_shape, smooth_random_state
 
 
@@ -162,3 +164,51 @@ def test_boundary_fills(c_oracle):
         np.testing.assert_array_equal(N[g:-g, -g - 1 + k], N[g:-g, -g - k])
         np.testing.assert_array_equal(P[g:-g, g - k], P[g:-g, g - k + n])
         np.testing.assert_array_equal(P[g - k, :], P[g - k + n, :])
+
+
+def _structure_cases():
+    rows = []
+    with open(os.path.join(GOLDEN, "structure_cube_cases.txt")) as f:
+        for line in f:
+            if line.startswith("#") or not line.strip():
+                continue
+            dim, n, bc, H, p, seed, dg, mx = line.split()
+            rows.append((int(dim), tuple(int(v) for v in n.split(",")), bc, int(H), float(p),
+                         int(seed), dg, float(mx)))
+    return rows
+
+
+@pytest.mark.parametrize("case", _structure_cases(), ids=lambda c: "d%d_%s_H%d_p%g" % (
+    c[0], c[2], c[3], c[4]))
+def test_c_oracle_structure_cube_matches_reference(c_oracle, case):
+    """structure_common.hpp:39-160 through the reference's own code: bit for bit."""
+    dim, n, bc, H, p, seed, dg, mx = case
+    st = smooth_random_state(seed, dim, n, 2)
+    out = c_oracle.structure_cube(dim, n, 2, bc, H, p, st)
+    assert digest(out) == dg
+    assert out.max() == mx
+
+
+@pytest.mark.parametrize("bc", ["periodic", "neumann"])
+def test_c_oracle_structure_functions_against_reference_build(c_oracle, ref_oracle, bc):
+    for dim, n in ((2, (9, 11)), (3, (5, 6, 4))):
+        st = smooth_random_state(4242 + dim, dim, n, 3)
+        for H, p in ((7, 2.0), (3, 1.5)):
+            np.testing.assert_array_equal(c_oracle.structure_cube(dim, n, 3, bc, H, p, st),
+                                          ref_oracle.structure_cube(dim, n, 3, bc, H, p, st))
+
+
+def test_structure_basic_small_case_by_hand(c_oracle):
+    """StructureBasic.cpp:74-118 on a 1-D ramp: |u_i - u_{i+h}| = h*step away from the edge."""
+    n = 8
+    st = np.zeros(padded_shape(1, (n,), 2))
+    st[:, 0, 0, 2:-2] = np.arange(n, dtype=float)
+    out = c_oracle.structure_basic(1, (n,), 2, "neumann", 0, 4, 1.0, st)
+    # Neumann clamps: sum_i |i - min(i+h, n-1)| / n
+    for h in range(4):
+        expect = sum(abs(i - min(i + h, n - 1)) for i in range(n)) / n
+        assert out[0, h] == pytest.approx(expect, rel=1e-15)
+    per = c_oracle.structure_basic(1, (n,), 2, "periodic", 0, 4, 2.0, st)
+    for h in range(4):
+        expect = sum((i - (i + h) % n) ** 2 for i in range(n)) / n
+        assert per[0, h] == pytest.approx(expect, rel=1e-15)
