@@ -1,6 +1,7 @@
 // C ABI of the MLP surrogate (include/als_surrogate.h): parameter layout,
 // workspaces, the training step as one captured CUDA graph, inference in
 // row chunks.  The kernels are in mlp_kernels.cuh / mlp_tc.cuh.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -20,7 +21,7 @@ using namespace mlpk;
 
 namespace {
 
-constexpr long long kInferChunk = 32768;   // rows per inference chunk (multiple of 128)
+constexpr long long kInferChunk = 65536;   // rows per inference chunk (multiple of 128)
 
 int mlp_fail(int code, const std::string& msg) {
     return als::report_error(code, msg.c_str());
@@ -72,6 +73,10 @@ struct als_mlp {
     // inference workspace (kInferChunk rows)
     __nv_bfloat16* xi = nullptr;
     __nv_bfloat16* hi[2] = {nullptr, nullptr};
+    // tensor maps of the inference operands (width 256): packed inputs, the
+    // two activation buffers, every hidden weight matrix
+    bool tma = false;
+    CUtensorMap tm_x, tm_h[2], tm_w[6];
     std::vector<void*> allocations;
 };
 
@@ -118,13 +123,73 @@ Operand columns_of(const __nv_bfloat16* p, long long ld) {
     return Operand{p, 1, ld};
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// BF16 matrix rows x cols (row-major, cols contiguous) as a 2-D tensor map
+// with a box of box_rows x 64 elements and 128-byte swizzle.
+int encode_bf16_map(CUtensorMap* map, const void* base, long long rows, int cols, int box_rows) {
+    static EncodeTiledFn encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+            return mlp_fail(ALS_E_CUDA, "cuTensorMapEncodeTiled is not available");
+        }
+        encode = reinterpret_cast<EncodeTiledFn>(fn);
+    }
+    const cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+    const cuuint64_t strides[1] = {cuuint64_t(cols) * 2};
+    const cuuint32_t box[2] = {cuuint32_t(kChunkK), cuuint32_t(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
+                              dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        return mlp_fail(ALS_E_CUDA, "cuTensorMapEncodeTiled failed");
+    }
+    return ALS_OK;
+}
+
+// Tensor maps of the inference path; only the 256-wide network with K of 64
+// (inputs) and 256 (hidden) takes it.
+int setup_tma(als_mlp* s) {
+    s->tma = false;
+    if (s->cfg.width != 256 || s->layers[0].kpad != 64) {
+        return ALS_OK;
+    }
+    MLP_TRY(encode_bf16_map(&s->tm_x, s->xi, kInferChunk, 64, kTileM));
+    MLP_TRY(encode_bf16_map(&s->tm_h[0], s->hi[0], kInferChunk, 256, kTileM));
+    MLP_TRY(encode_bf16_map(&s->tm_h[1], s->hi[1], kInferChunk, 256, kTileM));
+    for (int l = 0; l < s->cfg.hidden; ++l) {
+        MLP_TRY(encode_bf16_map(&s->tm_w[l], s->layers[l].wb, 256, s->layers[l].kpad, 256));
+    }
+    s->tma = true;
+    return ALS_OK;
+}
+
+template <int NK, bool HEAD>
+int launch_tma_forward(const CUtensorMap& a, const CUtensorMap& b, const GemmArgs& g,
+                       const float* head_w, const float* head_b, float* y, long long rows_valid,
+                       cudaStream_t st) {
+    gemm_tma_forward<NK, HEAD><<<g.M / kTileM, kTmaThreads, gemm_tma_smem_bytes<NK>(), st>>>(
+        a, b, g, head_w, head_b, y, rows_valid);
+    MLP_CUDA(cudaGetLastError());
+    return ALS_OK;
+}
+
 // Forward pass of `rows_pad` rows (multiple of 128) from packed inputs `x`
 // through the hidden layers into `hout` (the last activation), storing
 // pre-activations when `zs` is given (training), ping-ponging `hbuf`
 // otherwise (inference).
 int forward_hidden(als_mlp* s, const __nv_bfloat16* x, long long rows_pad,
                    const std::vector<float*>* zs, const std::vector<__nv_bfloat16*>* hs,
-                   __nv_bfloat16* const* hbuf, const __nv_bfloat16** hout, cudaStream_t st) {
+                   __nv_bfloat16* const* hbuf, const __nv_bfloat16** hout, cudaStream_t st,
+                   float* y_fused = nullptr, long long rows_valid = 0) {
     const int nh = s->cfg.hidden;
     const __nv_bfloat16* in = x;
     long long ld_in = s->layers[0].kpad;
@@ -144,7 +209,23 @@ int forward_hidden(als_mlp* s, const __nv_bfloat16* x, long long rows_pad,
         a.error = s->error;
         // training batches: narrow N tiles for more CTAs; inference: the
         // whole layer width per CTA, so each activation tile is read once
-        if (zs || L.out % 128 != 0) {
+        if (!zs && s->tma) {
+            // inference, 256 wide: TMA-fed tiles (K = 64 inputs, K = 256
+            // hidden); the last layer also applies the output head when the
+            // caller passes y_fused
+            const CUtensorMap& ta = l == 0 ? s->tm_x : s->tm_h[(l - 1) & 1];
+            const Layer& head = s->layers[nh];
+            const bool fuse = y_fused && l == nh - 1;
+            const float* hw = s->p + head.w_off;
+            const float* hb = s->p + head.b_off;
+            if (L.kpad == 64) {
+                MLP_TRY(fuse ? (launch_tma_forward<1, true>(ta, s->tm_w[l], a, hw, hb, y_fused, rows_valid, st))
+                             : (launch_tma_forward<1, false>(ta, s->tm_w[l], a, hw, hb, nullptr, 0, st)));
+            } else {
+                MLP_TRY(fuse ? (launch_tma_forward<4, true>(ta, s->tm_w[l], a, hw, hb, y_fused, rows_valid, st))
+                             : (launch_tma_forward<4, false>(ta, s->tm_w[l], a, hw, hb, nullptr, 0, st)));
+            }
+        } else if (zs || L.out % 128 != 0) {
             MLP_TRY((launch_gemm<64, EPI_FORWARD>(a, L.out, st)));
         } else if (L.out % 256 != 0) {
             MLP_TRY((launch_gemm<128, EPI_FORWARD>(a, L.out, st)));
@@ -191,7 +272,7 @@ int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, floa
     const long long rp = round_up(rows, kTileM);
     const Layer& L0 = s->layers[0];
     const Layer& head = s->layers[nh];
-    pack_inputs<<<grid_for(rp * L0.kpad, 256), 256, 0, st>>>(x, rows, s->cfg.inputs, s->xb, rp,
+    pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, st>>>(x, rows, s->cfg.inputs, s->xb, rp,
                                                              L0.kpad);
     MLP_CUDA(cudaGetLastError());
     const __nv_bfloat16* last = nullptr;
@@ -273,6 +354,14 @@ int configure_one() {
 // Dynamic shared memory limits of every GEMM instantiation, set on the
 // current device before any launch (and before any graph capture).
 int configure_kernels() {
+    MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<1, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<1>()));
+    MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<1, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<1>()));
+    MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<4, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<4>()));
+    MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<4, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<4>()));
     MLP_TRY((configure_one<64, EPI_FORWARD>()));
     MLP_TRY((configure_one<128, EPI_FORWARD>()));
     MLP_TRY((configure_one<256, EPI_FORWARD>()));
@@ -359,6 +448,7 @@ int als_mlp_create(const als_mlp_config* cfg, int device, als_mlp** out) {
         return cleanup(rc);
     }
     rc = configure_kernels();
+    rc = rc ? rc : setup_tma(s);
     if (rc) {
         return cleanup(rc);
     }
@@ -450,14 +540,17 @@ int als_mlp_forward(als_mlp* s, const float* x_dev, long long rows, float* y_dev
     for (long long r0 = 0; r0 < rows; r0 += kInferChunk) {
         const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
         const long long rp = (n + kTileM - 1) / kTileM * kTileM;
-        pack_inputs<<<grid_for(rp * L0.kpad, 256), 256, 0, st>>>(
+        pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, st>>>(
             x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, s->xi, rp, L0.kpad);
         MLP_CUDA(cudaGetLastError());
         const __nv_bfloat16* last = nullptr;
-        MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st));
-        head_forward<<<grid_for(n * 32, 256), 256, 0, st>>>(last, s->cfg.width, s->p + head.w_off,
-                                                            s->p + head.b_off, n, y_dev + r0);
-        MLP_CUDA(cudaGetLastError());
+        MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st,
+                               s->tma ? y_dev + r0 : nullptr, n));
+        if (!s->tma) {
+            head_forward<<<grid_for(n * 32, 256), 256, 0, st>>>(last, s->cfg.width,
+                s->p + head.w_off, s->p + head.b_off, n, y_dev + r0);
+            MLP_CUDA(cudaGetLastError());
+        }
     }
     return check_error_flag(s);
 }

@@ -3,6 +3,8 @@
 // output head, its loss and backward, column sums for bias gradients, Adam).
 #pragma once
 
+#include <cuda.h>
+
 #include "mlp_tc.cuh"
 
 namespace mlpk {
@@ -157,16 +159,152 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
     }
 }
 
-// x (rows x nin, FP32) -> xb (rows_pad x kpad, BF16), zero padded.
+// Inference forward layer through TMA: H_out = bf16(gelu(H_in W^T + b)) for
+// a 128 x 256 tile, K = 64 * NK (NK <= 4).  Every K chunk has its own
+// shared-memory stage (48 KB: A 128 x 64, B 256 x 64, both SWIZZLE_128B),
+// so thread 0 issues all TMA loads at once, then the MMAs of each chunk as
+// its stage lands, then one commit.  Sixteen warps share the epilogue: warp
+// w reads TMEM lane quarter w % 4 (the rows it may access) and columns
+// 64 (w / 4) .. 64 (w / 4) + 63.  With HEAD the last hidden layer also
+// applies the 256 -> 1 output layer: y = sum_n bf16(gelu(z_n)) w_n + b,
+// partial sums per column group combined through shared memory, so the
+// last activation never goes to memory.
+constexpr int kTmaThreads = 512;
+
+template <int NK>
+constexpr int gemm_tma_smem_bytes() {
+    return NK * (kTileM * kChunkK * 2 + 256 * kChunkK * 2) + 1024;
+}
+
+template <int NK, bool HEAD>
+__global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB,
+                                                                GemmArgs g, const float* head_w,
+                                                                const float* head_b, float* y,
+                                                                long long rows_valid) {
+    constexpr int BN = 256;
+    constexpr uint32_t kABytes = kTileM * kChunkK * 2;
+    constexpr uint32_t kBBytes = BN * kChunkK * 2;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t full[NK];
+    __shared__ uint64_t done;
+    __shared__ uint32_t tmem_base;
+    __shared__ float head_part[4][kTileM];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kTileM;
+    if (warp == 0) {
+        tmem_alloc(&tmem_base, BN);
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < NK; ++c) {
+            mbar_init(&full[c], 1);
+        }
+        mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < NK; ++c) {
+            unsigned char* sa = base + c * (kABytes + kBBytes);
+            mbar_expect_tx(&full[c], kABytes + kBBytes);
+            tma_load_2d(sa, &tmA, c * kChunkK, m0, &full[c]);
+            tma_load_2d(sa + kABytes, &tmB, c * kChunkK, 0, &full[c]);
+        }
+        const uint32_t idesc = instr_desc_bf16(kTileM, BN);
+        int issued = 0;
+        for (int c = 0; c < NK; ++c) {
+            if (!mbar_wait(&full[c], 0)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(base + c * (kABytes + kBBytes));
+            const uint32_t b0 = a0 + kABytes;
+#pragma unroll
+            for (int j = 0; j < kChunkK / 16; ++j) {
+                mma_bf16(tmem, smem_desc_sw128(a0 + j * 32), smem_desc_sw128(b0 + j * 32), idesc,
+                         (c > 0 || j > 0) ? 1u : 0u);
+            }
+            issued = c + 1;
+        }
+        if (!ok) {
+            // the loads that did land must not be overwritten mid-flight:
+            // wait (bounded) for the rest before the block leaves
+            for (int c = issued; c < NK; ++c) {
+                mbar_wait(&full[c], 0);
+            }
+        }
+        mma_commit(&done);
+    }
+    ok = mbar_wait(&done, 0) && ok;
+    const bool failed = __syncthreads_or(!ok);
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(g.error, 1);
+        }
+    } else {
+        tc_fence_after();
+        const int quarter = warp & 3;
+        const int cg = warp >> 2;
+        const int row = quarter * 32 + lane;
+        const long long m = m0 + row;
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16);
+        float hsum = 0.0f;
+#pragma unroll 1
+        for (int c0 = cg * 64; c0 < cg * 64 + 64; c0 += 16) {
+            float v[16];
+            tmem_load16(lane_base + uint32_t(c0), v);
+            if (HEAD) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float h = __bfloat162float(__float2bfloat16_rn(gelu(v[i] + g.bias[c0 + i])));
+                    hsum += h * head_w[c0 + i];
+                }
+            } else {
+                epilogue16<BN, EPI_FORWARD>(g, m, c0, v, BN);
+            }
+        }
+        if (HEAD) {
+            head_part[cg][row] = hsum;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (HEAD && !failed && threadIdx.x < kTileM && m0 + threadIdx.x < rows_valid) {
+        const int row = threadIdx.x;
+        y[m0 + row] = ((head_part[0][row] + head_part[1][row]) + (head_part[2][row] +
+                       head_part[3][row])) + head_b[0];
+    }
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free(tmem, BN);
+    }
+}
+
+// x (rows x nin, FP32) -> xb (rows_pad x kpad, BF16), zero padded; one
+// 16-byte store of 8 values per work item.
 __global__ void pack_inputs(const float* __restrict__ x, long long rows, int nin,
                             __nv_bfloat16* __restrict__ xb, long long rows_pad, int kpad) {
-    const long long total = rows_pad * kpad;
+    const int groups = kpad >> 3;
+    const long long total = rows_pad * groups;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long r = i / kpad;
-        const int k = int(i - r * kpad);
-        const float v = (r < rows && k < nin) ? x[r * nin + k] : 0.0f;
-        xb[i] = __float2bfloat16_rn(v);
+        const long long r = i / groups;
+        const int k0 = int(i - r * groups) * 8;
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int k = k0 + j;
+            v[j] = __float2bfloat16_rn((r < rows && k < nin) ? x[r * nin + k] : 0.0f);
+        }
+        *reinterpret_cast<uint4*>(xb + r * kpad + k0) = *reinterpret_cast<const uint4*>(v);
     }
 }
 

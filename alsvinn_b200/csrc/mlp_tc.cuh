@@ -52,15 +52,27 @@ struct GemmArgs {
     int* error;                 // set to 1 when a wait gave up
 };
 
+// GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear Units",
+// 2016): gelu(z) = z/2 (1 + tanh(k (z + a z^3))), k = sqrt(2/pi), a = 0.044715,
+// with the hardware tanh (tanh.approx.f32, relative error about 2^-11, below
+// the BF16 resolution of the activations it produces).
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ float gelu(float z) {
-    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+    const float u = 0.79788456080286536f * (z + 0.044715f * z * z * z);
+    return 0.5f * z * (1.0f + tanh_hw(u));
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
-    // d/dz [z Phi(z)] = Phi(z) + z phi(z)
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+    // d/dz: (1 + t)/2 + z/2 (1 - t^2) k (1 + 3 a z^2), t = tanh(u)
+    const float u = 0.79788456080286536f * (z + 0.044715f * z * z * z);
+    const float t = tanh_hw(u);
+    return 0.5f * (1.0f + t) +
+        0.5f * z * (1.0f - t * t) * 0.79788456080286536f * (1.0f + 0.134145f * z * z);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -160,6 +172,32 @@ __device__ __forceinline__ void tmem_load16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) {
         v[i] = __uint_as_float(r[i]);
     }
+}
+
+// --- TMA (inference path): operands land in shared memory through
+// cp.async.bulk.tensor with 128-byte swizzle, the canonical K-major
+// SWIZZLE_128B UMMA layout (8 rows x 128 bytes per atom, atoms 1024 bytes
+// apart); a K = 16 step advances the descriptor start by 32 bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t(1) << 16) |
+        (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// 2-D tiled TMA load of box (x = innermost coordinate in elements, y = row)
+// into shared memory, completion counted on `bar`.  No multicast.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y),
+          "r"(smem_u32(bar))
+        : "memory");
 }
 
 // Byte offset of element (r, k) of a staged rows x 64 chunk.

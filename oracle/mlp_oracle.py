@@ -6,7 +6,7 @@ file restates the network's mathematics in NumPy FP64:
 
     H_0 = x,  Z_l = H_{l-1} W_l^T + b_l,  H_l = gelu(Z_l)  (l = 1..hidden),
     y = H_hidden w + b,  loss = (1/B) sum_r (y_r - t_r)^2,
-    gelu(z) = z Phi(z),  gelu'(z) = Phi(z) + z phi(z),
+    gelu(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))  (tanh form),
 
 with back-propagation written out by hand.  ``bf16=True`` rounds at the
 same points as the GPU path (inputs, hidden weight matrices, activations
@@ -16,10 +16,6 @@ parameter layout is the one of include/als_surrogate.h: per layer the
 weight matrix (out x in, row-major) then the bias.
 """
 import numpy as np
-from scipy.special import erf
-
-SQRT1_2 = 0.70710678118654752
-INV_SQRT_2PI = 0.39894228040143268
 
 
 def bf16(a):
@@ -30,12 +26,18 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+K_GELU = 0.79788456080286536   # sqrt(2/pi)
+A_GELU = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z * SQRT1_2))
+    """GELU, tanh form (Hendrycks and Gimpel 2016)."""
+    return 0.5 * z * (1.0 + np.tanh(K_GELU * (z + A_GELU * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z * SQRT1_2)) + z * INV_SQRT_2PI * np.exp(-0.5 * z * z)
+    t = np.tanh(K_GELU * (z + A_GELU * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * K_GELU * (1.0 + 3.0 * A_GELU * z * z)
 
 
 def layer_shapes(inputs, width, hidden):
