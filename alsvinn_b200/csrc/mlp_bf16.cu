@@ -176,8 +176,15 @@ template <int NK, bool HEAD>
 int launch_tma_forward(const CUtensorMap& a, const CUtensorMap& b, const GemmArgs& g,
                        const float* head_w, const float* head_b, float* y, long long rows_valid,
                        cudaStream_t st) {
-    gemm_tma_forward<NK, HEAD><<<g.M / kTileM, kTmaThreads, gemm_tma_smem_bytes<NK>(), st>>>(
-        a, b, g, head_w, head_b, y, rows_valid);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        MLP_CUDA(cudaGetDevice(&dev));
+        MLP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int tiles = g.M / kTileM;
+    gemm_tma_forward<NK, HEAD><<<tiles < sms ? tiles : sms, kTmaThreads, gemm_tma_smem_bytes(),
+                                 st>>>(a, b, g, head_w, head_b, y, rows_valid);
     MLP_CUDA(cudaGetLastError());
     return ALS_OK;
 }
@@ -355,13 +362,13 @@ int configure_one() {
 // current device before any launch (and before any graph capture).
 int configure_kernels() {
     MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<1, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<1>()));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
     MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<1, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<1>()));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
     MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<4, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<4>()));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
     MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<4, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes<4>()));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
     MLP_TRY((configure_one<64, EPI_FORWARD>()));
     MLP_TRY((configure_one<128, EPI_FORWARD>()));
     MLP_TRY((configure_one<256, EPI_FORWARD>()));

@@ -159,21 +159,37 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
     }
 }
 
-// Inference forward layer through TMA: H_out = bf16(gelu(H_in W^T + b)) for
-// a 128 x 256 tile, K = 64 * NK (NK <= 4).  Every K chunk has its own
-// shared-memory stage (48 KB: A 128 x 64, B 256 x 64, both SWIZZLE_128B),
-// so thread 0 issues all TMA loads at once, then the MMAs of each chunk as
-// its stage lands, then one commit.  Sixteen warps share the epilogue: warp
-// w reads TMEM lane quarter w % 4 (the rows it may access) and columns
-// 64 (w / 4) .. 64 (w / 4) + 63.  With HEAD the last hidden layer also
-// applies the 256 -> 1 output layer: y = sum_n bf16(gelu(z_n)) w_n + b,
-// partial sums per column group combined through shared memory, so the
-// last activation never goes to memory.
-constexpr int kTmaThreads = 512;
+// Inference forward layer, persistent and warp-specialised:
+// H_out = bf16(gelu(H_in W^T + b)) over 128 x 256 tiles, K = 64 * NK (NK <= 4).
+//   warp 0  TMA producer: the whole weight matrix once into shared memory
+//           (NK x 32 KB, resident for every tile), then the activation
+//           chunks (128 x 64, 16 KB) through a ring of kRing stages;
+//   warp 1  MMA issuer: per tile, NK x 4 tcgen05.mma into one of two TMEM
+//           accumulators (2 x 256 columns), tcgen05.commit freeing each ring
+//           stage and finally marking the accumulator full;
+//   warps 4..19  epilogue: warp w reads TMEM lane quarter w % 4 and 64
+//           columns, applies bias + GELU and stores BF16 (or, with HEAD,
+//           folds the 256 -> 1 output layer in), then releases the
+//           accumulator, so the epilogue of tile i overlaps the MMAs of i+1.
+// All operands are 128-byte swizzled (the canonical K-major SWIZZLE_128B
+// UMMA layout).  Every wait is bounded; a timeout sets the error flag and
+// the roles drain and return.
+constexpr int kTmaThreads = 640;
+constexpr int kRing = 4;
+constexpr int kEpiWarp0 = 4;
 
-template <int NK>
+// Dynamic shared memory of every instantiation: the NK = 4 footprint, so that
+// one block per SM owns all 512 TMEM columns whatever NK is.
 constexpr int gemm_tma_smem_bytes() {
-    return NK * (kTileM * kChunkK * 2 + 256 * kChunkK * 2) + 1024;
+    return 4 * 256 * kChunkK * 2 + kRing * kTileM * kChunkK * 2 + 1024;
+}
+
+__device__ __forceinline__ void named_barrier_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 template <int NK, bool HEAD>
@@ -183,108 +199,175 @@ __global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_con
                                                                 const float* head_b, float* y,
                                                                 long long rows_valid) {
     constexpr int BN = 256;
-    constexpr uint32_t kABytes = kTileM * kChunkK * 2;
-    constexpr uint32_t kBBytes = BN * kChunkK * 2;
+    constexpr uint32_t kABytes = kTileM * kChunkK * 2;   // one ring stage
+    constexpr uint32_t kBBytes = BN * kChunkK * 2;       // one K chunk of the weights
     extern __shared__ unsigned char smem_raw[];
-    __shared__ uint64_t full[NK];
-    __shared__ uint64_t done;
+    __shared__ uint64_t b_full;
+    __shared__ uint64_t a_full[kRing];
+    __shared__ uint64_t a_empty[kRing];
+    __shared__ uint64_t t_full[2];
+    __shared__ uint64_t t_empty[2];
+    __shared__ uint64_t drain;
     __shared__ uint32_t tmem_base;
-    __shared__ float head_part[4][kTileM];
+    __shared__ int abort_flag;
+    __shared__ float head_part[2][4][kTileM];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sB = base;                       // NK x 32 KB
+    unsigned char* sA = base + NK * kBBytes;        // kRing x 16 KB
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kTileM;
+    const int tiles = g.M / kTileM;
     if (warp == 0) {
-        tmem_alloc(&tmem_base, BN);
+        tmem_alloc(&tmem_base, 2 * BN);
     }
     if (threadIdx.x == 0) {
-        for (int c = 0; c < NK; ++c) {
-            mbar_init(&full[c], 1);
+        mbar_init(&b_full, 1);
+        for (int r = 0; r < kRing; ++r) {
+            mbar_init(&a_full[r], 1);
+            mbar_init(&a_empty[r], 1);
         }
-        mbar_init(&done, 1);
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&t_full[k], 1);
+            mbar_init(&t_empty[k], 16);      // one arrival per epilogue warp
+        }
+        mbar_init(&drain, 1);
+        abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
-    bool ok = true;
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < NK; ++c) {
-            unsigned char* sa = base + c * (kABytes + kBBytes);
-            mbar_expect_tx(&full[c], kABytes + kBBytes);
-            tma_load_2d(sa, &tmA, c * kChunkK, m0, &full[c]);
-            tma_load_2d(sa + kABytes, &tmB, c * kChunkK, 0, &full[c]);
+    volatile int* abort_v = &abort_flag;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // the weights, once
+            mbar_expect_tx(&b_full, NK * kBBytes);
+            for (int c = 0; c < NK; ++c) {
+                tma_load_2d(sB + c * kBBytes, &tmB, c * kChunkK, 0, &b_full);
+            }
+            long long it = 0;
+            for (int t = blockIdx.x; t < tiles && !*abort_v; t += gridDim.x) {
+                for (int c = 0; c < NK; ++c, ++it) {
+                    const int slot = int(it % kRing);
+                    if (it >= kRing && !mbar_wait(&a_empty[slot], unsigned((it / kRing - 1) & 1))) {
+                        *abort_v = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&a_full[slot], kABytes);
+                    tma_load_2d(sA + slot * kABytes, &tmA, c * kChunkK, t * kTileM, &a_full[slot]);
+                }
+            }
         }
-        const uint32_t idesc = instr_desc_bf16(kTileM, BN);
-        int issued = 0;
-        for (int c = 0; c < NK; ++c) {
-            if (!mbar_wait(&full[c], 0)) {
-                ok = false;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc_bf16(kTileM, BN);
+            bool ok = mbar_wait(&b_full, 0);
+            long long it = 0;
+            int lt = 0;
+            for (int t = blockIdx.x; ok && t < tiles && !*abort_v; t += gridDim.x, ++lt) {
+                const int acc = lt & 1;
+                if (lt >= 2 && !mbar_wait(&t_empty[acc], unsigned(((lt >> 1) - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int c = 0; c < NK; ++c, ++it) {
+                    const int slot = int(it % kRing);
+                    if (!mbar_wait(&a_full[slot], unsigned((it / kRing) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(sA + slot * kABytes);
+                    const uint32_t b0 = smem_u32(sB + c * kBBytes);
+#pragma unroll
+                    for (int j = 0; j < kChunkK / 16; ++j) {
+                        mma_bf16(tmem + uint32_t(acc * BN), smem_desc_sw128(a0 + j * 32),
+                                 smem_desc_sw128(b0 + j * 32), idesc, (c > 0 || j > 0) ? 1u : 0u);
+                    }
+                    mma_commit(&a_empty[slot]);
+                }
+                if (!ok) {
+                    break;
+                }
+                mma_commit(&t_full[acc]);
+            }
+            if (!ok) {
+                *abort_v = 1;
+            }
+            // every MMA this thread issued is complete before TMEM is freed
+            mma_commit(&drain);
+            mbar_wait(&drain, 0);
+        }
+    } else if (warp >= kEpiWarp0) {
+        const int ew = warp - kEpiWarp0;          // 0..15
+        const int quarter = warp & 3;
+        const int cg = ew >> 2;
+        const int row = quarter * 32 + lane;
+        int lt = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++lt) {
+            const int acc = lt & 1;
+            bool ok = !*abort_v && mbar_wait(&t_full[acc], unsigned((lt >> 1) & 1));
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) {
+                *abort_v = 1;
+            }
+            float hsum = 0.0f;
+            if (ok) {
+                tc_fence_after();
+                const long long m = (long long)t * kTileM + row;
+                const uint32_t lane_base = tmem + uint32_t(acc * BN) + (uint32_t(quarter * 32) << 16);
+#pragma unroll 1
+                for (int c0 = cg * 64; c0 < cg * 64 + 64; c0 += 16) {
+                    float v[16];
+                    tmem_load16(lane_base + uint32_t(c0), v);
+                    if (HEAD) {
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const float h =
+                                __bfloat162float(__float2bfloat16_rn(gelu(v[i] + g.bias[c0 + i])));
+                            hsum += h * head_w[c0 + i];
+                        }
+                    } else {
+                        epilogue16<BN, EPI_FORWARD>(g, m, c0, v, BN);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&t_empty[acc]);
+                }
+            }
+            if (HEAD) {
+                head_part[acc][cg][row] = hsum;
+                named_barrier_sync(1, 16 * 32);
+                const int et = ew * 32 + lane;       // 0..511
+                if (ok && et < kTileM) {
+                    const long long m = (long long)t * kTileM + et;
+                    if (m < rows_valid) {
+                        y[m] = ((head_part[acc][0][et] + head_part[acc][1][et]) +
+                                (head_part[acc][2][et] + head_part[acc][3][et])) + head_b[0];
+                    }
+                }
+            }
+            // with HEAD every epilogue warp passes the named barrier once per
+            // tile of this block, aborted or not; without it a warp may leave
+            if (!HEAD && !ok) {
                 break;
             }
-            tc_fence_after();
-            const uint32_t a0 = smem_u32(base + c * (kABytes + kBBytes));
-            const uint32_t b0 = a0 + kABytes;
-#pragma unroll
-            for (int j = 0; j < kChunkK / 16; ++j) {
-                mma_bf16(tmem, smem_desc_sw128(a0 + j * 32), smem_desc_sw128(b0 + j * 32), idesc,
-                         (c > 0 || j > 0) ? 1u : 0u);
-            }
-            issued = c + 1;
-        }
-        if (!ok) {
-            // the loads that did land must not be overwritten mid-flight:
-            // wait (bounded) for the rest before the block leaves
-            for (int c = issued; c < NK; ++c) {
-                mbar_wait(&full[c], 0);
-            }
-        }
-        mma_commit(&done);
-    }
-    ok = mbar_wait(&done, 0) && ok;
-    const bool failed = __syncthreads_or(!ok);
-    if (failed) {
-        if (threadIdx.x == 0) {
-            atomicExch(g.error, 1);
-        }
-    } else {
-        tc_fence_after();
-        const int quarter = warp & 3;
-        const int cg = warp >> 2;
-        const int row = quarter * 32 + lane;
-        const long long m = m0 + row;
-        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16);
-        float hsum = 0.0f;
-#pragma unroll 1
-        for (int c0 = cg * 64; c0 < cg * 64 + 64; c0 += 16) {
-            float v[16];
-            tmem_load16(lane_base + uint32_t(c0), v);
-            if (HEAD) {
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float h = __bfloat162float(__float2bfloat16_rn(gelu(v[i] + g.bias[c0 + i])));
-                    hsum += h * head_w[c0 + i];
-                }
-            } else {
-                epilogue16<BN, EPI_FORWARD>(g, m, c0, v, BN);
-            }
-        }
-        if (HEAD) {
-            head_part[cg][row] = hsum;
         }
     }
-    tc_fence_before();
     __syncthreads();
-    if (HEAD && !failed && threadIdx.x < kTileM && m0 + threadIdx.x < rows_valid) {
-        const int row = threadIdx.x;
-        y[m0 + row] = ((head_part[0][row] + head_part[1][row]) + (head_part[2][row] +
-                       head_part[3][row])) + head_b[0];
+    if (threadIdx.x == 0 && *abort_v) {
+        atomicExch(g.error, 1);
     }
     if (warp == 0) {
+        __syncwarp();
         tc_fence_after();
-        tmem_free(tmem, BN);
+        tmem_free(tmem, 2 * BN);
     }
 }
 
