@@ -8,6 +8,7 @@
 //   HLL3                     alsfvm/include/alsfvm/numflux/euler/HLL3.hpp:52-149
 //   Central                  alsfvm/include/alsfvm/numflux/Central.hpp:39-56
 //   WENO2                    alsfvm/include/alsfvm/reconstruction/WENO2.hpp:31-91
+//   MC, MM                   alsfvm/include/alsfvm/reconstruction/MC.hpp, MM.hpp, minmod.hpp
 //   ENO2/3/4                 alsfvm/src/reconstruction/ENOCPU.cpp:41-267,
 //                            alsfvm/src/reconstruction/ENOCoefficients.cpp:27-49
 // Only the velocity component along the face normal is formed: the
@@ -18,11 +19,13 @@
 
 namespace als {
 
-enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4 };
+enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4,
+             RECON_MC = 5, RECON_MM = 6 };
 enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2 };
 
 __host__ __device__ constexpr int recon_ghosts(int recon) {
-    return recon == RECON_NONE ? 1 : (recon == RECON_WENO2 || recon == RECON_ENO2) ? 2
+    return recon == RECON_NONE ? 1
+        : (recon == RECON_WENO2 || recon == RECON_ENO2 || recon == RECON_MC || recon == RECON_MM) ? 2
         : (recon == RECON_ENO3 ? 3 : 4);
 }
 
@@ -241,6 +244,25 @@ __device__ __forceinline__ R twice_reciprocal(R d, R recip) {
     return out;
 }
 
+// sign and minmod (alsfvm/include/alsfvm/reconstruction/sign.hpp,
+// minmod.hpp): sign is 1, 0 or -1; minmod is sign(a) times the smallest
+// magnitude when all signs agree, else 0.
+template<class R>
+__device__ __forceinline__ R sign_of(R a) {
+    return a > R(0) ? R(1) : (a == R(0) ? R(0) : R(-1));
+}
+
+template<class R>
+__device__ __forceinline__ R minmod2(R a, R b) {
+    return sign_of(a) == sign_of(b) ? sign_of(a) * fmin(fabs(a), fabs(b)) : R(0);
+}
+
+template<class R>
+__device__ __forceinline__ R minmod3(R a, R b, R c) {
+    return (sign_of(a) == sign_of(b) && sign_of(b) == sign_of(c))
+        ? sign_of(a) * fmin(fabs(a), fmin(fabs(b), fabs(c))) : R(0);
+}
+
 template<class R, int NV, int RECON, class Fetch>
 __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right) {
     if (RECON == RECON_NONE) {
@@ -275,6 +297,22 @@ __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right)
             const R up = f.at(v, 1);
             left[v] = R(0.5) * (w1Left * um + cl * u0 - w0Left * up);
             right[v] = R(0.5) * (w0Right * up + cr * u0 - w1Right * um);
+        }
+    } else if (RECON == RECON_MC || RECON == RECON_MM) {
+        // MC.hpp:30-50 / MM.hpp:29-48, per variable
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const R l = f.at(v, -1);
+            const R m = f.at(v, 0);
+            const R r = f.at(v, 1);
+            R sigma;
+            if (RECON == RECON_MC) {
+                sigma = minmod3(R(2) * (r - m), (r - l) / R(2), R(2) * (m - l));
+            } else {
+                sigma = minmod2(r - m, m - l);
+            }
+            left[v] = m - sigma / R(2);
+            right[v] = m + sigma / R(2);
         }
     } else {
         constexpr int ORDER = RECON == RECON_ENO2 ? 2 : (RECON == RECON_ENO3 ? 3 : 4);

@@ -87,6 +87,8 @@ cudaError_t launch_stage_dim(int recon, int flux, int kind, const StageParams& P
     case RECON_ENO2: return launch_stage_flux<R, DIM, RECON_ENO2>(flux, kind, P, b, s);
     case RECON_ENO3: return launch_stage_flux<R, DIM, RECON_ENO3>(flux, kind, P, b, s);
     case RECON_ENO4: return launch_stage_flux<R, DIM, RECON_ENO4>(flux, kind, P, b, s);
+    case RECON_MC: return launch_stage_flux<R, DIM, RECON_MC>(flux, kind, P, b, s);
+    case RECON_MM: return launch_stage_flux<R, DIM, RECON_MM>(flux, kind, P, b, s);
     default: return cudaErrorInvalidValue;
     }
 }

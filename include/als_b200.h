@@ -41,6 +41,8 @@ extern "C" {
 #define ALS_RECON_ENO2 2            /* "eno2",  reconstruction/ENOCPU.cpp */
 #define ALS_RECON_ENO3 3            /* "eno3" */
 #define ALS_RECON_ENO4 4            /* "eno4" */
+#define ALS_RECON_MC 5              /* "mc", reconstruction/MC.hpp */
+#define ALS_RECON_MM 6              /* "mm", reconstruction/MM.hpp */
 #define ALS_INT_FORWARD_EULER 0     /* "forwardeuler", integrator/ForwardEuler.cpp */
 #define ALS_INT_RK2 1               /* "rungekutta2",  integrator/RungeKutta2.cpp */
 #define ALS_INT_RK3 2               /* "rungekutta3",  integrator/RungeKutta3.cpp */

@@ -204,6 +204,8 @@ int orc_ghost_cells(int flux, int recon) {
     case ORC_RECON_ENO2: rg = 2; break;
     case ORC_RECON_ENO3: rg = 3; break;
     case ORC_RECON_ENO4: rg = 4; break;
+    case ORC_RECON_MC: rg = 2; break;
+    case ORC_RECON_MM: rg = 2; break;
     default: return -1;
     }
     return rg > 1 ? rg : 1;
@@ -332,6 +334,24 @@ static double eno_coef(int order, int r, int j) {
     }
 }
 
+static double sign_of(double a) {
+    return a > 0 ? 1.0 : (a == 0 ? 0.0 : -1.0);
+}
+
+static double minmod2(double a, double b) {
+    if (sign_of(a) == sign_of(b)) {
+        return sign_of(a) * fmin(fabs(a), fabs(b));
+    }
+    return 0;
+}
+
+static double minmod3(double a, double b, double c) {
+    if (sign_of(a) == sign_of(b) && sign_of(b) == sign_of(c)) {
+        return sign_of(a) * fmin(fabs(a), fmin(fabs(b), fabs(c)));
+    }
+    return 0;
+}
+
 /* Reconstructs cell c (index into the planes) along stride s.
  * left/right receive nvar values. */
 static void reconstruct_cell(const orc_config* cfg, const double* in, long plane,
@@ -361,6 +381,18 @@ static void reconstruct_cell(const orc_config* cfg, const double* in, long plane
             const double up = in[var * plane + c + s];
             left[var] = 0.5 * (w1Left * um + (3 * w0Left + w1Left) * u0 - w0Left * up);
             right[var] = 0.5 * (w0Right * up + (3 * w1Right + w0Right) * u0 - w1Right * um);
+        }
+    } else if (cfg->recon == ORC_RECON_MC || cfg->recon == ORC_RECON_MM) {
+        /* MC.hpp:30-50 / MM.hpp:29-48 with minmod.hpp, sign.hpp, per variable */
+        for (var = 0; var < nvar; ++var) {
+            const double l = in[var * plane + c - s];
+            const double m = in[var * plane + c];
+            const double r = in[var * plane + c + s];
+            const double sigma = cfg->recon == ORC_RECON_MC
+                ? minmod3(2 * (r - m), (r - l) / 2, 2 * (m - l))
+                : minmod2(r - m, m - l);
+            left[var] = m - sigma / 2;
+            right[var] = m + sigma / 2;
         }
     } else {
         /* ENOCPU.cpp:140-180.  Level-l undivided differences of rho:

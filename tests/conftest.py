@@ -51,12 +51,13 @@ def load_golden(name):
 
 def flux_cases():
     rows = []
-    with open(os.path.join(GOLDEN, "compute_flux_cases.txt")) as f:
-        for line in f:
-            if line.startswith("#"):
-                continue
-            p = line.split()
-            rows.append({"dim": int(p[0]), "n": tuple(int(v) for v in p[1].split(",")),
-                         "recon": p[2], "flux": p[3], "bc": p[4], "seed": int(p[5]),
-                         "filled": p[6], "net": p[7], "ws": p[8], "ws_max": float(p[9])})
+    for name in ("compute_flux_cases.txt", "compute_flux_cases_limiters.txt"):
+        with open(os.path.join(GOLDEN, name)) as f:
+            for line in f:
+                if line.startswith("#"):
+                    continue
+                p = line.split()
+                rows.append({"dim": int(p[0]), "n": tuple(int(v) for v in p[1].split(",")),
+                             "recon": p[2], "flux": p[3], "bc": p[4], "seed": int(p[5]),
+                             "filled": p[6], "net": p[7], "ws": p[8], "ws_max": float(p[9])})
     return rows

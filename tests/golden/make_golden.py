@@ -50,6 +50,13 @@ SIMULATIONS = {
                                      "weno2", "rungekutta3", "periodic", 0.4, 0.03, "seed:13"),
     "rand3d_8x8x8_eno2_central_rk2": (3, (8, 8, 8), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "central",
                                       "eno2", "rungekutta2", "neumann", 0.3, 0.02, "seed:14"),
+    # slope-limited reconstructions (MC.hpp, MM.hpp)
+    "sod256_mc_hll3_rk3": (1, (256,), (-1.0,), (1.0,), "hll3", "mc", "rungekutta3", "neumann",
+                           0.45, 0.2, "sod"),
+    "kh24_mm_hll_rk2": (2, (24, 24), (0.0, 0.0), (1.0, 1.0), "hll", "mm", "rungekutta2", "periodic",
+                        0.4, 0.1, "kh"),
+    "rand3d_9x8x7_mc_hll3_rk3": (3, (9, 8, 7), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3", "mc",
+                                 "rungekutta3", "periodic", 0.4, 0.03, "seed:15"),
 }
 
 
@@ -61,6 +68,27 @@ def initial_state(kind, dim, n, g):
         return init.sod(n[0], g)
     params = np.asarray(RefOracle().stlmersenne(40, 0, 1)[0])
     return init.kelvin_helmholtz(n[0], params, g, dimension=3 if kind == "kh3" else 2)
+
+
+def write_limiter_cases(ref):
+    """One spatial-operator evaluation per (dim, MC/MM, flux, boundary)."""
+    cases = []
+    seed = 2000
+    for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
+        for recon in ("mc", "mm"):
+            for flux in ("hll", "hll3", "central"):
+                for bc in ("neumann", "periodic"):
+                    seed += 1
+                    st = smooth_random_state(seed, dim, n, 2)
+                    filled, net, ws = ref.compute_flux(dim, n, [0.0] * dim, [1.0] * dim, flux,
+                                                       recon, bc, 1.4, st)
+                    cases.append((dim, ",".join(map(str, n)), recon, flux, bc, seed,
+                                  digest(filled), digest(net), digest(ws), float(ws.max())))
+    with open(os.path.join(HERE, "compute_flux_cases_limiters.txt"), "w") as f:
+        f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
+                "sha256(wave speeds) max_wave_speed\n")
+        for c in cases:
+            f.write("%d %s %s %s %s %d %s %s %s %.17g\n" % c)
 
 
 def main():
@@ -97,6 +125,7 @@ def main():
                     filled, net, ws = ref.compute_flux(dim, n, lo, hi, flux, recon, bc, 1.4, st)
                     cases.append((dim, ",".join(map(str, n)), recon, flux, bc, seed,
                                   digest(filled), digest(net), digest(ws), float(ws.max())))
+    write_limiter_cases(ref)
     with open(os.path.join(HERE, "compute_flux_cases.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
                 "sha256(wave speeds) max_wave_speed\n")
