@@ -153,7 +153,7 @@ struct PlaneFetch {
 // cells [G-1, N-G] along dir, interior across (ReconstructionCPU.cpp:71-96).
 template<class R, int NV, int RECON>
 __global__ void __launch_bounds__(256) reconstruct_dir(Planes<R> in, Planes<R> left,
-    Planes<R> right, int dim, int N0, int N1, int N2, int G, int dir) {
+    Planes<R> right, int dim, int N0, int N1, int N2, int G, int dir, double gamma) {
     const int e0 = dir == 0 ? N0 - 2 * G + 2 : N0 - 2 * G;
     const int e1 = dim > 1 ? (dir == 1 ? N1 - 2 * G + 2 : N1 - 2 * G) : 1;
     const int e2 = dim > 2 ? (dir == 2 ? N2 - 2 * G + 2 : N2 - 2 * G) : 1;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(256) reconstruct_dir(Planes<R> in, Planes<R> l
         const long long idx = ((long long)z * N1 + y) * N0 + x;
         PlaneFetch<R, NV> f{&in, idx, s};
         R l[NV], r[NV];
-        reconstruct_f<R, NV, RECON>(f, l, r);
+        reconstruct_f<R, NV, RECON>(f, l, r, R(gamma));
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             left.p[v][idx] = l[v];

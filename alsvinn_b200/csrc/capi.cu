@@ -51,7 +51,7 @@ int grid_blocks(long long work, int threads) {
 
 bool valid_choice(int flux, int recon) {
     return flux >= ALS_FLUX_HLL && flux <= ALS_FLUX_CENTRAL && recon >= ALS_RECON_NONE &&
-        recon <= ALS_RECON_MM;
+        recon <= ALS_RECON_WENOF2;
 }
 
 cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
@@ -310,7 +310,7 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
     }
     const int nvar = grid->dimension + 2;
     if (direction < 0 || direction >= grid->dimension || reconstruction < ALS_RECON_NONE ||
-        reconstruction > ALS_RECON_MM) {
+        reconstruction > ALS_RECON_WENOF2) {
         return fail(ALS_E_INVALID, "invalid reconstruction arguments");
     }
     rc = check_planes((const void* const*)in, nvar);
@@ -349,7 +349,7 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
     const als::Planes<double> pr = planes_of<double>((void* const*)right, nvar);
 #define ALS_RECON_CASE(NV, RC)                                                               \
     als::reconstruct_dir<double, NV, RC><<<blocks, 256, 0, s>>>(pin, pl, pr, dim, N[0], N[1], \
-        N[2], G, direction)
+        N[2], G, direction, grid->gamma)
 #define ALS_RECON_NV(NV)                                                                     \
     switch (reconstruction) {                                                                \
     case ALS_RECON_WENO2: ALS_RECON_CASE(NV, als::RECON_WENO2); break;                       \
@@ -357,6 +357,7 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
     case ALS_RECON_ENO3: ALS_RECON_CASE(NV, als::RECON_ENO3); break;                         \
     case ALS_RECON_MC: ALS_RECON_CASE(NV, als::RECON_MC); break;                             \
     case ALS_RECON_MM: ALS_RECON_CASE(NV, als::RECON_MM); break;                             \
+    case ALS_RECON_WENOF2: ALS_RECON_CASE(NV, als::RECON_WENOF2); break;                     \
     default: ALS_RECON_CASE(NV, als::RECON_ENO4); break;                                     \
     }
     if (dim == 1) {

@@ -9,6 +9,7 @@
 //   Central                  alsfvm/include/alsfvm/numflux/Central.hpp:39-56
 //   WENO2                    alsfvm/include/alsfvm/reconstruction/WENO2.hpp:31-91
 //   MC, MM                   alsfvm/include/alsfvm/reconstruction/MC.hpp, MM.hpp, minmod.hpp
+//   WENOF2                   alsfvm/include/alsfvm/reconstruction/WENOF2.hpp
 //   ENO2/3/4                 alsfvm/src/reconstruction/ENOCPU.cpp:41-267,
 //                            alsfvm/src/reconstruction/ENOCoefficients.cpp:27-49
 // Only the velocity component along the face normal is formed: the
@@ -20,12 +21,13 @@
 namespace als {
 
 enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4,
-             RECON_MC = 5, RECON_MM = 6 };
+             RECON_MC = 5, RECON_MM = 6, RECON_WENOF2 = 7 };
 enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2 };
 
 __host__ __device__ constexpr int recon_ghosts(int recon) {
     return recon == RECON_NONE ? 1
-        : (recon == RECON_WENO2 || recon == RECON_ENO2 || recon == RECON_MC || recon == RECON_MM) ? 2
+        : (recon == RECON_WENO2 || recon == RECON_ENO2 || recon == RECON_MC || recon == RECON_MM ||
+           recon == RECON_WENOF2) ? 2
         : (recon == RECON_ENO3 ? 3 : 4);
 }
 
@@ -263,8 +265,75 @@ __device__ __forceinline__ R minmod3(R a, R b, R c) {
         ? sign_of(a) * fmin(fabs(a), fmin(fabs(b), fabs(c))) : R(0);
 }
 
+// Primitive variables of one cell (Euler.hpp:290-297): u = m/rho,
+// p = (gamma-1)(E - 0.5 m.m / rho).
+template<class R, int NSD, class Fetch>
+__device__ __forceinline__ void primitive_at(const Fetch& f, int o, R gamma, R& rho, R* u, R& p) {
+    rho = f.at(0, o);
+    R dot = f.at(1, o) * f.at(1, o);
+#pragma unroll
+    for (int k = 1; k < NSD; ++k) {
+        dot = dot + f.at(1 + k, o) * f.at(1 + k, o);
+    }
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        u[k] = f.at(1 + k, o) / rho;
+    }
+    const R ie = f.at(NSD + 1, o) - R(0.5) * dot / rho;
+    p = (gamma - R(1)) * ie;
+}
+
+// One side of WENOF2 (WENOF2.hpp:70-121): the bounded primitive slope dP,
+// the limiter a = 0.5 sqrt(R / max(R, LL)), then computeConserved of
+// mid -+ a dP (Euler.hpp:236-245).
+template<class R, int NSD, bool RIGHT>
+__device__ __forceinline__ void wenof2_side(R w0, R w1, R gamma, const R* rho, const R (*u)[NSD],
+    const R* p, R* out) {
+    const R BOUND = R(1.9);
+    R dr = w1 * (rho[1] - rho[0]) + w0 * (rho[2] - rho[1]);
+    R du[NSD];
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        du[k] = w1 * (u[1][k] - u[0][k]) + w0 * (u[2][k] - u[1][k]);
+    }
+    R dp = w1 * (p[1] - p[0]) + w0 * (p[2] - p[1]);
+    dr = fmax(-BOUND * rho[1], fmin(BOUND * rho[1], dr));
+    dp = fmax(-BOUND * p[1], fmin(BOUND * p[1], dp));
+    R dudu = du[0] * du[0];
+    R umdu = u[1][0] * du[0];
+#pragma unroll
+    for (int k = 1; k < NSD; ++k) {
+        dudu = dudu + du[k] * du[k];
+        umdu = umdu + u[1][k] * du[k];
+    }
+    const R LL = R(0.125) * rho[1] * dudu - R(0.5) * fmin(R(0), dr * umdu) +
+        R(0.5) * dr * dr * dudu / rho[1];
+    const R Rr = p[1] / (gamma - R(1));
+    const R a = R(0.5) * sqrt(Rr / fmax(Rr, LL));
+    R pr, pu[NSD], pp;
+    if (RIGHT) {
+        pr = rho[1] + a * dr;
+        pp = p[1] + a * dp;
+    } else {
+        pr = rho[1] - a * dr;
+        pp = p[1] - a * dp;
+    }
+    R dot = R(0);
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        pu[k] = RIGHT ? u[1][k] + a * du[k] : u[1][k] - a * du[k];
+        dot = k == 0 ? pu[0] * pu[0] : dot + pu[k] * pu[k];
+    }
+    out[0] = pr;
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        out[1 + k] = pu[k] * pr;
+    }
+    out[NSD + 1] = pp / (gamma - R(1)) + R(0.5) * pr * dot;
+}
+
 template<class R, int NV, int RECON, class Fetch>
-__device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right) {
+__device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right, R gamma) {
     if (RECON == RECON_NONE) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -298,6 +367,32 @@ __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right)
             left[v] = R(0.5) * (w1Left * um + cl * u0 - w0Left * up);
             right[v] = R(0.5) * (w0Right * up + cr * u0 - w1Right * um);
         }
+    } else if (RECON == RECON_WENOF2) {
+        // WENOF2.hpp:37-121: WENO2 weights of rho, slopes in primitive variables
+        constexpr int NSD = NV - 2;
+        const R eps = R(1e-8);
+        const R i0 = f.at(0, 0);
+        const R dp = f.at(0, 1) - i0;
+        const R dm = i0 - f.at(0, -1);
+        const R b0 = dp * dp;
+        const R b1 = dm * dm;
+        const R d0 = R(3) * (eps + b0) * (eps + b0);
+        const R d1 = R(3) * (eps + b1) * (eps + b1);
+        const R a0Left = R(1) / d0;
+        const R a1Right = R(1) / d1;
+        const R a1Left = twice_reciprocal(d1, a1Right);
+        const R a0Right = twice_reciprocal(d0, a0Left);
+        const R w0Left = a0Left / (a0Left + a1Left);
+        const R w1Left = a1Left / (a0Left + a1Left);
+        const R w0Right = a0Right / (a0Right + a1Right);
+        const R w1Right = a1Right / (a0Right + a1Right);
+        R rho[3], u[3][NSD], p[3];
+#pragma unroll
+        for (int o = -1; o <= 1; ++o) {
+            primitive_at<R, NSD>(f, o, gamma, rho[o + 1], u[o + 1], p[o + 1]);
+        }
+        wenof2_side<R, NSD, false>(w0Left, w1Left, gamma, rho, u, p, left);
+        wenof2_side<R, NSD, true>(w0Right, w1Right, gamma, rho, u, p, right);
     } else if (RECON == RECON_MC || RECON == RECON_MM) {
         // MC.hpp:30-50 / MM.hpp:29-48, per variable
 #pragma unroll
@@ -362,9 +457,10 @@ struct StridedFetch {
 };
 
 template<class R, int NV, int RECON>
-__device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R* left, R* right) {
+__device__ __forceinline__ void reconstruct(const R* src, int vstride, int s, R* left, R* right,
+    R gamma) {
     StridedFetch<R, int> f{src, vstride, s};
-    reconstruct_f<R, NV, RECON>(f, left, right);
+    reconstruct_f<R, NV, RECON>(f, left, right, gamma);
 }
 
 } // namespace als

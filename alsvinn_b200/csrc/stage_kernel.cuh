@@ -222,7 +222,7 @@ __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, con
         const int bz = DIM > 2 ? ez - (D == 2 ? 1 : 0) + G : 0;
         const R* src = box + (bz * Lay::BY + by) * Lay::BX + bx;
         R l[NV], r[NV];
-        reconstruct<R, NV, RECON>(src, Lay::BOX, S, l, r);
+        reconstruct<R, NV, RECON>(src, Lay::BOX, S, l, r, gamma);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             rec[v * RC + i] = l[v];

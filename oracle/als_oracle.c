@@ -206,6 +206,7 @@ int orc_ghost_cells(int flux, int recon) {
     case ORC_RECON_ENO4: rg = 4; break;
     case ORC_RECON_MC: rg = 2; break;
     case ORC_RECON_MM: rg = 2; break;
+    case ORC_RECON_WENOF2: rg = 2; break;
     default: return -1;
     }
     return rg > 1 ? rg : 1;
@@ -381,6 +382,72 @@ static void reconstruct_cell(const orc_config* cfg, const double* in, long plane
             const double up = in[var * plane + c + s];
             left[var] = 0.5 * (w1Left * um + (3 * w0Left + w1Left) * u0 - w0Left * up);
             right[var] = 0.5 * (w0Right * up + (3 * w1Right + w0Right) * u0 - w1Right * um);
+        }
+    } else if (cfg->recon == ORC_RECON_WENOF2) {
+        /* WENOF2.hpp:37-121: weights as WENO2, slopes of the primitive
+         * variables (Euler.hpp:290-297) bounded, limited, back to conserved
+         * variables (Euler.hpp:236-245) */
+        const int nsd = nvar - 2;
+        const double BOUND = 1.9;
+        const double gm1 = cfg->gamma - 1;
+        const double i0 = in[c];
+        const double b0 = (in[c + s] - i0) * (in[c + s] - i0);
+        const double b1 = (i0 - in[c - s]) * (i0 - in[c - s]);
+        const double a0Left = 1 / (3 * (WENO_EPS + b0) * (WENO_EPS + b0));
+        const double a1Left = 2 / (3 * (WENO_EPS + b1) * (WENO_EPS + b1));
+        const double w0Left = a0Left / (a0Left + a1Left);
+        const double w1Left = a1Left / (a0Left + a1Left);
+        const double a0Right = 2 / (3 * (WENO_EPS + b0) * (WENO_EPS + b0));
+        const double a1Right = 1 / (3 * (WENO_EPS + b1) * (WENO_EPS + b1));
+        const double w0Right = a0Right / (a0Right + a1Right);
+        const double w1Right = a1Right / (a0Right + a1Right);
+        double rho[3], u[3][3], p[3];
+        int o, k, side;
+        for (o = 0; o < 3; ++o) {
+            const long cc = c + (o - 1) * s;
+            double dot = in[plane + cc] * in[plane + cc];
+            for (k = 1; k < nsd; ++k) {
+                dot = dot + in[(1 + k) * plane + cc] * in[(1 + k) * plane + cc];
+            }
+            rho[o] = in[cc];
+            for (k = 0; k < nsd; ++k) {
+                u[o][k] = in[(1 + k) * plane + cc] / rho[o];
+            }
+            p[o] = gm1 * (in[(nsd + 1) * plane + cc] - 0.5 * dot / rho[o]);
+        }
+        for (side = 0; side < 2; ++side) {
+            const double w0 = side == 0 ? w0Left : w0Right;
+            const double w1 = side == 0 ? w1Left : w1Right;
+            double* out = side == 0 ? left : right;
+            double dr = w1 * (rho[1] - rho[0]) + w0 * (rho[2] - rho[1]);
+            double du[3], dp, dudu, umdu, LL, Rr, a, pr, pu[3], pp, dot;
+            for (k = 0; k < nsd; ++k) {
+                du[k] = w1 * (u[1][k] - u[0][k]) + w0 * (u[2][k] - u[1][k]);
+            }
+            dp = w1 * (p[1] - p[0]) + w0 * (p[2] - p[1]);
+            dr = fmax(-BOUND * rho[1], fmin(BOUND * rho[1], dr));
+            dp = fmax(-BOUND * p[1], fmin(BOUND * p[1], dp));
+            dudu = du[0] * du[0];
+            umdu = u[1][0] * du[0];
+            for (k = 1; k < nsd; ++k) {
+                dudu = dudu + du[k] * du[k];
+                umdu = umdu + u[1][k] * du[k];
+            }
+            LL = 0.125 * rho[1] * dudu - 0.5 * fmin(0.0, dr * umdu) + 0.5 * dr * dr * dudu / rho[1];
+            Rr = p[1] / (cfg->gamma - 1);
+            a = 0.5 * sqrt(Rr / fmax(Rr, LL));
+            pr = side == 0 ? rho[1] - a * dr : rho[1] + a * dr;
+            pp = side == 0 ? p[1] - a * dp : p[1] + a * dp;
+            dot = 0;
+            for (k = 0; k < nsd; ++k) {
+                pu[k] = side == 0 ? u[1][k] - a * du[k] : u[1][k] + a * du[k];
+                dot = k == 0 ? pu[0] * pu[0] : dot + pu[k] * pu[k];
+            }
+            out[0] = pr;
+            for (k = 0; k < nsd; ++k) {
+                out[1 + k] = pr * pu[k];
+            }
+            out[nsd + 1] = pp / (cfg->gamma - 1) + 0.5 * pr * dot;
         }
     } else if (cfg->recon == ORC_RECON_MC || cfg->recon == ORC_RECON_MM) {
         /* MC.hpp:30-50 / MM.hpp:29-48 with minmod.hpp, sign.hpp, per variable */

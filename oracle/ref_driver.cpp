@@ -28,6 +28,7 @@
 #include "alsfvm/reconstruction/WENO2.hpp"
 #include "alsfvm/reconstruction/MC.hpp"
 #include "alsfvm/reconstruction/MM.hpp"
+#include "alsfvm/reconstruction/WENOF2.hpp"
 #include "alsfvm/reconstruction/ENOCPU.hpp"
 #include "alsfvm/reconstruction/NoReconstruction.hpp"
 #include "alsfvm/integrator/ForwardEuler.hpp"
@@ -109,6 +110,8 @@ std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Object
         return std::make_shared<reconstruction::ENOCPU<4>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
     } else if (s.recon == "mc") {
         return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::MC<Eq>, Eq>>(*o.params);
+    } else if (s.recon == "wenof2") {
+        return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::WENOF2<Eq>, Eq>>(*o.params);
     } else if (s.recon == "mm") {
         return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::MM<Eq>, Eq>>(*o.params);
     } else if (s.recon == "none") {

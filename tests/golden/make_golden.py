@@ -57,6 +57,11 @@ SIMULATIONS = {
                         0.4, 0.1, "kh"),
     "rand3d_9x8x7_mc_hll3_rk3": (3, (9, 8, 7), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3", "mc",
                                  "rungekutta3", "periodic", 0.4, 0.03, "seed:15"),
+    # WENO2 in primitive variables with bounds (WENOF2.hpp)
+    "sod512_wenof2_hll3_rk3": (1, (512,), (-1.0,), (1.0,), "hll3", "wenof2", "rungekutta3",
+                               "neumann", 0.45, 0.2, "sod"),
+    "kh32_wenof2_hll3_rk3": (2, (32, 32), (0.0, 0.0), (1.0, 1.0), "hll3", "wenof2", "rungekutta3",
+                             "periodic", 0.4, 0.2, "kh"),
 }
 
 
@@ -71,7 +76,7 @@ def initial_state(kind, dim, n, g):
 
 
 def write_limiter_cases(ref):
-    """One spatial-operator evaluation per (dim, MC/MM, flux, boundary)."""
+    """One spatial-operator evaluation per (dim, MC/MM/WENOF2, flux, boundary)."""
     cases = []
     seed = 2000
     for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
@@ -84,6 +89,16 @@ def write_limiter_cases(ref):
                                                        recon, bc, 1.4, st)
                     cases.append((dim, ",".join(map(str, n)), recon, flux, bc, seed,
                                   digest(filled), digest(net), digest(ws), float(ws.max())))
+    seed = 2500
+    for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
+        for flux in ("hll", "hll3", "central"):
+            for bc in ("neumann", "periodic"):
+                seed += 1
+                st = smooth_random_state(seed, dim, n, 2)
+                filled, net, ws = ref.compute_flux(dim, n, [0.0] * dim, [1.0] * dim, flux,
+                                                   "wenof2", bc, 1.4, st)
+                cases.append((dim, ",".join(map(str, n)), "wenof2", flux, bc, seed,
+                              digest(filled), digest(net), digest(ws), float(ws.max())))
     with open(os.path.join(HERE, "compute_flux_cases_limiters.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
                 "sha256(wave speeds) max_wave_speed\n")

@@ -21,7 +21,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 
 FLUX = {"hll": 0, "hll3": 1, "central": 2}
-RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6}
+RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
+         "wenof2": 7}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
 BC = {"neumann": 0, "periodic": 1}
 
@@ -35,7 +36,8 @@ def _dptr(a):
 
 
 def ghost_cells(recon):
-    return {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 2, "mm": 2}[recon]
+    return {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 2, "mm": 2,
+            "wenof2": 2}[recon]
 
 
 def padded_shape(dim, n, g):
