@@ -46,6 +46,9 @@
 #include "alsfvm/DeviceConfiguration.hpp"
 #include "alsuq/generator/STLMersenne.hpp"
 #include "alsfvm/functional/structure_common.hpp"
+#ifdef ALSREF_WITH_B200
+#include "adapter/NumericalFluxB200.hpp"
+#endif
 
 #include <algorithm>
 #include <chrono>
@@ -120,9 +123,34 @@ std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Object
     THROW("unknown reconstruction " << s.recon);
 }
 
+#ifdef ALSREF_WITH_B200
+// Flux platform of the next builds: "cpu" (the reference's NumericalFluxCPU)
+// or "b200" (numflux::NumericalFluxB200 over the B200 library).
+std::string g_flux_platform = "cpu";
+
+int b200_code(const std::string& name, const char* const* names, int count) {
+    for (int i = 0; i < count; ++i) {
+        if (name == names[i]) {
+            return i;
+        }
+    }
+    THROW("no B200 code for " << name);
+}
+#endif
+
 template<int d>
 std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
     typedef equation::euler::Euler<d> Eq;
+#ifdef ALSREF_WITH_B200
+    if (g_flux_platform == "b200") {
+        // names in the order of the ALS_FLUX_* / ALS_RECON_* codes
+        static const char* const fluxes[] = {"hll", "hll3", "central"};
+        static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
+            "wenof2"};
+        return std::make_shared<numflux::NumericalFluxB200>(*o.grid, b200_code(s.flux, fluxes, 3),
+            b200_code(s.recon, recons, 8), s.gamma);
+    }
+#endif
     if (s.flux == "hll") {
         return std::make_shared<numflux::NumericalFluxCPU<numflux::euler::HLL<d>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
     } else if (s.flux == "hll3") {
@@ -479,5 +507,18 @@ int alsref_structure_cube(int dim, const int* n, int ghosts, const char* bc, int
         return -1;
     }
 }
+
+#ifdef ALSREF_WITH_B200
+// Selects the flux platform of the following calls ("cpu" or "b200").
+int alsref_set_flux_platform(const char* platform) {
+    const std::string p(platform ? platform : "");
+    if (p != "cpu" && p != "b200") {
+        g_last_error = "unknown flux platform " + p;
+        return -1;
+    }
+    g_flux_platform = p;
+    return 0;
+}
+#endif
 
 } // extern "C"

@@ -167,8 +167,8 @@ def ref_library_path():
 class RefOracle:
     """The reference's own CPU code (only where ``make -C oracle ref`` ran)."""
 
-    def __init__(self):
-        path = ref_library_path()
+    def __init__(self, path=None):
+        path = path or ref_library_path()
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = ctypes.CDLL(path)
@@ -284,3 +284,19 @@ def digest(*arrays):
     for a in arrays:
         h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
     return h.hexdigest()
+
+
+def ref_b200_library_path():
+    return os.path.join(ROOT, "oracle", "_ref", "libalsref_b200.so")
+
+
+class RefB200Oracle(RefOracle):
+    """The reference's time loop whose flux can be numflux::NumericalFluxB200
+    (oracle/adapter/), built by ``make -C oracle ref-b200``."""
+
+    def __init__(self):
+        super().__init__(ref_b200_library_path())
+        self.lib.alsref_set_flux_platform.argtypes = [ctypes.c_char_p]
+
+    def set_flux_platform(self, platform):
+        self._check(self.lib.alsref_set_flux_platform(platform.encode()))

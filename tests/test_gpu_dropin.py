@@ -1,0 +1,52 @@
+"""The drop-in boundary end to end: the reference's own time loop
+(ForwardEuler / RungeKutta2 / RungeKutta3 over ConservedSystem, BoundaryCPU,
+the end-time adjuster) with numflux::NumericalFluxB200 — the adapter class
+of INTEGRATION.md, compiled against the reference's headers
+(oracle/adapter/NumericalFluxB200.hpp) — in place of NumericalFluxCPU.
+Every whole simulation must equal the reference's own, bit for bit.
+"""
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle_lib import RefB200Oracle, ghost_cells, ref_b200_library_path, smooth_random_state
+
+pytestmark = pytest.mark.gpu
+
+CASES = []
+for _dim, _n in ((1, (32,)), (2, (14, 12)), (3, (8, 9, 8))):
+    for _recon in ("weno2", "eno3", "mc", "wenof2", "none"):
+        for _flux, _integ, _bc in (("hll3", "rungekutta3", "periodic"),
+                                   ("hll", "rungekutta2", "neumann"),
+                                   ("central", "forwardeuler", "periodic")):
+            CASES.append((_dim, _n, _recon, _flux, _integ, _bc))
+
+
+@pytest.fixture(scope="module")
+def ref_b200():
+    if not os.path.exists(ref_b200_library_path()):
+        pytest.skip("oracle/_ref/libalsref_b200.so not built (make -C oracle ref-b200)")
+    return RefB200Oracle()
+
+
+@pytest.mark.parametrize("dim,n,recon,flux,integ,bc", CASES,
+                         ids=["d%d-%s-%s-%s-%s" % (c[0], c[2], c[3], c[4], c[5]) for c in CASES])
+def test_reference_time_loop_with_b200_flux(ref_b200, dim, n, recon, flux, integ, bc):
+    g = ghost_cells(recon)
+    seed = zlib.crc32(("dropin-%d-%s-%s-%s" % (dim, recon, flux, integ)).encode()) % 100000
+    st = smooth_random_state(seed, dim, n, g)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    out = {}
+    for platform in ("cpu", "b200"):
+        ref_b200.set_flux_platform(platform)
+        out[platform] = ref_b200.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, 0.4, 0.03,
+                                          st)
+    ref_b200.set_flux_platform("cpu")
+    a, b = out["cpu"], out["b200"]
+    assert a[0] == b[0]            # status
+    assert a[3] == b[3] >= 1       # steps
+    assert a[4] == b[4]            # final time
+    np.testing.assert_array_equal(a[2], b[2])   # every dt
+    np.testing.assert_array_equal(a[1], b[1])   # final state, ghosts included

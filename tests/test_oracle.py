@@ -213,3 +213,22 @@ def test_structure_basic_small_case_by_hand(c_oracle):
     for h in range(4):
         expect = sum((i - (i + h) % n) ** 2 for i in range(n)) / n
         assert per[0, h] == pytest.approx(expect, rel=1e-15)
+
+
+def test_reference_driver_with_adapter_loads_and_matches_on_cpu(ref_oracle):
+    """oracle/_ref/libalsref_b200.so (the reference time loop that can take the
+    B200 flux adapter) gives the plain reference's results with its CPU flux."""
+    from oracle_lib import RefB200Oracle, ref_b200_library_path
+    if not os.path.exists(ref_b200_library_path()):
+        pytest.skip("libalsref_b200.so not built")
+    rb = RefB200Oracle()
+    rb.set_flux_platform("cpu")
+    st = smooth_random_state(8, 2, (10, 12), 2)
+    a = ref_oracle.simulate(2, (10, 12), (0, 0), (1, 1), "hll3", "weno2", "rungekutta3",
+                            "periodic", 1.4, 0.4, 0.02, st)
+    b = rb.simulate(2, (10, 12), (0, 0), (1, 1), "hll3", "weno2", "rungekutta3", "periodic",
+                    1.4, 0.4, 0.02, st)
+    assert a[0] == b[0] and a[3] == b[3] and a[4] == b[4]
+    np.testing.assert_array_equal(a[1], b[1])
+    with pytest.raises(RuntimeError):
+        rb.set_flux_platform("tpu")
