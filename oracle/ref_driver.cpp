@@ -48,6 +48,7 @@
 #include "alsfvm/functional/structure_common.hpp"
 #ifdef ALSREF_WITH_B200
 #include "adapter/NumericalFluxB200.hpp"
+#include "adapter/B200Adapters.hpp"
 #endif
 
 #include <algorithm>
@@ -100,9 +101,32 @@ struct Objects {
     std::string eqName;
 };
 
+#ifdef ALSREF_WITH_B200
+// Flux platform of the next builds: "cpu" (the reference's NumericalFluxCPU)
+// or "b200" (numflux::NumericalFluxB200 over the B200 library).
+std::string g_flux_platform = "cpu";
+
+int b200_code(const std::string& name, const char* const* names, int count) {
+    for (int i = 0; i < count; ++i) {
+        if (name == names[i]) {
+            return i;
+        }
+    }
+    THROW("no B200 code for " << name);
+}
+#endif
+
 template<int d>
 std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Objects& o) {
     typedef equation::euler::Euler<d> Eq;
+#ifdef ALSREF_WITH_B200
+    if (g_flux_platform == "b200-parts") {
+        // the reference's NumericalFluxCPU over the B200 reconstruction
+        static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
+            "wenof2"};
+        return std::make_shared<b200::ReconstructionB200>(d, b200_code(s.recon, recons, 8), s.gamma);
+    }
+#endif
     if (s.recon == "weno2") {
         return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::WENO2<Eq>, Eq>>(*o.params);
     } else if (s.recon == "eno2") {
@@ -123,26 +147,12 @@ std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Object
     THROW("unknown reconstruction " << s.recon);
 }
 
-#ifdef ALSREF_WITH_B200
-// Flux platform of the next builds: "cpu" (the reference's NumericalFluxCPU)
-// or "b200" (numflux::NumericalFluxB200 over the B200 library).
-std::string g_flux_platform = "cpu";
-
-int b200_code(const std::string& name, const char* const* names, int count) {
-    for (int i = 0; i < count; ++i) {
-        if (name == names[i]) {
-            return i;
-        }
-    }
-    THROW("no B200 code for " << name);
-}
-#endif
 
 template<int d>
 std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
     typedef equation::euler::Euler<d> Eq;
 #ifdef ALSREF_WITH_B200
-    if (g_flux_platform == "b200") {
+    if (g_flux_platform == "b200" || g_flux_platform == "b200-all") {
         // names in the order of the ALS_FLUX_* / ALS_RECON_* codes
         static const char* const fluxes[] = {"hll", "hll3", "central"};
         static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
@@ -207,6 +217,16 @@ Objects build(const Setup& s) {
     } else {
         o.boundary = std::make_shared<boundary::BoundaryCPU<boundary::Periodic>>(o.ghosts);
     }
+#ifdef ALSREF_WITH_B200
+    if (g_flux_platform == "b200-parts" || g_flux_platform == "b200-all") {
+        // the boundary and the integrator as B200 adapters too
+        o.boundary = std::make_shared<b200::BoundaryB200>(
+            t == boundary::Type::NEUMANN ? ALS_BC_NEUMANN : ALS_BC_PERIODIC, int(o.ghosts));
+        static const char* const integs[] = {"forwardeuler", "rungekutta2", "rungekutta3"};
+        o.integ = std::make_shared<b200::IntegratorB200>(b200_code(s.integrator, integs, 3),
+            o.system);
+    }
+#endif
     o.volumeFactory = std::make_shared<volume::VolumeFactory>(o.eqName, o.memoryFactory);
     return o;
 }
@@ -509,10 +529,13 @@ int alsref_structure_cube(int dim, const int* n, int ghosts, const char* bc, int
 }
 
 #ifdef ALSREF_WITH_B200
-// Selects the flux platform of the following calls ("cpu" or "b200").
+// Selects the classes of the following builds: "cpu" (the reference's),
+// "b200" (NumericalFluxB200), "b200-parts" (the reference's NumericalFluxCPU
+// over ReconstructionB200, with BoundaryB200 and IntegratorB200) or
+// "b200-all" (NumericalFluxB200, BoundaryB200, IntegratorB200).
 int alsref_set_flux_platform(const char* platform) {
     const std::string p(platform ? platform : "");
-    if (p != "cpu" && p != "b200") {
+    if (p != "cpu" && p != "b200" && p != "b200-parts" && p != "b200-all") {
         g_last_error = "unknown flux platform " + p;
         return -1;
     }

@@ -1,9 +1,10 @@
 """The drop-in boundary end to end: the reference's own time loop
-(ForwardEuler / RungeKutta2 / RungeKutta3 over ConservedSystem, BoundaryCPU,
-the end-time adjuster) with numflux::NumericalFluxB200 — the adapter class
-of INTEGRATION.md, compiled against the reference's headers
-(oracle/adapter/NumericalFluxB200.hpp) — in place of NumericalFluxCPU.
-Every whole simulation must equal the reference's own, bit for bit.
+(Simulator::incrementSolution's substep loop over ConservedSystem, the
+end-time adjuster, the constraint check) with the adapter classes of
+INTEGRATION.md — compiled against the reference's headers
+(oracle/adapter/) — in place of the reference's NumericalFluxCPU,
+Reconstruction, BoundaryCPU and integrators.  Every whole simulation must
+equal the reference's own, bit for bit.
 """
 import os
 import zlib
@@ -31,20 +32,23 @@ def ref_b200():
     return RefB200Oracle()
 
 
+@pytest.mark.parametrize("platform", ["b200", "b200-parts", "b200-all"])
 @pytest.mark.parametrize("dim,n,recon,flux,integ,bc", CASES,
                          ids=["d%d-%s-%s-%s-%s" % (c[0], c[2], c[3], c[4], c[5]) for c in CASES])
-def test_reference_time_loop_with_b200_flux(ref_b200, dim, n, recon, flux, integ, bc):
+def test_reference_time_loop_with_b200_classes(ref_b200, platform, dim, n, recon, flux, integ, bc):
+    """b200: NumericalFluxB200 as the flux; b200-parts: the reference's
+    NumericalFluxCPU over ReconstructionB200, with BoundaryB200 and
+    IntegratorB200; b200-all: NumericalFluxB200, BoundaryB200, IntegratorB200."""
     g = ghost_cells(recon)
     seed = zlib.crc32(("dropin-%d-%s-%s-%s" % (dim, recon, flux, integ)).encode()) % 100000
     st = smooth_random_state(seed, dim, n, g)
     lo, hi = [0.0] * dim, [1.0] * dim
     out = {}
-    for platform in ("cpu", "b200"):
-        ref_b200.set_flux_platform(platform)
-        out[platform] = ref_b200.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, 0.4, 0.03,
-                                          st)
+    for p in ("cpu", platform):
+        ref_b200.set_flux_platform(p)
+        out[p] = ref_b200.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, 0.4, 0.03, st)
     ref_b200.set_flux_platform("cpu")
-    a, b = out["cpu"], out["b200"]
+    a, b = out["cpu"], out[platform]
     assert a[0] == b[0]            # status
     assert a[3] == b[3] >= 1       # steps
     assert a[4] == b[4]            # final time
