@@ -215,6 +215,8 @@ def run_batch(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dim, levels = BATCHES[args.workload]
+    if (args.n or args.members) and len(levels) == 1:
+        levels = [(args.n or levels[0][0], args.members or levels[0][1])]
     precision = "fp64" if args.workload == "kh3d" else args.precision
     nvar = dim + 2
     elem = 8 if precision == "fp64" else 4
@@ -231,6 +233,11 @@ def run_batch(args, rank, world, local):
                                for j in range(k)])
             sim.set_state(states, first_member=lev["first"] + a)
         first += lev["members"]
+    if args.kernels_only:
+        sim.advance(args.warmup + args.steps)
+        sim.synchronize()
+        sim.close()
+        return
     schedule = sim.tune(steps=2)
     sim.advance(args.warmup)
     sim.synchronize()
@@ -498,6 +505,10 @@ def main():
                     help="kh1024 (default, the plain FP64 drop-in), an ensemble workload, or "
                          "uq (time-to-error of the surrogate control variate)")
     ap.add_argument("--samples", type=int, default=1024, help="plain MC samples of --workload uq")
+    ap.add_argument("--n", type=int, default=0,
+                    help="grid size of a one-level batch workload (profiler captures)")
+    ap.add_argument("--members", type=int, default=0,
+                    help="members of a one-level batch workload (profiler captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="member precision of the ensemble workloads")
     args = ap.parse_args()
