@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <random>
 #include <sstream>
@@ -22,6 +23,7 @@ using namespace mlpk;
 namespace {
 
 constexpr long long kInferChunk = 65536;   // rows per inference chunk (multiple of 128)
+constexpr int kMaxSplits = 16;             // K splits of a weight gradient, row splits of a column sum
 
 int mlp_fail(int code, const std::string& msg) {
     return als::report_error(code, msg.c_str());
@@ -70,6 +72,8 @@ struct als_mlp {
     float* y = nullptr;
     float* dy = nullptr;
     float* loss1 = nullptr;         // loss of a gradient evaluation
+    float* split_scratch = nullptr; // K-split partial weight gradients
+    float* col_scratch = nullptr;   // row-split partial column sums
     // inference workspace (kInferChunk rows)
     __nv_bfloat16* xi = nullptr;
     __nv_bfloat16* hi[2] = {nullptr, nullptr};
@@ -104,12 +108,12 @@ int grid_for(long long work, int threads) {
 }
 
 template <int BN, int EPI>
-int launch_gemm(const GemmArgs& a, int n_valid, cudaStream_t s) {
-    if (a.M % kTileM || a.N % BN || a.K % kChunkK || a.K <= 0) {
+int launch_gemm(const GemmArgs& a, int n_valid, cudaStream_t s, int splits = 1) {
+    if (a.M % kTileM || a.N % BN || a.K % kChunkK || a.K <= 0 || splits < 1 || splits > 65535) {
         return mlp_fail(ALS_E_INVALID, "GEMM shape is not a multiple of the tile");
     }
     constexpr int smem = gemm_smem_bytes<BN>();   // limit set by configure_kernels()
-    dim3 grid(a.M / kTileM, a.N / BN);
+    dim3 grid(a.M / kTileM, a.N / BN, splits);
     gemm_kernel<BN, EPI><<<grid, kThreads, smem, s>>>(a, n_valid);
     MLP_CUDA(cudaGetLastError());
     return ALS_OK;
@@ -270,6 +274,34 @@ int join_caller(als_mlp* s, void* stream) {
 
 namespace {
 
+// Column sums of a rows x cols matrix (weighted by wt when given) into out:
+// row splits on separate blocks, then the splits added in order.
+template <typename T>
+int col_sums(als_mlp* s, const T* x, int rows, int cols, long long ld, const float* wt, float* out,
+             cudaStream_t st) {
+    int splits = kMaxSplits;
+    if (rows < 8 * splits) {
+        splits = std::max(1, rows / 8);
+    }
+    const int per = (rows + splits - 1) / splits;
+    dim3 grid((cols + 31) / 32, splits);
+    column_sums<T><<<grid, 256, 0, st>>>(x, rows, cols, ld, wt, s->col_scratch, per);
+    sum_splits<<<grid_for(cols, 256), 256, 0, st>>>(s->col_scratch, splits, cols, out);
+    MLP_CUDA(cudaGetLastError());
+    return ALS_OK;
+}
+
+// Largest divisor of the K chunks (K / 64) not above kMaxSplits.
+int k_splits(long long K) {
+    const long long chunks = K / kChunkK;
+    for (int sp = kMaxSplits; sp > 1; --sp) {
+        if (chunks % sp == 0) {
+            return sp;
+        }
+    }
+    return 1;
+}
+
 // Forward + MSE backward of one batch (rows <= max_batch), gradients into
 // s->g.  `loss`/`base` select where the loss goes (see head_backward).
 int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, float* loss,
@@ -299,29 +331,32 @@ int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, floa
                                                   s->dy, s->dz[(nh - 1) & 1], s->step, loss, base);
     MLP_CUDA(cudaGetLastError());
     // head gradients: dw = sum_r dy_r h_r, db = sum_r dy_r
-    column_sums<__nv_bfloat16><<<(W + 31) / 32, 256, 0, st>>>(last, rows, W, W, s->dy,
-                                                              s->g + head.w_off);
-    column_sums<float><<<1, 256, 0, st>>>(s->dy, rows, 1, 1, nullptr, s->g + head.b_off);
-    MLP_CUDA(cudaGetLastError());
+    MLP_TRY(col_sums<__nv_bfloat16>(s, last, rows, W, W, s->dy, s->g + head.w_off, st));
+    MLP_TRY(col_sums<float>(s, s->dy, rows, 1, 1, nullptr, s->g + head.b_off, st));
     for (int l = nh - 1; l >= 0; --l) {
         const Layer& L = s->layers[l];
         const __nv_bfloat16* dzl = s->dz[l & 1];
         const __nv_bfloat16* hin = l > 0 ? s->h[l - 1] : s->xb;
         const long long ld_in = l > 0 ? s->layers[l - 1].out : L0.kpad;
         // dW = dZ^T H_in : M = out, N = kpad(in), K = rows (padded rows are zero in dZ)
+        // K (the batch) split over CTAs; the partial products are added in
+        // split order by sum_splits
+        const int splits = k_splits(rp);
         GemmArgs a = {};
         a.a = columns_of(dzl, L.out);
         a.b = columns_of(hin, ld_in);
         a.M = L.out;
         a.N = L.kpad;
-        a.K = int(rp);
-        a.g = s->g + L.w_off;
+        a.K = int(rp / splits);
+        a.g = s->split_scratch;
         a.ldg = L.in;
+        a.split_stride = (long long)L.out * L.in;
         a.error = s->error;
-        MLP_TRY((launch_gemm<64, EPI_WGRAD>(a, L.in, st)));
-        column_sums<__nv_bfloat16><<<(L.out + 31) / 32, 256, 0, st>>>(dzl, rows, L.out, L.out,
-                                                                       nullptr, s->g + L.b_off);
+        MLP_TRY((launch_gemm<64, EPI_WGRAD>(a, L.in, st, splits)));
+        sum_splits<<<grid_for((long long)L.out * L.in, 256), 256, 0, st>>>(
+            s->split_scratch, splits, (long long)L.out * L.in, s->g + L.w_off);
         MLP_CUDA(cudaGetLastError());
+        MLP_TRY(col_sums<__nv_bfloat16>(s, dzl, rows, L.out, L.out, nullptr, s->g + L.b_off, st));
         if (l > 0) {
             // dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}) : M = rows, N = in, K = out
             GemmArgs b = {};
@@ -447,6 +482,8 @@ int als_mlp_create(const als_mlp_config* cfg, int device, als_mlp** out) {
     rc = rc ? rc : dev_alloc(s, &s->dz[0], B * Wd);
     rc = rc ? rc : dev_alloc(s, &s->dz[1], B * Wd);
     rc = rc ? rc : dev_alloc(s, &s->y, B);
+    rc = rc ? rc : dev_alloc(s, &s->split_scratch, size_t(kMaxSplits) * Wd * std::max<size_t>(Wd, 64));
+    rc = rc ? rc : dev_alloc(s, &s->col_scratch, size_t(kMaxSplits) * Wd);
     rc = rc ? rc : dev_alloc(s, &s->dy, B);
     rc = rc ? rc : dev_alloc(s, &s->xi, size_t(kInferChunk) * s->layers[0].kpad);
     rc = rc ? rc : dev_alloc(s, &s->hi[0], size_t(kInferChunk) * Wd);

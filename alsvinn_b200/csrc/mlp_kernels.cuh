@@ -51,7 +51,7 @@ __device__ __forceinline__ void epilogue16(const GemmArgs& g, long long m, int n
         dh[0] = reinterpret_cast<const uint4*>(hb)[0];
         dh[1] = reinterpret_cast<const uint4*>(hb)[1];
     } else {
-        float* dst = g.g + m * g.ldg + n;
+        float* dst = g.g + blockIdx.z * g.split_stride + m * g.ldg + n;
         if (n + 16 <= n_valid && (g.ldg & 3) == 0) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -68,7 +68,9 @@ __device__ __forceinline__ void epilogue16(const GemmArgs& g, long long m, int n
     }
 }
 
-// D[128 x BN tile] = A * B^T over K, then the epilogue.  Grid: (M/128, N/BN).
+// D[128 x BN tile] = A * B^T over K, then the epilogue.  Grid: (M/128, N/BN,
+// splits): split z covers K range [z K, (z+1) K) and, with EPI_WGRAD, writes
+// its partial product z * split_stride further (summed by sum_splits).
 // `n_valid` limits the stored columns of EPI_WGRAD (padded inputs).
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid) {
@@ -87,6 +89,7 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
     const int lane = threadIdx.x & 31;
     const long long m0 = (long long)blockIdx.x * kTileM;
     const long long n0 = (long long)blockIdx.y * BN;
+    const int kb = blockIdx.z * g.K;
 
     if (warp == 0) {
         tmem_alloc(&tmem_base, BN);
@@ -115,8 +118,8 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
             failed = true;
             break;
         }
-        stage_operand<kTileM>(sa[s], g.a, m0, c * kChunkK);
-        stage_operand<BN>(sb[s], g.b, n0, c * kChunkK);
+        stage_operand<kTileM>(sa[s], g.a, m0, kb + c * kChunkK);
+        stage_operand<BN>(sb[s], g.b, n0, kb + c * kChunkK);
         fence_async_shared();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -457,18 +460,23 @@ __global__ void head_backward(const float* __restrict__ y, const float* __restri
     }
 }
 
-// out[n] = sum_r wt[r] * X[r][n] (wt null: weights 1), deterministic order.
-// Block: 32 columns x 8 row groups.
+// out[split][n] = sum over rows [split*rows_per_split, ...) of wt[r] * X[r][n]
+// (wt null: weights 1), deterministic order; sum_splits adds the splits.
+// Block: 32 columns x 8 row groups; grid (columns / 32, splits).
 template <typename T>
 __global__ void column_sums(const T* __restrict__ x, int rows, int cols, long long ld,
-                            const float* __restrict__ wt, float* __restrict__ out) {
+                            const float* __restrict__ wt, float* __restrict__ out,
+                            int rows_per_split) {
     __shared__ float part[8][33];
     const int cx = threadIdx.x & 31;
     const int gy = threadIdx.x >> 5;
     const int n = blockIdx.x * 32 + cx;
+    const int r0 = blockIdx.y * rows_per_split;
+    const int r1 = r0 + rows_per_split < rows ? r0 + rows_per_split : rows;
+    out += (long long)blockIdx.y * cols;
     float acc = 0.0f;
     if (n < cols) {
-        for (int r = gy; r < rows; r += 8) {
+        for (int r = r0 + gy; r < r1; r += 8) {
             float v;
             if constexpr (sizeof(T) == 2) {
                 v = __bfloat162float(x[(long long)r * ld + n]);
@@ -486,6 +494,19 @@ __global__ void column_sums(const T* __restrict__ x, int rows, int cols, long lo
             s += part[i][cx];
         }
         out[n] = s;
+    }
+}
+
+// out[i] = sum over s < splits of partial[s * count + i], in split order.
+__global__ void sum_splits(const float* __restrict__ partial, int splits, long long count,
+                           float* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int k = 0; k < splits; ++k) {
+            s += partial[k * count + i];
+        }
+        out[i] = s;
     }
 }
 

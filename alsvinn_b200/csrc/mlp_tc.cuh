@@ -49,6 +49,7 @@ struct GemmArgs {
     const float* zin;           // EPI_BACKWARD: pre-activations; ld = ldz
     float* g;                   // EPI_WGRAD output; ld = ldg
     long long ldz, ldh, ldg;
+    long long split_stride;     // EPI_WGRAD: elements between the outputs of K splits
     int* error;                 // set to 1 when a wait gave up
 };
 
