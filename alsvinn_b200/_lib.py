@@ -102,6 +102,9 @@ PROTOTYPES = {
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_double, _VP,
                                                 ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
                                                 _VP, _VP]),
+    "als_write_netcdf": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _I, ctypes.c_int, _PP,
+                                        _PP, ctypes.c_double, ctypes.c_int, _PP, _PP]),
+    "als_solver_write_netcdf": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     # include/als_surrogate.h
     "als_mlp_create": (ctypes.c_int, [ctypes.POINTER(MlpConfig), ctypes.c_int, _PP]),
     "als_mlp_destroy": (ctypes.c_int, [_VP]),

@@ -901,6 +901,61 @@ int als_solver_get_state(als_solver* s, double* host, int first_member, int coun
     return ALS_OK;
 }
 
+int als_solver_write_netcdf(als_solver* s, int member, const char* basename, int snapshot) {
+    const int l = s ? range_level(s, member, 1) : -1;
+    if (!s || l < 0 || !basename || snapshot < 0) {
+        return fail(ALS_E_INVALID, "invalid write_netcdf arguments");
+    }
+    const SolverLevel& L = s->levels[l];
+    const int dim = s->cfg.dimension;
+    std::vector<double> padded(size_t(L.member_elems));
+    int rc = als_solver_get_state(s, padded.data(), member, 1);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    als_member_info info;
+    rc = als_solver_info(s, member, &info);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    // Volume::copyInternalCells (HostMemory.cpp:239-258): interior, x fastest
+    const int* n = L.grid.n;
+    const int* N = L.grid.N;
+    const int G[3] = {s->g, dim > 1 ? s->g : 0, dim > 2 ? s->g : 0};
+    const size_t cells = size_t(n[0]) * n[1] * n[2];
+    std::vector<std::vector<double>> interior(size_t(s->nv), std::vector<double>(cells));
+    for (int v = 0; v < s->nv; ++v) {
+        const double* plane = padded.data() + size_t(v) * size_t(L.grid.plane);
+        size_t k = 0;
+        for (int z = 0; z < n[2]; ++z) {
+            for (int y = 0; y < n[1]; ++y) {
+                for (int x = 0; x < n[0]; ++x) {
+                    interior[size_t(v)][k++] =
+                        plane[(size_t(z + G[2]) * N[1] + size_t(y + G[1])) * N[0] + size_t(x + G[0])];
+                }
+            }
+        }
+    }
+    // Euler<d>::conservedVariables (alsfvm/src/equation/euler/Euler.cpp:20-75)
+    static const char* const names1[] = {"rho", "mx", "E"};
+    static const char* const names2[] = {"rho", "mx", "my", "E"};
+    static const char* const names3[] = {"rho", "mx", "my", "mz", "E"};
+    const char* const* names = dim == 1 ? names1 : (dim == 2 ? names2 : names3);
+    std::vector<const double*> ptrs;
+    for (const auto& v : interior) {
+        ptrs.push_back(v.data());
+    }
+    const std::string steps = std::to_string(info.steps);
+    const std::string prec = s->cfg.precision == ALS_FP64 ? "fp64" : "fp32";
+    const char* anames[] = {"alsvinn_b200.software", "alsvinn_b200.steps", "alsvinn_b200.precision"};
+    const char* avalues[] = {"alsvinn_b200", steps.c_str(), prec.c_str()};
+    // io_utils.cpp:34-40 and NetCDFWriter.cpp:139-146: <base>_<snapshot>.nc
+    const std::string path = std::string(basename) + "_" + std::to_string(snapshot) + ".nc";
+    int nn[3] = {n[0], n[1], n[2]};
+    return als_write_netcdf(path.c_str(), dim, nn, s->nv, names, ptrs.data(), info.t, 3, anames,
+        avalues);
+}
+
 int als_solver_state_pointer(als_solver* s, void** dev) {
     if (!s || !dev) {
         return fail(ALS_E_INVALID, "null argument");

@@ -206,6 +206,12 @@ class Simulator:
                                              ctypes.byref(ms)))
         return {"blocks_per_sm": bps.value, "level_order": list(order), "ms_per_step": ms.value}
 
+    def write_netcdf(self, basename, snapshot=0, member=0):
+        """Writes member's state to <basename>_<snapshot>.nc (NetCDFWriter layout)."""
+        _lib.check(self._lib.als_solver_write_netcdf(self._h, member, basename.encode(),
+                                                     int(snapshot)))
+        return "%s_%d.nc" % (basename, snapshot)
+
     def region_sums(self, first_member=0, count=None, lo=None, hi=None):
         """FP64 sums of each conserved variable over the interior box [lo, hi)
         (interior cell coordinates, default the whole interior): (count, nvar)."""

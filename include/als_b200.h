@@ -257,6 +257,24 @@ int als_stats_moments(als_stats* st, long long* n, double** mean, double** m2);
 /* Writes mean and variance (device arrays of `count` doubles; either may be NULL). */
 int als_stats_result(als_stats* st, double* mean, double* variance, void* stream);
 
+/* ------------------------------------------------------------- output
+ * Snapshot files with the layout of alsfvm::io::NetCDFWriter
+ * (alsfvm/src/io/NetCDFWriter.cpp:32-146) in the classic NetCDF format
+ * (version 2, 64-bit offsets; the reference writes NetCDF-4 through
+ * libnetcdf, which readers open alike): dimensions t = 1, x, y, z; a double
+ * variable "time"; one double variable per conserved variable with
+ * dimensions (x, y, z) holding the interior cells in the order
+ * Volume::copyInternalCells gives them (x fastest); global text attributes.
+ * `interior` holds nvar host arrays of n[0]*n[1]*n[2] doubles (1 for
+ * inactive directions). */
+int als_write_netcdf(const char* path, int dimension, const int* n, int nvar,
+    const char* const* names, const double* const* interior, double time, int nattr,
+    const char* const* attr_names, const char* const* attr_values);
+/* The current state of one member, its time and the reference's variable
+ * names (rho, mx, [my, [mz,]] E) into <basename>_<snapshot>.nc
+ * (alsfvm/src/io/io_utils.cpp:34-40). */
+int als_solver_write_netcdf(als_solver* s, int member, const char* basename, int snapshot);
+
 /* ------------------------------------------------- structure functions
  * Structure-function statistics of `members` states (device memory, FP64
  * or FP32, `member_stride` elements apart, dimension+2 padded planes each)
