@@ -254,3 +254,25 @@ def test_fp32_members_stay_close_to_fp64():
     # (my starts at zero, so its own norm is no scale)
     rel = np.abs(a - b).sum(axis=(2, 3, 4)) / np.abs(a[:, :1]).sum(axis=(2, 3, 4))
     assert rel.max() < 1e-4, rel
+
+
+@pytest.mark.parametrize("dim,n,steps", [(2, (1024, 1024), 6), (3, (128, 128, 128), 2)])
+def test_full_size_steps_match_oracle(c_oracle, dim, n, steps):
+    """The benchmark sizes themselves (KH 1024^2, KH 128^3; WENO2 + HLL3,
+    RK3, periodic, FP64): a few whole time steps bit for bit, step for step."""
+    g = 2
+    params = als.uniform_draws(40, 3, 1)[0]
+    st = als.kelvin_helmholtz(n[0], params, g, dimension=dim)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    cfg = c_oracle.config(dim, n, lo, hi, "hll3", "weno2", "rungekutta3", "periodic", 1.4)
+    rc, U_ref, dts, done, t = c_oracle.simulate(cfg, st, 0.4, 10.0, max_steps=steps)
+    assert rc == 0 and done == steps
+    with als.Simulator(dim, n, lo, hi, flux="hll3", reconstruction="weno2",
+                       integrator="rungekutta3", boundary="periodic", cfl=0.4,
+                       end_time=10.0, max_steps=steps) as sim:
+        sim.set_state(st)
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["steps"] == steps and info["t"] == t and info["dt"] == dts[steps - 1]
+    np.testing.assert_array_equal(U, U_ref)
