@@ -154,9 +154,12 @@ struct PlaneFetch {
 template<class R, int NV, int RECON>
 __global__ void __launch_bounds__(256) reconstruct_dir(Planes<R> in, Planes<R> left,
     Planes<R> right, int dim, int N0, int N1, int N2, int G, int dir, double gamma) {
-    const int e0 = dir == 0 ? N0 - 2 * G + 2 : N0 - 2 * G;
-    const int e1 = dim > 1 ? (dir == 1 ? N1 - 2 * G + 2 : N1 - 2 * G) : 1;
-    const int e2 = dim > 2 ? (dir == 2 ? N2 - 2 * G + 2 : N2 - 2 * G) : 1;
+    // WENOCPU<3> also reconstructs every cell across the direction, ghosts
+    // included (WENOCPU.cpp:100-106); the others only the interior
+    const int gt = RECON == RECON_WENO3 ? 0 : G;
+    const int e0 = dir == 0 ? N0 - 2 * G + 2 : N0 - 2 * gt;
+    const int e1 = dim > 1 ? (dir == 1 ? N1 - 2 * G + 2 : N1 - 2 * gt) : 1;
+    const int e2 = dim > 2 ? (dir == 2 ? N2 - 2 * G + 2 : N2 - 2 * gt) : 1;
     const long long count = (long long)e0 * e1 * e2;
     const long long s = dir == 0 ? 1 : (dir == 1 ? N0 : (long long)N0 * N1);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
@@ -164,9 +167,9 @@ __global__ void __launch_bounds__(256) reconstruct_dir(Planes<R> in, Planes<R> l
         const int a = int(i % e0);
         const int b = int((i / e0) % e1);
         const int c = int(i / ((long long)e0 * e1));
-        const int x = a + G - (dir == 0 ? 1 : 0);
-        const int y = dim > 1 ? b + G - (dir == 1 ? 1 : 0) : 0;
-        const int z = dim > 2 ? c + G - (dir == 2 ? 1 : 0) : 0;
+        const int x = dir == 0 ? a + G - 1 : a + gt;
+        const int y = dim > 1 ? (dir == 1 ? b + G - 1 : b + gt) : 0;
+        const int z = dim > 2 ? (dir == 2 ? c + G - 1 : c + gt) : 0;
         const long long idx = ((long long)z * N1 + y) * N0 + x;
         PlaneFetch<R, NV> f{&in, idx, s};
         R l[NV], r[NV];

@@ -51,7 +51,7 @@ int grid_blocks(long long work, int threads) {
 
 bool valid_choice(int flux, int recon) {
     return flux >= ALS_FLUX_HLL && flux <= ALS_FLUX_CENTRAL && recon >= ALS_RECON_NONE &&
-        recon <= ALS_RECON_WENOF2;
+        recon <= ALS_RECON_WENO3;
 }
 
 cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
@@ -310,7 +310,7 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
     }
     const int nvar = grid->dimension + 2;
     if (direction < 0 || direction >= grid->dimension || reconstruction < ALS_RECON_NONE ||
-        reconstruction > ALS_RECON_WENOF2) {
+        reconstruction > ALS_RECON_WENO3) {
         return fail(ALS_E_INVALID, "invalid reconstruction arguments");
     }
     rc = check_planes((const void* const*)in, nvar);
@@ -358,6 +358,7 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
     case ALS_RECON_MC: ALS_RECON_CASE(NV, als::RECON_MC); break;                             \
     case ALS_RECON_MM: ALS_RECON_CASE(NV, als::RECON_MM); break;                             \
     case ALS_RECON_WENOF2: ALS_RECON_CASE(NV, als::RECON_WENOF2); break;                     \
+    case ALS_RECON_WENO3: ALS_RECON_CASE(NV, als::RECON_WENO3); break;                       \
     default: ALS_RECON_CASE(NV, als::RECON_ENO4); break;                                     \
     }
     if (dim == 1) {

@@ -21,14 +21,14 @@
 namespace als {
 
 enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4,
-             RECON_MC = 5, RECON_MM = 6, RECON_WENOF2 = 7 };
+             RECON_MC = 5, RECON_MM = 6, RECON_WENOF2 = 7, RECON_WENO3 = 8 };
 enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2 };
 
 __host__ __device__ constexpr int recon_ghosts(int recon) {
     return recon == RECON_NONE ? 1
         : (recon == RECON_WENO2 || recon == RECON_ENO2 || recon == RECON_MC || recon == RECON_MM ||
            recon == RECON_WENOF2) ? 2
-        : (recon == RECON_ENO3 ? 3 : 4);
+        : ((recon == RECON_ENO3 || recon == RECON_WENO3) ? 3 : 4);
 }
 
 // Left/right face state of one cell along direction D.
@@ -366,6 +366,59 @@ __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right,
             const R up = f.at(v, 1);
             left[v] = R(0.5) * (w1Left * um + cl * u0 - w0Left * up);
             right[v] = R(0.5) * (w0Right * up + cr * u0 - w1Right * um);
+        }
+    } else if (RECON == RECON_WENO3) {
+        // WENOCPU<3> (WENOCPU.cpp:34-187), WENOCoefficients<3>
+        // (WENOCoefficients.hpp:52-66, WENOCoefficients.cpp:24-37): smoothness
+        // of rho on the three ENO3 stencils, weights c_i / (beta_i + eps)^2
+        // summed from i = 2 down, ENO3 candidate values combined per variable
+        // (std::pow(x, 2) with its constant exponent is x*x)
+        const R eps = R(1e-8);
+        const R v0 = f.at(0, -2), v1 = f.at(0, -1), v2 = f.at(0, 0), v3 = f.at(0, 1), v4 = f.at(0, 2);
+        const R c1312 = R(13.0 / 12.0);
+        const R quarter = R(1 / 4.0);
+        R q = v2 - R(2) * v3 + v4;
+        R beta0 = c1312 * (q * q);
+        q = R(3) * v2 - R(4) * v3 + v4;
+        beta0 = beta0 + quarter * (q * q);
+        q = v1 - R(2) * v2 + v3;
+        R beta1 = c1312 * (q * q);
+        q = v1 - v3;
+        beta1 = beta1 + quarter * (q * q);
+        q = v0 - R(2) * v1 + v2;
+        R beta2 = c1312 * (q * q);
+        q = v0 - R(4) * v1 + R(3) * v2;
+        beta2 = beta2 + quarter * (q * q);
+        const R cw0 = R(3.0 / 10.0), cw1 = R(3.0 / 5.0), cw2 = R(1.0 / 10.0);
+        const R d2 = (beta2 + eps) * (beta2 + eps);
+        const R d1 = (beta1 + eps) * (beta1 + eps);
+        const R d0 = (beta0 + eps) * (beta0 + eps);
+        R ar[3], al[3];
+        ar[2] = cw2 / d2;
+        al[2] = cw0 / d2;
+        ar[1] = cw1 / d1;
+        al[1] = cw1 / d1;
+        ar[0] = cw0 / d0;
+        al[0] = cw2 / d0;
+        const R sr = ((R(0) + ar[2]) + ar[1]) + ar[0];
+        const R sl = ((R(0) + al[2]) + al[1]) + al[0];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R lw = R(0), rw = R(0);
+#pragma unroll
+            for (int shift = 0; shift < 3; ++shift) {
+                R lv = R(0), rv = R(0);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const R value = f.at(v, j - shift);
+                    lv += eno_coef<R, 3>(shift, j) * value;
+                    rv += eno_coef<R, 3>(shift + 1, j) * value;
+                }
+                lw += lv * (al[shift] / sl);
+                rw += rv * (ar[shift] / sr);
+            }
+            left[v] = lw;
+            right[v] = rw;
         }
     } else if (RECON == RECON_WENOF2) {
         // WENOF2.hpp:37-121: WENO2 weights of rho, slopes in primitive variables

@@ -90,6 +90,7 @@ cudaError_t launch_stage_dim(int recon, int flux, int kind, const StageParams& P
     case RECON_MC: return launch_stage_flux<R, DIM, RECON_MC>(flux, kind, P, b, s);
     case RECON_MM: return launch_stage_flux<R, DIM, RECON_MM>(flux, kind, P, b, s);
     case RECON_WENOF2: return launch_stage_flux<R, DIM, RECON_WENOF2>(flux, kind, P, b, s);
+    case RECON_WENO3: return launch_stage_flux<R, DIM, RECON_WENO3>(flux, kind, P, b, s);
     default: return cudaErrorInvalidValue;
     }
 }

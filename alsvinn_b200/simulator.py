@@ -18,7 +18,7 @@ from .initial_data import padded_shape
 
 FLUX = {"hll": 0, "hll3": 1, "central": 2}
 RECONSTRUCTION = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
-                  "wenof2": 7}
+                  "wenof2": 7, "weno3": 8}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
 BOUNDARY = {"neumann": 0, "periodic": 1}
 PRECISION = {"fp64": 0, "fp32": 1}

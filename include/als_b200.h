@@ -44,6 +44,7 @@ extern "C" {
 #define ALS_RECON_MC 5              /* "mc", reconstruction/MC.hpp */
 #define ALS_RECON_MM 6              /* "mm", reconstruction/MM.hpp */
 #define ALS_RECON_WENOF2 7          /* "wenof2", reconstruction/WENOF2.hpp (WENO2 in primitive variables, bounded) */
+#define ALS_RECON_WENO3 8           /* "weno3", reconstruction/WENOCPU.cpp (order 3, three ghost cells) */
 #define ALS_INT_FORWARD_EULER 0     /* "forwardeuler", integrator/ForwardEuler.cpp */
 #define ALS_INT_RK2 1               /* "rungekutta2",  integrator/RungeKutta2.cpp */
 #define ALS_INT_RK3 2               /* "rungekutta3",  integrator/RungeKutta3.cpp */

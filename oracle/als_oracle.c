@@ -207,6 +207,7 @@ int orc_ghost_cells(int flux, int recon) {
     case ORC_RECON_MC: rg = 2; break;
     case ORC_RECON_MM: rg = 2; break;
     case ORC_RECON_WENOF2: rg = 2; break;
+    case ORC_RECON_WENO3: rg = 3; break;
     default: return -1;
     }
     return rg > 1 ? rg : 1;
@@ -383,6 +384,51 @@ static void reconstruct_cell(const orc_config* cfg, const double* in, long plane
             left[var] = 0.5 * (w1Left * um + (3 * w0Left + w1Left) * u0 - w0Left * up);
             right[var] = 0.5 * (w0Right * up + (3 * w1Right + w0Right) * u0 - w1Right * um);
         }
+    } else if (cfg->recon == ORC_RECON_WENO3) {
+        /* WENOCPU<3> (WENOCPU.cpp:34-187) with WENOCoefficients<3>
+         * (WENOCoefficients.hpp:52-66, WENOCoefficients.cpp:24-37); the
+         * reference's std::pow(x, 2) has a constant exponent and is x*x */
+        static const double c3[3] = {3.0 / 10.0, 3.0 / 5.0, 1.0 / 10.0};
+        const double eps = 1e-8;
+        double V[5], beta[3], al[3], ar[3], sl = 0.0, sr = 0.0, q;
+        int i, shift, j;
+        for (i = -2; i <= 2; ++i) {
+            V[i + 2] = in[c + i * s];
+        }
+        q = V[2] - 2 * V[3] + V[4];
+        beta[0] = 13.0 / 12.0 * (q * q);
+        q = 3 * V[2] - 4 * V[3] + V[4];
+        beta[0] = beta[0] + 1 / 4.0 * (q * q);
+        q = V[1] - 2 * V[2] + V[3];
+        beta[1] = 13.0 / 12.0 * (q * q);
+        q = V[1] - V[3];
+        beta[1] = beta[1] + 1 / 4.0 * (q * q);
+        q = V[0] - 2 * V[1] + V[2];
+        beta[2] = 13.0 / 12.0 * (q * q);
+        q = V[0] - 4 * V[1] + 3 * V[2];
+        beta[2] = beta[2] + 1 / 4.0 * (q * q);
+        for (i = 2; i >= 0; --i) {
+            const double d = (beta[i] + eps) * (beta[i] + eps);
+            ar[i] = c3[i] / d;
+            sr += ar[i];
+            al[i] = c3[2 - i] / d;
+            sl += al[i];
+        }
+        for (var = 0; var < nvar; ++var) {
+            double lw = 0.0, rw = 0.0;
+            for (shift = 0; shift < 3; ++shift) {
+                double lv = 0.0, rv = 0.0;
+                for (j = 0; j < 3; ++j) {
+                    const double value = in[var * plane + c - (long)(shift - j) * s];
+                    lv += eno_coef(3, shift, j) * value;
+                    rv += eno_coef(3, shift + 1, j) * value;
+                }
+                lw += lv * (al[shift] / sl);
+                rw += rv * (ar[shift] / sr);
+            }
+            left[var] = lw;
+            right[var] = rw;
+        }
     } else if (cfg->recon == ORC_RECON_WENOF2) {
         /* WENOF2.hpp:37-121: weights as WENO2, slopes of the primitive
          * variables (Euler.hpp:290-297) bounded, limited, back to conserved
@@ -514,6 +560,11 @@ void orc_reconstruct(const orc_config* cfg, int dir, const double* in, double* l
         const int gd = d < cfg->dim ? g : 0;
         lo[d] = gd - (d == dir ? 1 : 0);
         hi[d] = N[d] - gd + (d == dir ? 1 : 0);
+        if (cfg->recon == ORC_RECON_WENO3 && d != dir) {
+            /* WENOCPU.cpp:100-106: every cell across the direction, ghosts included */
+            lo[d] = 0;
+            hi[d] = N[d];
+        }
     }
     for (z = lo[2]; z < hi[2]; ++z) {
         for (y = lo[1]; y < hi[1]; ++y) {

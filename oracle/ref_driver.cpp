@@ -29,6 +29,7 @@
 #include "alsfvm/reconstruction/MC.hpp"
 #include "alsfvm/reconstruction/MM.hpp"
 #include "alsfvm/reconstruction/WENOF2.hpp"
+#include "alsfvm/reconstruction/WENOCPU.hpp"
 #include "alsfvm/reconstruction/ENOCPU.hpp"
 #include "alsfvm/reconstruction/NoReconstruction.hpp"
 #include "alsfvm/integrator/ForwardEuler.hpp"
@@ -123,8 +124,8 @@ std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Object
     if (g_flux_platform == "b200-parts") {
         // the reference's NumericalFluxCPU over the B200 reconstruction
         static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
-            "wenof2"};
-        return std::make_shared<b200::ReconstructionB200>(d, b200_code(s.recon, recons, 8), s.gamma);
+            "wenof2", "weno3"};
+        return std::make_shared<b200::ReconstructionB200>(d, b200_code(s.recon, recons, 9), s.gamma);
     }
 #endif
     if (s.recon == "weno2") {
@@ -137,6 +138,8 @@ std::shared_ptr<reconstruction::Reconstruction> makeRecon(const Setup& s, Object
         return std::make_shared<reconstruction::ENOCPU<4>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
     } else if (s.recon == "mc") {
         return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::MC<Eq>, Eq>>(*o.params);
+    } else if (s.recon == "weno3") {
+        return std::make_shared<reconstruction::WENOCPU<3>>();
     } else if (s.recon == "wenof2") {
         return std::make_shared<reconstruction::ReconstructionCPU<reconstruction::WENOF2<Eq>, Eq>>(*o.params);
     } else if (s.recon == "mm") {
@@ -156,9 +159,9 @@ std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
         // names in the order of the ALS_FLUX_* / ALS_RECON_* codes
         static const char* const fluxes[] = {"hll", "hll3", "central"};
         static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
-            "wenof2"};
+            "wenof2", "weno3"};
         return std::make_shared<numflux::NumericalFluxB200>(*o.grid, b200_code(s.flux, fluxes, 3),
-            b200_code(s.recon, recons, 8), s.gamma);
+            b200_code(s.recon, recons, 9), s.gamma);
     }
 #endif
     if (s.flux == "hll") {

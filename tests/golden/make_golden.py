@@ -62,6 +62,11 @@ SIMULATIONS = {
                                "neumann", 0.45, 0.2, "sod"),
     "kh32_wenof2_hll3_rk3": (2, (32, 32), (0.0, 0.0), (1.0, 1.0), "hll3", "wenof2", "rungekutta3",
                              "periodic", 0.4, 0.2, "kh"),
+    # WENO of order 3 (WENOCPU<3>)
+    "sod256_weno3_hll_rk3": (1, (256,), (-1.0,), (1.0,), "hll", "weno3", "rungekutta3", "neumann",
+                             0.45, 0.2, "sod"),
+    "kh24_weno3_hll3_rk3": (2, (24, 24), (0.0, 0.0), (1.0, 1.0), "hll3", "weno3", "rungekutta3",
+                            "periodic", 0.4, 0.2, "kh"),
 }
 
 
@@ -76,7 +81,7 @@ def initial_state(kind, dim, n, g):
 
 
 def write_limiter_cases(ref):
-    """One spatial-operator evaluation per (dim, MC/MM/WENOF2, flux, boundary)."""
+    """One spatial-operator evaluation per (dim, MC/MM/WENOF2/WENO3, flux, boundary)."""
     cases = []
     seed = 2000
     for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
@@ -98,6 +103,16 @@ def write_limiter_cases(ref):
                 filled, net, ws = ref.compute_flux(dim, n, [0.0] * dim, [1.0] * dim, flux,
                                                    "wenof2", bc, 1.4, st)
                 cases.append((dim, ",".join(map(str, n)), "wenof2", flux, bc, seed,
+                              digest(filled), digest(net), digest(ws), float(ws.max())))
+    seed = 2700
+    for dim, n in ((1, (16,)), (2, (10, 9)), (3, (8, 8, 9))):
+        for flux in ("hll", "hll3", "central"):
+            for bc in ("neumann", "periodic"):
+                seed += 1
+                st = smooth_random_state(seed, dim, n, 3)
+                filled, net, ws = ref.compute_flux(dim, n, [0.0] * dim, [1.0] * dim, flux,
+                                                   "weno3", bc, 1.4, st)
+                cases.append((dim, ",".join(map(str, n)), "weno3", flux, bc, seed,
                               digest(filled), digest(net), digest(ws), float(ws.max())))
     with open(os.path.join(HERE, "compute_flux_cases_limiters.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "

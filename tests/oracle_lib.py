@@ -22,7 +22,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 
 FLUX = {"hll": 0, "hll3": 1, "central": 2}
 RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
-         "wenof2": 7}
+         "wenof2": 7, "weno3": 8}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
 BC = {"neumann": 0, "periodic": 1}
 
@@ -37,7 +37,7 @@ def _dptr(a):
 
 def ghost_cells(recon):
     return {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 2, "mm": 2,
-            "wenof2": 2}[recon]
+            "wenof2": 2, "weno3": 3}[recon]
 
 
 def padded_shape(dim, n, g):

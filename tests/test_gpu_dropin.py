@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 CASES = []
 for _dim, _n in ((1, (32,)), (2, (14, 12)), (3, (8, 9, 8))):
-    for _recon in ("weno2", "eno3", "mc", "wenof2", "none"):
+    for _recon in ("weno2", "eno3", "mc", "wenof2", "weno3", "none"):
         for _flux, _integ, _bc in (("hll3", "rungekutta3", "periodic"),
                                    ("hll", "rungekutta2", "neumann"),
                                    ("central", "forwardeuler", "periodic")):

@@ -56,7 +56,7 @@ def test_sod_1024_reference_numbers():
 
 CASES = []
 for _dim, _n in ((1, (40,)), (2, (19, 21)), (3, (10, 9, 11))):
-    for _recon in ("none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2"):
+    for _recon in ("none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2", "weno3"):
         if min(_n) < 2 * ghost_cells(_recon):
             continue
         for _flux in ("hll", "hll3", "central"):
@@ -111,7 +111,7 @@ def test_plugin_boundary_and_flux_match_reference(case):
 
 
 @pytest.mark.parametrize("dim,n", [(1, (20,)), (2, (11, 12)), (3, (8, 9, 10))])
-@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2"])
+@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2", "weno3"])
 def test_plugin_reconstruction_matches_oracle(c_oracle, dim, n, recon):
     g = ghost_cells(recon)
     if min(n) < 2 * g:

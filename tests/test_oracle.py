@@ -62,14 +62,14 @@ def test_c_oracle_meanvar_matches_reference(c_oracle):
 
 
 @pytest.mark.parametrize("dim,n", [(1, (24,)), (2, (10, 11)), (3, (8, 9, 8))])
-@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2"])
+@pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2", "weno3"])
 def test_c_oracle_matches_reference_build(c_oracle, ref_oracle, dim, n, recon):
     """Fresh random cases against the reference build (skipped without it)."""
     g = ghost_cells(recon)
     if min(n) < 2 * g:
         pytest.skip("grid smaller than two ghost widths")
     seed = 5000 + 17 * dim + 3 * ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
-                                  "wenof2"].index(recon)
+                                  "wenof2", "weno3"].index(recon)
     for flux in ("hll", "hll3", "central"):
         for bc in ("neumann", "periodic"):
             st = smooth_random_state(seed, dim, n, g)
