@@ -117,6 +117,7 @@ PROTOTYPES = {
                                          ctypes.POINTER(ctypes.c_float), _VP]),
     "als_mlp_train": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      _VP, _VP]),
+    "als_mlp_test_wait_timeout": (ctypes.c_int, [_VP, ctypes.c_uint, ctypes.c_int]),
     "als_mlp_sample_uniform": (ctypes.c_int, [_VP, ctypes.c_longlong, ctypes.c_ulonglong, _VP]),
 }
 

@@ -64,6 +64,8 @@ struct als_mlp {
     float* v = nullptr;
     long long* step = nullptr;      // Adam step counter (device)
     int* error = nullptr;           // set by a GEMM whose wait gave up
+    unsigned wait_limit = 0;        // als_mlp_test_wait_timeout
+    int withhold_commit = 0;
     // training workspace (max_batch rows)
     __nv_bfloat16* xb = nullptr;    // packed inputs (rows x kpad0)
     std::vector<float*> z;          // pre-activations per hidden layer
@@ -101,6 +103,13 @@ int dev_alloc(als_mlp* s, T** p, size_t count) {
             return rc_;           \
         }                         \
     } while (0)
+
+// The error flag and wait settings every tcgen05 GEMM of `s` receives.
+void arm(const als_mlp* s, GemmArgs& a) {
+    a.error = s->error;
+    a.wait_limit = s->wait_limit;
+    a.withhold_commit = s->withhold_commit;
+}
 
 int grid_for(long long work, int threads) {
     long long b = (work + threads - 1) / threads;
@@ -217,7 +226,7 @@ int forward_hidden(als_mlp* s, const __nv_bfloat16* x, long long rows_pad,
         a.h = hs ? (*hs)[l] : hbuf[l & 1];
         a.ldz = L.out;
         a.ldh = L.out;
-        a.error = s->error;
+        arm(s, a);
         // training batches: narrow N tiles for more CTAs; inference: the
         // whole layer width per CTA, so each activation tile is read once
         if (!zs && s->tma) {
@@ -351,7 +360,7 @@ int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, floa
         a.g = s->split_scratch;
         a.ldg = L.in;
         a.split_stride = (long long)L.out * L.in;
-        a.error = s->error;
+        arm(s, a);
         MLP_TRY((launch_gemm<64, EPI_WGRAD>(a, L.in, st, splits)));
         sum_splits<<<grid_for((long long)L.out * L.in, 256), 256, 0, st>>>(
             s->split_scratch, splits, (long long)L.out * L.in, s->g + L.w_off);
@@ -369,7 +378,7 @@ int enqueue_gradients(als_mlp* s, const float* x, const float* t, int rows, floa
             b.h = s->dz[(l - 1) & 1];
             b.ldz = L.in;
             b.ldh = L.in;
-            b.error = s->error;
+            arm(s, b);
             MLP_TRY((launch_gemm<64, EPI_BACKWARD>(b, L.in, st)));
         }
     }
@@ -689,6 +698,15 @@ int als_mlp_train(als_mlp* s, const float* x_dev, const float* t_dev, int rows, 
                                         cudaGetErrorString(le != cudaSuccess ? le : se));
     }
     return check_error_flag(s);
+}
+
+int als_mlp_test_wait_timeout(als_mlp* s, unsigned wait_limit, int withhold_commit) {
+    if (!s) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument");
+    }
+    s->wait_limit = wait_limit;
+    s->withhold_commit = withhold_commit ? 1 : 0;
+    return ALS_OK;
 }
 
 int als_mlp_sample_uniform(float* x_dev, long long count, unsigned long long seed, void* stream) {

@@ -77,11 +77,13 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
     static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM columns: power of two");
     extern __shared__ unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
+    __shared__ uint64_t drain;
     __shared__ uint32_t tmem_base;
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     constexpr int kABytes = kTileM * kChunkK * 2;
     constexpr int kBBytes = BN * kChunkK * 2;
+    const unsigned limit = g.wait_limit ? g.wait_limit : kWaitLimit;
     unsigned char* sa[2] = {base, base + kABytes + kBBytes};
     unsigned char* sb[2] = {base + kABytes, base + 2 * kABytes + kBBytes};
 
@@ -97,6 +99,7 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&drain, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
         const int s = c & 1;
         bool ok = true;
         if (c >= 2) {
-            ok = mbar_wait(&bars[s], unsigned((c - 2) >> 1) & 1u);
+            ok = mbar_wait(&bars[s], unsigned((c - 2) >> 1) & 1u, limit);
         }
         if (__syncthreads_or(!ok)) {
             failed = true;
@@ -131,18 +134,23 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int n_valid)
                 mma_bf16(tmem, smem_desc(a0 + j * 256, 128, 1024),
                          smem_desc(b0 + j * 256, 128, 1024), idesc, (c > 0 || j > 0) ? 1u : 0u);
             }
-            mma_commit(&bars[s]);
+            if (!g.withhold_commit) {
+                mma_commit(&bars[s]);
+            }
         }
         last = c;
     }
     bool done = false;
     if (last >= 0) {
-        done = mbar_wait(&bars[last & 1], unsigned(last >> 1) & 1u);
+        done = mbar_wait(&bars[last & 1], unsigned(last >> 1) & 1u, limit);
     }
     if (__syncthreads_or(!done) || failed) {
         if (threadIdx.x == 0) {
             atomicExch(g.error, 1);
+            // every MMA issued so far completes before TMEM is freed
+            mma_commit(&drain);
         }
+        mbar_wait(&drain, 0, kWaitLimit);
     } else {
         tc_fence_after();
         const long long m = m0 + warp * 32 + lane;

@@ -51,6 +51,9 @@ struct GemmArgs {
     long long ldz, ldh, ldg;
     long long split_stride;     // EPI_WGRAD: elements between the outputs of K splits
     int* error;                 // set to 1 when a wait gave up
+    unsigned wait_limit;        // polls per wait; 0: kWaitLimit
+    int withhold_commit;        // failure-detection test: no chunk is committed, so
+                                // the waits run out and the error flag is set
 };
 
 // GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear Units",
@@ -113,8 +116,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 }
 
 // Bounded wait for the completion of phase `parity` of `bar`.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-    for (unsigned i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned limit = kWaitLimit) {
+    for (unsigned i = 0; i < limit; ++i) {
         if (mbar_try_wait(bar, parity)) {
             return true;
         }

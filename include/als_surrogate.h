@@ -69,6 +69,17 @@ int als_mlp_gradients(als_mlp* h, const float* x_dev, const float* t_dev, int ro
 int als_mlp_train(als_mlp* h, const float* x_dev, const float* t_dev, int rows, int steps,
                   float lr, float* loss_dev, void* stream);
 
+/* Failure-detection hook for tests.  Every wait of the tensor-core GEMMs
+ * that compute gradients and train (and of inference when width is not
+ * 256) polls its barrier at most `wait_limit` times (0: the default, about
+ * 4 M polls) and, after a timeout, sets the handle's error flag, waits for
+ * its own MMAs in flight, frees its tensor memory and returns; the call then
+ * returns ALS_E_CUDA ("tensor-core GEMM wait timed out") and the handle and
+ * the CUDA context stay usable.  With `withhold_commit` nonzero these GEMMs
+ * issue no completion commit, so their waits run out (nothing else is
+ * skipped); 0 restores normal operation. */
+int als_mlp_test_wait_timeout(als_mlp* h, unsigned wait_limit, int withhold_commit);
+
 /* U[0,1) draws (24-bit, counter based on `seed` and the index) into
  * x_dev[0 .. count). */
 int als_mlp_sample_uniform(float* x_dev, long long count, unsigned long long seed, void* stream);
