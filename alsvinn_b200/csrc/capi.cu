@@ -50,8 +50,18 @@ int grid_blocks(long long work, int threads) {
 }
 
 bool valid_choice(int flux, int recon) {
-    return flux >= ALS_FLUX_HLL && flux <= ALS_FLUX_CENTRAL && recon >= ALS_RECON_NONE &&
+    return flux >= ALS_FLUX_HLL && flux <= ALS_FLUX_TECNO6 && recon >= ALS_RECON_NONE &&
         recon <= ALS_RECON_WENO3;
+}
+
+// The TeCNO fluxes are built with reconstruction "none", the way the
+// reference pairs them (the high-order part of the TeCNO scheme sits in its
+// diffusion operator); the stencil fluxes tecno4/6 read the cell values.
+int check_supported(int flux, int recon) {
+    if (flux >= ALS_FLUX_TECNO1 && recon != ALS_RECON_NONE) {
+        return fail(ALS_E_UNSUPPORTED, "the TeCNO fluxes are built for reconstruction \"none\"");
+    }
+    return ALS_OK;
 }
 
 cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
@@ -207,8 +217,12 @@ int als_ghost_cells(int flux, int reconstruction) {
     if (!valid_choice(flux, reconstruction)) {
         return fail(ALS_E_INVALID, "unknown flux or reconstruction");
     }
-    // every in-scope flux uses the two-point stencil {0, 1} (numflux_util.hpp:52-60)
-    return std::max(1, als::recon_ghosts(reconstruction));
+    const int rc = check_supported(flux, reconstruction);
+    if (rc != ALS_OK) {
+        return rc;
+    }
+    // max(stencil size - 1, reconstruction ghosts) (NumericalFluxCPU.cpp:225-231)
+    return als::stage_ghosts(reconstruction, flux);
 }
 
 int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, int nvar,
@@ -242,6 +256,10 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     }
     if (!valid_choice(flux, reconstruction) || !wave_speed) {
         return fail(ALS_E_INVALID, "invalid flux arguments");
+    }
+    rc = check_supported(flux, reconstruction);
+    if (rc != ALS_OK) {
+        return rc;
     }
     const int nvar = grid->dimension + 2;
     rc = check_planes((const void* const*)in, nvar);
@@ -674,6 +692,9 @@ int check_config(const als_solver_config* cfg) {
         return fail(ALS_E_INVALID, "invalid solver configuration");
     }
     const int g = als_ghost_cells(cfg->flux, cfg->reconstruction);
+    if (g < 0) {
+        return g;
+    }
     for (int d = 0; d < cfg->dimension; ++d) {
         // ConservedSystem splits the update into an interior and 2*dim side
         // regions of width g (ConservedSystem.cpp:59-96); with fewer than 2g
@@ -1588,6 +1609,10 @@ extern "C" int als_compute_flux_static(const als_grid* grid, int flux, int recon
     }
     if (!valid_choice(flux, reconstruction) || !in || !out || !wave_speed) {
         return fail(ALS_E_INVALID, "invalid flux arguments");
+    }
+    rc = check_supported(flux, reconstruction);
+    if (rc != ALS_OK) {
+        return rc;
     }
     if (members < 1 || members > kStaticFluxMembers) {
         return fail(ALS_E_INVALID, "als_compute_flux_static takes 1 to 1024 states per call");

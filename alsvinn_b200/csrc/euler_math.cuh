@@ -22,13 +22,30 @@ namespace als {
 
 enum Recon { RECON_NONE = 0, RECON_WENO2 = 1, RECON_ENO2 = 2, RECON_ENO3 = 3, RECON_ENO4 = 4,
              RECON_MC = 5, RECON_MM = 6, RECON_WENOF2 = 7, RECON_WENO3 = 8 };
-enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2 };
+enum Flux { FLUX_HLL = 0, FLUX_HLL3 = 1, FLUX_CENTRAL = 2, FLUX_TECNO1 = 3, FLUX_TECNO4 = 4,
+            FLUX_TECNO6 = 5 };
 
 __host__ __device__ constexpr int recon_ghosts(int recon) {
     return recon == RECON_NONE ? 1
         : (recon == RECON_WENO2 || recon == RECON_ENO2 || recon == RECON_MC || recon == RECON_MM ||
            recon == RECON_WENOF2) ? 2
         : ((recon == RECON_ENO3 || recon == RECON_WENO3) ? 3 : 4);
+}
+
+// Ghost cells the flux's stencil needs: stencil size - 1 (NumericalFluxCPU.cpp:225-231);
+// TecnoCombined4/6 read {-1..2} / {-2..3} (TecnoCombined4.hpp:62-66,
+// TecnoCombined6.hpp:67-71), every other flux the two-point {0, 1}.
+__host__ __device__ constexpr int flux_ghosts(int flux) {
+    return flux == FLUX_TECNO4 ? 3 : (flux == FLUX_TECNO6 ? 5 : 1);
+}
+
+// Stencil fluxes read the cell values themselves (reconstruction "none").
+__host__ __device__ constexpr bool stencil_flux(int flux) {
+    return flux == FLUX_TECNO4 || flux == FLUX_TECNO6;
+}
+
+__host__ __device__ constexpr int stage_ghosts(int recon, int flux) {
+    return recon_ghosts(recon) > flux_ghosts(flux) ? recon_ghosts(recon) : flux_ghosts(flux);
 }
 
 // Left/right face state of one cell along direction D.
@@ -105,10 +122,11 @@ __device__ __forceinline__ R flux_hll(const FaceState<R, NSD>& L, const FaceStat
     return fmax(fabs(sL), fabs(sR));
 }
 
-template<class R, int NSD, int D>
-__device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
-    R gamma, R* F) {
-    constexpr int NV = NSD + 2;
+// HLL3::computeHLLSpeeds (HLL3.hpp:120-160): Roe-averaged speeds with the
+// shock correction.
+template<class R, int NSD>
+__device__ __forceinline__ void hll3_speeds(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R& sL, R& sR) {
     const R wl = sqrt(L.c[0]);
     const R wr = sqrt(Rt.c[0]);
     const R rho = (L.c[0] + Rt.c[0]) / R(2);
@@ -118,8 +136,16 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
     const R cfR = sqrt(gamma * Rt.p / Rt.c[0]);
     const R correct = R(0.5) * fmax(R(0), L.ud - Rt.ud);
     const R cs = sqrt(gamma * p / rho);
-    const R sL = fmin(L.ud + correct - cfL, ud - cs);
-    const R sR = fmax(Rt.ud - correct + cfR, ud + cs);
+    sL = fmin(L.ud + correct - cfL, ud - cs);
+    sR = fmax(Rt.ud - correct + cfR, ud + cs);
+}
+
+template<class R, int NSD, int D>
+__device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    R sL, sR;
+    hll3_speeds<R, NSD>(L, Rt, gamma, sL, sR);
     if (sL == R(0)) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
@@ -184,6 +210,89 @@ __device__ __forceinline__ R flux_central(const FaceState<R, NSD>& L, const Face
         fabs(Rt.ud) + sqrt(gamma * Rt.p / Rt.c[0]));
 }
 
+// Logarithmic mean (b - a) / (log b - log a), 0 when either difference is 0
+// (tecno_utils.hpp:30-38), and F over it, 0 when that mean is 0 (:42-50).
+template<class R>
+__device__ __forceinline__ R log_mean(R a, R b) {
+    const R d = b - a;
+    const R dl = log(b) - log(a);
+    if (d == R(0) || dl == R(0)) {
+        return R(0);
+    }
+    return d / dl;
+}
+
+template<class R>
+__device__ __forceinline__ R over_log_mean(R a, R b, R F) {
+    const R m = log_mean(a, b);
+    return m == R(0) ? R(0) : F / m;
+}
+
+// Parameter vector z = (sqrt(rho/p), sqrt(rho/p) u, sqrt(rho p))
+// (Euler.hpp:290-320), from the primitive variables u = m/rho and
+// p = (gamma-1)(E - 0.5 m.m/rho).
+template<class R, int NSD>
+__device__ __forceinline__ void tecno_z(const FaceState<R, NSD>& s, R* z) {
+    const R q = sqrt(s.c[0] / s.p);
+#pragma unroll
+    for (int k = 0; k < NSD; ++k) {
+        z[1 + k] = (s.c[1 + k] / s.c[0]) * q;
+    }
+    z[0] = q;
+    z[NSD + 1] = sqrt(s.c[0] * s.p);
+}
+
+// Entropy-conservative flux of Fjordholm, Mishra and Tadmor (SINUM 2012,
+// eq. 6.11) as the reference states it (numflux/euler/Tecno1.hpp:51-180):
+// the point flux when both states are equal; otherwise built from
+// arithmetic means of z and logarithmic means of z_0 and z_last.  The
+// reference writes the 2-D formulas for every dimension: in 3-D the
+// z-momentum flux is 0 and the z-direction flux stays 0 unless the states
+// are equal.  The wave speed is max |s| of the HLL3 speeds.
+template<class R, int NSD, int D>
+__device__ __forceinline__ R flux_tecno1(const FaceState<R, NSD>& L, const FaceState<R, NSD>& Rt,
+    R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    bool same = true;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        same = same && (L.c[k] == Rt.c[k]);
+    }
+    if (same) {
+        point_flux<R, NSD, D>(L, F);
+    } else if (NSD == 3 && D == 2) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = R(0);
+        }
+    } else {
+        R zl[NV], zr[NV];
+        tecno_z<R, NSD>(L, zl);
+        tecno_z<R, NSD>(Rt, zr);
+        auto bar = [&](int k) { return (zl[k] + zr[k]) / R(2); };
+        F[0] = bar(1 + D) * log_mean(zl[NSD + 1], zr[NSD + 1]);
+#pragma unroll
+        for (int k = 0; k < NSD; ++k) {
+            if (NSD == 3 && k == 2) {
+                F[1 + k] = R(0);
+            } else if (k == D) {
+                F[1 + k] = bar(NSD + 1) / bar(0) + bar(1 + D) / bar(0) * F[0];
+            } else {
+                F[1 + k] = bar(1 + k) / bar(0) * F[0];
+            }
+        }
+        R e = (gamma + R(1)) / (gamma - R(1)) * over_log_mean(zl[0], zr[0], F[0]);
+        e = e + bar(1) * F[1];
+        if (NSD > 1) {
+            e = e + bar(2) * F[2];
+        }
+        F[NSD + 1] = R(1) / (R(2) * bar(0)) * e;
+    }
+    R sL, sR;
+    hll3_speeds<R, NSD>(L, Rt, gamma, sL, sR);
+    return fmax(fabs(sL), fabs(sR));
+}
+
 // F(U-, U+) at one face along D.  ul = right-reconstructed value of the cell
 // left of the face, ur = left-reconstructed value of the cell to its right
 // (numflux_util.hpp:62-92).  Returns the face wave speed.
@@ -196,6 +305,8 @@ __device__ __forceinline__ R face_flux(const R* ul, const R* ur, R gamma, R* F) 
         return flux_hll<R, NSD, D>(L, Rt, gamma, F);
     } else if (FLUX == FLUX_HLL3) {
         return flux_hll3<R, NSD, D>(L, Rt, gamma, F);
+    } else if (FLUX == FLUX_TECNO1) {
+        return flux_tecno1<R, NSD, D>(L, Rt, gamma, F);
     } else {
         return flux_central<R, NSD, D>(L, Rt, gamma, F);
     }

@@ -16,7 +16,7 @@ namespace als {
 // there are work items.
 template<class R, int DIM, int RECON, int FLUX, int KIND>
 cudaError_t launch_stage_one(const StageParams& P, int blocks_per_sm, cudaStream_t stream) {
-    typedef StageLayout<R, DIM, RECON> Lay;
+    typedef StageLayout<R, DIM, RECON, FLUX> Lay;
     auto kernel = stage_kernel<R, DIM, RECON, FLUX, KIND>;
     // raising the dynamic shared-memory limit is idempotent and cheap; it is
     // done on every launch so that every device the process uses is covered
@@ -74,8 +74,18 @@ cudaError_t launch_stage_flux(int flux, int kind, const StageParams& P, int b, c
     case FLUX_HLL: return launch_stage_kind<R, DIM, RECON, FLUX_HLL>(kind, P, b, s);
     case FLUX_HLL3: return launch_stage_kind<R, DIM, RECON, FLUX_HLL3>(kind, P, b, s);
     case FLUX_CENTRAL: return launch_stage_kind<R, DIM, RECON, FLUX_CENTRAL>(kind, P, b, s);
-    default: return cudaErrorInvalidValue;
+    default: break;
     }
+    // the TeCNO fluxes are built for reconstruction "none" only
+    if constexpr (RECON == RECON_NONE) {
+        switch (flux) {
+        case FLUX_TECNO1: return launch_stage_kind<R, DIM, RECON, FLUX_TECNO1>(kind, P, b, s);
+        case FLUX_TECNO4: return launch_stage_kind<R, DIM, RECON, FLUX_TECNO4>(kind, P, b, s);
+        case FLUX_TECNO6: return launch_stage_kind<R, DIM, RECON, FLUX_TECNO6>(kind, P, b, s);
+        default: break;
+        }
+    }
+    return cudaErrorInvalidValue;
 }
 
 template<class R, int DIM>

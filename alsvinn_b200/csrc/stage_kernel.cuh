@@ -91,10 +91,11 @@ template<> struct TileShape<3> {
         B = ALS_STAGE3_BLOCKS;
 };
 
-template<class R, int DIM, int RECON>
+template<class R, int DIM, int RECON, int FLUX>
 struct StageLayout {
     static constexpr int NV = DIM + 2;
-    static constexpr int G = recon_ghosts(RECON);
+    static constexpr int G = stage_ghosts(RECON, FLUX);
+    static constexpr bool STENCIL = stencil_flux(FLUX);
     static constexpr int TX = TileShape<DIM>::X;
     static constexpr int TY = TileShape<DIM>::Y;
     static constexpr int TZ = TileShape<DIM>::Z;
@@ -109,7 +110,9 @@ struct StageLayout {
     static constexpr int REC0 = (TX + 2) * TY * TZ;
     static constexpr int REC1 = DIM > 1 ? TX * (TY + 2) * TZ : 0;
     static constexpr int REC2 = DIM > 2 ? TX * TY * (TZ + 2) : 0;
-    static constexpr int REC = REC0 > REC1 ? (REC0 > REC2 ? REC0 : REC2) : (REC1 > REC2 ? REC1 : REC2);
+    // stencil fluxes read the staged cells directly and need no reconstructed values
+    static constexpr int REC = STENCIL ? 0
+        : (REC0 > REC1 ? (REC0 > REC2 ? REC0 : REC2) : (REC1 > REC2 ? REC1 : REC2));
     static constexpr int FAC0 = (TX + 1) * TY * TZ;
     static constexpr int FAC1 = DIM > 1 ? TX * (TY + 1) * TZ : 0;
     static constexpr int FAC2 = DIM > 2 ? TX * TY * (TZ + 1) : 0;
@@ -187,6 +190,53 @@ __device__ __forceinline__ bool obeys_constraints(const R* U, R gamma) {
     return ok && isfinite(p) && (U[0] > R(0)) && (p > R(0));
 }
 
+// The stencil flux across the face between staged cells `src` and src + S
+// (S: the stride along D): TecnoCombined4 / TecnoCombined6
+// (TecnoCombined4.hpp:40-60, TecnoCombined6.hpp:40-65) over the
+// entropy-conservative two-point flux, combined per component as the
+// reference does, with the largest wave speed of its parts.  The
+// reference's six-point stencil {-2, -1, 0, 1, 2, 3} lives in an ivec6
+// whose constructor stores 0 as the sixth entry (alsutils/vec6.hpp:36-39):
+// its u_{i+3} is u_i, so the last term is F(u_i, u_i), the point flux.
+template<class R, int NSD, int FLUX, int D>
+__device__ __forceinline__ R stencil_face_flux(const R* src, int box, int S, R gamma, R* F) {
+    constexpr int NV = NSD + 2;
+    R w = R(0);
+    auto pair = [&](int a, int b, R* out) {
+        R ua[NV], ub[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            ua[v] = src[v * box + a * S];
+            ub[v] = src[v * box + b * S];
+        }
+        FaceState<R, NSD> A, B;
+        make_state<R, NSD, D>(ua, gamma, A);
+        make_state<R, NSD, D>(ub, gamma, B);
+        w = fmax(w, flux_tecno1<R, NSD, D>(A, B, gamma, out));
+    };
+    R f01[NV], fm11[NV], f02[NV];
+    pair(0, 1, f01);
+    pair(-1, 1, fm11);
+    pair(0, 2, f02);
+    if (FLUX == FLUX_TECNO4) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = R(4.0 / 3.0) * f01[k] - R(1.0 / 6.0) * (fm11[k] + f02[k]);
+        }
+    } else {
+        R fm21[NV], fm12[NV], f00[NV];
+        pair(-2, 1, fm21);
+        pair(-1, 2, fm12);
+        pair(0, 0, f00);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            F[k] = (R(3.0 / 2.0) * f01[k] - R(3.0 / 10.0) * (fm11[k] + f02[k])) +
+                R(1.0 / 30.0) * ((fm21[k] + fm12[k]) + f00[k]);
+        }
+    }
+    return w;
+}
+
 template<class R>
 __device__ __forceinline__ R warp_max(R v) {
 #pragma unroll
@@ -198,8 +248,8 @@ __device__ __forceinline__ R warp_max(R v) {
 
 template<class R, int DIM, int RECON, int FLUX, int KIND, int D>
 __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, const R* box, R* rec,
-    R* flx, R (&acc)[StageLayout<R, DIM, RECON>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
-    typedef StageLayout<R, DIM, RECON> Lay;
+    R* flx, R (&acc)[StageLayout<R, DIM, RECON, FLUX>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
+    typedef StageLayout<R, DIM, RECON, FLUX> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
     // extents of the reconstructed-cell index space (x fastest), offset -1 along D
@@ -213,7 +263,7 @@ __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, con
     constexpr int S = D == 0 ? 1 : (D == 1 ? Lay::BX : Lay::BX * Lay::BY);
     const int tid = threadIdx.x;
 
-    for (int i = tid; i < RC; i += Lay::THREADS) {
+    for (int i = tid; i < (Lay::STENCIL ? 0 : RC); i += Lay::THREADS) {
         const int ex = i % E0;
         const int ey = (i / E0) % E1;
         const int ez = i / (E0 * E1);
@@ -237,16 +287,27 @@ __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, con
         const int fx = i % F0;
         const int fy = (i / F0) % F1;
         const int fz = i / (F0 * F1);
-        // face between reconstructed cells (fx,fy,fz) and its +D neighbour in E space
-        const int rl = (fz * E1 + fy) * E0 + fx;
-        const int rr = rl + (D == 0 ? 1 : (D == 1 ? E0 : E0 * E1));
-        R ul[NV], ur[NV], F[NV];
+        R F[NV];
+        R w;
+        if constexpr (Lay::STENCIL) {
+            // the face's left cell, staged at tile cell (fx,fy,fz) - 1 along D
+            const int bx = fx - (D == 0 ? 1 : 0) + G;
+            const int by = DIM > 1 ? fy - (D == 1 ? 1 : 0) + G : 0;
+            const int bz = DIM > 2 ? fz - (D == 2 ? 1 : 0) + G : 0;
+            w = stencil_face_flux<R, DIM, FLUX, D>(box + (bz * Lay::BY + by) * Lay::BX + bx,
+                Lay::BOX, S, gamma, F);
+        } else {
+            // face between reconstructed cells (fx,fy,fz) and its +D neighbour in E space
+            const int rl = (fz * E1 + fy) * E0 + fx;
+            const int rr = rl + (D == 0 ? 1 : (D == 1 ? E0 : E0 * E1));
+            R ul[NV], ur[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            ul[v] = rec[(NV + v) * RC + rl];
-            ur[v] = rec[v * RC + rr];
+            for (int v = 0; v < NV; ++v) {
+                ul[v] = rec[(NV + v) * RC + rl];
+                ur[v] = rec[v * RC + rr];
+            }
+            w = face_flux<R, DIM, FLUX, D>(ul, ur, gamma, F);
         }
-        const R w = face_flux<R, DIM, FLUX, D>(ul, ur, gamma, F);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             flx[v * FC + i] = F[v];
@@ -317,7 +378,7 @@ __device__ __forceinline__ void finish_step(StepState* st) {
 template<class R, int DIM, int RECON, int FLUX, int KIND>
 __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc& L, int tile,
     int member, unsigned char* smem) {
-    typedef StageLayout<R, DIM, RECON> Lay;
+    typedef StageLayout<R, DIM, RECON, FLUX> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
     constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
@@ -546,7 +607,7 @@ __device__ __forceinline__ void stage_item(const StageParams& P, long long w, un
 // from the counter until the list is exhausted, and the last block to
 // leave resets the counter for the next launch.
 template<class R, int DIM, int RECON, int FLUX, int KIND>
-__global__ void __launch_bounds__((StageLayout<R, DIM, RECON>::THREADS), (StageLayout<R, DIM, RECON>::BLOCKS))
+__global__ void __launch_bounds__((StageLayout<R, DIM, RECON, FLUX>::THREADS), (StageLayout<R, DIM, RECON, FLUX>::BLOCKS))
 stage_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ long long item;

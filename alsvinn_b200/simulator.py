@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from .initial_data import padded_shape
 
-FLUX = {"hll": 0, "hll3": 1, "central": 2}
+FLUX = {"hll": 0, "hll3": 1, "central": 2, "tecno1": 3, "tecno4": 4, "tecno6": 5}
 RECONSTRUCTION = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
                   "wenof2": 7, "weno3": 8}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}

@@ -36,6 +36,10 @@ extern "C" {
 #define ALS_FLUX_HLL 0              /* "hll",     numflux/euler/HLL.hpp */
 #define ALS_FLUX_HLL3 1             /* "hll3",    numflux/euler/HLL3.hpp */
 #define ALS_FLUX_CENTRAL 2          /* "central", numflux/Central.hpp */
+/* TeCNO fluxes, with reconstruction "none" (ALS_E_UNSUPPORTED otherwise): */
+#define ALS_FLUX_TECNO1 3           /* "tecno1",  numflux/euler/Tecno1.hpp (entropy conservative) */
+#define ALS_FLUX_TECNO4 4           /* "tecno4",  numflux/TecnoCombined4.hpp (stencil -1..2, 3 ghost cells) */
+#define ALS_FLUX_TECNO6 5           /* "tecno6",  numflux/TecnoCombined6.hpp (stencil -2..3, 5 ghost cells) */
 #define ALS_RECON_NONE 0            /* "none",  reconstruction/NoReconstruction.cpp */
 #define ALS_RECON_WENO2 1           /* "weno2", reconstruction/WENO2.hpp */
 #define ALS_RECON_ENO2 2            /* "eno2",  reconstruction/ENOCPU.cpp */

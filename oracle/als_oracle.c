@@ -193,11 +193,154 @@ static double flux_central(int nsd, int d, double gamma, const state_t* L,
             fabs(R->u[d]) + sqrt(gamma * R->p / R->rho));
 }
 
+/* ---------------------------------------------------------------- TeCNO */
+
+/* bar and ln of tecno_utils.hpp:22-38: the logarithmic mean is 0 when
+ * either difference is 0; divLn (tecno_utils.hpp:42-50) gives 0 over it. */
+static double tecno_bar(double a, double b) {
+    return (a + b) / 2;
+}
+
+static double tecno_ln(double a, double b) {
+    if (b - a == 0 || log(b) - log(a) == 0) {
+        return 0;
+    }
+    return (b - a) / (log(b) - log(a));
+}
+
+static double tecno_div_ln(double a, double b, double F) {
+    const double div = tecno_ln(a, b);
+    return div == 0 ? 0 : F / div;
+}
+
+/* z = (sqrt(rho/p), sqrt(rho/p) u, sqrt(rho p)) from the primitive
+ * variables u = m/rho, p = (gamma-1)(E - 0.5 m.m/rho) (Euler.hpp:290-320);
+ * z has nsd+2 entries. */
+static void tecno_z(int nsd, double gamma, const state_t* s, double* z) {
+    double dot = s->m[0] * s->m[0];
+    double p, q;
+    int k;
+    if (nsd > 1) {
+        dot = dot + s->m[1] * s->m[1];
+    }
+    if (nsd > 2) {
+        dot = dot + s->m[2] * s->m[2];
+    }
+    p = (gamma - 1) * (s->E - 0.5 * dot / s->rho);
+    q = sqrt(s->rho / p);
+    z[0] = q;
+    for (k = 0; k < nsd; ++k) {
+        z[1 + k] = (s->m[k] / s->rho) * q;
+    }
+    z[1 + nsd] = sqrt(s->rho * p);
+}
+
+/* Speeds of HLL3::computeHLLSpeeds (HLL3.hpp:120-160), as in flux_hll3. */
+static double hll3_speed(int d, double gamma, const state_t* L, const state_t* R) {
+    const double wl = sqrt(L->rho);
+    const double wr = sqrt(R->rho);
+    const double rho = (L->rho + R->rho) / 2;
+    const double ud = (wl * L->u[d] + wr * R->u[d]) / (wl + wr);
+    const double p = (wl * L->p + wr * R->p) / (wl + wr);
+    const double cfL = sqrt(gamma * L->p / L->rho);
+    const double cfR = sqrt(gamma * R->p / R->rho);
+    const double correct = 0.5 * fmax(0.0, L->u[d] - R->u[d]);
+    const double cs = sqrt(gamma * p / rho);
+    const double sL = fmin(L->u[d] + correct - cfL, ud - cs);
+    const double sR = fmax(R->u[d] - correct + cfR, ud + cs);
+    return fmax(fabs(sL), fabs(sR));
+}
+
+/* Tecno1 (numflux/euler/Tecno1.hpp:51-180).  The reference writes the 2-D
+ * formulas for all dimensions: in 3-D the z-momentum flux is 0, and along z
+ * the flux keeps its zero initial value unless both states are equal. */
+static double flux_tecno1(int nsd, int d, double gamma, const state_t* L, const state_t* R,
+    double* F) {
+    const int nv = nsd + 2;
+    int same = L->rho == R->rho && L->E == R->E;
+    int k;
+    for (k = 0; k < nsd; ++k) {
+        same = same && L->m[k] == R->m[k];
+    }
+    if (same) {
+        point_flux(nsd, d, L, F);
+    } else if (nsd == 3 && d == 2) {
+        for (k = 0; k < nv; ++k) {
+            F[k] = 0;
+        }
+    } else {
+        double zl[5], zr[5], e;
+        const int last = nsd + 1;
+        tecno_z(nsd, gamma, L, zl);
+        tecno_z(nsd, gamma, R, zr);
+        F[0] = tecno_bar(zl[1 + d], zr[1 + d]) * tecno_ln(zl[last], zr[last]);
+        for (k = 0; k < nsd; ++k) {
+            if (nsd == 3 && k == 2) {
+                F[1 + k] = 0;
+            } else if (k == d) {
+                F[1 + k] = tecno_bar(zl[last], zr[last]) / tecno_bar(zl[0], zr[0]) +
+                    tecno_bar(zl[1 + d], zr[1 + d]) / tecno_bar(zl[0], zr[0]) * F[0];
+            } else {
+                F[1 + k] = tecno_bar(zl[1 + k], zr[1 + k]) / tecno_bar(zl[0], zr[0]) * F[0];
+            }
+        }
+        e = (gamma + 1) / (gamma - 1) * tecno_div_ln(zl[0], zr[0], F[0]) +
+            tecno_bar(zl[1], zr[1]) * F[1];
+        if (nsd > 1) {
+            e = e + tecno_bar(zl[2], zr[2]) * F[2];
+        }
+        F[last] = 1.0 / (2 * tecno_bar(zl[0], zr[0])) * e;
+    }
+    return hll3_speed(d, gamma, L, R);
+}
+
+/* TecnoCombined4 / TecnoCombined6 (TecnoCombined4.hpp:40-60,
+ * TecnoCombined6.hpp:40-65) at the face between cells c and c+s of `in`.
+ * TecnoCombined6's stencil {-2, -1, 0, 1, 2, 3} is held in an ivec6 whose
+ * constructor stores 0 for the sixth entry (alsutils/vec6.hpp:36-39), so
+ * its "u_{i+3}" is u_i and the last term is F(u_i, u_i), the point flux. */
+static double flux_tecno_stencil(const orc_config* cfg, int d, const double* in, long plane,
+    long c, long s, double* F) {
+    const int nsd = cfg->dim;
+    const int nv = nsd + 2;
+    double w = 0;
+    double f[6][5];
+    /* pairs (a, b): F(u_{c+a}, u_{c+b}) */
+    static const int pairs[6][2] = {{0, 1}, {-1, 1}, {0, 2}, {-2, 1}, {-1, 2}, {0, 0}};
+    const int np = cfg->flux == ORC_FLUX_TECNO4 ? 3 : 6;
+    int k, q;
+    for (q = 0; q < np; ++q) {
+        state_t A, B;
+        double ua[5], ub[5];
+        int v;
+        for (v = 0; v < nv; ++v) {
+            ua[v] = in[v * plane + c + pairs[q][0] * s];
+            ub[v] = in[v * plane + c + pairs[q][1] * s];
+        }
+        make_all(nsd, cfg->gamma, ua[0], ua + 1, ua[1 + nsd], &A);
+        make_all(nsd, cfg->gamma, ub[0], ub + 1, ub[1 + nsd], &B);
+        w = fmax(w, flux_tecno1(nsd, d, cfg->gamma, &A, &B, f[q]));
+    }
+    for (k = 0; k < nv; ++k) {
+        if (np == 3) {
+            F[k] = 4.0 / 3.0 * f[0][k] - 1.0 / 6.0 * (f[1][k] + f[2][k]);
+        } else {
+            F[k] = (3.0 / 2.0 * f[0][k] - 3.0 / 10.0 * (f[1][k] + f[2][k])) +
+                1.0 / 30.0 * ((f[3][k] + f[4][k]) + f[5][k]);
+        }
+    }
+    return w;
+}
+
 /* -------------------------------------------------------------- helpers */
 
 int orc_ghost_cells(int flux, int recon) {
     int rg = 1;
-    (void)flux; /* every in-scope flux has the two-point stencil {0, 1} */
+    /* stencil size - 1: 3 for tecno4, 5 for tecno6, else 1 (numflux_util.hpp:52-60) */
+    const int fg = flux == ORC_FLUX_TECNO4 ? 3 : (flux == ORC_FLUX_TECNO6 ? 5 : 1);
+    if (flux < ORC_FLUX_HLL || flux > ORC_FLUX_TECNO6) {
+        return -1;
+    }
     switch (recon) {
     case ORC_RECON_NONE: rg = 1; break;
     case ORC_RECON_WENO2: rg = 2; break;
@@ -210,7 +353,7 @@ int orc_ghost_cells(int flux, int recon) {
     case ORC_RECON_WENO3: rg = 3; break;
     default: return -1;
     }
-    return rg > 1 ? rg : 1;
+    return rg > fg ? rg : fg;
 }
 
 int orc_configure(orc_config* cfg, int dim, const int* n, const double* lower,
@@ -592,11 +735,13 @@ static double face_flux(const orc_config* cfg, int d, const double* ul, const do
     switch (cfg->flux) {
     case ORC_FLUX_HLL: return flux_hll(nsd, d, cfg->gamma, &L, &R, F);
     case ORC_FLUX_HLL3: return flux_hll3(nsd, d, cfg->gamma, &L, &R, F);
+    case ORC_FLUX_TECNO1: return flux_tecno1(nsd, d, cfg->gamma, &L, &R, F);
     default: return flux_central(nsd, d, cfg->gamma, &L, &R, F);
     }
 }
 
 void orc_net_flux(const orc_config* cfg, const double* in, double* out, double ws[3]) {
+    const int stencil = cfg->flux == ORC_FLUX_TECNO4 || cfg->flux == ORC_FLUX_TECNO6;
     int N[3];
     const int g = cfg->g;
     const int nvar = cfg->dim + 2;
@@ -614,6 +759,9 @@ void orc_net_flux(const orc_config* cfg, const double* in, double* out, double w
         }
     }
     ws[0] = ws[1] = ws[2] = 0;
+    if (stencil && cfg->recon != ORC_RECON_NONE) {
+        return; /* stencil fluxes are restated for reconstruction none only */
+    }
     for (d = 0; d < cfg->dim; ++d) {
         const long s = d == 0 ? 1 : (d == 1 ? N[0] : (long)N[0] * N[1]);
         const int len = N[d];
@@ -643,7 +791,13 @@ void orc_net_flux(const orc_config* cfg, const double* in, double* out, double w
                     for (i = g - 1; i < len - g; ++i) {
                         const double* ul = rec + (size_t)i * 2 * nvar + nvar;
                         const double* ur = rec + (size_t)(i + 1) * 2 * nvar;
-                        const double w = face_flux(cfg, d, ul, ur, flux + (size_t)i * nvar);
+                        /* stencil fluxes read the "left" volume, a copy of
+                         * the cells under reconstruction none
+                         * (numflux_util.hpp:94-116) */
+                        const double w = stencil
+                            ? flux_tecno_stencil(cfg, d, in, plane, base + i * s, s,
+                                  flux + (size_t)i * nvar)
+                            : face_flux(cfg, d, ul, ur, flux + (size_t)i * nvar);
                         if (wmax < w) { /* std::max(waveSpeedComputed, local) */
                             wmax = w;
                         }

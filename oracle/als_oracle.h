@@ -21,7 +21,8 @@
 extern "C" {
 #endif
 
-enum { ORC_FLUX_HLL = 0, ORC_FLUX_HLL3 = 1, ORC_FLUX_CENTRAL = 2 };
+enum { ORC_FLUX_HLL = 0, ORC_FLUX_HLL3 = 1, ORC_FLUX_CENTRAL = 2, ORC_FLUX_TECNO1 = 3,
+       ORC_FLUX_TECNO4 = 4, ORC_FLUX_TECNO6 = 5 };
 enum { ORC_RECON_NONE = 0, ORC_RECON_WENO2 = 1, ORC_RECON_ENO2 = 2,
        ORC_RECON_ENO3 = 3, ORC_RECON_ENO4 = 4, ORC_RECON_MC = 5, ORC_RECON_MM = 6,
        ORC_RECON_WENOF2 = 7, ORC_RECON_WENO3 = 8 };

@@ -24,6 +24,9 @@
 #include "alsfvm/numflux/euler/HLL.hpp"
 #include "alsfvm/numflux/euler/HLL3.hpp"
 #include "alsfvm/numflux/Central.hpp"
+#include "alsfvm/numflux/TecnoCombined4.hpp"
+#include "alsfvm/numflux/TecnoCombined6.hpp"
+#include "alsfvm/numflux/euler/Tecno1.hpp"
 #include "alsfvm/reconstruction/ReconstructionCPU.hpp"
 #include "alsfvm/reconstruction/WENO2.hpp"
 #include "alsfvm/reconstruction/MC.hpp"
@@ -157,10 +160,11 @@ std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
 #ifdef ALSREF_WITH_B200
     if (g_flux_platform == "b200" || g_flux_platform == "b200-all") {
         // names in the order of the ALS_FLUX_* / ALS_RECON_* codes
-        static const char* const fluxes[] = {"hll", "hll3", "central"};
+        static const char* const fluxes[] = {"hll", "hll3", "central", "tecno1", "tecno4",
+            "tecno6"};
         static const char* const recons[] = {"none", "weno2", "eno2", "eno3", "eno4", "mc", "mm",
             "wenof2", "weno3"};
-        return std::make_shared<numflux::NumericalFluxB200>(*o.grid, b200_code(s.flux, fluxes, 3),
+        return std::make_shared<numflux::NumericalFluxB200>(*o.grid, b200_code(s.flux, fluxes, 6),
             b200_code(s.recon, recons, 9), s.gamma);
     }
 #endif
@@ -170,6 +174,12 @@ std::shared_ptr<numflux::NumericalFlux> makeFlux(const Setup& s, Objects& o) {
         return std::make_shared<numflux::NumericalFluxCPU<numflux::euler::HLL3<d>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
     } else if (s.flux == "central") {
         return std::make_shared<numflux::NumericalFluxCPU<numflux::Central<Eq>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    } else if (s.flux == "tecno1") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::euler::Tecno1<d>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    } else if (s.flux == "tecno4") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::TecnoCombined4<Eq, numflux::euler::Tecno1<d>>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
+    } else if (s.flux == "tecno6") {
+        return std::make_shared<numflux::NumericalFluxCPU<numflux::TecnoCombined6<Eq, numflux::euler::Tecno1<d>>, Eq, d>>(*o.grid, o.recon, o.params, o.device);
     }
     THROW("unknown flux " << s.flux);
 }

@@ -121,6 +121,34 @@ def write_limiter_cases(ref):
             f.write("%d %s %s %s %s %d %s %s %s %.17g\n" % c)
 
 
+# TeCNO fluxes (reconstruction none), prefixed "tecno_": the CUDA path calls
+# the device log, so these are matched to a tolerance on the GPU; the oracle
+# matches them bit for bit
+TECNO_SIMULATIONS = {
+    "tecno_kh32_tecno1_rk3": (2, (32, 32), (0.0, 0.0), (1.0, 1.0), "tecno1", "none",
+                              "rungekutta3", "periodic", 0.4, 0.05, "kh"),
+    "tecno_rand2d_18x20_tecno4_rk2": (2, (18, 20), (0.0, 0.0), (1.0, 1.0), "tecno4", "none",
+                                      "rungekutta2", "neumann", 0.4, 0.04, "seed:21"),
+    "tecno_rand1d_64_tecno6_rk3": (1, (64,), (0.0,), (1.0,), "tecno6", "none", "rungekutta3",
+                                   "periodic", 0.4, 0.05, "seed:22"),
+    "tecno_rand3d_10x11x10_tecno4_fe": (3, (10, 11, 10), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "tecno4",
+                                        "none", "forwardeuler", "periodic", 0.3, 0.02, "seed:23"),
+}
+
+
+def write_tecno_fixtures(ref):
+    for name, (dim, n, lo, hi, flux, recon, integ, bc, cfl, T, kind) in TECNO_SIMULATIONS.items():
+        g = ghost_cells(recon, flux)
+        U0 = initial_state(kind, dim, n, g)
+        rc, U, dts, steps, t = ref.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, cfl, T, U0)
+        assert rc == 0, name
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), initial=U0, final=U, dts=dts,
+                            steps=steps, t=t, dim=dim, n=np.array(n), lower=np.array(lo),
+                            upper=np.array(hi), flux=flux, recon=recon, integrator=integ, bc=bc,
+                            cfl=cfl, end_time=T, gamma=1.4)
+        print(name, "steps=%d t=%r" % (steps, t))
+
+
 def main():
     ref = RefOracle()
     out = {}
@@ -156,6 +184,7 @@ def main():
                     cases.append((dim, ",".join(map(str, n)), recon, flux, bc, seed,
                                   digest(filled), digest(net), digest(ws), float(ws.max())))
     write_limiter_cases(ref)
+    write_tecno_fixtures(ref)
     with open(os.path.join(HERE, "compute_flux_cases.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
                 "sha256(wave speeds) max_wave_speed\n")

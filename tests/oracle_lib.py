@@ -20,7 +20,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 
-FLUX = {"hll": 0, "hll3": 1, "central": 2}
+FLUX = {"hll": 0, "hll3": 1, "central": 2, "tecno1": 3, "tecno4": 4, "tecno6": 5}
 RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
          "wenof2": 7, "weno3": 8}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
@@ -35,9 +35,10 @@ def _dptr(a):
     return a.ctypes.data_as(_D)
 
 
-def ghost_cells(recon):
-    return {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 2, "mm": 2,
-            "wenof2": 2, "weno3": 3}[recon]
+def ghost_cells(recon, flux="hll"):
+    g = {"none": 1, "weno2": 2, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 2, "mm": 2,
+         "wenof2": 2, "weno3": 3}[recon]
+    return max(g, {"tecno4": 3, "tecno6": 5}.get(flux, 1))
 
 
 def padded_shape(dim, n, g):

@@ -39,6 +39,11 @@ def test_ghost_cells():
     assert alsvinn_b200.ghost_cells("hll3", "eno3") == 3
     assert alsvinn_b200.ghost_cells("central", "eno4") == 4
     assert alsvinn_b200.ghost_cells("hll", "none") == 1
+    assert alsvinn_b200.ghost_cells("tecno1", "none") == 1
+    assert alsvinn_b200.ghost_cells("tecno4", "none") == 3
+    assert alsvinn_b200.ghost_cells("tecno6", "none") == 5
+    with pytest.raises(_lib.AlsError):
+        alsvinn_b200.ghost_cells("tecno4", "weno2")   # TeCNO fluxes: reconstruction "none"
     with pytest.raises(_lib.AlsError):
         alsvinn_b200.ghost_cells(7, 1)
 

@@ -54,3 +54,34 @@ def test_reference_time_loop_with_b200_classes(ref_b200, platform, dim, n, recon
     assert a[4] == b[4]            # final time
     np.testing.assert_array_equal(a[2], b[2])   # every dt
     np.testing.assert_array_equal(a[1], b[1])   # final state, ghosts included
+
+
+TECNO_CASES = [(1, (32,), "tecno6", "rungekutta3", "periodic"),
+               (2, (14, 12), "tecno1", "rungekutta2", "neumann"),
+               (2, (14, 12), "tecno4", "rungekutta3", "periodic"),
+               (3, (10, 11, 10), "tecno4", "forwardeuler", "periodic")]
+
+
+@pytest.mark.parametrize("platform", ["b200", "b200-all"])
+@pytest.mark.parametrize("dim,n,flux,integ,bc", TECNO_CASES,
+                         ids=["d%d-%s-%s-%s" % (c[0], c[2], c[3], c[4]) for c in TECNO_CASES])
+def test_reference_time_loop_with_b200_tecno_flux(ref_b200, platform, dim, n, flux, integ, bc):
+    """The TeCNO fluxes (reconstruction none) through NumericalFluxB200 in the
+    reference's time loop: same status and step count as the reference's own
+    NumericalFluxCPU; states within relative 1e-10 (the device log and the C
+    library's log may differ in the last bit)."""
+    g = ghost_cells("none", flux)
+    seed = zlib.crc32(("dropin-tecno-%d-%s-%s" % (dim, flux, integ)).encode()) % 100000
+    st = smooth_random_state(seed, dim, n, g)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    out = {}
+    for p in ("cpu", platform):
+        ref_b200.set_flux_platform(p)
+        out[p] = ref_b200.simulate(dim, n, lo, hi, flux, "none", integ, bc, 1.4, 0.4, 0.03, st)
+    ref_b200.set_flux_platform("cpu")
+    a, b = out["cpu"], out[platform]
+    assert a[0] == b[0] == 0
+    assert a[3] == b[3] >= 1
+    assert abs(a[4] - b[4]) <= 1e-15
+    np.testing.assert_allclose(a[2], b[2], rtol=1e-10)
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-10, atol=1e-12)
