@@ -5,14 +5,14 @@ C ABI in ``include/als_b200.h``); this package is the Python face of it.
 """
 from . import _lib
 from .initial_data import (kelvin_helmholtz, kh_ensemble, padded_shape, sod, uniform_draws)
-from .simulator import (Boundary, Integrator, MeanVariance, NumericalFlux, Reconstruction,
-                        Simulator, ghost_cells)
+from .simulator import (Boundary, DiffusionOperator, Integrator, MeanVariance, NumericalFlux,
+                        Reconstruction, Simulator, diffusion_ghost_cells, ghost_cells)
 from .surrogate import Surrogate
 from . import uq
 
 __all__ = [
-    "Boundary", "Integrator", "MeanVariance", "NumericalFlux", "Reconstruction", "Simulator",
-    "Surrogate", "ghost_cells", "uq",
+    "Boundary", "DiffusionOperator", "Integrator", "MeanVariance", "NumericalFlux",
+    "Reconstruction", "Simulator", "Surrogate", "diffusion_ghost_cells", "ghost_cells", "uq",
     "kelvin_helmholtz", "kh_ensemble", "padded_shape", "sod", "uniform_draws",
 ]
 

@@ -105,6 +105,10 @@ PROTOTYPES = {
     "als_write_netcdf": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _I, ctypes.c_int, _PP,
                                         _PP, ctypes.c_double, ctypes.c_int, _PP, _PP]),
     "als_solver_write_netcdf": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "als_diffusion_ghost_cells": (ctypes.c_int, [ctypes.c_int]),
+    "als_diffusion_create": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _PP]),
+    "als_diffusion_apply": (ctypes.c_int, [_VP, _PP, _PP, _VP]),
+    "als_diffusion_destroy": (ctypes.c_int, [_VP]),
     # include/als_surrogate.h
     "als_mlp_create": (ctypes.c_int, [ctypes.POINTER(MlpConfig), ctypes.c_int, _PP]),
     "als_mlp_destroy": (ctypes.c_int, [_VP]),

@@ -108,6 +108,7 @@ als::GridDesc make_grid(int dim, const int* n, int g, const int* lo, const int* 
         gd.tiles[d] = std::max(1, (gd.hi[d] - gd.lo[d] + t - 1) / t);
     }
     gd.plane = (long long)gd.N[0] * gd.N[1] * gd.N[2];
+    gd.ghosts = g;
     return gd;
 }
 
@@ -269,11 +270,10 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     if (rc != ALS_OK) {
         return rc;
     }
+    // wider planes are fine: the reference sizes ghosts as the maximum of
+    // the flux's and the diffusion operator's (ConservedSystem.cpp:109-114)
     if (grid->ghosts < als_ghost_cells(flux, reconstruction)) {
-        return fail(ALS_E_INVALID, "planes have fewer ghost cells than the reconstruction needs");
-    }
-    if (grid->ghosts != als_ghost_cells(flux, reconstruction)) {
-        return fail(ALS_E_UNSUPPORTED, "planes must have exactly the ghost width of the reconstruction");
+        return fail(ALS_E_INVALID, "planes have fewer ghost cells than the flux needs");
     }
     int lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {
@@ -1617,8 +1617,8 @@ extern "C" int als_compute_flux_static(const als_grid* grid, int flux, int recon
     if (members < 1 || members > kStaticFluxMembers) {
         return fail(ALS_E_INVALID, "als_compute_flux_static takes 1 to 1024 states per call");
     }
-    if (grid->ghosts != als_ghost_cells(flux, reconstruction)) {
-        return fail(ALS_E_UNSUPPORTED, "planes must have exactly the ghost width of the reconstruction");
+    if (grid->ghosts < als_ghost_cells(flux, reconstruction)) {
+        return fail(ALS_E_INVALID, "planes have fewer ghost cells than the flux needs");
     }
     void* scratch = nullptr;
     rc = static_flux_scratch(&scratch);

@@ -420,16 +420,19 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     }
 
     // stage the tile and its halo; U1 = (dt/dx)*L + U^n is formed here for the
-    // second stage (RungeKutta{2,3}.cpp: output *= dt/dx; output += U)
+    // second stage (RungeKutta{2,3}.cpp: output *= dt/dx; output += U).
+    // Planes may carry more ghost cells than the stencil needs (a diffusion
+    // operator with a wider stencil sets the width): `sh` skips the extra ones.
+    const int sh = gd.ghosts - G;
     for (int i = tid; i < NV * Lay::BOX; i += Lay::THREADS) {
         const int v = i / Lay::BOX;
         const int b = i - v * Lay::BOX;
         const int bx = b % Lay::BX;
         const int by = (b / Lay::BX) % Lay::BY;
         const int bz = b / (Lay::BX * Lay::BY);
-        const int px = x0 + bx;
-        const int py = DIM > 1 ? y0 + by : 0;
-        const int pz = DIM > 2 ? z0 + bz : 0;
+        const int px = x0 + bx + sh;
+        const int py = DIM > 1 ? y0 + by + sh : 0;
+        const int pz = DIM > 2 ? z0 + bz + sh : 0;
         R val = R(0);
         if (px < gd.N[0] && py < gd.N[1] && pz < gd.N[2]) {
             const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
@@ -476,9 +479,9 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         if (gx >= gd.hi[0] || (DIM > 1 && gy >= gd.hi[1]) || (DIM > 2 && gz >= gd.hi[2])) {
             continue;
         }
-        const int px = gx + G;
-        const int py = DIM > 1 ? gy + G : 0;
-        const int pz = DIM > 2 ? gz + G : 0;
+        const int px = gx + gd.ghosts;
+        const int py = DIM > 1 ? gy + gd.ghosts : 0;
+        const int pz = DIM > 2 ? gz + gd.ghosts : 0;
         const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
         const int bidx = ((DIM > 2 ? cz + G : 0) * Lay::BY + (DIM > 1 ? cy + G : 0)) * Lay::BX + cx + G;
         R val[NV];
@@ -514,9 +517,9 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         }
         if (P.write_ghosts) {
             int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
-            const int nxi = boundary_images(gx, gd.n[0], G, P.bc, ix);
-            const int nyi = DIM > 1 ? boundary_images(gy, gd.n[1], G, P.bc, iy) : 1;
-            const int nzi = DIM > 2 ? boundary_images(gz, gd.n[2], G, P.bc, iz) : 1;
+            const int nxi = boundary_images(gx, gd.n[0], gd.ghosts, P.bc, ix);
+            const int nyi = DIM > 1 ? boundary_images(gy, gd.n[1], gd.ghosts, P.bc, iy) : 1;
+            const int nzi = DIM > 2 ? boundary_images(gz, gd.n[2], gd.ghosts, P.bc, iz) : 1;
             if (nxi * nyi * nzi > 1) {
                 for (int a = 0; a < nzi; ++a) {
                     for (int b = 0; b < nyi; ++b) {

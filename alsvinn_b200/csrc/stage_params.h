@@ -44,6 +44,7 @@ struct GridDesc {
     int tiles[3];      // tiles covering the region [lo, hi)
     int lo[3], hi[3];  // region of interior cells to update (interior coordinates)
     long long plane;   // padded cells per plane
+    int ghosts;        // ghost width of the planes (>= the stencil's)
 };
 
 // One grid level of a launch: its geometry, its planes (one pointer per

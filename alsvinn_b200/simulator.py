@@ -304,13 +304,15 @@ def _stream(stream):
 class NumericalFlux:
     """numflux::NumericalFlux (NumericalFlux.hpp:25-53) on device planes."""
 
-    def __init__(self, dimension, n, flux="hll", reconstruction="weno2", gamma=1.4):
+    def __init__(self, dimension, n, flux="hll", reconstruction="weno2", gamma=1.4, ghosts=None):
+        """``ghosts``: the planes' ghost width when wider than the flux needs
+        (a diffusion operator with a wider stencil sets it)."""
         self.dimension = dimension
         self.n = tuple(n)
         self.flux = _choice(FLUX, flux, "flux")
         self.reconstruction = _choice(RECONSTRUCTION, reconstruction, "reconstruction")
         self.gamma = gamma
-        self.ghosts = ghost_cells(self.flux, self.reconstruction)
+        self.ghosts = ghosts or ghost_cells(self.flux, self.reconstruction)
 
     def getNumberOfGhostCells(self):
         return self.ghosts
@@ -366,13 +368,77 @@ class Boundary:
                                        planes.shape[0], _stream(stream)))
 
 
+DIFFUSION = {"tecnoroe": 0, "tecnorusanov": 1}
+TECNO_RECONSTRUCTION = {"none": 0, "eno2": 2, "eno3": 3, "eno4": 4}
+
+
+def diffusion_ghost_cells(reconstruction):
+    """Ghost cells of a TeCNO diffusion operator over ``reconstruction``."""
+    lib = _lib.load()
+    return _lib.check(lib.als_diffusion_ghost_cells(
+        _choice(TECNO_RECONSTRUCTION, reconstruction, "TeCNO reconstruction")))
+
+
+class DiffusionOperator:
+    """diffusion::DiffusionOperator (DiffusionOperator.hpp:25-47) as
+    DiffusionFactory builds it for the Euler equations: TecnoDiffusionCPU with
+    the "tecnoroe" or "tecnorusanov" matrix over the TeCNO reconstruction
+    "none", "eno2", "eno3" or "eno4" of the scaled entropy variables.  Its
+    work arrays persist between calls, as the reference's do."""
+
+    def __init__(self, dimension, n, diffusion="tecnoroe", reconstruction="eno2", gamma=1.4,
+                 ghosts=None):
+        self.dimension = dimension
+        self.n = tuple(n)
+        self.kind = _choice(DIFFUSION, diffusion, "diffusion")
+        self.reconstruction = _choice(TECNO_RECONSTRUCTION, reconstruction, "TeCNO reconstruction")
+        self.ghosts = ghosts or diffusion_ghost_cells(reconstruction)
+        self.gamma = gamma
+        self._lib = _lib.load()
+        g = _grid(dimension, self.n, self.ghosts, gamma)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.als_diffusion_create(ctypes.byref(g), self.kind, self.reconstruction,
+                                                  ctypes.byref(h)))
+        self._h = h
+
+    def getNumberOfGhostCells(self):
+        return diffusion_ghost_cells({v: k for k, v in TECNO_RECONSTRUCTION.items()}[
+            self.reconstruction])
+
+    def applyDiffusion(self, output, conserved, stream=0):
+        """output += the diffusion of ``conserved`` ((nvar, ...) FP64 device
+        tensors, ghosts filled)."""
+        _lib.check(self._lib.als_diffusion_apply(self._h, _lib.plane_pointers(conserved),
+                                                 _lib.plane_pointers(output), _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.als_diffusion_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Integrator:
     """integrator::Integrator (Integrator.hpp:52-115): the stage combination
-    of performSubstep and computeTimestep, around a NumericalFlux."""
+    of performSubstep and computeTimestep, around the system L(U) of a
+    NumericalFlux and, optionally, a DiffusionOperator added to it
+    (ConservedSystem.cpp:31-103)."""
 
-    def __init__(self, name, numerical_flux, cfl):
+    def __init__(self, name, numerical_flux, cfl, diffusion=None):
         self.integrator = _choice(INTEGRATOR, name, "integrator")
         self.flux = numerical_flux
+        self.diffusion = diffusion
         self.cfl = cfl
 
     def getNumberOfSubsteps(self):
@@ -389,6 +455,8 @@ class Integrator:
         """volumes[k] = U_k (device tensors); returns dt (computed at substep 0)."""
         lib = _lib.load()
         ws = self.flux.computeFlux(volumes[substep], out, stream=stream)
+        if self.diffusion is not None:
+            self.diffusion.applyDiffusion(out, volumes[substep], stream=stream)
         if substep == 0:
             dt = self.computeTimestep(ws, cell_lengths, t, end_time)
         c = dt / cell_lengths[0]

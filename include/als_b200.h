@@ -301,6 +301,41 @@ int als_structure_functions(const als_grid* grid, int boundary, int kind, int di
     double p, const void* states, int precision, long long member_stride, int members,
     double* out, void* stream);
 
+/* ------------------------------------------------------- TeCNO diffusion
+ * DiffusionOperator for the Euler equations: TecnoDiffusionCPU with the Roe
+ * or Rusanov diffusion matrix over a TeCNO reconstruction of the scaled
+ * entropy variables (alsfvm/src/diffusion/TecnoDiffusionCPU.cpp:23-170,
+ * DiffusionFactory.cpp:41-95, reconstruction/tecno/).  FP64. */
+#define ALS_DIFFUSION_TECNOROE 0        /* "tecnoroe",     diffusion/RoeMatrix.hpp */
+#define ALS_DIFFUSION_TECNORUSANOV 1    /* "tecnorusanov", diffusion/RusanovMatrix.hpp */
+#define ALS_TECNO_RECON_NONE 0          /* "none", reconstruction/tecno/NoReconstruction */
+#define ALS_TECNO_RECON_ENO2 2          /* "eno2", reconstruction/tecno/ENOCPU<2> */
+#define ALS_TECNO_RECON_ENO3 3          /* "eno3" */
+#define ALS_TECNO_RECON_ENO4 4          /* "eno4" */
+typedef struct als_diffusion als_diffusion;
+
+/* Ghost cells the operator needs (1 for none, the order for ENO); replaces
+ * TecnoDiffusionCPU::getNumberOfGhostCells (TecnoDiffusionCPU.cpp:172-176).
+ * A simulation's planes carry max(this, als_ghost_cells(flux, recon))
+ * (ConservedSystem.cpp:109-114). */
+int als_diffusion_ghost_cells(int reconstruction);
+
+/* One operator for planes of `grid` (grid->ghosts >= the operator's ghost
+ * cells) on the current device.  It owns work arrays that persist between
+ * calls like the reference's work volumes, whose entries the reference
+ * partly reads before writing; results depend on earlier calls in the same
+ * way.  Replaces DiffusionFactory::createDiffusionOperator. */
+int als_diffusion_create(const als_grid* grid, int kind, int reconstruction, als_diffusion** out);
+
+/* out += the diffusion of `conserved` (nvar device planes each, ghosts
+ * filled), on every cell the reference updates (ghost cells included,
+ * which a later boundary fill overwrites).  Replaces
+ * DiffusionOperator::applyDiffusion(output, conservedVolume).  Stream-ordered;
+ * calls on one operator must not overlap. */
+int als_diffusion_apply(als_diffusion* h, const double* const* conserved, double* const* out,
+    void* stream);
+int als_diffusion_destroy(als_diffusion* h);
+
 /* ------------------------------------------------------- UQ sampling
  * Parameter draws of samples [first_sample, first_sample+count) for a
  * parameter of length `dimension`: out[k*dimension + c].  Same numbers as

@@ -1,10 +1,11 @@
-// boundary::Boundary, reconstruction::Reconstruction and integrator::Integrator
-// backed by the B200 library — the other adapter classes a maintainer adds
+// boundary::Boundary, reconstruction::Reconstruction, integrator::Integrator
+// and diffusion::DiffusionOperator backed by the B200 library — the other adapter classes a maintainer adds
 // beside numflux::NumericalFluxB200, compiled
 // against the reference's headers:
 //   alsfvm/include/alsfvm/boundary/Boundary.hpp:25-35
 //   alsfvm/include/alsfvm/reconstruction/Reconstruction.hpp:40-58
 //   alsfvm/include/alsfvm/integrator/Integrator.hpp:52-100
+//   alsfvm/include/alsfvm/diffusion/DiffusionOperator.hpp:25-47
 //
 // TEST INFRASTRUCTURE in this repository (built only into
 // oracle/_ref/libalsref_b200.so): the reference's time loop drives them and
@@ -17,6 +18,7 @@
 #include <vector>
 
 #include "alsfvm/boundary/Boundary.hpp"
+#include "alsfvm/diffusion/DiffusionOperator.hpp"
 #include "alsfvm/grid/Grid.hpp"
 #include "alsfvm/integrator/Integrator.hpp"
 #include "alsfvm/integrator/System.hpp"
@@ -201,6 +203,49 @@ public:
 private:
     int code;
     alsfvm::shared_ptr<integrator::System> system;
+    Staging stage;
+};
+
+// diffusion::DiffusionOperator (DiffusionOperator.hpp:25-47) backed by an
+// als_diffusion operator, created on the first call for the volume's shape.
+class DiffusionB200 : public diffusion::DiffusionOperator {
+public:
+    DiffusionB200(int dimension, int kind, int reconstruction, real gamma)
+        : dimension(dimension), kind(kind), reconstruction(reconstruction), gamma(gamma) {}
+
+    ~DiffusionB200() override {
+        als_diffusion_destroy(op);
+    }
+
+    void applyDiffusion(volume::Volume& outputVolume, const volume::Volume& conservedVolume) override {
+        if (!op) {
+            als_grid g;
+            g.dimension = dimension;
+            g.n[0] = int(conservedVolume.getNumberOfXCells());
+            g.n[1] = int(conservedVolume.getNumberOfYCells());
+            g.n[2] = int(conservedVolume.getNumberOfZCells());
+            g.ghosts = int(conservedVolume.getNumberOfXGhostCells());
+            g.gamma = gamma;
+            check_als(als_diffusion_create(&g, kind, reconstruction, &op), "als_diffusion_create");
+        }
+        std::vector<double*> u = stage.put(0, conservedVolume, true);
+        std::vector<double*> o = stage.put(1, outputVolume, true);
+        std::vector<const double*> cu(u.begin(), u.end());
+        check_als(als_diffusion_apply(op, cu.data(), o.data(), nullptr), "als_diffusion_apply");
+        check_cuda(cudaDeviceSynchronize());
+        stage.get(1, outputVolume);
+    }
+
+    size_t getNumberOfGhostCells() const override {
+        return size_t(als_diffusion_ghost_cells(reconstruction));
+    }
+
+private:
+    int dimension;
+    int kind;
+    int reconstruction;
+    real gamma;
+    als_diffusion* op = nullptr;
     Staging stage;
 };
 

@@ -69,7 +69,9 @@ public:
         g.n[0] = n.x;
         g.n[1] = n.y;
         g.n[2] = n.z;
-        g.ghosts = int(getNumberOfGhostCells());
+        // the volume's ghost width: at least the flux's, wider when a
+        // diffusion operator needs more (ConservedSystem.cpp:109-114)
+        g.ghosts = int(U.getNumberOfXGhostCells());
         g.gamma = gamma;
         const int s[3] = {start.x, start.y, start.z};
         const int e[3] = {end.x, end.y, end.z};

@@ -363,6 +363,7 @@ int orc_configure(orc_config* cfg, int dim, const int* n, const double* lower,
         return -1;
     }
     memset(cfg, 0, sizeof(*cfg));
+    cfg->diffusion = -1;
     cfg->dim = dim;
     for (d = 0; d < 3; ++d) {
         cfg->n[d] = d < dim ? n[d] : 1;
@@ -861,6 +862,7 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
     const size_t bytes = sizeof(double) * (size_t)nvar * (size_t)plane;
     const int substeps = cfg->integrator == ORC_INT_FE ? 1 : (cfg->integrator == ORC_INT_RK2 ? 2 : 3);
     double* vol[4];
+    double* diff_state = NULL;
     double t = 0;
     long steps = 0, i;
     int s, status = 0, d;
@@ -874,6 +876,14 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
     }
     memcpy(vol[0], planes, bytes);
     orc_fill_ghosts(cfg, vol[0], nvar);
+    if (cfg->diffusion >= 0) {
+        /* the operator's work arrays live as long as the simulator */
+        const long vol4 = 4L * nvar * plane;
+        diff_state = (double*)calloc((size_t)(vol4 + 3 * plane), sizeof(double));
+        for (i = 0; i < vol4; ++i) {
+            diff_state[i] = 42.0;
+        }
+    }
     while (t < end_time && steps < max_steps) {
         double dt = 0;
         for (s = 0; s < substeps; ++s) {
@@ -883,6 +893,9 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
             const double* U0 = vol[0];
             double c;
             orc_net_flux(cfg, Us, out, ws);
+            if (diff_state) {
+                orc_diffusion_apply(cfg, cfg->diffusion, cfg->diffusion_recon, diff_state, Us, out);
+            }
             if (s == 0) {
                 /* Integrator.cpp:20-46 then the end-time clamp */
                 double total = 0;
@@ -936,6 +949,7 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
     for (s = 0; s <= substeps; ++s) {
         free(vol[s]);
     }
+    free(diff_state);
     if (steps_out) {
         *steps_out = steps;
     }
@@ -1098,4 +1112,347 @@ void orc_structure_basic(int dim, const int* n, int g, int bc, int nvar, int dir
             }
         }
     }
+}
+
+/* ------------------------------------------------------- TeCNO diffusion */
+
+/* Conserved state rotated into direction d's frame, the "rotation trick"
+ * of Euler<2/3>::computeEigenVectorMatrix / computeEigenValues
+ * (Euler.hpp:409-425, 506-517): 2-D d=1 m -> (m_y, -m_x); 3-D d=1
+ * (m_y, -m_x, m_z), d=2 (m_z, m_y, -m_x).  Returns u (rotated), p, a. */
+static void rotated_primitive(int nsd, int d, double gamma, const double* U, double* u,
+    double* p, double* a) {
+    double m[3] = {0, 0, 0}, dot;
+    int k;
+    for (k = 0; k < nsd; ++k) {
+        m[k] = U[1 + k];
+    }
+    if (nsd == 2 && d == 1) {
+        const double mx = m[0];
+        m[0] = m[1];
+        m[1] = -mx;
+    } else if (nsd == 3 && d == 1) {
+        const double mx = m[0];
+        m[0] = m[1];
+        m[1] = -mx;
+    } else if (nsd == 3 && d == 2) {
+        const double mx = m[0];
+        m[0] = m[2];
+        m[2] = -mx;
+    }
+    /* computePrimitiveVariables (Euler.hpp:290-297) */
+    dot = m[0] * m[0];
+    if (nsd > 1) {
+        dot = dot + m[1] * m[1];
+    }
+    if (nsd > 2) {
+        dot = dot + m[2] * m[2];
+    }
+    for (k = 0; k < nsd; ++k) {
+        u[k] = m[k] / U[0];
+    }
+    *p = (gamma - 1) * (U[1 + nsd] - 0.5 * dot / U[0]);
+    *a = sqrt(gamma * *p / U[0]);
+}
+
+static double udot(int nsd, const double* u) {
+    double s = u[0] * u[0];
+    if (nsd > 1) {
+        s = s + u[1] * u[1];
+    }
+    if (nsd > 2) {
+        s = s + u[2] * u[2];
+    }
+    return s;
+}
+
+/* Eigenvector matrix R[row][col] of Euler<nsd>::computeEigenVectorMatrix<d>
+ * (Euler.hpp:409-466 normalised columns in 3-D, with the norm's square
+ * root taken in single precision as mat.hpp:96-110 does; 506-553 in 2-D;
+ * 586-623 scaled columns in 1-D). */
+static void eigenvectors(int nsd, int d, double gamma, const double* U, double R[5][5]) {
+    double u[3], p, a, H;
+    int r, c;
+    rotated_primitive(nsd, d, gamma, U, u, &p, &a);
+    H = (U[1 + nsd] + p) / U[0];
+    memset(R, 0, sizeof(double) * 25);
+    if (nsd == 1) {
+        const double rho = U[0];
+        const double a1 = sqrt(rho / (2 * gamma));
+        const double a2 = sqrt(rho * (gamma - 1) / gamma);
+        const double a4 = a1;
+        R[0][0] = a1;
+        R[0][1] = a2;
+        R[0][2] = a4;
+        R[1][0] = a1 * (u[0] - a);
+        R[1][1] = a2 * u[0];
+        R[1][2] = a4 * (u[0] + a);
+        R[2][0] = a1 * (H - u[0] * a);
+        R[2][1] = 0.5 * a2 * udot(1, u);
+        R[2][2] = a4 * (H + u[0] * a);
+    } else if (nsd == 2) {
+        R[0][0] = 1; R[0][1] = 1; R[0][2] = 0; R[0][3] = 1;
+        R[1][0] = u[0] - a; R[1][1] = u[0]; R[1][2] = 0; R[1][3] = u[0] + a;
+        R[2][0] = u[1]; R[2][1] = u[1]; R[2][2] = 1; R[2][3] = u[1];
+        R[3][0] = H - u[0] * a; R[3][1] = 0.5 * udot(2, u); R[3][2] = u[1];
+        R[3][3] = H + u[0] * a;
+    } else {
+        R[0][0] = 1; R[0][1] = 1; R[0][2] = 0; R[0][3] = 0; R[0][4] = 1;
+        R[1][0] = u[0] - a; R[1][1] = u[0]; R[1][2] = 0; R[1][3] = 0; R[1][4] = u[0] + a;
+        R[2][0] = u[1]; R[2][1] = u[1]; R[2][2] = 1; R[2][3] = 0; R[2][4] = u[1];
+        R[3][0] = u[2]; R[3][1] = u[2]; R[3][2] = 0; R[3][3] = 1; R[3][4] = u[2];
+        R[4][0] = H - u[0] * a; R[4][1] = 0.5 * udot(3, u); R[4][2] = u[1]; R[4][3] = u[2];
+        R[4][4] = H + u[0] * a;
+        for (c = 0; c < 5; ++c) {
+            double norm = 0;
+            for (r = 0; r < 5; ++r) {
+                norm += R[r][c] * R[r][c];
+            }
+            norm = sqrtf((float)norm);
+            for (r = 0; r < 5; ++r) {
+                R[r][c] = R[r][c] / norm;
+            }
+        }
+    }
+}
+
+/* Eigenvalues of the rotated flux Jacobian: u-a, u (nsd times), u+a
+ * (Euler.hpp:470-498, 555-580, 646-657). */
+static void eigenvalues(int nsd, int d, double gamma, const double* U, double* ev) {
+    double u[3], p, a;
+    int k;
+    rotated_primitive(nsd, d, gamma, U, u, &p, &a);
+    ev[0] = u[0] - a;
+    for (k = 1; k <= nsd; ++k) {
+        ev[k] = u[0];
+    }
+    ev[nsd + 1] = u[0] + a;
+}
+
+/* Entropy variables v(u) for E = -rho s/(gamma-1), s = log p - gamma log rho
+ * (Euler.hpp:323-348). */
+static void entropy_variables(int nsd, double gamma, const double* U, double* v) {
+    double u[3], dot = U[1] * U[1], p, s;
+    int k;
+    if (nsd > 1) {
+        dot = dot + U[2] * U[2];
+    }
+    if (nsd > 2) {
+        dot = dot + U[3] * U[3];
+    }
+    for (k = 0; k < nsd; ++k) {
+        u[k] = U[1 + k] / U[0];
+    }
+    p = (gamma - 1) * (U[1 + nsd] - 0.5 * dot / U[0]);
+    s = log(p) - gamma * log(U[0]);
+    v[0] = (gamma - s) / (gamma - 1) - (U[0] * udot(nsd, u)) / (2 * p);
+    for (k = 0; k < nsd; ++k) {
+        v[1 + k] = U[1 + k] / p;
+    }
+    v[1 + nsd] = -U[0] / p;
+}
+
+/* y = M x with the column-major accumulation of mat.hpp:47-60 (transpose:
+ * M(row, col) = R[col][row]). */
+static void mat_vec(int nv, double R[5][5], int transpose, const double* x, double* y) {
+    int r, c;
+    for (r = 0; r < nv; ++r) {
+        y[r] = 0;
+    }
+    for (c = 0; c < nv; ++c) {
+        for (r = 0; r < nv; ++r) {
+            y[r] += (transpose ? R[c][r] : R[r][c]) * x[c];
+        }
+    }
+}
+
+int orc_diffusion_ghost_cells(int recon) {
+    /* tecno::NoReconstruction: 1 (NoReconstruction.hpp:40-42); ENOCPU<order>: order */
+    return recon == 0 ? 1 : recon;
+}
+
+static void load_cell(const double* planes, long plane, int nvar, long c, double* U) {
+    int v;
+    for (v = 0; v < nvar; ++v) {
+        U[v] = planes[v * plane + c];
+    }
+}
+
+/* The diffusion flux D(l, r) = 0.5 R (Lambda (left[r] - right[l])), both at
+ * the mean of U[l] and U[r] (TecnoDiffusionCPU.cpp:70-88). */
+static void diffusion_term(const orc_config* cfg, int d, int kind, const double* U,
+    const double* rec_left, const double* rec_right, long plane, long l, long r, double* D) {
+    const int nsd = cfg->dim, nv = nsd + 2;
+    double Ul[5], Ur[5], avg[5], ev[5], R[5][5], diff[5], t[5], y[5];
+    int k;
+    load_cell(U, plane, nv, l, Ul);
+    load_cell(U, plane, nv, r, Ur);
+    for (k = 0; k < nv; ++k) {
+        avg[k] = 0.5 * (Ur[k] + Ul[k]);
+        diff[k] = rec_left[k * plane + r] - rec_right[k * plane + l];
+    }
+    eigenvalues(nsd, d, cfg->gamma, avg, ev);
+    if (kind == 0) {
+        /* RoeMatrix: diag |lambda_i| (RoeMatrix.hpp:36-45) */
+        for (k = 0; k < nv; ++k) {
+            t[k] = fabs(ev[k]) * diff[k];
+        }
+    } else {
+        /* RusanovMatrix: max_i |lambda_i| (RusanovMatrix.hpp:36-54) */
+        double mx = 0.0;
+        for (k = 0; k < nv; ++k) {
+            mx = fmax(fabs(ev[k]), mx);
+        }
+        for (k = 0; k < nv; ++k) {
+            t[k] = mx * diff[k];
+        }
+    }
+    eigenvectors(nsd, d, cfg->gamma, avg, R);
+    mat_vec(nv, R, 0, t, y);
+    for (k = 0; k < nv; ++k) {
+        D[k] = 0.5 * y[k];
+    }
+}
+
+void orc_diffusion_apply(const orc_config* cfg, int kind, int recon, double* state,
+    const double* U, double* out) {
+    int N[3];
+    const int nsd = cfg->dim, nv = nsd + 2;
+    const long plane = orc_plane_size(cfg);
+    double* EL = state;
+    double* ER = state + (long)nv * plane;
+    double* OL = state + 2L * nv * plane;
+    double* OR = state + 3L * nv * plane;
+    double* DD = state + 4L * nv * plane;
+    int d, x, y, z, k;
+    padded(cfg, N);
+    for (d = 0; d < nsd; ++d) {
+        const long s = d == 0 ? 1 : (d == 1 ? N[0] : (long)N[0] * N[1]);
+        /* pass 1: scaled entropy variables at both sides of face m-1|m for
+         * m in [1, N_d - 2] along d, every transverse cell
+         * (TecnoDiffusionCPU.cpp:40-58; volume_foreach.hpp:72-99) */
+        for (z = 0; z < N[2]; ++z) {
+            for (y = 0; y < N[1]; ++y) {
+                for (x = 0; x < N[0]; ++x) {
+                    const int c[3] = {x, y, z};
+                    const long m = idx3(N, x, y, z);
+                    double Um[5], Ul[5], avg[5], R[5][5], vm[5], vl[5], a[5], b[5];
+                    if (c[d] < 1 || c[d] > N[d] - 2) {
+                        continue;
+                    }
+                    load_cell(U, plane, nv, m, Um);
+                    load_cell(U, plane, nv, m - s, Ul);
+                    for (k = 0; k < nv; ++k) {
+                        avg[k] = 0.5 * (Um[k] + Ul[k]);
+                    }
+                    eigenvectors(nsd, d, cfg->gamma, avg, R);
+                    entropy_variables(nsd, cfg->gamma, Um, vm);
+                    entropy_variables(nsd, cfg->gamma, Ul, vl);
+                    mat_vec(nv, R, 1, vm, a);
+                    mat_vec(nv, R, 1, vl, b);
+                    for (k = 0; k < nv; ++k) {
+                        EL[k * plane + m] = a[k];
+                        ER[k * plane + m - s] = b[k];
+                    }
+                }
+            }
+        }
+        /* pass 2: reconstruction of the pair (tecno/NoReconstruction.cpp:20-44
+         * copies every cell; tecno/ENOCPU.cpp:35-139 for cells
+         * [order-1, N_d - order + 1) along d, every transverse cell) */
+        if (recon == 0) {
+            memcpy(OL, EL, sizeof(double) * (size_t)nv * (size_t)plane);
+            memcpy(OR, ER, sizeof(double) * (size_t)nv * (size_t)plane);
+        } else {
+            const int order = recon;
+            int var, level;
+            long i;
+            for (var = 0; var < nv; ++var) {
+                const double* L = EL + var * plane;
+                const double* Rt = ER + var * plane;
+                /* undivided differences into the operator's persistent
+                 * arrays (ENOCPU.cpp:205-267): level k writes
+                 * dd[k-1][j - s] for cells j with k <= c_d < N_d - k, every
+                 * transverse cell; level 1 from (left, right), level k > 1
+                 * from level k - 1.  Entries outside that range keep what
+                 * an earlier variable, direction or call left there. */
+                for (level = 1; level < order; ++level) {
+                    double* out_dd = DD + (long)(level - 1) * plane;
+                    const double* a = level == 1 ? L : DD + (long)(level - 2) * plane;
+                    const double* b = level == 1 ? Rt : a;
+                    for (i = 0; i < plane; ++i) {
+                        const int c[3] = {(int)(i % N[0]), (int)((i / N[0]) % N[1]),
+                            (int)(i / ((long)N[0] * N[1]))};
+                        if (c[d] < level || c[d] >= N[d] - level) {
+                            continue;
+                        }
+                        out_dd[i - s] = a[i] - b[i - s];
+                    }
+                }
+                /* ENOCPU.cpp:84-136 for cells [order-1, N_d - order + 1) */
+                for (i = 0; i < plane; ++i) {
+                    const int c[3] = {(int)(i % N[0]), (int)((i / N[0]) % N[1]),
+                        (int)(i / ((long)N[0] * N[1]))};
+                    double w[7], uli = 0, uri = 0;
+                    int shift = 0, l;
+                    if (c[d] < order - 1 || c[d] >= N[d] - order + 1) {
+                        continue;
+                    }
+                    for (level = 0; level < order - 1; ++level) {
+                        /* |dd(left)| < |dd(right)| moves the stencil left */
+                        if (fabs(DD[(long)level * plane + i - s]) < fabs(DD[(long)level * plane + i])) {
+                            ++shift;
+                        }
+                    }
+                    /* the stencil values are rebuilt from level-1 differences
+                     * at flat offsets +l and -l-1 (ENOCPU.cpp:118-123), i.e.
+                     * x-neighbours whatever the direction; kept as is */
+                    w[order - 1] = L[i];
+                    for (l = 0; l < order - 1; ++l) {
+                        w[order + l] = w[order + l - 1] + DD[i + l];
+                        w[order - l - 2] = w[order - l - 1] - DD[i - l - 1];
+                    }
+                    for (l = 0; l < order; ++l) {
+                        uli += eno_coef(order, shift, l) * w[order - 1 - shift + l];
+                        uri += eno_coef(order, shift + 1, l) * w[order - 1 - shift + l];
+                    }
+                    OL[var * plane + i] = uli;
+                    OR[var * plane + i] = uri + (Rt[i] - L[i]);
+                }
+            }
+        }
+        /* pass 3: out[m] += D(m, m+1) - D(m-1, m) for m in [1, N_d - 2]
+         * along d, every transverse cell (TecnoDiffusionCPU.cpp:62-92) */
+        for (z = 0; z < N[2]; ++z) {
+            for (y = 0; y < N[1]; ++y) {
+                for (x = 0; x < N[0]; ++x) {
+                    const int c[3] = {x, y, z};
+                    const long m = idx3(N, x, y, z);
+                    double Dr[5], Dl[5];
+                    if (c[d] < 1 || c[d] > N[d] - 2) {
+                        continue;
+                    }
+                    diffusion_term(cfg, d, kind, U, OL, OR, plane, m, m + s, Dr);
+                    diffusion_term(cfg, d, kind, U, OL, OR, plane, m - s, m, Dl);
+                    for (k = 0; k < nv; ++k) {
+                        out[k * plane + m] = out[k * plane + m] + (Dr[k] - Dl[k]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+int orc_set_diffusion(orc_config* cfg, int kind, int recon) {
+    int g;
+    if ((kind != 0 && kind != 1) || (recon != 0 && (recon < 2 || recon > 4))) {
+        return -1;
+    }
+    cfg->diffusion = kind;
+    cfg->diffusion_recon = recon;
+    g = orc_diffusion_ghost_cells(recon);
+    if (g > cfg->g) {
+        cfg->g = g;
+    }
+    return 0;
 }

@@ -36,6 +36,8 @@ typedef struct {
     double gamma;
     int flux, recon, integrator, bc;
     double dx[3];     /* cell lengths; 1 for inactive directions */
+    int diffusion;    /* -1 none, 0 tecnoroe, 1 tecnorusanov (orc_set_diffusion) */
+    int diffusion_recon;
 } orc_config;
 
 /* Ghost width max(stencil-1, reconstruction ghosts), NumericalFluxCPU.cpp:227-231. */
@@ -87,6 +89,27 @@ void orc_structure_basic(int dim, const int* n, int g, int bc, int nvar, int dir
 /* Constraint check of CPUCellComputer::obeysConstraints (CPUCellComputer.cpp:80-128)
  * over all cells; returns 1 when every cell obeys. */
 int orc_obeys_constraints(const orc_config* cfg, const double* planes);
+
+/* TeCNO diffusion, TecnoDiffusionCPU::applyDiffusion (TecnoDiffusionCPU.cpp:
+ * 23-170): kind 0 tecnoroe (RoeMatrix), 1 tecnorusanov (RusanovMatrix);
+ * recon 0 none, 2/3/4 ENO of that order (reconstruction/tecno/).  Adds the
+ * diffusion to `out` (every cell the reference touches, ghosts included).
+ * `state` holds the operator's persistent work arrays: four volumes
+ * (scaled entropy variables left/right, their reconstructions left/right;
+ * 4 * nvar planes), which the caller fills with 42 once, as HostMemory does
+ * (HostMemory.cpp:36-37), then the ENO's three difference planes, filled
+ * with 0 (ENOCPU.cpp:27-33, 196-203).  The caller keeps them between calls:
+ * the reference reads entries its passes do not write (the last cells along
+ * each direction), so results depend on what earlier calls, directions and
+ * variables left there. */
+int orc_diffusion_ghost_cells(int recon);
+
+/* Adds a TeCNO diffusion operator to the system of orc_simulate
+ * (ConservedSystem.cpp:102) and widens cfg->g to
+ * max(flux ghosts, diffusion ghosts) (ConservedSystem.cpp:109-114). */
+int orc_set_diffusion(orc_config* cfg, int kind, int recon);
+void orc_diffusion_apply(const orc_config* cfg, int kind, int recon, double* state,
+    const double* U, double* out);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,11 @@
 #include "alsfvm/simulator/SimulatorParameters.hpp"
 #include "alsfvm/simulator/TimestepInformation.hpp"
 #include "alsfvm/diffusion/NoDiffusion.hpp"
+#include "alsfvm/diffusion/TecnoDiffusionCPU.hpp"
+#include "alsfvm/diffusion/RoeMatrix.hpp"
+#include "alsfvm/diffusion/RusanovMatrix.hpp"
+#include "alsfvm/reconstruction/tecno/ENOCPU.hpp"
+#include "alsfvm/reconstruction/tecno/NoReconstruction.hpp"
 #include "alsfvm/volume/VolumeFactory.hpp"
 #include "alsfvm/memory/MemoryFactory.hpp"
 #include "alsfvm/equation/euler/EulerParameters.hpp"
@@ -98,12 +103,60 @@ struct Objects {
     std::shared_ptr<reconstruction::Reconstruction> recon;
     std::shared_ptr<numflux::NumericalFlux> flux;
     std::shared_ptr<integrator::System> system;
+    std::shared_ptr<diffusion::DiffusionOperator> diffusion;
     std::shared_ptr<integrator::Integrator> integ;
     std::shared_ptr<boundary::Boundary> boundary;
     std::shared_ptr<volume::VolumeFactory> volumeFactory;
     size_t ghosts = 0;
     std::string eqName;
 };
+
+// Diffusion operator of the next builds: "none" or "tecnoroe" /
+// "tecnorusanov" over the TeCNO reconstruction g_diffusion_recon
+// ("none", "eno2", "eno3", "eno4"), as DiffusionFactory.cpp:41-95 builds them.
+std::string g_diffusion = "none";
+std::string g_diffusion_recon = "none";
+
+#ifdef ALSREF_WITH_B200
+extern std::string g_flux_platform;
+#endif
+
+template<int d>
+std::shared_ptr<diffusion::DiffusionOperator> makeDiffusion(const Setup& s, Objects& o) {
+    typedef equation::euler::Euler<d> Eq;
+    if (g_diffusion == "none") {
+        return std::make_shared<diffusion::NoDiffusion>();
+    }
+#ifdef ALSREF_WITH_B200
+    if (g_flux_platform == "b200-all") {
+        const int kind = g_diffusion == "tecnoroe" ? ALS_DIFFUSION_TECNOROE : ALS_DIFFUSION_TECNORUSANOV;
+        const int rec = g_diffusion_recon == "none" ? ALS_TECNO_RECON_NONE
+            : (g_diffusion_recon == "eno2" ? ALS_TECNO_RECON_ENO2
+            : (g_diffusion_recon == "eno3" ? ALS_TECNO_RECON_ENO3 : ALS_TECNO_RECON_ENO4));
+        return std::make_shared<b200::DiffusionB200>(d, kind, rec, s.gamma);
+    }
+#endif
+    std::shared_ptr<reconstruction::tecno::TecnoReconstruction> rec;
+    if (g_diffusion_recon == "none") {
+        rec = std::make_shared<reconstruction::tecno::NoReconstruction>();
+    } else if (g_diffusion_recon == "eno2") {
+        rec = std::make_shared<reconstruction::tecno::ENOCPU<2>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else if (g_diffusion_recon == "eno3") {
+        rec = std::make_shared<reconstruction::tecno::ENOCPU<3>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else if (g_diffusion_recon == "eno4") {
+        rec = std::make_shared<reconstruction::tecno::ENOCPU<4>>(o.memoryFactory, s.n.x, s.n.y, s.n.z);
+    } else {
+        THROW("unknown diffusion reconstruction " << g_diffusion_recon);
+    }
+    if (g_diffusion == "tecnoroe") {
+        return std::make_shared<diffusion::TecnoDiffusionCPU<Eq, diffusion::RoeMatrix>>(
+            *o.volumeFactory, rec, *o.params);
+    } else if (g_diffusion == "tecnorusanov") {
+        return std::make_shared<diffusion::TecnoDiffusionCPU<Eq, diffusion::RusanovMatrix>>(
+            *o.volumeFactory, rec, *o.params);
+    }
+    THROW("unknown diffusion " << g_diffusion);
+}
 
 #ifdef ALSREF_WITH_B200
 // Flux platform of the next builds: "cpu" (the reference's NumericalFluxCPU)
@@ -206,15 +259,14 @@ Objects build(const Setup& s) {
     std::array<boundary::Type, 6> bcs = {t, t, t, t, t, t};
     o.grid = std::make_shared<grid::Grid>(s.lower, s.upper, s.n, bcs);
 
+    o.volumeFactory = std::make_shared<volume::VolumeFactory>(o.eqName, o.memoryFactory);
     switch (s.dim) {
-    case 1: o.recon = makeRecon<1>(s, o); o.flux = makeFlux<1>(s, o); break;
-    case 2: o.recon = makeRecon<2>(s, o); o.flux = makeFlux<2>(s, o); break;
-    case 3: o.recon = makeRecon<3>(s, o); o.flux = makeFlux<3>(s, o); break;
+    case 1: o.recon = makeRecon<1>(s, o); o.flux = makeFlux<1>(s, o); o.diffusion = makeDiffusion<1>(s, o); break;
+    case 2: o.recon = makeRecon<2>(s, o); o.flux = makeFlux<2>(s, o); o.diffusion = makeDiffusion<2>(s, o); break;
+    case 3: o.recon = makeRecon<3>(s, o); o.flux = makeFlux<3>(s, o); o.diffusion = makeDiffusion<3>(s, o); break;
     default: THROW("dimension must be 1, 2 or 3");
     }
-    std::shared_ptr<diffusion::DiffusionOperator> diffusion =
-        std::make_shared<diffusion::NoDiffusion>();
-    o.system = std::make_shared<simulator::ConservedSystem>(o.flux, diffusion);
+    o.system = std::make_shared<simulator::ConservedSystem>(o.flux, o.diffusion);
     if (s.integrator == "forwardeuler") {
         o.integ = std::make_shared<integrator::ForwardEuler>(o.system);
     } else if (s.integrator == "rungekutta2") {
@@ -240,7 +292,6 @@ Objects build(const Setup& s) {
             o.system);
     }
 #endif
-    o.volumeFactory = std::make_shared<volume::VolumeFactory>(o.eqName, o.memoryFactory);
     return o;
 }
 
@@ -536,6 +587,55 @@ int alsref_structure_cube(int dim, const int* n, int ghosts, const char* bc, int
         }
         return 0;
     } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Selects the diffusion operator of the following builds (see g_diffusion).
+int alsref_set_diffusion(const char* kind, const char* recon) {
+    const std::string k(kind ? kind : ""), r(recon ? recon : "");
+    if ((k != "none" && k != "tecnoroe" && k != "tecnorusanov") ||
+        (r != "none" && r != "eno2" && r != "eno3" && r != "eno4")) {
+        g_last_error = "unknown diffusion " + k + " / " + r;
+        return -1;
+    }
+    g_diffusion = k;
+    g_diffusion_recon = r;
+    return 0;
+}
+
+// DiffusionOperator::applyDiffusion of one operator object, called `calls`
+// times: call k adds the diffusion of state k to output k (both nvar padded
+// planes of the ghost width the reference picks, flux hll + reconstruction
+// none + this diffusion).  The operator keeps its work volumes between
+// calls, as in a time loop.  *ghosts receives that width.
+int alsref_apply_diffusion(int dim, const int* n, const char* kind, const char* recon,
+    double gamma, int calls, const double* states, double* outs, int* ghosts) {
+    const std::string k0 = g_diffusion, r0 = g_diffusion_recon;
+    try {
+        if (alsref_set_diffusion(kind, recon) != 0) {
+            return -1;
+        }
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", "neumann", gamma, 0.5);
+        auto o = build(s);
+        g_diffusion = k0;
+        g_diffusion_recon = r0;
+        *ghosts = int(o.ghosts);
+        auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, o.ghosts);
+        auto out = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, o.ghosts);
+        const size_t size = paddedCells(*u) * u->getNumberOfVariables();
+        for (int c = 0; c < calls; ++c) {
+            copyIn(*u, states + size_t(c) * size);
+            copyIn(*out, outs + size_t(c) * size);
+            o.diffusion->applyDiffusion(*out, *u);
+            copyOut(*out, outs + size_t(c) * size);
+        }
+        return 0;
+    } catch (std::exception& e) {
+        g_diffusion = k0;
+        g_diffusion_recon = r0;
         g_last_error = e.what();
         return -1;
     }

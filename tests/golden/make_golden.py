@@ -149,6 +149,59 @@ def write_tecno_fixtures(ref):
         print(name, "steps=%d t=%r" % (steps, t))
 
 
+# TeCNO diffusion in the reference's time loop (ConservedSystem with
+# TecnoDiffusionCPU), prefixed "tecnodiff_": (..., diffusion, its reconstruction)
+DIFFUSION_SIMULATIONS = {
+    "tecnodiff_rand1d_64_tecno1_roe_eno2_rk3": (1, (64,), (0.0,), (1.0,), "tecno1", "none",
+                                                "rungekutta3", "periodic", 0.4, 0.05, "seed:31",
+                                                "tecnoroe", "eno2"),
+    "tecnodiff_sod128_tecno4_rusanov_eno3_rk2": (1, (128,), (-1.0,), (1.0,), "tecno4", "none",
+                                                 "rungekutta2", "neumann", 0.4, 0.05, "sod",
+                                                 "tecnorusanov", "eno3"),
+    "tecnodiff_rand2d_14x12_tecno1_roe_eno2_rk3": (2, (14, 12), (0.0, 0.0), (1.0, 1.0), "tecno1",
+                                                   "none", "rungekutta3", "periodic", 0.4, 0.01,
+                                                   "seed:32", "tecnoroe", "eno2"),
+    "tecnodiff_rand3d_10x11x10_tecno1_rusanov_eno4_rk3": (3, (10, 11, 10), (0.0, 0.0, 0.0),
+                                                          (1.0, 1.0, 1.0), "tecno1", "none",
+                                                          "rungekutta3", "neumann", 0.4, 0.01,
+                                                          "seed:33", "tecnorusanov", "eno4"),
+}
+
+
+def diffusion_ghosts(flux, recon, diffusion_recon):
+    return max(ghost_cells(recon, flux), 1 if diffusion_recon == "none" else int(diffusion_recon[-1]))
+
+
+def write_diffusion_fixtures(ref):
+    for name, (dim, n, lo, hi, flux, recon, integ, bc, cfl, T, kind, dkind, drec) in \
+            DIFFUSION_SIMULATIONS.items():
+        g = diffusion_ghosts(flux, recon, drec)
+        U0 = initial_state(kind, dim, n, g)
+        ref.set_diffusion(dkind, drec)
+        rc, U, dts, steps, t = ref.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, cfl, T, U0)
+        ref.set_diffusion("none")
+        assert rc == 0, name
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), initial=U0, final=U, dts=dts,
+                            steps=steps, t=t, dim=dim, n=np.array(n), lower=np.array(lo),
+                            upper=np.array(hi), flux=flux, recon=recon, integrator=integ, bc=bc,
+                            cfl=cfl, end_time=T, gamma=1.4, diffusion=dkind,
+                            diffusion_recon=drec)
+        print(name, "steps=%d t=%r" % (steps, t))
+    # one operator applied three times in a row (its work arrays carry over)
+    for dim, n, dkind, drec, seed in ((2, (12, 11), "tecnoroe", "eno3", 41),
+                                      (3, (9, 10, 8), "tecnorusanov", "eno2", 42)):
+        g = 1 if drec == "none" else int(drec[-1])
+        states = np.stack([smooth_random_state(seed + k, dim, n, g) for k in range(3)])
+        outs = np.stack([np.random.default_rng(seed + k).uniform(-1, 1, states.shape[1:])
+                         for k in range(3)])
+        res = ref.apply_diffusion(dim, n, dkind, drec, 1.4, states, outs)
+        name = "diffusion_apply_%dd_%s_%s" % (dim, dkind, drec)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), states=states, outs=outs,
+                            result=res, dim=dim, n=np.array(n), ghosts=g, diffusion=dkind,
+                            diffusion_recon=drec, gamma=1.4)
+        print(name)
+
+
 def main():
     ref = RefOracle()
     out = {}
@@ -185,6 +238,7 @@ def main():
                                   digest(filled), digest(net), digest(ws), float(ws.max())))
     write_limiter_cases(ref)
     write_tecno_fixtures(ref)
+    write_diffusion_fixtures(ref)
     with open(os.path.join(HERE, "compute_flux_cases.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
                 "sha256(wave speeds) max_wave_speed\n")

@@ -24,6 +24,8 @@ FLUX = {"hll": 0, "hll3": 1, "central": 2, "tecno1": 3, "tecno4": 4, "tecno6": 5
 RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
          "wenof2": 7, "weno3": 8}
 INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
+DIFFUSION = {"tecnoroe": 0, "tecnorusanov": 1}
+DIFFUSION_RECON = {"none": 0, "eno2": 2, "eno3": 3, "eno4": 4}
 BC = {"neumann": 0, "periodic": 1}
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -59,6 +61,8 @@ class _Config(ctypes.Structure):
         ("integrator", ctypes.c_int),
         ("bc", ctypes.c_int),
         ("dx", ctypes.c_double * 3),
+        ("diffusion", ctypes.c_int),
+        ("diffusion_recon", ctypes.c_int),
     ]
 
 
@@ -86,6 +90,10 @@ class COracle:
         L.orc_fill_ghosts.argtypes = [ctypes.POINTER(_Config), _D, ctypes.c_int]
         L.orc_meanvar.argtypes = [ctypes.c_long, ctypes.c_long, _D, _D, _D]
         L.orc_obeys_constraints.argtypes = [ctypes.POINTER(_Config), _D]
+        L.orc_diffusion_apply.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, ctypes.c_int,
+                                          _D, _D, _D]
+        L.orc_diffusion_ghost_cells.argtypes = [ctypes.c_int]
+        L.orc_set_diffusion.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, ctypes.c_int]
         L.orc_structure_cube.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D]
         L.orc_structure_basic.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
@@ -140,6 +148,32 @@ class COracle:
         self.lib.orc_meanvar(count, st.shape[0], _dptr(st), _dptr(mean), _dptr(var))
         return mean.reshape(st.shape[1:]), var.reshape(st.shape[1:])
 
+    def set_diffusion(self, cfg, kind, recon):
+        """Adds a TeCNO diffusion operator to cfg's system (widens cfg.g)."""
+        assert self.lib.orc_set_diffusion(ctypes.byref(cfg), DIFFUSION[kind],
+                                          DIFFUSION_RECON[recon]) == 0
+        return cfg
+
+    def diffusion_state(self, cfg):
+        """The persistent work arrays of a diffusion operator as the
+        reference creates them: four volumes from HostMemory (every entry
+        42), then three zeroed difference planes."""
+        shp = padded_shape(cfg.dim, list(cfg.n), cfg.g)
+        plane = int(np.prod(shp[1:]))
+        st = np.zeros(4 * shp[0] * plane + 3 * plane)
+        st[:4 * shp[0] * plane] = 42.0
+        return st
+
+    def apply_diffusion(self, cfg, kind, recon, state, planes, out):
+        """Adds the TeCNO diffusion of `planes` to a copy of `out`; `state`
+        (from diffusion_state) is updated in place."""
+        assert state.flags["C_CONTIGUOUS"] and state.dtype == np.float64
+        inp = np.ascontiguousarray(planes, dtype=np.float64)
+        res = np.ascontiguousarray(out, dtype=np.float64).copy()
+        self.lib.orc_diffusion_apply(ctypes.byref(cfg), DIFFUSION[kind], DIFFUSION_RECON[recon],
+                                     _dptr(state), _dptr(inp), _dptr(res))
+        return res
+
     def obeys_constraints(self, cfg, planes):
         p = np.ascontiguousarray(planes, dtype=np.float64)
         return bool(self.lib.orc_obeys_constraints(ctypes.byref(cfg), _dptr(p)))
@@ -192,6 +226,26 @@ class RefOracle:
         L.alsref_ghost_cells.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]
         L.alsref_structure_cube.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_char_p,
                                             ctypes.c_int, ctypes.c_double, _D, _D]
+        L.alsref_set_diffusion.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.alsref_apply_diffusion.argtypes = [ctypes.c_int, _I, ctypes.c_char_p, ctypes.c_char_p,
+                                             ctypes.c_double, ctypes.c_int, _D, _D,
+                                             ctypes.POINTER(ctypes.c_int)]
+
+    def set_diffusion(self, kind, recon="none"):
+        """Diffusion operator of the following simulations (none by default)."""
+        self._check(self.lib.alsref_set_diffusion(kind.encode(), recon.encode()))
+
+    def apply_diffusion(self, dim, n, kind, recon, gamma, states, outs):
+        """One operator object applied to states[k], adding into outs[k] in
+        turn; returns the new outputs."""
+        st = np.ascontiguousarray(states, dtype=np.float64)
+        out = np.ascontiguousarray(outs, dtype=np.float64).copy()
+        g = ctypes.c_int()
+        self._check(self.lib.alsref_apply_diffusion(dim, self._vec(n, ctypes.c_int, 1),
+                                                    kind.encode(), recon.encode(), gamma,
+                                                    st.shape[0], _dptr(st), _dptr(out),
+                                                    ctypes.byref(g)))
+        return out
 
     def _check(self, rc):
         if rc < 0:

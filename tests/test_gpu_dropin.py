@@ -85,3 +85,38 @@ def test_reference_time_loop_with_b200_tecno_flux(ref_b200, platform, dim, n, fl
     assert abs(a[4] - b[4]) <= 1e-15
     np.testing.assert_allclose(a[2], b[2], rtol=1e-10)
     np.testing.assert_allclose(a[1], b[1], rtol=1e-10, atol=1e-12)
+
+
+DIFFUSION_CASES = [(1, (32,), "tecno1", "tecnoroe", "eno2", "rungekutta3", "periodic", 0.03),
+                   (1, (40,), "tecno4", "tecnorusanov", "eno3", "rungekutta2", "neumann", 0.03),
+                   (2, (14, 12), "tecno1", "tecnoroe", "eno2", "rungekutta3", "periodic", 0.01),
+                   (3, (10, 11, 10), "tecno1", "tecnorusanov", "eno4", "rungekutta3", "neumann",
+                    0.01)]
+
+
+@pytest.mark.parametrize("dim,n,flux,dkind,drec,integ,bc,T", DIFFUSION_CASES,
+                         ids=["d%d-%s-%s-%s" % (c[0], c[2], c[3], c[4]) for c in DIFFUSION_CASES])
+def test_reference_time_loop_with_b200_diffusion(ref_b200, dim, n, flux, dkind, drec, integ, bc, T):
+    """The reference's time loop with every part from the B200 library
+    (NumericalFluxB200, DiffusionB200, BoundaryB200, IntegratorB200) against
+    the reference's own classes, TeCNO diffusion in the system: same status
+    and steps, states within relative 1e-10 (device vs C library log)."""
+    g = max(ghost_cells("none", flux), 1 if drec == "none" else int(drec[-1]))
+    seed = zlib.crc32(("dropin-diff-%d-%s-%s" % (dim, flux, drec)).encode()) % 100000
+    st = smooth_random_state(seed, dim, n, g)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    out = {}
+    ref_b200.set_diffusion(dkind, drec)
+    try:
+        for p in ("cpu", "b200-all"):
+            ref_b200.set_flux_platform(p)
+            out[p] = ref_b200.simulate(dim, n, lo, hi, flux, "none", integ, bc, 1.4, 0.4, T, st)
+    finally:
+        ref_b200.set_flux_platform("cpu")
+        ref_b200.set_diffusion("none")
+    a, b = out["cpu"], out["b200-all"]
+    assert a[0] == b[0] == 0
+    assert a[3] == b[3] >= 1
+    assert abs(a[4] - b[4]) <= 1e-15
+    np.testing.assert_allclose(a[2], b[2], rtol=1e-10)
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-10, atol=1e-12)

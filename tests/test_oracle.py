@@ -313,3 +313,67 @@ def test_tecno_entropy_production(c_oracle, dim, n):
     assert abs(production("tecno4")) < 1e-14
     assert abs(production("tecno6")) > 1e-7
     assert production("hll3") < -1e-3
+
+
+# --------------------------------------------------------------------------
+# TeCNO diffusion (TecnoDiffusionCPU with the tecno reconstructions)
+
+DIFFUSION_FIXTURES = sorted(f[:-4] for f in os.listdir(GOLDEN)
+                            if f.startswith("tecnodiff_") and f.endswith(".npz"))
+DIFFUSION_APPLY_FIXTURES = sorted(f[:-4] for f in os.listdir(GOLDEN)
+                                  if f.startswith("diffusion_apply_") and f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", DIFFUSION_FIXTURES)
+def test_c_oracle_reproduces_reference_diffusion_simulation(c_oracle, name):
+    """Time loops with a TeCNO diffusion operator in the system, made by the
+    reference build, reproduced bit for bit."""
+    z = load_golden(name)
+    dim = int(z["dim"])
+    cfg = c_oracle.config(dim, z["n"], z["lower"], z["upper"], str(z["flux"]), str(z["recon"]),
+                          str(z["integrator"]), str(z["bc"]), float(z["gamma"]))
+    c_oracle.set_diffusion(cfg, str(z["diffusion"]), str(z["diffusion_recon"]))
+    rc, U, dts, steps, t = c_oracle.simulate(cfg, z["initial"], float(z["cfl"]),
+                                             float(z["end_time"]))
+    assert rc == 0 and steps == z["steps"] and t == z["t"]
+    np.testing.assert_array_equal(dts, z["dts"])
+    np.testing.assert_array_equal(U, z["final"])
+
+
+@pytest.mark.parametrize("name", DIFFUSION_APPLY_FIXTURES)
+def test_c_oracle_reproduces_reference_diffusion_calls(c_oracle, name):
+    """One operator applied to three states in a row: the reference reads
+    entries of its work arrays that only earlier calls wrote, and the
+    oracle's persistent state reproduces that bit for bit."""
+    z = load_golden(name)
+    dim = int(z["dim"])
+    cfg = c_oracle.config(dim, z["n"], [0.0] * dim, [1.0] * dim, "hll", "none", "rungekutta3",
+                          "neumann", float(z["gamma"]))
+    cfg.g = int(z["ghosts"])
+    st = c_oracle.diffusion_state(cfg)
+    for k in range(z["states"].shape[0]):
+        res = c_oracle.apply_diffusion(cfg, str(z["diffusion"]), str(z["diffusion_recon"]), st,
+                                       z["states"][k], z["outs"][k])
+        np.testing.assert_array_equal(res, z["result"][k])
+
+
+@pytest.mark.parametrize("dim,n", [(1, (24,)), (2, (12, 11)), (3, (9, 10, 8))])
+@pytest.mark.parametrize("kind", ["tecnoroe", "tecnorusanov"])
+@pytest.mark.parametrize("recon", ["none", "eno2", "eno3", "eno4"])
+def test_c_oracle_diffusion_matches_reference_build(c_oracle, ref_oracle, dim, n, kind, recon):
+    """Every operator of the reference's diffusion factory for the Euler
+    equations, three calls in a row on fresh random states (skipped without
+    the reference build)."""
+    g = 1 if recon == "none" else int(recon[-1])
+    seed = 6000 + 31 * dim + 7 * ["none", "eno2", "eno3", "eno4"].index(recon) + len(kind)
+    states = np.stack([smooth_random_state(seed + k, dim, n, g) for k in range(3)])
+    outs = np.stack([np.random.default_rng(seed + k).uniform(-1, 1, states.shape[1:])
+                     for k in range(3)])
+    ref = ref_oracle.apply_diffusion(dim, n, kind, recon, 1.4, states, outs)
+    cfg = c_oracle.config(dim, n, [0.0] * dim, [1.0] * dim, "hll", "none", "rungekutta3",
+                          "neumann", 1.4)
+    cfg.g = g
+    st = c_oracle.diffusion_state(cfg)
+    for k in range(3):
+        np.testing.assert_array_equal(
+            c_oracle.apply_diffusion(cfg, kind, recon, st, states[k], outs[k]), ref[k])
