@@ -65,6 +65,8 @@ PROTOTYPES = {
                                        _PP, _VP]),
     "als_integrator_combine": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,
                                               ctypes.c_size_t, ctypes.c_double, _VP]),
+    "als_integrator_combine_rk4": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, ctypes.c_size_t,
+                                                  ctypes.c_double, _VP]),
     "als_compute_timestep": (ctypes.c_double, [_D, _D, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double]),
     "als_solver_create": (ctypes.c_int, [ctypes.POINTER(SolverConfig), ctypes.c_int,

@@ -75,12 +75,21 @@ __global__ void __launch_bounds__(256) fe_update(const R* L, R* un, long long pl
 //   integrator 1 (RK2): s0 as FE; s1: ((c*L + Us) + U0) * 0.5
 //   integrator 2 (RK3): s0 as FE; s1: ((c*L + Us) * 1/3 + U0) * 3/4;
 //                       s2: ((c*L + Us) * 2 + U0) * 1/3
+//   integrator 3 (RK4): s0, s1: (c*L) * 0.5 + U0; s2: c*L + U0
+//                       (RungeKutta4.cpp:66-78; s3 is combine_rk4_final)
 template<class R>
 __global__ void __launch_bounds__(256) combine(R* out, const R* us, const R* u0, long long count,
     R c, int integrator, int substep) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x) {
         R x = out[i] * c;
+        if (integrator == 3) {
+            if (substep < 2) {
+                x = x * R(0.5);
+            }
+            out[i] = x + u0[i];
+            continue;
+        }
         x = x + us[i];
         if (integrator == 2 && substep == 1) {
             x = x * R(1. / 3.);
@@ -94,6 +103,25 @@ __global__ void __launch_bounds__(256) combine(R* out, const R* us, const R* u0,
             x = x + u0[i];
             x = x * R(0.5);
         }
+        out[i] = x;
+    }
+}
+
+// RK4's last stage, Volume::addLinearCombination (Volume.cpp:359-370,
+// HostMemory.cpp:261-280): out = a1 L + a2 U1 + a3 U2 + a4 U3 + a5 U0,
+// summed left to right, with a1 = (1/6)(dt/dx), a2 = a4 = 1/3, a3 = 2/3,
+// a5 = -1/3 (RungeKutta4.cpp:80-87).
+template<class R>
+__global__ void __launch_bounds__(256) combine_rk4_final(R* out, const R* u0, const R* u1,
+    const R* u2, const R* u3, long long count, R a1) {
+    const R a2 = R(1.0 / 3.0), a3 = R(2.0 / 3.0), a4 = R(1.0 / 3.0), a5 = R(-1.0 / 3.0);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        R x = a1 * out[i];
+        x = x + a2 * u1[i];
+        x = x + a3 * u2[i];
+        x = x + a4 * u3[i];
+        x = x + a5 * u0[i];
         out[i] = x;
     }
 }

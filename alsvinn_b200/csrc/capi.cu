@@ -395,12 +395,28 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
 int als_integrator_combine(int integrator, int substep, double* out, const double* us,
     const double* u0, size_t count, double c, void* stream) {
     const int substeps = integrator + 1;
-    if (integrator < ALS_INT_FORWARD_EULER || integrator > ALS_INT_RK3 || substep < 0 ||
-        substep >= substeps || !out || !us || (substep > 0 && !u0)) {
+    if (integrator < ALS_INT_FORWARD_EULER || integrator > ALS_INT_RK4 || substep < 0 ||
+        substep >= substeps || !out || !us || ((substep > 0 || integrator == ALS_INT_RK4) && !u0)) {
         return fail(ALS_E_INVALID, "invalid combine arguments");
+    }
+    if (integrator == ALS_INT_RK4 && substep == 3) {
+        return fail(ALS_E_INVALID, "RK4's last stage combines five volumes: als_integrator_combine_rk4");
     }
     als::combine<double><<<grid_blocks((long long)count, 256), 256, 0, (cudaStream_t)stream>>>(
         out, us, u0, (long long)count, c, integrator, substep);
+    ALS_CUDA(cudaGetLastError());
+    return ALS_OK;
+}
+
+int als_integrator_combine_rk4(double* out, const double* u0, const double* u1, const double* u2,
+    const double* u3, size_t count, double c, void* stream) {
+    if (!out || !u0 || !u1 || !u2 || !u3) {
+        return fail(ALS_E_INVALID, "invalid combine arguments");
+    }
+    // a1 = (1.0 / 6.0) * cellScaling.x (RungeKutta4.cpp:81)
+    const double a1 = (1.0 / 6.0) * c;
+    als::combine_rk4_final<double><<<grid_blocks((long long)count, 256), 256, 0,
+        (cudaStream_t)stream>>>(out, u0, u1, u2, u3, (long long)count, a1);
     ALS_CUDA(cudaGetLastError());
     return ALS_OK;
 }
@@ -684,6 +700,10 @@ int range_level(const als_solver* s, int first, int count) {
 }
 
 int check_config(const als_solver_config* cfg) {
+    if (cfg->integrator == ALS_INT_RK4) {
+        return fail(ALS_E_UNSUPPORTED,
+            "RK4 runs through the plug-in integrator (als_integrator_combine, als_integrator_combine_rk4)");
+    }
     if (cfg->dimension < 1 || cfg->dimension > 3 || !valid_choice(cfg->flux, cfg->reconstruction) ||
         cfg->integrator < ALS_INT_FORWARD_EULER || cfg->integrator > ALS_INT_RK3 ||
         (cfg->boundary != ALS_BC_NEUMANN && cfg->boundary != ALS_BC_PERIODIC) ||

@@ -19,7 +19,7 @@ from .initial_data import padded_shape
 FLUX = {"hll": 0, "hll3": 1, "central": 2, "tecno1": 3, "tecno4": 4, "tecno6": 5}
 RECONSTRUCTION = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
                   "wenof2": 7, "weno3": 8}
-INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
+INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2, "rungekutta4": 3}
 BOUNDARY = {"neumann": 0, "periodic": 1}
 PRECISION = {"fp64": 0, "fp32": 1}
 EQUATION = {"euler1": 1, "euler2": 2, "euler3": 3}
@@ -460,7 +460,14 @@ class Integrator:
         if substep == 0:
             dt = self.computeTimestep(ws, cell_lengths, t, end_time)
         c = dt / cell_lengths[0]
-        _lib.check(lib.als_integrator_combine(self.integrator, substep, _ptr(out),
-                                              _ptr(volumes[substep]), _ptr(volumes[0]),
-                                              out.numel(), c, _stream(stream)))
+        if self.integrator == 3 and substep == 3:
+            # RungeKutta4.cpp:80-87
+            _lib.check(lib.als_integrator_combine_rk4(_ptr(out), _ptr(volumes[0]),
+                                                      _ptr(volumes[1]), _ptr(volumes[2]),
+                                                      _ptr(volumes[3]), out.numel(), c,
+                                                      _stream(stream)))
+        else:
+            _lib.check(lib.als_integrator_combine(self.integrator, substep, _ptr(out),
+                                                  _ptr(volumes[substep]), _ptr(volumes[0]),
+                                                  out.numel(), c, _stream(stream)))
         return dt

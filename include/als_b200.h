@@ -52,6 +52,7 @@ extern "C" {
 #define ALS_INT_FORWARD_EULER 0     /* "forwardeuler", integrator/ForwardEuler.cpp */
 #define ALS_INT_RK2 1               /* "rungekutta2",  integrator/RungeKutta2.cpp */
 #define ALS_INT_RK3 2               /* "rungekutta3",  integrator/RungeKutta3.cpp */
+#define ALS_INT_RK4 3               /* "rungekutta4",  integrator/RungeKutta4.cpp (plug-in path only) */
 #define ALS_BC_NEUMANN 0            /* "neumann",  boundary/Neumann.hpp */
 #define ALS_BC_PERIODIC 1           /* "periodic", boundary/Periodic.hpp */
 #define ALS_FP64 0
@@ -127,10 +128,16 @@ int als_reconstruct(const als_grid* grid, int reconstruction, int direction,
 
 /* Stage combination of Integrator::performSubstep
  * (alsfvm/include/alsfvm/integrator/Integrator.hpp:59-80; ForwardEuler.cpp:32-51,
- * RungeKutta2.cpp:37-67, RungeKutta3.cpp:49-86) over `count` elements:
- * on entry out = L(U_substep); us = U_substep, u0 = U_0; c = dt/dx. */
+ * RungeKutta2.cpp:37-67, RungeKutta3.cpp:49-86, RungeKutta4.cpp:66-78) over
+ * `count` elements: on entry out = L(U_substep); us = U_substep, u0 = U_0;
+ * c = dt/dx.  RK4's substep 3 takes als_integrator_combine_rk4. */
 int als_integrator_combine(int integrator, int substep, double* out, const double* us,
     const double* u0, size_t count, double c, void* stream);
+
+/* RK4's last stage (RungeKutta4.cpp:80-87, Volume::addLinearCombination):
+ * out = (c/6) L(U_3) + U_1/3 + 2 U_2/3 + U_3/3 - U_0/3, on entry out = L(U_3). */
+int als_integrator_combine_rk4(double* out, const double* u0, const double* u1, const double* u2,
+    const double* u3, size_t count, double c, void* stream);
 
 /* Integrator::computeTimestep + adjustTimestep with an end-time clamp
  * (alsfvm/src/integrator/Integrator.cpp:20-46, alsfvm/src/io/FixedIntervalWriter.cpp:45-53):

@@ -176,7 +176,7 @@ public:
         : code(integratorCode), system(system) {}
 
     size_t getNumberOfSubsteps() const override {
-        return code == ALS_INT_FORWARD_EULER ? 1 : (code == ALS_INT_RK2 ? 2 : 3);
+        return size_t(code + 1);
     }
 
     real performSubstep(std::vector<alsfvm::shared_ptr<volume::Volume>>& inputConserved,
@@ -191,9 +191,19 @@ public:
         std::vector<double*> us = stage.put(1, *inputConserved[substep], true);
         std::vector<double*> u0 = stage.put(2, *inputConserved[0], true);
         const size_t cells = padded_cells(output);
-        for (size_t k = 0; k < o.size(); ++k) {
-            check_als(als_integrator_combine(code, int(substep), o[k], us[k], u0[k], cells,
-                dt / spatialCellSizes.x, nullptr), "als_integrator_combine");
+        if (code == ALS_INT_RK4 && substep == 3) {
+            // out = (c/6) L + U1/3 + 2 U2/3 + U3/3 - U0/3 (RungeKutta4.cpp:80-87)
+            std::vector<double*> u1 = stage.put(3, *inputConserved[1], true);
+            std::vector<double*> u2 = stage.put(4, *inputConserved[2], true);
+            for (size_t k = 0; k < o.size(); ++k) {
+                check_als(als_integrator_combine_rk4(o[k], u0[k], u1[k], u2[k], us[k], cells,
+                    dt / spatialCellSizes.x, nullptr), "als_integrator_combine_rk4");
+            }
+        } else {
+            for (size_t k = 0; k < o.size(); ++k) {
+                check_als(als_integrator_combine(code, int(substep), o[k], us[k], u0[k], cells,
+                    dt / spatialCellSizes.x, nullptr), "als_integrator_combine");
+            }
         }
         check_cuda(cudaDeviceSynchronize());
         stage.get(0, output);

@@ -860,8 +860,8 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
     const int nvar = cfg->dim + 2;
     const long plane = orc_plane_size(cfg);
     const size_t bytes = sizeof(double) * (size_t)nvar * (size_t)plane;
-    const int substeps = cfg->integrator == ORC_INT_FE ? 1 : (cfg->integrator == ORC_INT_RK2 ? 2 : 3);
-    double* vol[4];
+    const int substeps = cfg->integrator + 1;
+    double* vol[5];
     double* diff_state = NULL;
     double t = 0;
     long steps = 0, i;
@@ -910,6 +910,27 @@ int orc_simulate(const orc_config* cfg, double cfl, double end_time, long max_st
             }
             c = dt / cfg->dx[0];
             /* the Volume operations run over every cell; ghosts are refilled below */
+            if (cfg->integrator == ORC_INT_RK4) {
+                /* RungeKutta4.cpp:66-87; the last stage is
+                 * addLinearCombination (HostMemory.cpp:261-280) */
+                const double a1 = (1.0 / 6.0) * c;
+                for (i = 0; i < nvar * plane; ++i) {
+                    double v = out[i];
+                    if (s < 3) {
+                        v *= c;
+                        if (s < 2) {
+                            v *= 0.5;
+                        }
+                        v += U0[i];
+                    } else {
+                        v = a1 * v + 1.0 / 3.0 * vol[1][i] + 2.0 / 3.0 * vol[2][i] +
+                            1.0 / 3.0 * vol[3][i] + -1.0 / 3.0 * U0[i];
+                    }
+                    out[i] = v;
+                }
+                orc_fill_ghosts(cfg, out, nvar);
+                continue;
+            }
             for (i = 0; i < nvar * plane; ++i) {
                 double v = out[i];
                 v *= c;

@@ -26,7 +26,7 @@ enum { ORC_FLUX_HLL = 0, ORC_FLUX_HLL3 = 1, ORC_FLUX_CENTRAL = 2, ORC_FLUX_TECNO
 enum { ORC_RECON_NONE = 0, ORC_RECON_WENO2 = 1, ORC_RECON_ENO2 = 2,
        ORC_RECON_ENO3 = 3, ORC_RECON_ENO4 = 4, ORC_RECON_MC = 5, ORC_RECON_MM = 6,
        ORC_RECON_WENOF2 = 7, ORC_RECON_WENO3 = 8 };
-enum { ORC_INT_FE = 0, ORC_INT_RK2 = 1, ORC_INT_RK3 = 2 };
+enum { ORC_INT_FE = 0, ORC_INT_RK2 = 1, ORC_INT_RK3 = 2, ORC_INT_RK4 = 3 };
 enum { ORC_BC_NEUMANN = 0, ORC_BC_PERIODIC = 1 };
 
 typedef struct {

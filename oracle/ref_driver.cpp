@@ -38,6 +38,7 @@
 #include "alsfvm/integrator/ForwardEuler.hpp"
 #include "alsfvm/integrator/RungeKutta2.hpp"
 #include "alsfvm/integrator/RungeKutta3.hpp"
+#include "alsfvm/integrator/RungeKutta4.hpp"
 #include "alsfvm/integrator/TimestepAdjuster.hpp"
 #include "alsfvm/simulator/ConservedSystem.hpp"
 #include "alsfvm/simulator/SimulatorParameters.hpp"
@@ -273,6 +274,8 @@ Objects build(const Setup& s) {
         o.integ = std::make_shared<integrator::RungeKutta2>(o.system);
     } else if (s.integrator == "rungekutta3") {
         o.integ = std::make_shared<integrator::RungeKutta3>(o.system);
+    } else if (s.integrator == "rungekutta4") {
+        o.integ = std::make_shared<integrator::RungeKutta4>(o.system);
     } else {
         THROW("unknown integrator " << s.integrator);
     }
@@ -287,8 +290,9 @@ Objects build(const Setup& s) {
         // the boundary and the integrator as B200 adapters too
         o.boundary = std::make_shared<b200::BoundaryB200>(
             t == boundary::Type::NEUMANN ? ALS_BC_NEUMANN : ALS_BC_PERIODIC, int(o.ghosts));
-        static const char* const integs[] = {"forwardeuler", "rungekutta2", "rungekutta3"};
-        o.integ = std::make_shared<b200::IntegratorB200>(b200_code(s.integrator, integs, 3),
+        static const char* const integs[] = {"forwardeuler", "rungekutta2", "rungekutta3",
+            "rungekutta4"};
+        o.integ = std::make_shared<b200::IntegratorB200>(b200_code(s.integrator, integs, 4),
             o.system);
     }
 #endif

@@ -202,6 +202,30 @@ def write_diffusion_fixtures(ref):
         print(name)
 
 
+# RungeKutta4 (the plug-in integrator path), prefixed "rk4_"
+RK4_SIMULATIONS = {
+    "rk4_sod256_weno2_hll3": (1, (256,), (-1.0,), (1.0,), "hll3", "weno2", "rungekutta4",
+                              "neumann", 0.45, 0.2, "sod"),
+    "rk4_kh32_eno2_hll": (2, (32, 32), (0.0, 0.0), (1.0, 1.0), "hll", "eno2", "rungekutta4",
+                          "periodic", 0.4, 0.1, "kh"),
+    "rk4_rand3d_9x8x10_weno2_hll3": (3, (9, 8, 10), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3",
+                                     "weno2", "rungekutta4", "periodic", 0.4, 0.03, "seed:51"),
+}
+
+
+def write_rk4_fixtures(ref):
+    for name, (dim, n, lo, hi, flux, recon, integ, bc, cfl, T, kind) in RK4_SIMULATIONS.items():
+        g = ghost_cells(recon, flux)
+        U0 = initial_state(kind, dim, n, g)
+        rc, U, dts, steps, t = ref.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, cfl, T, U0)
+        assert rc == 0, name
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), initial=U0, final=U, dts=dts,
+                            steps=steps, t=t, dim=dim, n=np.array(n), lower=np.array(lo),
+                            upper=np.array(hi), flux=flux, recon=recon, integrator=integ, bc=bc,
+                            cfl=cfl, end_time=T, gamma=1.4)
+        print(name, "steps=%d t=%r" % (steps, t))
+
+
 def main():
     ref = RefOracle()
     out = {}
@@ -239,6 +263,7 @@ def main():
     write_limiter_cases(ref)
     write_tecno_fixtures(ref)
     write_diffusion_fixtures(ref)
+    write_rk4_fixtures(ref)
     with open(os.path.join(HERE, "compute_flux_cases.txt"), "w") as f:
         f.write("# dim n recon flux bc seed sha256(ghost-filled input) sha256(net flux) "
                 "sha256(wave speeds) max_wave_speed\n")

@@ -23,7 +23,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 FLUX = {"hll": 0, "hll3": 1, "central": 2, "tecno1": 3, "tecno4": 4, "tecno6": 5}
 RECON = {"none": 0, "weno2": 1, "eno2": 2, "eno3": 3, "eno4": 4, "mc": 5, "mm": 6,
          "wenof2": 7, "weno3": 8}
-INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2}
+INTEGRATOR = {"forwardeuler": 0, "rungekutta2": 1, "rungekutta3": 2, "rungekutta4": 3}
 DIFFUSION = {"tecnoroe": 0, "tecnorusanov": 1}
 DIFFUSION_RECON = {"none": 0, "eno2": 2, "eno3": 3, "eno4": 4}
 BC = {"neumann": 0, "periodic": 1}

@@ -18,6 +18,7 @@ import torch
 import alsvinn_b200 as als
 from conftest import GOLDEN, load_golden
 from oracle_lib import smooth_random_state
+from plugin_loop import run_plugin_time_loop
 
 pytestmark = pytest.mark.gpu
 
@@ -68,43 +69,12 @@ def test_diffusion_operator_reproduces_reference_calls(name):
             np.testing.assert_allclose(out.cpu().numpy(), z["result"][k], rtol=RTOL, atol=ATOL)
 
 
-def _run_plugin_time_loop(z):
-    """The reference's time loop (Simulator::incrementSolution) driven with
-    the plug-in classes: NumericalFlux + DiffusionOperator as the system,
-    Integrator for the stages, Boundary after each stage."""
-    dim = int(z["dim"])
-    n = tuple(int(v) for v in z["n"])
-    flux, recon = str(z["flux"]), str(z["recon"])
-    g = max(als.ghost_cells(flux, recon), als.diffusion_ghost_cells(str(z["diffusion_recon"])))
-    lengths = [(float(z["upper"][d]) - float(z["lower"][d])) / n[d] for d in range(dim)]
-    lengths += [0.0] * (3 - dim)
-    bc = als.Boundary(dim, n, g, str(z["bc"]))
-    nf = als.NumericalFlux(dim, n, flux, recon, ghosts=g)
-    with als.DiffusionOperator(dim, n, str(z["diffusion"]), str(z["diffusion_recon"]),
-                               ghosts=g) as op:
-        integ = als.Integrator(str(z["integrator"]), nf, float(z["cfl"]), diffusion=op)
-        substeps = integ.getNumberOfSubsteps()
-        vols = [_dev(z["initial"]) for _ in range(substeps + 1)]
-        bc.applyBoundaryConditions(vols[0])
-        t, steps, T = 0.0, 0, float(z["end_time"])
-        while t < T:
-            dt = 0.0
-            for s in range(substeps):
-                dt = integ.performSubstep(vols, lengths, dt, vols[s + 1], s, t, T)
-                bc.applyBoundaryConditions(vols[s + 1])
-            vols[0], vols[substeps] = vols[substeps], vols[0]
-            t += dt
-            steps += 1
-        torch.cuda.synchronize()
-        return vols[0].cpu().numpy(), steps, t
-
-
 @pytest.mark.parametrize("name", _fixtures("tecnodiff_"))
 def test_plugin_time_loop_with_diffusion_reproduces_reference(name):
     """Whole simulations with flux + TeCNO diffusion through the plug-in
     classes against the reference's own time loop (relative 1e-10)."""
     z = load_golden(name)
-    U, steps, t = _run_plugin_time_loop(z)
+    U, steps, t = run_plugin_time_loop(z, str(z["diffusion"]), str(z["diffusion_recon"]))
     assert steps == int(z["steps"])
     assert abs(t - float(z["t"])) <= 1e-15
     np.testing.assert_allclose(U, z["final"], rtol=RTOL, atol=ATOL)

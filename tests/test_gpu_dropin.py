@@ -120,3 +120,25 @@ def test_reference_time_loop_with_b200_diffusion(ref_b200, dim, n, flux, dkind, 
     assert abs(a[4] - b[4]) <= 1e-15
     np.testing.assert_allclose(a[2], b[2], rtol=1e-10)
     np.testing.assert_allclose(a[1], b[1], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("dim,n,recon,flux,bc", [(1, (32,), "weno2", "hll3", "periodic"),
+                                                 (2, (14, 12), "eno2", "hll", "neumann"),
+                                                 (3, (8, 9, 8), "weno2", "hll3", "periodic")])
+def test_reference_time_loop_with_b200_rk4(ref_b200, dim, n, recon, flux, bc):
+    """RungeKutta4 in the reference's own loop with IntegratorB200 (and the
+    other B200 classes) against the reference's RungeKutta4, bit for bit."""
+    g = ghost_cells(recon, flux)
+    seed = zlib.crc32(("dropin-rk4-%d-%s-%s" % (dim, recon, flux)).encode()) % 100000
+    st = smooth_random_state(seed, dim, n, g)
+    lo, hi = [0.0] * dim, [1.0] * dim
+    out = {}
+    for p in ("cpu", "b200-all"):
+        ref_b200.set_flux_platform(p)
+        out[p] = ref_b200.simulate(dim, n, lo, hi, flux, recon, "rungekutta4", bc, 1.4, 0.4, 0.03,
+                                   st)
+    ref_b200.set_flux_platform("cpu")
+    a, b = out["cpu"], out["b200-all"]
+    assert a[0] == b[0] and a[3] == b[3] >= 1 and a[4] == b[4]
+    np.testing.assert_array_equal(a[2], b[2])
+    np.testing.assert_array_equal(a[1], b[1])

@@ -74,7 +74,7 @@ def test_c_oracle_matches_reference_build(c_oracle, ref_oracle, dim, n, recon):
         for bc in ("neumann", "periodic"):
             st = smooth_random_state(seed, dim, n, g)
             lo, hi = [0.0] * dim, [1.0] * dim
-            for integ in ("forwardeuler", "rungekutta2", "rungekutta3"):
+            for integ in ("forwardeuler", "rungekutta2", "rungekutta3", "rungekutta4"):
                 cfg = c_oracle.config(dim, n, lo, hi, flux, recon, integ, bc, 1.4)
                 r = ref_oracle.simulate(dim, n, lo, hi, flux, recon, integ, bc, 1.4, 0.4, 0.03, st)
                 c = c_oracle.simulate(cfg, st, 0.4, 0.03)
@@ -377,3 +377,22 @@ def test_c_oracle_diffusion_matches_reference_build(c_oracle, ref_oracle, dim, n
     for k in range(3):
         np.testing.assert_array_equal(
             c_oracle.apply_diffusion(cfg, kind, recon, st, states[k], outs[k]), ref[k])
+
+
+RK4_FIXTURES = sorted(f[:-4] for f in os.listdir(GOLDEN)
+                      if f.startswith("rk4_") and f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", RK4_FIXTURES)
+def test_c_oracle_reproduces_reference_rk4_simulation(c_oracle, name):
+    """RungeKutta4 time loops made by the reference build (RungeKutta4.cpp),
+    reproduced bit for bit."""
+    z = load_golden(name)
+    dim = int(z["dim"])
+    cfg = c_oracle.config(dim, z["n"], z["lower"], z["upper"], str(z["flux"]), str(z["recon"]),
+                          str(z["integrator"]), str(z["bc"]), float(z["gamma"]))
+    rc, U, dts, steps, t = c_oracle.simulate(cfg, z["initial"], float(z["cfl"]),
+                                             float(z["end_time"]))
+    assert rc == 0 and steps == z["steps"] and t == z["t"]
+    np.testing.assert_array_equal(dts, z["dts"])
+    np.testing.assert_array_equal(U, z["final"])
