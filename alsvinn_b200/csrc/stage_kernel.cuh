@@ -352,7 +352,10 @@ __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, con
             acc[k][v] = acc[k][v] + (tr + (-tl));
         }
     }
-    __syncthreads();
+    // No barrier here: the next direction's reconstruction writes only `rec`,
+    // which this phase does not read, and its face phase (which overwrites
+    // `flx`) starts after the barrier that ends that reconstruction, which
+    // every thread reaches only after finishing this loop.
 }
 
 // Advances the time bookkeeping of a member once its last tile of the last

@@ -610,14 +610,16 @@ def main():
     # from pinned memory, advance the same number of steps, download it
     pinned_in = torch.from_numpy(state).pin_memory()
     pinned_out = torch.empty_like(pinned_in).pin_memory()
+    # the warm-up runs the same three calls once (first calls set up staging)
+    out = pinned_out.numpy()
     sim.set_state(pinned_in.numpy())
     sim.advance(args.warmup)
+    sim._lib.als_solver_get_state(sim._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0, 1)
     sim.synchronize()
     e2e_steps = args.steps
     t0 = time.perf_counter()
     sim.set_state(pinned_in.numpy())
     sim.advance(e2e_steps)
-    out = pinned_out.numpy()
     sim._lib.als_solver_get_state(sim._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0, 1)
     e2e_secs = time.perf_counter() - t0
     tt = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
