@@ -15,6 +15,13 @@ _PP = ctypes.POINTER(ctypes.c_void_p)   # array of plane pointers
 _LL = ctypes.POINTER(ctypes.c_longlong)
 
 
+class FunctionalParams(ctypes.Structure):
+    _fields_ = [("degree", ctypes.c_int), ("degree_k", ctypes.c_int), ("degree_n", ctypes.c_int),
+                ("degree_m", ctypes.c_int), ("min_value", ctypes.c_double),
+                ("max_value", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3)]
+
+
 class Grid(ctypes.Structure):
     _fields_ = [("dimension", ctypes.c_int), ("n", ctypes.c_int * 3), ("ghosts", ctypes.c_int),
                 ("gamma", ctypes.c_double)]
@@ -107,6 +114,11 @@ PROTOTYPES = {
     "als_write_netcdf": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _I, ctypes.c_int, _PP,
                                         _PP, ctypes.c_double, ctypes.c_int, _PP, _PP]),
     "als_solver_write_netcdf": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "als_functional_size": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, _LL]),
+    "als_functional": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int,
+                                      ctypes.POINTER(FunctionalParams), _VP, ctypes.c_int,
+                                      ctypes.c_longlong, ctypes.c_int, _VP, ctypes.c_longlong,
+                                      ctypes.c_double, _VP]),
     "als_diffusion_ghost_cells": (ctypes.c_int, [ctypes.c_int]),
     "als_diffusion_create": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _PP]),
     "als_diffusion_apply": (ctypes.c_int, [_VP, _PP, _PP, _VP]),

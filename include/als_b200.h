@@ -308,6 +308,40 @@ int als_structure_functions(const als_grid* grid, int boundary, int kind, int di
     double p, const void* states, int precision, long long member_stride, int members,
     double* out, void* stream);
 
+/* ------------------------------------------------------- functionals
+ * Functional::operator()(out, U, weight, grid) (alsfvm/src/functional/,
+ * Functional.hpp:41-60): out += weight * f(U), batched over `members`
+ * states (`states` + m * member_stride elements, nvar padded planes of
+ * `precision` each; ghosts as `grid`).  Results are FP64, per member
+ * nvar blocks of als_functional_size elements (out + m * out_member_stride):
+ *   IDENTITY            interior cells, x fastest        (Identity.cpp:25-48)
+ *   MOMENT              padded cells, U^degree          (Moment.cpp:27-37)
+ *   LOG_ENTROPY         1 value, in the energy block     (LogEntropy.cpp:30-80)
+ *   LEGENDRE            1 value per variable, 2-D        (Legendre.cpp:36-98)
+ *   LEGENDRE_POINTWISE  interior cells, 2-D              (LegendrePointWise.cpp:32-87)
+ *   BV                  1 value per variable, 1-D/2-D    (BoundedVariation.cpp:24-52)
+ * Cell midpoints and volumes follow Grid.cpp:24-41 (a direction with one
+ * cell has length 1).  Sums over cells are reduced in a fixed order
+ * (deterministic; equal to the reference's sequential sums to rounding).
+ * Stream-ordered. */
+#define ALS_FUNCTIONAL_IDENTITY 0            /* "identity" */
+#define ALS_FUNCTIONAL_MOMENT 1              /* "moment" */
+#define ALS_FUNCTIONAL_LOG_ENTROPY 2         /* "log_entropy" */
+#define ALS_FUNCTIONAL_LEGENDRE 3            /* "legendre" */
+#define ALS_FUNCTIONAL_LEGENDRE_POINTWISE 4  /* "legendre_pointwise" */
+#define ALS_FUNCTIONAL_BV 5                  /* "bv" */
+typedef struct {
+    int degree;                        /* moment, legendre_pointwise, bv (the power p) */
+    int degree_k, degree_n, degree_m;  /* legendre: x, y and value degrees */
+    double min_value, max_value;       /* legendre*: value scaled to (u - min)/(max - min) */
+    double gamma;                      /* log_entropy */
+    double lower[3], upper[3];         /* domain corners (Grid origin and top) */
+} als_functional_params;
+int als_functional_size(const als_grid* grid, int kind, long long* elements_per_variable);
+int als_functional(const als_grid* grid, int kind, const als_functional_params* params,
+    const void* states, int precision, long long member_stride, int members, double* out,
+    long long out_member_stride, double weight, void* stream);
+
 /* ------------------------------------------------------- TeCNO diffusion
  * DiffusionOperator for the Euler equations: TecnoDiffusionCPU with the Roe
  * or Rusanov diffusion matrix over a TeCNO reconstruction of the scaled

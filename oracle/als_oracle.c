@@ -1477,3 +1477,141 @@ int orc_set_diffusion(orc_config* cfg, int kind, int recon) {
     }
     return 0;
 }
+
+/* ------------------------------------------------------------ functionals */
+
+/* boost::math::legendre_p's recurrence (Bonnet):
+ * P_{l+1} = ((2l+1) x P_l - l P_{l-1}) / (l+1), from P_0 = 1, P_1 = x. */
+static double legendre_p(int l, double x) {
+    double p0 = 1, p1 = x;
+    int m;
+    if (l == 0) {
+        return p0;
+    }
+    for (m = 1; m < l; ++m) {
+        const double next = ((2 * m + 1) * x * p1 - m * p0) / (m + 1);
+        p0 = p1;
+        p1 = next;
+    }
+    return p1;
+}
+
+long orc_functional_size(int dim, const int* n, int g, int kind) {
+    long cells = 1, plane = 1;
+    int d;
+    for (d = 0; d < 3; ++d) {
+        const int nd = d < dim ? n[d] : 1;
+        cells *= nd;
+        plane *= nd + (d < dim ? 2 * g : 0);
+    }
+    return kind == ORC_FUNCTIONAL_IDENTITY || kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE ? cells
+        : (kind == ORC_FUNCTIONAL_MOMENT ? plane : 1);
+}
+
+int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_params* p,
+    const double* planes, double* out, double weight) {
+    int N[3], nn[3], d, i, j, k, v;
+    long plane = 1;
+    double len[3], sides[3], dV;
+    const int nvar = dim + 2;
+    long per_var;
+    for (d = 0; d < 3; ++d) {
+        nn[d] = d < dim ? n[d] : 1;
+        N[d] = nn[d] + (d < dim ? 2 * g : 0);
+        plane *= N[d];
+        sides[d] = p->upper[d] - p->lower[d];
+        /* Grid.cpp:24-41 */
+        len[d] = (p->upper[d] - p->lower[d]) / (double)nn[d];
+        if (d > 0 && nn[d] == 1) {
+            len[d] = 1;
+        }
+    }
+    dV = len[0] * len[1] * len[2];
+    per_var = orc_functional_size(dim, n, g, kind);
+    if ((kind == ORC_FUNCTIONAL_LEGENDRE || kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE) && dim != 2) {
+        return -1;
+    }
+    if (kind == ORC_FUNCTIONAL_BV && dim > 2) {
+        return -1;
+    }
+    if (kind == ORC_FUNCTIONAL_MOMENT) {
+        /* HostMemory.cpp:293-301 over every cell */
+        long c;
+        for (v = 0; v < nvar; ++v) {
+            for (c = 0; c < plane; ++c) {
+                out[v * per_var + c] += weight * pow(planes[v * plane + c], (double)p->degree);
+            }
+        }
+        return 0;
+    }
+    if (kind == ORC_FUNCTIONAL_LOG_ENTROPY) {
+        /* LogEntropy.cpp:30-80, midpoint loop volume_foreach.hpp:441-480 */
+        double integral = 0.0;
+        for (k = 0; k < nn[2]; ++k) {
+            for (j = 0; j < nn[1]; ++j) {
+                for (i = 0; i < nn[0]; ++i) {
+                    const long idx = idx3(N, i + g, dim > 1 ? j + g : 0, dim > 2 ? k + g : 0);
+                    const double rho = planes[idx];
+                    const double E = planes[(nvar - 1) * plane + idx];
+                    double msq = 0.0, pressure, s, ent;
+                    int c;
+                    for (c = 0; c < dim; ++c) {
+                        const double m = planes[(1 + c) * plane + idx];
+                        msq += m * m;
+                    }
+                    pressure = (p->gamma - 1) * (E - 1.0 / (2 * rho) * msq);
+                    s = log(pressure) - p->gamma * log(rho);
+                    ent = (-rho * s) / (p->gamma - 1);
+                    integral += ent * dV;
+                }
+            }
+        }
+        out[(nvar - 1) * per_var] += weight * integral;
+        return 0;
+    }
+    for (v = 0; v < nvar; ++v) {
+        double integral = 0.0;
+        for (k = 0; k < nn[2]; ++k) {
+            for (j = 0; j < nn[1]; ++j) {
+                for (i = 0; i < nn[0]; ++i) {
+                    const long idx = idx3(N, i + g, dim > 1 ? j + g : 0, dim > 2 ? k + g : 0);
+                    const long c = ((long)k * nn[1] + j) * nn[0] + i;
+                    const double u = planes[v * plane + idx];
+                    if (kind == ORC_FUNCTIONAL_IDENTITY) {
+                        /* Identity.cpp:25-48 */
+                        out[v * per_var + c] += weight * u;
+                    } else if (kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE) {
+                        /* LegendrePointWise.cpp:58-76 */
+                        const double value = (u - p->min_value) / (p->max_value - p->min_value);
+                        out[v * per_var + c] += legendre_p(p->degree, value) * weight;
+                    } else if (kind == ORC_FUNCTIONAL_LEGENDRE) {
+                        /* Legendre.cpp:62-90, midpoints Grid.cpp:148-171 */
+                        const double x = (p->lower[0] + len[0] * i) + len[0] / 2.0;
+                        const double y = (p->lower[1] + len[1] * j) + len[1] / 2.0;
+                        const double xs = 2 * (x - p->lower[0]) / sides[0] - 1;
+                        const double ys = 2 * (y - p->lower[1]) / sides[1] - 1;
+                        const double value = (u - p->min_value) / (p->max_value - p->min_value);
+                        integral += legendre_p(p->degree_k, xs) * legendre_p(p->degree_n, ys) *
+                            legendre_p(p->degree_m, value) * dV;
+                    } else {
+                        /* HostMemory::getTotalVariation (HostMemory.cpp:325-362):
+                         * cells after the first along x and, in 2-D, y */
+                        double dy = 0, dx;
+                        if (i == 0 || (dim > 1 && j == 0)) {
+                            continue;
+                        }
+                        if (dim > 1) {
+                            dy = u - planes[v * plane + idx - N[0]];
+                        }
+                        dx = u - planes[v * plane + idx - 1];
+                        integral += pow(sqrt(dy * dy + dx * dx), (double)p->degree);
+                    }
+                }
+            }
+        }
+        if (kind == ORC_FUNCTIONAL_LEGENDRE || kind == ORC_FUNCTIONAL_BV) {
+            out[v * per_var] += weight * integral;
+        }
+    }
+    return 0;
+}

@@ -90,6 +90,20 @@ void orc_structure_basic(int dim, const int* n, int g, int bc, int nvar, int dir
  * over all cells; returns 1 when every cell obeys. */
 int orc_obeys_constraints(const orc_config* cfg, const double* planes);
 
+/* Functionals (alsfvm/src/functional/): out += weight * f(U) for one state,
+ * sums in the reference's sequential order.  Output per variable:
+ * orc_functional_size elements (interior cells, padded cells or 1). */
+enum { ORC_FUNCTIONAL_IDENTITY = 0, ORC_FUNCTIONAL_MOMENT = 1, ORC_FUNCTIONAL_LOG_ENTROPY = 2,
+       ORC_FUNCTIONAL_LEGENDRE = 3, ORC_FUNCTIONAL_LEGENDRE_POINTWISE = 4, ORC_FUNCTIONAL_BV = 5 };
+typedef struct {
+    int degree, degree_k, degree_n, degree_m;
+    double min_value, max_value, gamma;
+    double lower[3], upper[3];
+} orc_functional_params;
+long orc_functional_size(int dim, const int* n, int g, int kind);
+int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_params* p,
+    const double* planes, double* out, double weight);
+
 /* TeCNO diffusion, TecnoDiffusionCPU::applyDiffusion (TecnoDiffusionCPU.cpp:
  * 23-170): kind 0 tecnoroe (RoeMatrix), 1 tecnorusanov (RusanovMatrix);
  * recon 0 none, 2/3/4 ENO of that order (reconstruction/tecno/).  Adds the

@@ -1,0 +1,147 @@
+"""The functionals of alsfvm/src/functional/ in the oracle (CPU).
+
+The reference's functional sources need Boost (property trees for their
+parameters, boost::math::legendre_p), which this image lacks, so the
+restatement is pinned to the reference's own unit tests for these classes
+(test/library_tests/src/fvm/functional/EntropyTest.cpp, LegendreTest.cpp),
+ported here with their inputs and tolerances, to SciPy's Legendre
+polynomials, and to direct NumPy evaluations of the stated formulas.
+"""
+import numpy as np
+import pytest
+import scipy.special
+
+from oracle_lib import padded_shape, smooth_random_state
+
+GAMMA = 1.4
+
+
+def _midpoints(n, lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0)):
+    """Cell midpoints origin + dx*i + dx/2 (Grid.cpp:148-171)."""
+    return [lower[d] + (upper[d] - lower[d]) / n[d] * np.arange(n[d]) +
+            (upper[d] - lower[d]) / n[d] / 2.0 for d in range(len(n))]
+
+
+def _euler2_state(n, g, E_of):
+    """fill_volume with rho = e, m_x = m_y = sin(2 pi x y) at the midpoints."""
+    shp = padded_shape(2, n, g)
+    U = np.zeros(shp)
+    x, y = _midpoints(n)
+    X, Y = np.meshgrid(x, y)
+    rho = np.full_like(X, np.exp(1.0))
+    m = np.sin(2 * np.pi * X * Y)
+    U[0, 0, g:-g, g:-g] = rho
+    U[1, 0, g:-g, g:-g] = m
+    U[2, 0, g:-g, g:-g] = m
+    U[3, 0, g:-g, g:-g] = E_of(rho, m)
+    return U
+
+
+def test_log_entropy_result_is_zero(c_oracle):
+    """EntropyTest.ResultIsZeroTest: p = e^1.4, rho = e, so s = 0."""
+    n, g = (3, 2), 2
+    U = _euler2_state(n, g, lambda rho, m: np.exp(1.4) / 0.4 + .5 * (2 * m * m) / rho)
+    out = c_oracle.functional(2, n, g, "log_entropy", U, weight=0.5, gamma=GAMMA)
+    assert abs(out[3, 0]) < 1e-8
+
+
+def test_log_entropy_result_is_one(c_oracle):
+    """EntropyTest.ResultIsOneTest: s = 0.4/e, so -rho s/(gamma-1) = -1 on
+    the unit square; weight -1 gives 1."""
+    n, g = (2, 2), 2
+    U = _euler2_state(n, g, lambda rho, m: np.exp(1.4 + 0.4 / np.exp(1)) / 0.4 +
+                      .5 * (2 * m * m) / rho)
+    out = c_oracle.functional(2, n, g, "log_entropy", U, weight=-1.0, gamma=GAMMA)
+    assert abs(out[3, 0] - 1.0) < 1e-8
+    assert np.all(out[:3] == 0)
+
+
+def test_legendre_constant(c_oracle):
+    """LegendreTest.ConstantTest: degrees 0, weight 0.5 -> 0.5 per variable
+    (ASSERT_DOUBLE_EQ: within 4 ulps)."""
+    n, g = (3, 2), 2
+    U = _euler2_state(n, g, lambda rho, m: np.sin(2 * np.pi * m))
+    out = c_oracle.functional(2, n, g, "legendre", U, weight=0.5, degree_k=0, degree_n=0,
+                              degree_m=0, min_value=-1, max_value=1)
+    assert np.all(np.abs(out[:, 0] - 0.5) <= 4 * np.spacing(0.5))
+
+
+@pytest.mark.parametrize("degree", range(12))
+def test_legendre_polynomials_against_scipy(c_oracle, degree):
+    """P_degree(u) through legendre_pointwise (min 0, max 1: the value is u)
+    against scipy.special.eval_legendre on [-1, 1]."""
+    n, g = (21, 5), 1
+    u = np.linspace(-1, 1, 21)
+    U = np.zeros(padded_shape(2, n, g))
+    U[:, 0, g:-g, g:-g] = u[None, None, :]
+    out = c_oracle.functional(2, n, g, "legendre_pointwise", U, degree=degree, min_value=0.0,
+                              max_value=1.0)
+    ref = scipy.special.eval_legendre(degree, u)
+    np.testing.assert_allclose(out[0].reshape(5, 21), np.broadcast_to(ref, (5, 21)), rtol=0,
+                               atol=1e-14)
+
+
+def test_legendre_integral_formula(c_oracle):
+    """legendre: sum over cells of P_k(x') P_n(y') P_m(u') dV with x', y' the
+    midpoints scaled to [-1, 1] and u' = (u - min)/(max - min)."""
+    n, g = (9, 7), 2
+    st = smooth_random_state(21, 2, n, g)
+    out = c_oracle.functional(2, n, g, "legendre", st, weight=1.5, degree_k=2, degree_n=3,
+                              degree_m=1, min_value=0.5, max_value=1.5)
+    x, y = _midpoints(n)
+    X, Y = np.meshgrid(2 * x - 1, 2 * y - 1)
+    for v in range(4):
+        val = (st[v, 0, g:-g, g:-g] - 0.5) / 1.0
+        ref = np.sum(scipy.special.eval_legendre(2, X) * scipy.special.eval_legendre(3, Y) *
+                     val) * (1 / 9) * (1 / 7)
+        assert abs(out[v, 0] - 1.5 * ref) < 1e-13
+
+
+@pytest.mark.parametrize("dim,n", [(1, (17,)), (2, (9, 8)), (3, (5, 6, 4))])
+def test_identity_and_moment(c_oracle, dim, n):
+    g = 2
+    st = smooth_random_state(31 + dim, dim, n, g)
+    ident = c_oracle.functional(dim, n, g, "identity", st, weight=0.25)
+    sl = tuple([slice(None)] + [slice(g, -g) if 3 - a <= dim else slice(None) for a in range(3)])
+    np.testing.assert_array_equal(ident, 0.25 * st[sl].reshape(dim + 2, -1))
+    mom = c_oracle.functional(dim, n, g, "moment", st, weight=2.0, degree=3)
+    np.testing.assert_allclose(mom, 2.0 * st.reshape(dim + 2, -1) ** 3, rtol=1e-15)
+
+
+@pytest.mark.parametrize("dim,n", [(1, (17,)), (2, (9, 8))])
+@pytest.mark.parametrize("p", [1, 2])
+def test_bounded_variation(c_oracle, dim, n, p):
+    """sum over interior cells after the first along x (and y) of
+    |(u - u_below, u - u_left)|^p (HostMemory::getTotalVariation)."""
+    g = 2
+    st = smooth_random_state(41 + dim, dim, n, g)
+    out = c_oracle.functional(dim, n, g, "bv", st, weight=1.0, degree=p)
+    for v in range(dim + 2):
+        if dim == 1:
+            u = st[v, 0, 0, g:-g]
+            ref = np.sum(np.abs(np.diff(u)) ** p)
+        else:
+            u = st[v, 0, g:-g, g:-g]
+            dx = u[1:, 1:] - u[1:, :-1]
+            dy = u[1:, 1:] - u[:-1, 1:]
+            ref = np.sum(np.sqrt(dx * dx + dy * dy) ** p)
+        assert abs(out[v, 0] - ref) < 1e-12 * max(1.0, abs(ref))
+
+
+def test_log_entropy_formula_3d(c_oracle):
+    n, g = (6, 5, 4), 2
+    st = smooth_random_state(51, 3, n, g)
+    out = c_oracle.functional(3, n, g, "log_entropy", st, weight=1.0, gamma=GAMMA,
+                              upper=(2.0, 1.0, 0.5))
+    U = st[:, g:-g, g:-g, g:-g]
+    msq = U[1] ** 2 + U[2] ** 2 + U[3] ** 2
+    p = (GAMMA - 1) * (U[4] - msq / (2 * U[0]))
+    s = np.log(p) - GAMMA * np.log(U[0])
+    ref = np.sum(-U[0] * s / (GAMMA - 1)) * (2.0 / 6) * (1.0 / 5) * (0.5 / 4)
+    assert abs(out[4, 0] - ref) < 1e-12 * abs(ref)
+
+
+def test_legendre_needs_two_dimensions(c_oracle):
+    st = smooth_random_state(1, 1, (8,), 1)
+    with pytest.raises(ValueError):
+        c_oracle.functional(1, (8,), 1, "legendre", st)

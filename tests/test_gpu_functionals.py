@@ -1,0 +1,78 @@
+"""The functionals (als_functional) on the GPU against the oracle.
+
+Pointwise functionals (identity, legendre_pointwise) evaluate the same
+operations in the same order and match exactly; moment calls pow, and the
+sums (log_entropy, legendre, bv) are reduced in a different (fixed) order
+than the reference's sequential loop and log_entropy calls log, so those
+match to a relative 1e-12 (moment: 1e-14).  FP32 members are converted to
+FP64 on load, so the oracle runs on the same values widened.
+"""
+import numpy as np
+import pytest
+import torch
+
+from alsvinn_b200 import functionals as fn
+from oracle_lib import smooth_random_state
+
+pytestmark = pytest.mark.gpu
+
+CASES = []
+for _dim, _n in ((1, (37,)), (2, (23, 19)), (3, (9, 8, 7))):
+    for _kind in ("identity", "moment", "log_entropy", "legendre", "legendre_pointwise", "bv"):
+        if _kind.startswith("legendre") and _dim != 2:
+            continue
+        if _kind == "bv" and _dim > 2:
+            continue
+        CASES.append((_dim, _n, _kind))
+
+PARAMS = dict(degree=2, degree_k=1, degree_n=2, degree_m=3, min_value=0.8, max_value=1.2,
+              gamma=1.4, lower=(0.0, -1.0, 0.0), upper=(2.0, 1.0, 1.0))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("dim,n,kind", CASES, ids=["d%d-%s" % (c[0], c[2]) for c in CASES])
+def test_functional_matches_oracle(c_oracle, dim, n, kind, precision):
+    g = 2
+    members = 3
+    states = np.stack([smooth_random_state(500 + 7 * k + dim, dim, n, g) for k in range(members)])
+    dtype = torch.float64 if precision == "fp64" else torch.float32
+    x = torch.from_numpy(states).to(dtype).cuda().contiguous()
+    widened = x.double().cpu().numpy()
+    start = torch.rand((members, dim + 2, fn.functional_size(dim, n, g, kind)),
+                       dtype=torch.float64, device="cuda")
+    out = fn.functional(x, dim, n, g, kind, weight=0.75, out=start.clone(), **PARAMS)
+    got = out.cpu().numpy()
+    for m in range(members):
+        ref = c_oracle.functional(dim, n, g, kind, widened[m], weight=0.75,
+                                  out=start[m].cpu().numpy(), **PARAMS)
+        if kind in ("identity", "legendre_pointwise"):
+            np.testing.assert_array_equal(got[m], ref)
+        else:
+            rtol = 1e-14 if kind == "moment" else 1e-12
+            np.testing.assert_allclose(got[m], ref, rtol=rtol, atol=1e-14)
+
+
+def test_functional_reductions_are_deterministic():
+    """The fixed-order sums give the same bits on every call."""
+    st = np.stack([smooth_random_state(9 + k, 2, (300, 257), 2) for k in range(4)])
+    x = torch.from_numpy(st).cuda()
+    a = fn.functional(x, 2, (300, 257), 2, "log_entropy", gamma=1.4).cpu().numpy()
+    for _ in range(3):
+        b = fn.functional(x, 2, (300, 257), 2, "log_entropy", gamma=1.4).cpu().numpy()
+        np.testing.assert_array_equal(a, b)
+
+
+def test_time_integrated_functional(c_oracle):
+    """TimeIntegrationFunctional: writes within the radius add dt * f."""
+    dim, n, g = 2, (16, 12), 2
+    tif = fn.TimeIntegratedFunctional(dim, n, g, "bv", time=0.5, radius=0.25, degree=1)
+    ref = np.zeros((1, 4, 1))
+    last = 0.0
+    for k, t in enumerate([0.1, 0.3, 0.45, 0.6, 0.8, 0.9]):
+        st = smooth_random_state(60 + k, dim, n, g)
+        tif.write(torch.from_numpy(st[None]).cuda().contiguous(), t)
+        if abs(t - 0.5) <= 0.25:
+            ref[0] = c_oracle.functional(dim, n, g, "bv", st, weight=t - last, out=ref[0],
+                                         degree=1)
+        last = t
+    np.testing.assert_allclose(tif.value.cpu().numpy(), ref, rtol=1e-12)
