@@ -19,7 +19,8 @@ class FunctionalParams(ctypes.Structure):
     _fields_ = [("degree", ctypes.c_int), ("degree_k", ctypes.c_int), ("degree_n", ctypes.c_int),
                 ("degree_m", ctypes.c_int), ("min_value", ctypes.c_double),
                 ("max_value", ctypes.c_double), ("gamma", ctypes.c_double),
-                ("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3)]
+                ("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3),
+                ("direction", ctypes.c_int), ("number_of_h", ctypes.c_int)]
 
 
 class Grid(ctypes.Structure):
@@ -115,6 +116,8 @@ PROTOTYPES = {
                                         _PP, ctypes.c_double, ctypes.c_int, _PP, _PP]),
     "als_solver_write_netcdf": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "als_functional_size": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, _LL]),
+    "als_functional_size2": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int,
+                                            ctypes.POINTER(FunctionalParams), _LL]),
     "als_functional": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int,
                                       ctypes.POINTER(FunctionalParams), _VP, ctypes.c_int,
                                       ctypes.c_longlong, ctypes.c_int, _VP, ctypes.c_longlong,

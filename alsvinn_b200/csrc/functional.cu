@@ -12,6 +12,12 @@
 //   legendre_pointwise  LegendrePointWise.cpp:32-87  out (interior) += w P_degree(u')
 //   bv                  BoundedVariation.cpp:24-52,  out[v] += w sum |grad U_v|^p
 //                       HostMemory.cpp:325-362
+//   bv_direction        alsuq/src/stats/BoundedVariationDirection.cpp:35-70,
+//                       HostMemory.cpp:364-401     out[v] += w sum |U(x) - U(x-e_d)|^p
+//   structure_2pt       alsuq/src/stats/StructureTwoPoints.cpp:48-92
+//                       out[v][h1 + H h2] += w sum (U(x+h1 e)-U)^2 (U(x+h2 e)-U) / cells
+//                       (shifts clamped at the last cell; the reference
+//                       uses direction1 for both shifts)
 //
 // Sums over cells (log_entropy, legendre, bv) are reduced in a fixed order
 // (per block: strided per-thread sums, then a shared-memory tree; the block
@@ -110,12 +116,15 @@ __global__ void __launch_bounds__(kThreads) pointwise(Geometry G, int kind, int 
 // Block partial sums of a reduced functional: partial[(m * nsum + s) * B + b].
 template<class R>
 __global__ void __launch_bounds__(kThreads) partial_sums(Geometry G, int kind, int p, int dk,
-    int dn, int dm, double lo, double hi, double gamma, const void* states,
+    int dn, int dm, double lo, double hi, double gamma, int dir, int H, const void* states,
     long long member_stride, int nvar, int nsum, double* partial) {
     const int b = blockIdx.x;
     const int m = blockIdx.y;
-    const int sidx = blockIdx.z;           // variable for legendre / bv, 0 for log_entropy
+    // the sum's index: the variable (legendre, bv, bv_direction), 0
+    // (log_entropy), or variable * H^2 + h1 + H h2 (structure_2pt)
+    const int sidx = blockIdx.z;
     const long long base = (long long)m * member_stride;
+    const long long stride = dir == 0 ? 1 : (dir == 1 ? G.N[0] : (long long)G.N[0] * G.N[1]);
     __shared__ double red[kThreads];
     double acc = 0;
     for (long long c = (long long)b * blockDim.x + threadIdx.x; c < G.cells;
@@ -142,6 +151,26 @@ __global__ void __launch_bounds__(kThreads) partial_sums(Geometry G, int kind, i
             const double value = (load<R>(states, base + (long long)sidx * G.plane + idx) - lo) /
                 (hi - lo);
             acc += legendre_p(dk, xs) * legendre_p(dn, ys) * legendre_p(dm, value) * G.dV;
+        } else if (kind == ALS_FUNCTIONAL_BV_DIRECTION) {
+            if (ijk[dir] == 0) {
+                continue;
+            }
+            const long long v0 = base + (long long)sidx * G.plane;
+            acc += pow(fabs(load<R>(states, v0 + idx) - load<R>(states, v0 + idx - stride)),
+                double(p));
+        } else if (kind == ALS_FUNCTIONAL_STRUCTURE_2PT) {
+            const int var = sidx / (H * H);
+            const int h1 = (sidx % (H * H)) % H;
+            const int h2 = (sidx % (H * H)) / H;
+            const long long v0 = base + (long long)var * G.plane;
+            const double u = load<R>(states, v0 + idx);
+            // shifted cells, clamped at the last interior cell along dir
+            const int last = G.n[dir] - 1;
+            const int s1 = min(ijk[dir] + h1, last) - ijk[dir];
+            const int s2 = min(ijk[dir] + h2, last) - ijk[dir];
+            const double u1 = load<R>(states, v0 + idx + s1 * stride);
+            const double u2 = load<R>(states, v0 + idx + s2 * stride);
+            acc += (u1 - u) * (u1 - u) * (u2 - u) / double(G.cells);
         } else {
             // bounded variation: cells after the first along x (and y in 2-D)
             if (ijk[0] == 0 || (G.dim > 1 && ijk[1] == 0)) {
@@ -169,9 +198,10 @@ __global__ void __launch_bounds__(kThreads) partial_sums(Geometry G, int kind, i
     }
 }
 
-// out slot += weight * (sum of the block partials in block order).
+// out slot += weight * (sum of the block partials in block order); sum s
+// goes to variable slot0 + s / inner, element s % inner.
 __global__ void __launch_bounds__(kThreads) finish_sums(const double* partial, int blocks,
-    int members, int nsum, int slot0, long long per_var, double* out,
+    int members, int nsum, int slot0, int inner, long long per_var, double* out,
     long long out_member_stride, double weight) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= members * nsum) {
@@ -183,8 +213,8 @@ __global__ void __launch_bounds__(kThreads) finish_sums(const double* partial, i
     for (int b = 0; b < blocks; ++b) {
         sum += partial[(long long)t * blocks + b];
     }
-    const int v = slot0 + s;
-    double* o = out + (long long)m * out_member_stride + (long long)v * per_var;
+    const int v = slot0 + s / inner;
+    double* o = out + (long long)m * out_member_stride + (long long)v * per_var + s % inner;
     *o = *o + weight * sum;
 }
 
@@ -196,13 +226,15 @@ int blocks_for(long long n) {
     return int(b < 148LL * 16 ? b : 148LL * 16);
 }
 
-long long elements_per_variable(const Geometry& G, int kind) {
+long long elements_per_variable(const Geometry& G, int kind, int H) {
     switch (kind) {
     case ALS_FUNCTIONAL_IDENTITY:
     case ALS_FUNCTIONAL_LEGENDRE_POINTWISE:
         return G.cells;
     case ALS_FUNCTIONAL_MOMENT:
         return G.plane;
+    case ALS_FUNCTIONAL_STRUCTURE_2PT:
+        return (long long)H * H;
     default:
         return 1;
     }
@@ -243,17 +275,23 @@ int make_geometry(const als_grid* grid, const als_functional_params* p, Geometry
 
 extern "C" {
 
-int als_functional_size(const als_grid* grid, int kind, long long* elements) {
+int als_functional_size2(const als_grid* grid, int kind, const als_functional_params* params,
+    long long* elements) {
     Geometry G;
     const int rc = make_geometry(grid, nullptr, G);
     if (rc != ALS_OK) {
         return rc;
     }
-    if (!elements || kind < ALS_FUNCTIONAL_IDENTITY || kind > ALS_FUNCTIONAL_BV) {
+    if (!elements || kind < ALS_FUNCTIONAL_IDENTITY || kind > ALS_FUNCTIONAL_STRUCTURE_2PT ||
+        (kind == ALS_FUNCTIONAL_STRUCTURE_2PT && (!params || params->number_of_h < 1))) {
         return als::report_error(ALS_E_INVALID, "invalid functional arguments");
     }
-    *elements = elements_per_variable(G, kind);
+    *elements = elements_per_variable(G, kind, params ? params->number_of_h : 0);
     return ALS_OK;
+}
+
+int als_functional_size(const als_grid* grid, int kind, long long* elements) {
+    return als_functional_size2(grid, kind, nullptr, elements);
 }
 
 int als_functional(const als_grid* grid, int kind, const als_functional_params* params,
@@ -265,17 +303,25 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
         return rc;
     }
     if (!params || !states || !out || members < 1 || member_stride < 0 ||
-        out_member_stride < 0 || kind < ALS_FUNCTIONAL_IDENTITY || kind > ALS_FUNCTIONAL_BV ||
-        (precision != ALS_FP64 && precision != ALS_FP32)) {
+        out_member_stride < 0 || kind < ALS_FUNCTIONAL_IDENTITY ||
+        kind > ALS_FUNCTIONAL_STRUCTURE_2PT || (precision != ALS_FP64 && precision != ALS_FP32)) {
         return als::report_error(ALS_E_INVALID, "invalid functional arguments");
     }
+    if ((kind == ALS_FUNCTIONAL_BV_DIRECTION || kind == ALS_FUNCTIONAL_STRUCTURE_2PT) &&
+        (params->direction < 0 || params->direction >= G.dim)) {
+        return als::report_error(ALS_E_INVALID, "direction outside the grid's dimensions");
+    }
+    if (kind == ALS_FUNCTIONAL_STRUCTURE_2PT && (params->number_of_h < 1 ||
+        params->number_of_h > 64)) {
+        return als::report_error(ALS_E_INVALID, "structure_2pt takes 1 <= number_of_h <= 64");
+    }
     const int nvar = G.dim + 2;
-    const long long per_var = elements_per_variable(G, kind);
+    const long long per_var = elements_per_variable(G, kind, params->number_of_h);
     if (members > 1 && (member_stride < nvar * G.plane || out_member_stride < nvar * per_var)) {
         return als::report_error(ALS_E_INVALID, "member strides smaller than one member");
     }
     if ((kind == ALS_FUNCTIONAL_MOMENT || kind == ALS_FUNCTIONAL_LEGENDRE_POINTWISE ||
-         kind == ALS_FUNCTIONAL_BV) && params->degree < 0) {
+         kind == ALS_FUNCTIONAL_BV || kind == ALS_FUNCTIONAL_BV_DIRECTION) && params->degree < 0) {
         return als::report_error(ALS_E_INVALID, "negative degree");
     }
     if (kind == ALS_FUNCTIONAL_LEGENDRE && (params->degree_k < 0 || params->degree_n < 0 ||
@@ -310,11 +356,21 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
         }
         err = cudaGetLastError();
     } else {
-        // log_entropy: one sum into the energy slot; legendre / bv: one per variable
-        const int nsum = kind == ALS_FUNCTIONAL_LOG_ENTROPY ? 1 : nvar;
+        // log_entropy: one sum into the energy slot; legendre, bv,
+        // bv_direction: one per variable; structure_2pt: H^2 per variable
+        const int H = params->number_of_h;
+        const int inner = kind == ALS_FUNCTIONAL_STRUCTURE_2PT ? H * H : 1;
+        const int nsum = kind == ALS_FUNCTIONAL_LOG_ENTROPY ? 1 : nvar * inner;
         const int slot0 = kind == ALS_FUNCTIONAL_LOG_ENTROPY ? nvar - 1 : 0;
+        if (members > 65535) {
+            return als::report_error(ALS_E_INVALID, "at most 65535 members per call");
+        }
         long long bl = (G.cells + kThreads - 1) / kThreads;
-        const int blocks = int(bl < kReduceBlocks ? (bl < 1 ? 1 : bl) : kReduceBlocks);
+        int blocks = int(bl < kReduceBlocks ? (bl < 1 ? 1 : bl) : kReduceBlocks);
+        // partial sums stay below 512 MB
+        while (blocks > 1 && (long long)members * nsum * blocks > (1LL << 26)) {
+            blocks /= 2;
+        }
         double* partial = nullptr;
         err = cudaMallocAsync((void**)&partial,
             sizeof(double) * size_t(members) * nsum * blocks, st);
@@ -323,17 +379,19 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
             if (precision == ALS_FP64) {
                 partial_sums<double><<<grid3, kThreads, 0, st>>>(G, kind, params->degree,
                     params->degree_k, params->degree_n, params->degree_m, params->min_value,
-                    params->max_value, params->gamma, states, member_stride, nvar, nsum, partial);
+                    params->max_value, params->gamma, params->direction, H, states,
+                    member_stride, nvar, nsum, partial);
             } else {
                 partial_sums<float><<<grid3, kThreads, 0, st>>>(G, kind, params->degree,
                     params->degree_k, params->degree_n, params->degree_m, params->min_value,
-                    params->max_value, params->gamma, states, member_stride, nvar, nsum, partial);
+                    params->max_value, params->gamma, params->direction, H, states,
+                    member_stride, nvar, nsum, partial);
             }
             err = cudaGetLastError();
             if (err == cudaSuccess) {
                 finish_sums<<<(members * nsum + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-                    partial, blocks, members, nsum, slot0, per_var, out, out_member_stride,
-                    weight);
+                    partial, blocks, members, nsum, slot0, inner, per_var, out,
+                    out_member_stride, weight);
                 err = cudaGetLastError();
             }
             const cudaError_t ferr = cudaFreeAsync(partial, st);

@@ -46,29 +46,36 @@ def structure_functions(states, dimension, n, ghosts, boundary="periodic", kind=
 
 
 FUNCTIONALS = {"identity": 0, "moment": 1, "log_entropy": 2, "legendre": 3,
-               "legendre_pointwise": 4, "bv": 5}
+               "legendre_pointwise": 4, "bv": 5, "bv_direction": 6, "structure_2pt": 7}
 
 
-def functional_size(dimension, n, ghosts, kind):
+def functional_size(dimension, n, ghosts, kind, number_of_h=1):
     """Elements per variable of a functional's output (Functional::getFunctionalSize)."""
     lib = _lib.load()
     g = _grid(dimension, n, ghosts, 1.4)
+    p = _lib.FunctionalParams()
+    p.number_of_h = int(number_of_h)
     size = ctypes.c_longlong()
-    _lib.check(lib.als_functional_size(ctypes.byref(g), _choice(FUNCTIONALS, kind, "functional"),
-                                       ctypes.byref(size)))
+    _lib.check(lib.als_functional_size2(ctypes.byref(g), _choice(FUNCTIONALS, kind, "functional"),
+                                        ctypes.byref(p), ctypes.byref(size)))
     return size.value
 
 
 def functional(states, dimension, n, ghosts, kind, weight=1.0, out=None, degree=1, degree_k=0,
                degree_n=0, degree_m=0, min_value=0.0, max_value=1.0, gamma=1.4,
-               lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0), stream=0):
+               lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0), direction=0, number_of_h=1,
+               stream=0):
     """out += weight * f(U) for every member of a (members, nvar, Nz, Ny, Nx)
     FP64 or FP32 CUDA tensor; ``out`` (created zero when None) is an FP64
     CUDA tensor (members, nvar, functional_size).  ``kind``: identity,
     moment (``degree``), log_entropy (``gamma``), legendre (``degree_k``,
     ``degree_n``, ``degree_m``, ``min_value``, ``max_value``),
-    legendre_pointwise (``degree``, ``min_value``, ``max_value``) or bv (the
-    power ``degree``); ``lower``/``upper`` are the domain corners."""
+    legendre_pointwise (``degree``, ``min_value``, ``max_value``), bv (the
+    power ``degree``), or the alsuq statistics bv_direction (``direction``,
+    ``degree``) and structure_2pt (``direction``, ``number_of_h``);
+    ``lower``/``upper`` are the domain corners.  An ensemble statistic of the
+    reference (onepointmoment, bv, functional, structure_2pt) is the mean of
+    these per-member results over the members."""
     import torch
     lib = _lib.load()
     if states.dim() != 5 or not states.is_cuda or not states.is_contiguous():
@@ -77,7 +84,7 @@ def functional(states, dimension, n, ghosts, kind, weight=1.0, out=None, degree=
     if precision is None:
         raise ValueError("states must be float64 or float32")
     members, nvar = states.shape[0], states.shape[1]
-    size = functional_size(dimension, n, ghosts, kind)
+    size = functional_size(dimension, n, ghosts, kind, number_of_h)
     if out is None:
         out = torch.zeros((members, nvar, size), dtype=torch.float64, device=states.device)
     if out.shape != (members, nvar, size) or out.dtype != torch.float64 or not out.is_contiguous():
@@ -86,6 +93,7 @@ def functional(states, dimension, n, ghosts, kind, weight=1.0, out=None, degree=
     p.degree, p.degree_k, p.degree_n, p.degree_m = int(degree), int(degree_k), int(degree_n), \
         int(degree_m)
     p.min_value, p.max_value, p.gamma = float(min_value), float(max_value), float(gamma)
+    p.direction, p.number_of_h = int(direction), int(number_of_h)
     for d in range(3):
         p.lower[d] = float(lower[d]) if d < len(lower) else 0.0
         p.upper[d] = float(upper[d]) if d < len(upper) else 0.0

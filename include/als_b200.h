@@ -320,6 +320,12 @@ int als_structure_functions(const als_grid* grid, int boundary, int kind, int di
  *   LEGENDRE            1 value per variable, 2-D        (Legendre.cpp:36-98)
  *   LEGENDRE_POINTWISE  interior cells, 2-D              (LegendrePointWise.cpp:32-87)
  *   BV                  1 value per variable, 1-D/2-D    (BoundedVariation.cpp:24-52)
+ *   BV_DIRECTION        1 value per variable: sum |u(x) - u(x - e_d)|^degree
+ *                       (alsuq BoundedVariationDirection.cpp:35-70,
+ *                       HostMemory::getTotalVariation(direction, ...))
+ *   STRUCTURE_2PT       number_of_h^2 values per variable (h1 fastest):
+ *                       sum (u(x+h1 e) - u)^2 (u(x+h2 e) - u) / cells, shifts
+ *                       clamped at the last cell (alsuq StructureTwoPoints.cpp:48-92)
  * Cell midpoints and volumes follow Grid.cpp:24-41 (a direction with one
  * cell has length 1).  Sums over cells are reduced in a fixed order
  * (deterministic; equal to the reference's sequential sums to rounding).
@@ -330,13 +336,20 @@ int als_structure_functions(const als_grid* grid, int boundary, int kind, int di
 #define ALS_FUNCTIONAL_LEGENDRE 3            /* "legendre" */
 #define ALS_FUNCTIONAL_LEGENDRE_POINTWISE 4  /* "legendre_pointwise" */
 #define ALS_FUNCTIONAL_BV 5                  /* "bv" */
+#define ALS_FUNCTIONAL_BV_DIRECTION 6        /* alsuq statistic "bv_direction" */
+#define ALS_FUNCTIONAL_STRUCTURE_2PT 7       /* alsuq statistic "structure_2pt" */
 typedef struct {
     int degree;                        /* moment, legendre_pointwise, bv (the power p) */
     int degree_k, degree_n, degree_m;  /* legendre: x, y and value degrees */
     double min_value, max_value;       /* legendre*: value scaled to (u - min)/(max - min) */
     double gamma;                      /* log_entropy */
     double lower[3], upper[3];         /* domain corners (Grid origin and top) */
+    int direction;                     /* bv_direction, structure_2pt (its direction1) */
+    int number_of_h;                   /* structure_2pt */
 } als_functional_params;
+/* elements per variable; STRUCTURE_2PT needs params (its number_of_h) */
+int als_functional_size2(const als_grid* grid, int kind, const als_functional_params* params,
+    long long* elements_per_variable);
 int als_functional_size(const als_grid* grid, int kind, long long* elements_per_variable);
 int als_functional(const als_grid* grid, int kind, const als_functional_params* params,
     const void* states, int precision, long long member_stride, int members, double* out,

@@ -1496,13 +1496,16 @@ static double legendre_p(int l, double x) {
     return p1;
 }
 
-long orc_functional_size(int dim, const int* n, int g, int kind) {
+long orc_functional_size(int dim, const int* n, int g, int kind, int number_of_h) {
     long cells = 1, plane = 1;
     int d;
     for (d = 0; d < 3; ++d) {
         const int nd = d < dim ? n[d] : 1;
         cells *= nd;
         plane *= nd + (d < dim ? 2 * g : 0);
+    }
+    if (kind == ORC_FUNCTIONAL_STRUCTURE_2PT) {
+        return (long)number_of_h * number_of_h;
     }
     return kind == ORC_FUNCTIONAL_IDENTITY || kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE ? cells
         : (kind == ORC_FUNCTIONAL_MOMENT ? plane : 1);
@@ -1527,12 +1530,73 @@ int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_
         }
     }
     dV = len[0] * len[1] * len[2];
-    per_var = orc_functional_size(dim, n, g, kind);
+    per_var = orc_functional_size(dim, n, g, kind, p->number_of_h);
     if ((kind == ORC_FUNCTIONAL_LEGENDRE || kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE) && dim != 2) {
         return -1;
     }
     if (kind == ORC_FUNCTIONAL_BV && dim > 2) {
         return -1;
+    }
+    if (kind == ORC_FUNCTIONAL_BV_DIRECTION || kind == ORC_FUNCTIONAL_STRUCTURE_2PT) {
+        const int dd = p->direction;
+        const long s = dd == 0 ? 1 : (dd == 1 ? N[0] : (long)N[0] * N[1]);
+        const int H = p->number_of_h;
+        if (dd < 0 || dd >= dim) {
+            return -1;
+        }
+        for (v = 0; v < nvar; ++v) {
+            if (kind == ORC_FUNCTIONAL_BV_DIRECTION) {
+                /* HostMemory::getTotalVariation(direction, p, start, end)
+                 * (HostMemory.cpp:364-401): from one cell after the start
+                 * along the direction */
+                double bv = 0;
+                for (k = 0; k < nn[2]; ++k) {
+                    for (j = 0; j < nn[1]; ++j) {
+                        for (i = 0; i < nn[0]; ++i) {
+                            const int c[3] = {i, j, k};
+                            const long idx = idx3(N, i + g, dim > 1 ? j + g : 0,
+                                dim > 2 ? k + g : 0);
+                            if (c[dd] == 0) {
+                                continue;
+                            }
+                            bv += pow(fabs(planes[v * plane + idx] - planes[v * plane + idx - s]),
+                                (double)p->degree);
+                        }
+                    }
+                }
+                out[v * per_var] += weight * bv;
+            } else {
+                /* StructureTwoPoints::computeStructure (StructureTwoPoints.cpp:48-92):
+                 * per cell, for h1 then h2, accumulated in place */
+                double* acc = (double*)calloc((size_t)H * H, sizeof(double));
+                int h1, h2;
+                const long cells = (long)nn[0] * nn[1] * nn[2];
+                for (k = 0; k < nn[2]; ++k) {
+                    for (j = 0; j < nn[1]; ++j) {
+                        for (i = 0; i < nn[0]; ++i) {
+                            const int c[3] = {i, j, k};
+                            const long idx = idx3(N, i + g, dim > 1 ? j + g : 0,
+                                dim > 2 ? k + g : 0);
+                            const double u = planes[v * plane + idx];
+                            for (h1 = 0; h1 < H; ++h1) {
+                                const int a = (c[dd] + h1 < nn[dd] - 1 ? c[dd] + h1 : nn[dd] - 1) - c[dd];
+                                const double u1 = planes[v * plane + idx + a * s];
+                                for (h2 = 0; h2 < H; ++h2) {
+                                    const int b = (c[dd] + h2 < nn[dd] - 1 ? c[dd] + h2 : nn[dd] - 1) - c[dd];
+                                    const double u2 = planes[v * plane + idx + b * s];
+                                    acc[h1 + H * h2] += (u1 - u) * (u1 - u) * (u2 - u) / (double)cells;
+                                }
+                            }
+                        }
+                    }
+                }
+                for (h1 = 0; h1 < H * H; ++h1) {
+                    out[v * per_var + h1] += weight * acc[h1];
+                }
+                free(acc);
+            }
+        }
+        return 0;
     }
     if (kind == ORC_FUNCTIONAL_MOMENT) {
         /* HostMemory.cpp:293-301 over every cell */

@@ -94,13 +94,15 @@ int orc_obeys_constraints(const orc_config* cfg, const double* planes);
  * sums in the reference's sequential order.  Output per variable:
  * orc_functional_size elements (interior cells, padded cells or 1). */
 enum { ORC_FUNCTIONAL_IDENTITY = 0, ORC_FUNCTIONAL_MOMENT = 1, ORC_FUNCTIONAL_LOG_ENTROPY = 2,
-       ORC_FUNCTIONAL_LEGENDRE = 3, ORC_FUNCTIONAL_LEGENDRE_POINTWISE = 4, ORC_FUNCTIONAL_BV = 5 };
+       ORC_FUNCTIONAL_LEGENDRE = 3, ORC_FUNCTIONAL_LEGENDRE_POINTWISE = 4, ORC_FUNCTIONAL_BV = 5,
+       ORC_FUNCTIONAL_BV_DIRECTION = 6, ORC_FUNCTIONAL_STRUCTURE_2PT = 7 };
 typedef struct {
     int degree, degree_k, degree_n, degree_m;
     double min_value, max_value, gamma;
     double lower[3], upper[3];
+    int direction, number_of_h;
 } orc_functional_params;
-long orc_functional_size(int dim, const int* n, int g, int kind);
+long orc_functional_size(int dim, const int* n, int g, int kind, int number_of_h);
 int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_params* p,
     const double* planes, double* out, double weight);
 

@@ -79,11 +79,12 @@ class FunctionalParams(ctypes.Structure):
     _fields_ = [("degree", ctypes.c_int), ("degree_k", ctypes.c_int), ("degree_n", ctypes.c_int),
                 ("degree_m", ctypes.c_int), ("min_value", ctypes.c_double),
                 ("max_value", ctypes.c_double), ("gamma", ctypes.c_double),
-                ("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3)]
+                ("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3),
+                ("direction", ctypes.c_int), ("number_of_h", ctypes.c_int)]
 
 
 FUNCTIONAL = {"identity": 0, "moment": 1, "log_entropy": 2, "legendre": 3,
-              "legendre_pointwise": 4, "bv": 5}
+              "legendre_pointwise": 4, "bv": 5, "bv_direction": 6, "structure_2pt": 7}
 
 
 class COracle:
@@ -105,7 +106,8 @@ class COracle:
                                           _D, _D, _D]
         L.orc_diffusion_ghost_cells.argtypes = [ctypes.c_int]
         L.orc_set_diffusion.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, ctypes.c_int]
-        L.orc_functional_size.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int]
+        L.orc_functional_size.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int]
         L.orc_functional_size.restype = ctypes.c_long
         L.orc_functional.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
                                      ctypes.POINTER(FunctionalParams), _D, _D, ctypes.c_double]
@@ -171,16 +173,17 @@ class COracle:
 
     def functional(self, dim, n, g, kind, planes, weight=1.0, out=None, degree=1, degree_k=0,
                    degree_n=0, degree_m=0, min_value=0.0, max_value=1.0, gamma=1.4,
-                   lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0)):
+                   lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0), direction=0, number_of_h=1):
         """out (nvar, size) += weight * f(planes) for one padded state."""
         nn = (ctypes.c_int * 3)(*[int(v) for v in (list(n) + [1, 1, 1])[:3]])
-        size = self.lib.orc_functional_size(dim, nn, g, FUNCTIONAL[kind])
+        size = self.lib.orc_functional_size(dim, nn, g, FUNCTIONAL[kind], int(number_of_h))
         res = np.zeros((dim + 2, size)) if out is None else np.array(out, dtype=np.float64)
         p = FunctionalParams(int(degree), int(degree_k), int(degree_n), int(degree_m),
                              float(min_value), float(max_value), float(gamma))
         for d in range(3):
             p.lower[d] = float(lower[d]) if d < len(lower) else 0.0
             p.upper[d] = float(upper[d]) if d < len(upper) else 0.0
+        p.direction, p.number_of_h = int(direction), int(number_of_h)
         inp = np.ascontiguousarray(planes, dtype=np.float64)
         rc = self.lib.orc_functional(dim, nn, g, FUNCTIONAL[kind], ctypes.byref(p), _dptr(inp),
                                      _dptr(res), float(weight))

@@ -145,3 +145,35 @@ def test_legendre_needs_two_dimensions(c_oracle):
     st = smooth_random_state(1, 1, (8,), 1)
     with pytest.raises(ValueError):
         c_oracle.functional(1, (8,), 1, "legendre", st)
+
+
+@pytest.mark.parametrize("dim,n,direction", [(1, (17,), 0), (2, (9, 8), 1), (3, (5, 6, 4), 2)])
+def test_bv_direction(c_oracle, dim, n, direction):
+    """alsuq bv_direction: sum of |u(x) - u(x - e_d)|^p from one cell after
+    the start along d."""
+    g = 2
+    st = smooth_random_state(71 + dim, dim, n, g)
+    out = c_oracle.functional(dim, n, g, "bv_direction", st, degree=2, direction=direction)
+    sl = tuple([slice(None)] + [slice(g, -g) if 3 - a <= dim else slice(None) for a in range(3)])
+    U = st[sl]
+    axis = 3 - direction
+    for v in range(dim + 2):
+        ref = np.sum(np.abs(np.diff(U[v], axis=axis - 1)) ** 2)
+        assert abs(out[v, 0] - ref) < 1e-12 * ref
+
+
+def test_structure_two_points(c_oracle):
+    """alsuq structure_2pt: (u(x+h1 e)-u)^2 (u(x+h2 e)-u) / cells summed,
+    shifts clamped at the last cell, h1 fastest."""
+    dim, n, g, H = 2, (11, 7), 2, 4
+    st = smooth_random_state(81, dim, n, g)
+    out = c_oracle.functional(dim, n, g, "structure_2pt", st, direction=0, number_of_h=H)
+    for v in range(4):
+        u = st[v, 0, g:-g, g:-g]
+        ref = np.zeros((H, H))
+        for h1 in range(H):
+            i1 = np.minimum(np.arange(n[0]) + h1, n[0] - 1)
+            for h2 in range(H):
+                i2 = np.minimum(np.arange(n[0]) + h2, n[0] - 1)
+                ref[h2, h1] = np.sum((u[:, i1] - u) ** 2 * (u[:, i2] - u)) / (n[0] * n[1])
+        np.testing.assert_allclose(out[v].reshape(H, H), ref, rtol=1e-12, atol=1e-16)

@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 
 CASES = []
 for _dim, _n in ((1, (37,)), (2, (23, 19)), (3, (9, 8, 7))):
-    for _kind in ("identity", "moment", "log_entropy", "legendre", "legendre_pointwise", "bv"):
+    for _kind in ("identity", "moment", "log_entropy", "legendre", "legendre_pointwise", "bv",
+                  "bv_direction", "structure_2pt"):
         if _kind.startswith("legendre") and _dim != 2:
             continue
         if _kind == "bv" and _dim > 2:
@@ -38,13 +39,14 @@ def test_functional_matches_oracle(c_oracle, dim, n, kind, precision):
     dtype = torch.float64 if precision == "fp64" else torch.float32
     x = torch.from_numpy(states).to(dtype).cuda().contiguous()
     widened = x.double().cpu().numpy()
-    start = torch.rand((members, dim + 2, fn.functional_size(dim, n, g, kind)),
+    params = dict(PARAMS, direction=dim - 1, number_of_h=5)
+    start = torch.rand((members, dim + 2, fn.functional_size(dim, n, g, kind, 5)),
                        dtype=torch.float64, device="cuda")
-    out = fn.functional(x, dim, n, g, kind, weight=0.75, out=start.clone(), **PARAMS)
+    out = fn.functional(x, dim, n, g, kind, weight=0.75, out=start.clone(), **params)
     got = out.cpu().numpy()
     for m in range(members):
         ref = c_oracle.functional(dim, n, g, kind, widened[m], weight=0.75,
-                                  out=start[m].cpu().numpy(), **PARAMS)
+                                  out=start[m].cpu().numpy(), **params)
         if kind in ("identity", "legendre_pointwise"):
             np.testing.assert_array_equal(got[m], ref)
         else:
