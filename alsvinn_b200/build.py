@@ -25,6 +25,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 EXACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 FAST32 = ["-fmad=true"]
+# FP32 ensemble members: contracted multiply-adds and the hardware-approximate
+# divide and square root (at most a few ulp; the FP64 path stays IEEE)
+STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]
 
 
 def nvcc_path():
@@ -40,7 +43,7 @@ def sources():
     for name in sorted(os.listdir(CSRC)):
         if not name.endswith(".cu"):
             continue
-        flags = FAST32 if ("_f32_" in name or name.startswith("mlp")) else EXACT
+        flags = STAGE32 if "_f32_" in name else (FAST32 if name.startswith("mlp") else EXACT)
         units.append((os.path.join(CSRC, name), flags))
     return units
 
