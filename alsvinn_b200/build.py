@@ -26,8 +26,13 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 EXACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 FAST32 = ["-fmad=true"]
 # FP32 ensemble members: contracted multiply-adds and the hardware-approximate
-# divide and square root (at most a few ulp; the FP64 path stays IEEE)
-STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+# divide and square root (at most a few ulp; the FP64 path stays IEEE), and
+# in 2-D three resident blocks per SM (the FP32 tile needs half the shared
+# memory and registers of the FP64 one).  Measured on 512 x 256^2 KH members
+# (member cell-updates/s): IEEE, 2 blocks 4.2e9; approximate, 2 blocks 5.1e9;
+# approximate, 3 blocks 5.9e9; 16x16 tiles / 288 threads / 4 blocks 5.3e9;
+# 32x8 / 320 / 4 3.9e9.
+STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-DALS_STAGE2_BLOCKS=3"]
 
 
 def nvcc_path():
@@ -59,13 +64,20 @@ def _headers_mtime():
 
 def _compile(nvcc, src, flags, force, obj_dir=OBJ_DIR):
     obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
-    if (not force and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
-            and os.path.getmtime(obj) > _headers_mtime()):
-        return obj
     cmd = [nvcc] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+    # the command an object was built with sits beside it: a change of flags
+    # rebuilds it like a change of its sources
+    stamp = obj + ".cmd"
+    same_cmd = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+    if (not force and same_cmd and os.path.exists(obj) and
+            os.path.getmtime(obj) > os.path.getmtime(src) and
+            os.path.getmtime(obj) > _headers_mtime()):
+        return obj
     res = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s" % (src, res.stdout))
+    with open(stamp, "w") as f:
+        f.write(" ".join(cmd))
     return obj
 
 
