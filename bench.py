@@ -135,15 +135,14 @@ def cpu_baseline(state, target_seconds=12.0):
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     if os.path.exists(ref_library_path()):
         ref = RefOracle()
-        steps = 2
-        while True:
-            rc, _, _, done, _ = ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC,
-                                             1.4, CFL, 2.0, state, max_steps=steps)
-            secs = ref.lib.alsref_last_loop_seconds()
-            if secs * 2 > target_seconds or steps >= 64:
-                break
-            steps = max(steps + 1, int(steps * target_seconds / max(secs, 1e-3) * 0.6))
-            steps = min(steps, 64)
+        # a 2-step probe sizes one timed sample of about target_seconds
+        ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC, 1.4, CFL, 2.0, state,
+                     max_steps=2)
+        per_step = max(ref.lib.alsref_last_loop_seconds() / 2, 1e-4)
+        steps = int(min(max(target_seconds / per_step, 2), 2000))
+        rc, _, _, done, _ = ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC,
+                                         1.4, CFL, 2.0, state, max_steps=steps)
+        secs = ref.lib.alsref_last_loop_seconds()
         kind, sample = "reference", "%d time steps of the same KH 1024^2 state" % done
         threads = int(os.environ.get("OMP_NUM_THREADS", cores))
     else:
