@@ -41,7 +41,11 @@ namespace als {
 //   32x8  / 320 threads / 3 blocks (64 regs)   0.454
 //   32x8  / 256 threads / 4 blocks (64 regs)   0.490
 //   32x16 / 256 threads / 2 blocks (~100 regs) 0.556
-// All of these are build-time knobs.
+//   32x12 / 384 threads / 3 blocks             0.507
+//   48x12 / 576 threads / 2 blocks             0.579
+// (the first row is 0.433 since the barrier at the end of each direction
+// went).  All of these are build-time knobs; the FP32 units build with three
+// blocks per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
 #endif
