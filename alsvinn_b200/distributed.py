@@ -14,7 +14,52 @@ Samples are independent, so the only exchange is the statistics at the end:
   (alsuq/src/stats/StatisticsHelper.cpp:35-79).
 
 No step of the solve itself communicates.
+
+``check_peers`` is the failure check before that exchange: every rank posts
+whether its share succeeded under a tag in the process group's key-value
+store and waits, with a time limit, for everyone else's; a failed or silent
+rank turns into a ``PeerFailure`` on every other rank, on the host, before
+any collective is launched.
 """
+import datetime
+
+
+class PeerFailure(RuntimeError):
+    """Raised by check_peers: ``failed`` ranks reported a failure, ``silent``
+    ranks did not report within the time limit."""
+
+    def __init__(self, tag, failed, silent):
+        super().__init__("ranks %s failed and ranks %s did not report before %r"
+                         % (failed, silent, tag))
+        self.failed = failed
+        self.silent = silent
+
+
+def check_peers(ok, tag, timeout_seconds=30.0, store=None, group=None):
+    """Posts this rank's status for ``tag`` and waits for every rank's.
+
+    Returns when all ranks posted success; raises PeerFailure otherwise
+    (after at most ``timeout_seconds`` per silent rank).  Each tag is used
+    once per run (e.g. "stats-step-100")."""
+    import torch.distributed as dist
+    if store is None:
+        store = dist.distributed_c10d._get_default_store()
+    rank = dist.get_rank(group)
+    world = dist.get_world_size(group)
+    store.set("%s/%d" % (tag, rank), b"1" if ok else b"0")
+    failed, silent = [], []
+    limit = datetime.timedelta(seconds=timeout_seconds)
+    for r in range(world):
+        key = "%s/%d" % (tag, r)
+        try:
+            store.wait([key], limit)
+        except Exception:
+            silent.append(r)
+            continue
+        if store.get(key) != b"1":
+            failed.append(r)
+    if failed or silent:
+        raise PeerFailure(tag, failed, silent)
 
 
 def samples_for_rank(total, world, rank):
@@ -79,20 +124,35 @@ def _device_view(ptr, count, device):
     return torch.as_tensor(_DeviceArray(ptr, count), device="cuda:%d" % device)
 
 
+_calls = 0
+
+
 def kh_observable_ensemble(n, total_samples, precision="fp64", end_time=2.0, group=None, **kw):
     """The UQ ensemble of uq.kh_observable_ensemble sharded over the ranks of
     `group`: each rank solves its block of samples on its own GPU; the
     observables are all-gathered (sample order) and the FP64 field
     statistics merged.  Returns (params, y, info) on every rank, info with
-    the merged "field_mean" / "field_var" and this rank's "solve_seconds"."""
+    the merged "field_mean" / "field_var" and this rank's "solve_seconds".
+    A rank whose solve fails makes every rank raise PeerFailure (check_peers)
+    before any collective starts."""
     import torch
     import torch.distributed as dist
     from . import uq
+    global _calls
+    _calls += 1
+    tag = "kh-ensemble-%d" % _calls
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     first, count = samples_for_rank(total_samples, world, rank)
-    params, y, info = uq.kh_observable_ensemble(n, first, count, precision=precision,
-                                                end_time=end_time, keep_statistics=True, **kw)
+    try:
+        params, y, info = uq.kh_observable_ensemble(n, first, count, precision=precision,
+                                                    end_time=end_time, keep_statistics=True,
+                                                    **kw)
+    except Exception:
+        # the others learn of it before they launch the exchange
+        check_peers(False, tag, group=group)
+        raise
+    check_peers(True, tag, group=group)
     local = info.pop("statistics")
     merged = merge_statistics(local, group)
     local.close()

@@ -83,3 +83,53 @@ def test_gathered_moments_merge_to_the_ensemble_statistics(world):
     # every rank merged in the same order: identical bits
     np.testing.assert_array_equal(res[0]["mean"], res[1]["mean"])
     np.testing.assert_array_equal(res[0]["var"], res[1]["var"])
+
+
+def _failing_worker(rank, world, port, out_dir, mode):
+    """Rank 1 fails before the statistics exchange: it reports the failure
+    ("report") or exits without a word ("silent"); rank 0 must learn of it on
+    the host through check_peers, within the time limit, and never enter the
+    collective."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    import time
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=20))
+    result = "no error"
+    t0 = time.time()
+    try:
+        if rank == 1:
+            try:
+                raise RuntimeError("injected failure of this rank's share")
+            except RuntimeError:
+                if mode == "report":
+                    distributed.check_peers(False, "stats-step-1", timeout_seconds=3.0)
+                result = "left"
+                return
+        distributed.check_peers(True, "stats-step-1", timeout_seconds=3.0)
+        distributed.gather_moments(1, torch.zeros(4, dtype=torch.float64),
+                                   torch.zeros(4, dtype=torch.float64))
+    except distributed.PeerFailure as e:
+        result = "PeerFailure failed=%s silent=%s" % (e.failed, e.silent)
+    finally:
+        with open(os.path.join(out_dir, "rank%d.txt" % rank), "w") as f:
+            f.write("%s|%.1f" % (result, time.time() - t0))
+        if rank == 0:
+            # keep the store (hosted by rank 0) alive until rank 1 is done
+            time.sleep(1.0)
+        torch.distributed.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", ["report", "silent"])
+def test_failed_rank_is_detected_on_the_host_before_the_exchange(mode):
+    with tempfile.TemporaryDirectory() as d:
+        mp.spawn(_failing_worker, args=(2, _free_port(), d, mode), nprocs=2, join=True)
+        r0 = open(os.path.join(d, "rank0.txt")).read().split("|")
+        r1 = open(os.path.join(d, "rank1.txt")).read().split("|")
+    assert r1[0] in ("left", "PeerFailure failed=[1] silent=[]")
+    if mode == "report":
+        assert r0[0] == "PeerFailure failed=[1] silent=[]"
+    else:
+        assert r0[0] == "PeerFailure failed=[] silent=[1]"
+        assert float(r0[1]) < 15.0      # the 3 s limit, not the 20 s group timeout
