@@ -126,6 +126,18 @@ def kh_state(sample):
     return als.kelvin_helmholtz(N, params, GHOSTS)
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the CPU records."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(state, target_seconds=12.0):
     """The reference's own CPU path (oracle/_ref) on a bounded sample of the
     same workload, all host threads; falls back to the C restatement."""
@@ -154,7 +166,8 @@ def cpu_baseline(state, target_seconds=12.0):
         secs = time.perf_counter() - t0
         kind, sample, threads = "port", "%d time steps of the same KH 1024^2 state" % done, 1
     return {"value": N * N * done / secs, "unit": "cell-updates/s", "cores": threads,
-            "kind": kind, "sample": sample, "seconds": secs}
+            "kind": kind, "sample": sample, "seconds": secs, "cpu_model": cpu_model(),
+            "host_threads": os.cpu_count()}
 
 
 def run_reference_arm(args, rank):
@@ -184,7 +197,7 @@ def run_reference_arm(args, rank):
            "cpu_baseline": {"value": value, "unit": "cell-updates/s",
                             "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
                             "sample": "%d time steps of KH 1024^2 (reference CPU sources, OpenMP)"
-                            % steps},
+                            % steps, "cpu_model": cpu_model(), "host_threads": os.cpu_count()},
            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
