@@ -330,11 +330,11 @@ UQ_ORACLE = os.path.join(ROOT, "tests", "golden", "uq_kh256_fp64_4096.npz")
 def run_uq(args, rank, world, local):
     """UQ time-to-error: plain batched Monte Carlo against the surrogate
     control variate, KH 256^2 to T = 2, observable = mean density over
-    [0.25, 0.75]^2, both judged by the 4096-sample FP64 ensemble.
+    [0.25, 0.75]^2, both measured against the 4096-sample FP64 ensemble.
 
     The surrogate (40 -> 256 x4 -> 1, BF16 tensor cores) is trained on the
     FP64 ensemble's samples 0..1023 (Adam, lr 1e-3, up to 2000 steps, early
-    stopping on samples 1024..2047) and judged on samples 2048..4095: there
+    stopping on samples 1024..2047) and evaluated on samples 2048..4095: there
     the residual variance Var(Y - b f) / Var(Y) (and the same for Y^2) says
     how many fewer solver samples the control-variate estimator needs for
     the RMS error of plain MC with M samples.  Both arms are then run for

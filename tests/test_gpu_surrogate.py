@@ -129,13 +129,13 @@ def test_device_uniform_draws_and_moments():
     assert m2 >= m1 * m1
 
 
-def _heldout_reduction(params, y, train, val, judge, steps=2000):
+def _heldout_reduction(params, y, train, val, held, steps=2000):
     with als.Surrogate(seed=0) as s:
         s.fit(params[train], y[train], steps=steps, lr=1e-3,
               validation=(params[val], y[val]), check_every=50)
-        f = s(params[judge]).double().cpu().numpy()
+        f = s(params[held]).double().cpu().numpy()
         m1, m2 = s.moments(1 << 20, seed=2)
-    yh = y[judge]
+    yh = y[held]
     fc = f - f.mean()
     beta = np.dot(fc, yh - yh.mean()) / np.dot(fc, fc)
     return np.var(yh - beta * f) / np.var(yh), f, m1, m2
@@ -163,7 +163,7 @@ def test_control_variate_gain_on_early_time_samples():
 
 def test_control_variate_gain_at_the_final_time():
     """The 4096-sample FP64 ensemble at T = 2 (committed fixture): trained on
-    samples 0..1023, early-stopped on 1024..2047, judged on 2048..4095.  At
+    samples 0..1023, early-stopped on 1024..2047, evaluated on 2048..4095.  At
     T = 2 the observable is dominated by the chaotic roll-up, so the gain is
     small, but the control variate must still remove variance, never add it."""
     z = load_golden("uq_kh256_fp64_4096")

@@ -84,7 +84,7 @@ def test_control_variate_reduces_the_error_of_plain_mc():
 
 
 def test_uq_oracle_ensemble_fixture():
-    """The committed FP64 ensemble that judges the UQ estimators."""
+    """The committed FP64 ensemble the UQ estimators are measured against."""
     from conftest import load_golden
     z = load_golden("uq_kh256_fp64_4096")
     y = z["y"]
