@@ -1,8 +1,8 @@
 // Snapshot writer with the layout of alsfvm::io::NetCDFWriter
 // (alsfvm/src/io/NetCDFWriter.cpp:32-146), host code.
 //
-// The reference writes NetCDF-4 through libnetcdf, which is not part of
-// this build; this writer produces the classic NetCDF format (version 2,
+// The reference writes NetCDF-4 through libnetcdf, which this library does
+// not link; this writer produces the classic NetCDF format (version 2,
 // 64-bit offsets), which the same readers open (libnetcdf, ncdump, xarray,
 // scipy.io.netcdf_file), with the reference's content:
 //   dimensions  t = 1, x = nx, y = ny, z = nz   (NetCDFWriter.cpp:50-53, 85-97)
