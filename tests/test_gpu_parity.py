@@ -276,3 +276,35 @@ def test_full_size_steps_match_oracle(c_oracle, dim, n, steps):
         U = sim.get_state()[0]
     assert info["steps"] == steps and info["t"] == t and info["dt"] == dts[steps - 1]
     np.testing.assert_array_equal(U, U_ref)
+
+
+def test_largest_grid_conserves_and_matches_its_halves():
+    """A grid far above the benchmark (KH 4096^2 FP64, 0.5 GB per state):
+    with periodic boundaries every conserved total stays at its start to
+    rounding (FP64 sums over 16.8 M cells), and its left and right halves,
+    run as two subdomains of a decomposition, give the same bits."""
+    from alsvinn_b200 import domain
+    n, g, steps = 4096, 2, 3
+    st = als.kelvin_helmholtz(n, als.uniform_draws(40, 9, 1)[0], g)
+    with als.Simulator(2, (n, n), (0, 0), (1, 1), flux="hll3", reconstruction="weno2",
+                       integrator="rungekutta3", boundary="periodic", cfl=0.4, end_time=10.0,
+                       max_steps=steps) as sim:
+        sim.set_state(st)
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["steps"] == steps and info["status"] == 0
+    inner = (slice(None), 0, slice(g, g + n), slice(g, g + n))
+    before = st[inner].sum(axis=(1, 2))
+    after = U[inner].sum(axis=(1, 2))
+    # (y-momentum starts at exactly 0: its scale is the final |m_y| total)
+    scale = np.maximum(np.abs(st[inner]).sum(axis=(1, 2)), np.abs(U[inner]).sum(axis=(1, 2)))
+    assert np.all(np.abs(after - before) <= 1e-13 * scale), (after - before) / scale
+    decs = [domain.CartesianDecomposition(2, (n, n), (2, 1), r, "periodic") for r in range(2)]
+    subs = [domain.Subdomain(d, "hll3", "weno2", "rungekutta3", 0.4, 1.4) for d in decs]
+    for s in subs:
+        s.set_state(st)
+    run = domain.DecomposedSimulation(subs, domain.LocalExchange(decs, g), [1.0 / n, 1.0 / n],
+                                      0.4, 10.0)
+    assert run.run(max_steps=steps) == (steps, info["t"])
+    np.testing.assert_array_equal(run.gather(U.shape), U[:, :, g:g + n, g:g + n])
