@@ -662,7 +662,8 @@ def main():
         "schedule": schedule,
         "clocks": clock_info,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU baseline is timed at N = 1 only
         result["cpu_baseline"] = cpu_baseline(state)
     if rank == 0:
         print(json.dumps(result))
