@@ -30,7 +30,8 @@ FAST32 = ["-fmad=true"]
 # in 2-D three resident blocks per SM (the FP32 tile needs half the shared
 # memory and registers of the FP64 one).  Measured on 512 x 256^2 KH members
 # (member cell-updates/s): IEEE, 2 blocks 4.2e9; approximate, 2 blocks 5.1e9;
-# approximate, 3 blocks 5.9e9; 16x16 tiles / 288 threads / 4 blocks 5.3e9;
+# approximate, 3 blocks 5.9e9 (6.3e9 with the reciprocal forms that
+# euler_math.cuh uses for FP32); 16x16 tiles / 288 threads / 4 blocks 5.3e9;
 # 32x8 / 320 / 4 3.9e9.
 STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-DALS_STAGE2_BLOCKS=3"]
 

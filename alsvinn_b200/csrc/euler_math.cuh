@@ -48,12 +48,27 @@ __host__ __device__ constexpr int stage_ghosts(int recon, int flux) {
     return recon_ghosts(recon) > flux_ghosts(flux) ? recon_ghosts(recon) : flux_ghosts(flux);
 }
 
+// FP32 ensemble members are compared with the FP64 path by tolerance, not
+// bit for bit, so their arithmetic may be regrouped: with ALS_F32_RECIP set,
+// every group of divisions by one denominator becomes one reciprocal and
+// products, and the WENO2 weights take their closed form.  This halves the
+// divisions of a WENO2 + HLL3 cell-stage.  FP64 code never takes these
+// branches and keeps the reference's operations in the reference's order.
+#ifndef ALS_F32_RECIP
+#define ALS_F32_RECIP 1
+#endif
+template<class R>
+__host__ __device__ constexpr bool fast_recip() {
+    return ALS_F32_RECIP != 0 && sizeof(R) == 4;
+}
+
 // Left/right face state of one cell along direction D.
 template<class R, int NSD>
 struct FaceState {
     R c[NSD + 2];   // rho, m_0..m_{NSD-1}, E
     R p;            // pressure
     R ud;           // velocity along the face normal
+    R ri;           // 1 / rho (set and used only when fast_recip<R>())
 };
 
 // computeExtra (Euler.hpp:204-211): ie = E - 0.5*(m.m)/rho, u = m/rho, p = (gamma-1)*ie.
@@ -70,9 +85,26 @@ __device__ __forceinline__ void make_state(const R* U, R gamma, FaceState<R, NSD
     if (NSD > 2) {
         dot = dot + U[3] * U[3];
     }
-    const R ie = U[NSD + 1] - R(0.5) * dot / U[0];
-    s.ud = U[1 + D] / U[0];
-    s.p = (gamma - R(1)) * ie;
+    if constexpr (fast_recip<R>()) {
+        const R ri = R(1) / U[0];
+        s.ri = ri;
+        s.ud = U[1 + D] * ri;
+        s.p = (gamma - R(1)) * (U[NSD + 1] - R(0.5) * dot * ri);
+    } else {
+        const R ie = U[NSD + 1] - R(0.5) * dot / U[0];
+        s.ud = U[1 + D] / U[0];
+        s.p = (gamma - R(1)) * ie;
+    }
+}
+
+// gamma p / rho of a face state (the squared sound speed).
+template<class R, int NSD>
+__device__ __forceinline__ R sound2(const FaceState<R, NSD>& s, R gamma) {
+    if constexpr (fast_recip<R>()) {
+        return gamma * s.p * s.ri;
+    } else {
+        return gamma * s.p / s.c[0];
+    }
 }
 
 // Point flux along D (Euler.hpp:172-181).
@@ -94,11 +126,18 @@ __device__ __forceinline__ R flux_hll(const FaceState<R, NSD>& L, const FaceStat
     const R wl = sqrt(L.c[0]);
     const R wr = sqrt(Rt.c[0]);
     const R rho = (L.c[0] + Rt.c[0]) / R(2);
-    const R ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
-    const R p = (L.p * wl + Rt.p * wr) / (wl + wr);
+    R ud, p;
+    if constexpr (fast_recip<R>()) {
+        const R iw = R(1) / (wl + wr);
+        ud = (wl * L.ud + wr * Rt.ud) * iw;
+        p = (L.p * wl + Rt.p * wr) * iw;
+    } else {
+        ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
+        p = (L.p * wl + Rt.p * wr) / (wl + wr);
+    }
     const R cs = sqrt(gamma * p / rho);
-    const R sL = fmin(L.ud - sqrt(gamma * L.p / L.c[0]), ud - cs);
-    const R sR = fmax(Rt.ud + sqrt(gamma * Rt.p / Rt.c[0]), ud + cs);
+    const R sL = fmin(L.ud - sqrt(sound2(L, gamma)), ud - cs);
+    const R sR = fmax(Rt.ud + sqrt(sound2(Rt, gamma)), ud + cs);
     if (sL == R(0)) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
@@ -114,9 +153,11 @@ __device__ __forceinline__ R flux_hll(const FaceState<R, NSD>& L, const FaceStat
         point_flux<R, NSD, D>(Rt, FR);
         const R srsl = sR * sL;
         const R den = sR - sL;
+        const R iden = fast_recip<R>() ? R(1) / den : R(0);
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            F[k] = (sR * FL[k] - sL * FR[k] + srsl * (Rt.c[k] - L.c[k])) / den;
+            const R num = sR * FL[k] - sL * FR[k] + srsl * (Rt.c[k] - L.c[k]);
+            F[k] = fast_recip<R>() ? num * iden : num / den;
         }
     }
     return fmax(fabs(sL), fabs(sR));
@@ -130,10 +171,17 @@ __device__ __forceinline__ void hll3_speeds(const FaceState<R, NSD>& L, const Fa
     const R wl = sqrt(L.c[0]);
     const R wr = sqrt(Rt.c[0]);
     const R rho = (L.c[0] + Rt.c[0]) / R(2);
-    const R ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
-    const R p = (wl * L.p + wr * Rt.p) / (wl + wr);
-    const R cfL = sqrt(gamma * L.p / L.c[0]);
-    const R cfR = sqrt(gamma * Rt.p / Rt.c[0]);
+    R ud, p;
+    if constexpr (fast_recip<R>()) {
+        const R iw = R(1) / (wl + wr);
+        ud = (wl * L.ud + wr * Rt.ud) * iw;
+        p = (wl * L.p + wr * Rt.p) * iw;
+    } else {
+        ud = (wl * L.ud + wr * Rt.ud) / (wl + wr);
+        p = (wl * L.p + wr * Rt.p) / (wl + wr);
+    }
+    const R cfL = sqrt(sound2(L, gamma));
+    const R cfR = sqrt(sound2(Rt, gamma));
     const R correct = R(0.5) * fmax(R(0), L.ud - Rt.ud);
     const R cs = sqrt(gamma * p / rho);
     sL = fmin(L.ud + correct - cfL, ud - cs);
@@ -162,7 +210,9 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
         const R udl = L.ud - sL;
         const R udr = Rt.ud - sR;
         const R aa = udr * Rt.c[0] - udl * L.c[0];
-        const R sm = (Rt.c[1 + D] * udr - L.c[1 + D] * udl + Rt.p - L.p) / aa;
+        const R iaa = fast_recip<R>() ? R(1) / aa : R(0);
+        auto over_aa = [&](R x) { return fast_recip<R>() ? x * iaa : x / aa; };
+        const R sm = over_aa(Rt.c[1 + D] * udr - L.c[1 + D] * udl + Rt.p - L.p);
         // us: transverse star velocities (the normal one is sm)
         R us[NSD];
 #pragma unroll
@@ -170,7 +220,7 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
             if (k == D) {
                 us[k] = sm;
             } else {
-                us[k] = (FR[1 + k] - FL[1 + k] - sR * Rt.c[1 + k] + sL * L.c[1 + k]) / aa;
+                us[k] = over_aa(FR[1 + k] - FL[1 + k] - sR * Rt.c[1 + k] + sL * L.c[1 + k]);
             }
         }
         const bool left = sm >= R(0);
@@ -179,14 +229,16 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
         const R udk = left ? udl : udr;
         const R* FK = left ? FL : FR;
         const R den = sm - sK;
+        const R iden = fast_recip<R>() ? R(1) / den : R(0);
+        auto over_den = [&](R x) { return fast_recip<R>() ? x * iden : x / den; };
         R mid[NV];
-        mid[0] = S.c[0] * udk / den;
+        mid[0] = over_den(S.c[0] * udk);
 #pragma unroll
         for (int k = 0; k < NSD; ++k) {
             mid[1 + k] = us[k] * mid[0];
         }
         const R ps = S.p + S.c[0] * (S.ud - sm) * udk;
-        mid[NSD + 1] = (udk * S.c[NSD + 1] + S.p * S.ud - ps * sm) / den;
+        mid[NSD + 1] = over_den(udk * S.c[NSD + 1] + S.p * S.ud - ps * sm);
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             F[k] = FK[k] + sK * (mid[k] - S.c[k]);
@@ -206,8 +258,7 @@ __device__ __forceinline__ R flux_central(const FaceState<R, NSD>& L, const Face
     for (int k = 0; k < NV; ++k) {
         F[k] = R(0.5) * (FL[k] + FR[k]);
     }
-    return fmax(fabs(L.ud) + sqrt(gamma * L.p / L.c[0]),
-        fabs(Rt.ud) + sqrt(gamma * Rt.p / Rt.c[0]));
+    return fmax(fabs(L.ud) + sqrt(sound2(L, gamma)), fabs(Rt.ud) + sqrt(sound2(Rt, gamma)));
 }
 
 // Logarithmic mean (b - a) / (log b - log a), 0 when either difference is 0
@@ -460,14 +511,27 @@ __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right,
         const R b1 = dm * dm;
         const R d0 = R(3) * (eps + b0) * (eps + b0);
         const R d1 = R(3) * (eps + b1) * (eps + b1);
-        const R a0Left = R(1) / d0;
-        const R a1Right = R(1) / d1;
-        const R a1Left = twice_reciprocal(d1, a1Right);
-        const R a0Right = twice_reciprocal(d0, a0Left);
-        const R w0Left = a0Left / (a0Left + a1Left);
-        const R w1Left = a1Left / (a0Left + a1Left);
-        const R w0Right = a0Right / (a0Right + a1Right);
-        const R w1Right = a1Right / (a0Right + a1Right);
+        R w0Left, w1Left, w0Right, w1Right;
+        if constexpr (fast_recip<R>()) {
+            // a0L = 1/d0, a1L = 2/d1, a0R = 2/d0, a1R = 1/d1 give w0L = d1/(d1 + 2 d0),
+            // w1L = 2 d0/(d1 + 2 d0), w0R = 2 d1/(2 d1 + d0), w1R = d0/(2 d1 + d0)
+            // (d stays finite in FP32 while neighbouring densities differ by < 1e9)
+            const R rl = R(1) / (d1 + R(2) * d0);
+            const R rr = R(1) / (R(2) * d1 + d0);
+            w0Left = d1 * rl;
+            w1Left = R(2) * d0 * rl;
+            w0Right = R(2) * d1 * rr;
+            w1Right = d0 * rr;
+        } else {
+            const R a0Left = R(1) / d0;
+            const R a1Right = R(1) / d1;
+            const R a1Left = twice_reciprocal(d1, a1Right);
+            const R a0Right = twice_reciprocal(d0, a0Left);
+            w0Left = a0Left / (a0Left + a1Left);
+            w1Left = a1Left / (a0Left + a1Left);
+            w0Right = a0Right / (a0Right + a1Right);
+            w1Right = a1Right / (a0Right + a1Right);
+        }
         const R cl = R(3) * w0Left + w1Left;
         const R cr = R(3) * w1Right + w0Right;
 #pragma unroll
@@ -542,14 +606,27 @@ __device__ __forceinline__ void reconstruct_f(const Fetch& f, R* left, R* right,
         const R b1 = dm * dm;
         const R d0 = R(3) * (eps + b0) * (eps + b0);
         const R d1 = R(3) * (eps + b1) * (eps + b1);
-        const R a0Left = R(1) / d0;
-        const R a1Right = R(1) / d1;
-        const R a1Left = twice_reciprocal(d1, a1Right);
-        const R a0Right = twice_reciprocal(d0, a0Left);
-        const R w0Left = a0Left / (a0Left + a1Left);
-        const R w1Left = a1Left / (a0Left + a1Left);
-        const R w0Right = a0Right / (a0Right + a1Right);
-        const R w1Right = a1Right / (a0Right + a1Right);
+        R w0Left, w1Left, w0Right, w1Right;
+        if constexpr (fast_recip<R>()) {
+            // a0L = 1/d0, a1L = 2/d1, a0R = 2/d0, a1R = 1/d1 give w0L = d1/(d1 + 2 d0),
+            // w1L = 2 d0/(d1 + 2 d0), w0R = 2 d1/(2 d1 + d0), w1R = d0/(2 d1 + d0)
+            // (d stays finite in FP32 while neighbouring densities differ by < 1e9)
+            const R rl = R(1) / (d1 + R(2) * d0);
+            const R rr = R(1) / (R(2) * d1 + d0);
+            w0Left = d1 * rl;
+            w1Left = R(2) * d0 * rl;
+            w0Right = R(2) * d1 * rr;
+            w1Right = d0 * rr;
+        } else {
+            const R a0Left = R(1) / d0;
+            const R a1Right = R(1) / d1;
+            const R a1Left = twice_reciprocal(d1, a1Right);
+            const R a0Right = twice_reciprocal(d0, a0Left);
+            w0Left = a0Left / (a0Left + a1Left);
+            w1Left = a1Left / (a0Left + a1Left);
+            w0Right = a0Right / (a0Right + a1Right);
+            w1Right = a1Right / (a0Right + a1Right);
+        }
         R rho[3], u[3][NSD], p[3];
 #pragma unroll
         for (int o = -1; o <= 1; ++o) {

@@ -44,8 +44,11 @@ namespace als {
 //   32x12 / 384 threads / 3 blocks             0.507
 //   48x12 / 576 threads / 2 blocks             0.579
 // (the first row is 0.433 since the barrier at the end of each direction
-// went).  All of these are build-time knobs; the FP32 units build with three
-// blocks per SM.
+// went, 0.430 since the constraint check skips its velocity divisions when
+// rho >= 1).  Keeping the tile's U^n in shared memory from the load phase
+// for the epilogue, instead of reading it there, ran slower (0.434 vs 0.430;
+// FP32 members 3 % slower).  All of these are build-time knobs; the FP32
+// units build with three blocks per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
 #endif
@@ -187,9 +190,14 @@ __device__ __forceinline__ bool obeys_constraints(const R* U, R gamma) {
     }
     const R ie = U[NV - 1] - R(0.5) * dot / U[0];
     const R p = (gamma - R(1)) * ie;
+    // with every U[k] finite and U[0] >= 1 each velocity U[k]/U[0] is at most
+    // |U[k]| in magnitude, hence finite: the divisions only decide the answer
+    // when U[0] < 1
+    if (!(U[0] >= R(1))) {
 #pragma unroll
-    for (int k = 1; k < NV - 1; ++k) {
-        ok = ok && isfinite(U[k] / U[0]);
+        for (int k = 1; k < NV - 1; ++k) {
+            ok = ok && isfinite(U[k] / U[0]);
+        }
     }
     return ok && isfinite(p) && (U[0] > R(0)) && (p > R(0));
 }
