@@ -226,6 +226,68 @@ int als_ghost_cells(int flux, int reconstruction) {
     return als::stage_ghosts(reconstruction, flux);
 }
 
+} // extern "C"
+
+namespace {
+
+// Three wave-speed accumulators per host thread and device for
+// als_compute_flux, allocated on first use and kept: a per-call
+// cudaMallocAsync/cudaFreeAsync pair costs a pool release and re-map at
+// every synchronisation (the default pool keeps nothing), several hundred
+// microseconds per call.  A call that reads them back synchronises before
+// it returns, so one thread never has two calls using them at once.
+struct ThreadWaveSpeeds {
+    std::vector<unsigned long long*> by_device;
+    ~ThreadWaveSpeeds() {
+        for (unsigned long long* p : by_device) {
+            if (p) {
+                cudaFree(p);   // at process exit the context may be gone: ignored
+            }
+        }
+    }
+};
+
+int thread_wave_speed_scratch(unsigned long long** out) {
+    thread_local ThreadWaveSpeeds slots;
+    int device = 0;
+    ALS_CUDA(cudaGetDevice(&device));
+    if (device < 0) {
+        return fail(ALS_E_CUDA, "no current device");
+    }
+    if (size_t(device) >= slots.by_device.size()) {
+        slots.by_device.resize(size_t(device) + 1, nullptr);
+    }
+    if (!slots.by_device[device]) {
+        ALS_CUDA(cudaMalloc((void**)&slots.by_device[device], 3 * sizeof(unsigned long long)));
+    }
+    *out = slots.by_device[device];
+    return ALS_OK;
+}
+
+// Write-only accumulators of the calls that want no wave speeds (one array
+// per device; concurrent calls only race on values nobody reads), and its
+// address per device, looked up once.
+static __device__ unsigned long long g_discarded_wave_speeds[3];
+std::mutex g_discard_mutex;
+void* g_discard_address[256] = {};
+
+unsigned long long* discard_wave_speeds() {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 256) {
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_discard_mutex);
+    if (!g_discard_address[device] &&
+        cudaGetSymbolAddress(&g_discard_address[device], g_discarded_wave_speeds) != cudaSuccess) {
+        g_discard_address[device] = nullptr;
+    }
+    return static_cast<unsigned long long*>(g_discard_address[device]);
+}
+
+} // namespace
+
+extern "C" {
+
 int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, int nvar,
     void* stream) {
     int rc = check_grid(grid);
@@ -255,7 +317,7 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     if (rc != ALS_OK) {
         return rc;
     }
-    if (!valid_choice(flux, reconstruction) || !wave_speed) {
+    if (!valid_choice(flux, reconstruction)) {
         return fail(ALS_E_INVALID, "invalid flux arguments");
     }
     rc = check_supported(flux, reconstruction);
@@ -295,23 +357,27 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
     P.write_ghosts = 0;
     P.gamma = grid->gamma;
     unsigned long long* ws_dev = nullptr;
-    ALS_CUDA(cudaMallocAsync((void**)&ws_dev, 3 * sizeof(unsigned long long), s));
-    ALS_CUDA(cudaMemsetAsync(ws_dev, 0, 3 * sizeof(unsigned long long), s));
-    P.level[0].ws_out = ws_dev;
+    if (wave_speed) {
+        rc = thread_wave_speed_scratch(&ws_dev);
+        if (rc != ALS_OK) {
+            return rc;
+        }
+        ALS_CUDA(cudaMemsetAsync(ws_dev, 0, 3 * sizeof(unsigned long long), s));
+    }
+    // without a destination the kernel still reduces the face speeds; the
+    // level's accumulators then go to a slot nobody reads
+    P.level[0].ws_out = ws_dev ? ws_dev : discard_wave_speeds();
     finish_params(P);
-    cudaError_t err = launch_stage(ALS_FP64, grid->dimension, reconstruction, flux,
-        als::KIND_FLUX0, P, 0, s);
+    if (!P.level[0].ws_out) {
+        return fail(ALS_E_CUDA, "wave-speed scratch unavailable");
+    }
+    ALS_CUDA(launch_stage(ALS_FP64, grid->dimension, reconstruction, flux, als::KIND_FLUX0, P, 0, s));
+    if (!wave_speed) {
+        return ALS_OK;
+    }
     unsigned long long host[3] = {0, 0, 0};
-    if (err == cudaSuccess) {
-        err = cudaMemcpyAsync(host, ws_dev, sizeof(host), cudaMemcpyDeviceToHost, s);
-    }
-    cudaFreeAsync(ws_dev, s);
-    if (err == cudaSuccess) {
-        err = cudaStreamSynchronize(s);
-    }
-    if (err != cudaSuccess) {
-        return fail(ALS_E_CUDA, std::string("compute_flux: ") + cudaGetErrorString(err));
-    }
+    ALS_CUDA(cudaMemcpyAsync(host, ws_dev, sizeof(host), cudaMemcpyDeviceToHost, s));
+    ALS_CUDA(cudaStreamSynchronize(s));
     for (int d = 0; d < 3; ++d) {
         double w;
         std::memcpy(&w, &host[d], sizeof(w));
@@ -1582,9 +1648,10 @@ int als_stats_result(als_stats* st, double* mean, double* variance, void* stream
 
 // ------------------------------------------- allocation-free flux evaluation
 //
-// als_compute_flux reserves three wave-speed accumulators per call with
-// cudaMallocAsync.  Some hosts of NumericalFlux::computeFlux cannot let a
-// library allocate device memory: a runtime that plans every byte of device
+// als_compute_flux allocates its three wave-speed accumulators once per
+// host thread and device (cudaMalloc on first use) and keeps them.  Some
+// hosts of NumericalFlux::computeFlux cannot let a library allocate device
+// memory at all: a runtime that plans every byte of device
 // memory up front (a memory pool owned by another framework, a fixed-budget
 // embedded or real-time deployment), or one that forbids allocation calls
 // while it drives the flux evaluation many times per time step.  For them,
@@ -1600,10 +1667,13 @@ static __device__ __align__(256) unsigned long long g_static_flux_wave_speeds[3 
 
 std::mutex g_static_flux_mutex;
 void* g_static_flux_address[256] = {};
+// one caller at a time per device uses the array (clear, kernel, read-back)
+std::mutex g_static_flux_calls[256];
 
 // Device address of the array on the current device, looked up once per
-// device (cudaGetSymbolAddress; the name itself is a host-side stand-in).
-int static_flux_scratch(void** address) {
+// device (cudaGetSymbolAddress; the name itself is a host-side stand-in),
+// and the device's ordinal.
+int static_flux_scratch(void** address, int* device_out) {
     int device = 0;
     ALS_CUDA(cudaGetDevice(&device));
     if (device < 0 || device >= 256) {
@@ -1616,6 +1686,7 @@ int static_flux_scratch(void** address) {
         g_static_flux_address[device] = p;
     }
     *address = g_static_flux_address[device];
+    *device_out = device;
     return ALS_OK;
 }
 
@@ -1641,10 +1712,12 @@ extern "C" int als_compute_flux_static(const als_grid* grid, int flux, int recon
         return fail(ALS_E_INVALID, "planes have fewer ghost cells than the flux needs");
     }
     void* scratch = nullptr;
-    rc = static_flux_scratch(&scratch);
+    int device = 0;
+    rc = static_flux_scratch(&scratch, &device);
     if (rc != ALS_OK) {
         return rc;
     }
+    std::lock_guard<std::mutex> turn(g_static_flux_calls[device]);
     int lo[3] = {0, 0, 0};
     int n[3];
     for (int d = 0; d < 3; ++d) {

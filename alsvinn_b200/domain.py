@@ -237,7 +237,8 @@ class DecomposedSimulation:
             dt = 0.0
             for s in range(substeps):
                 speeds = [sub.flux.computeFlux(sub.volumes[s], sub.volumes[s + 1],
-                                               stream=self.stream) for sub in self.subs]
+                                               stream=self.stream, compute_wave_speed=s == 0)
+                          for sub in self.subs]
                 if s == 0:
                     ws = self._max_speed(speeds)
                     dt = integ.computeTimestep(ws, self.lengths, self.t, self.end_time)

@@ -317,17 +317,21 @@ class NumericalFlux:
     def getNumberOfGhostCells(self):
         return self.ghosts
 
-    def computeFlux(self, conserved, out, start=(0, 0, 0), end=(0, 0, 0), stream=0):
+    def computeFlux(self, conserved, out, start=(0, 0, 0), end=(0, 0, 0), stream=0,
+                    compute_wave_speed=True):
         """Net flux of the region into ``out`` ((nvar, ...) FP64 device tensors);
-        returns the per-direction wave speeds."""
+        returns the per-direction wave speeds (the call then waits for the
+        stream), or None with ``compute_wave_speed`` False (the reference's
+        computeWaveSpeed flag: the flux is only enqueued)."""
         lib = _lib.load()
         g = _grid(self.dimension, self.n, self.ghosts, self.gamma)
-        ws = np.zeros(3)
+        ws = np.zeros(3) if compute_wave_speed else None
         s = (ctypes.c_int * 3)(*start)
         e = (ctypes.c_int * 3)(*end)
         _lib.check(lib.als_compute_flux(ctypes.byref(g), self.flux, self.reconstruction,
                                         _lib.plane_pointers(conserved), _lib.plane_pointers(out),
-                                        s, e, ws.ctypes.data_as(_D), _stream(stream)))
+                                        s, e, ws.ctypes.data_as(_D) if ws is not None else None,
+                                        _stream(stream)))
         return ws
 
 
@@ -454,7 +458,10 @@ class Integrator:
     def performSubstep(self, volumes, cell_lengths, dt, out, substep, t, end_time, stream=0):
         """volumes[k] = U_k (device tensors); returns dt (computed at substep 0)."""
         lib = _lib.load()
-        ws = self.flux.computeFlux(volumes[substep], out, stream=stream)
+        # only the first stage's wave speeds set dt (Integrator.cpp:20-46); the
+        # other stages are enqueued without a host round trip
+        ws = self.flux.computeFlux(volumes[substep], out, stream=stream,
+                                   compute_wave_speed=substep == 0)
         if self.diffusion is not None:
             self.diffusion.applyDiffusion(out, volumes[substep], stream=stream)
         if substep == 0:

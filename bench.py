@@ -512,6 +512,85 @@ def run_surrogate(args, rank, world, local):
     }
     print(json.dumps(result))
 
+def run_plugin(args, rank, world, local):
+    """KH 1024^2 FP64 through the plug-in classes: the reference's time loop
+    (Simulator.cpp:191-214) with NumericalFlux as the system, Integrator for
+    the stages and Boundary after every stage, each one C-ABI call -- what a
+    user of the reference gets by switching only the platform of those
+    objects.  The time step takes one host round trip per step (the wave
+    speeds of the first stage), as in the reference."""
+    import torch
+    import torch.distributed as dist
+    import alsvinn_b200 as als
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    n = (N, N)
+    lengths = [1.0 / N, 1.0 / N, 0.0]
+    nf = als.NumericalFlux(DIM, n, FLUX, RECON)
+    bc = als.Boundary(DIM, n, nf.getNumberOfGhostCells(), BC)
+    integ = als.Integrator(INTEG, nf, CFL)
+    substeps = integ.getNumberOfSubsteps()
+    first = torch.from_numpy(kh_state(rank)).cuda()
+    vols = [first] + [first.clone() for _ in range(substeps)]
+    bc.applyBoundaryConditions(vols[0])
+    state = {"t": 0.0}
+
+    def step():
+        dt = 0.0
+        for s in range(substeps):
+            dt = integ.performSubstep(vols, lengths, dt, vols[s + 1], s, state["t"], 1e9)
+            bc.applyBoundaryConditions(vols[s + 1])
+        vols[0], vols[substeps] = vols[substeps], vols[0]
+        state["t"] += dt
+
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        starts[k].record()
+        step()
+        ends[k].record()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    cells = N * N
+    result = {
+        "metric": "cell-updates/s (KH 1024^2 FP64 through the plug-in classes)",
+        "value": world * cells * args.steps / (total_ms * 1e-3), "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Kelvin-Helmholtz initial data, sample index = rank)",
+        "config": dict(WORKLOAD, parallelism="independent replicas",
+                       path="NumericalFlux.computeFlux + Integrator.performSubstep + "
+                            "Boundary.applyBoundaryConditions per stage"),
+        "gpu_launches": args.steps * substeps * 3,
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(result))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -522,9 +601,10 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only run warmup+steps time steps (for profiler captures)")
     ap.add_argument("--workload", default="kh1024",
-                    choices=sorted(["kh1024", "uq", "surrogate"] + list(BATCHES)),
-                    help="kh1024 (default, the plain FP64 drop-in), an ensemble workload, or "
-                         "uq (time-to-error of the surrogate control variate)")
+                    choices=sorted(["kh1024", "plugin", "uq", "surrogate"] + list(BATCHES)),
+                    help="kh1024 (default, the plain FP64 drop-in through the fused solver), "
+                         "plugin (the same through the plug-in classes), an ensemble workload, "
+                         "or uq (time-to-error of the surrogate control variate)")
     ap.add_argument("--samples", type=int, default=1024, help="plain MC samples of --workload uq")
     ap.add_argument("--n", type=int, default=0,
                     help="grid size of a one-level batch workload (profiler captures)")
@@ -548,6 +628,9 @@ def main():
         return
     if args.workload == "surrogate":
         run_surrogate(args, rank, world, local)
+        return
+    if args.workload == "plugin":
+        run_plugin(args, rank, world, local)
         return
     if args.workload != "kh1024":
         run_batch(args, rank, world, local)

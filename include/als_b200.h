@@ -96,7 +96,12 @@ int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, i
  * [start, n+end) (start/end as in the reference: offsets from the interior
  * bounds, end <= 0); other cells are left untouched.  `wave_speed` (host,
  * 3 doubles) receives the maximal face wave speed per direction; the call
- * synchronises `stream` to read it back, like the reference's CUDA path. */
+ * synchronises `stream` to read it back, like the reference's CUDA path.
+ * With `wave_speed` null (the reference's computeWaveSpeed == false) the
+ * flux is only enqueued on `stream`: no wave speeds, no synchronisation.
+ * The wave-speed accumulators are three words of device memory that each
+ * host thread allocates once per device and reuses (a call that reads them
+ * back has finished with them when it returns). */
 int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* const* in,
     double* const* out, const int* start, const int* end, double* wave_speed, void* stream);
 
@@ -113,9 +118,10 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
  * cudaMalloc, cudaFree or allocating routine is called.  The first call on a
  * device looks the array's address up (cudaGetSymbolAddress): make that first
  * call before any stream capture.  Calls share the array and the call
- * clears what it uses, so calls that overlap on the GPU (from several
- * threads or streams) race; the call synchronises `stream` before it
- * returns.  More than 1024 states is rejected with ALS_E_INVALID. */
+ * clears what it uses; calls on one device from several threads take
+ * turns (a lock held from the clearing of the array to the read-back), and
+ * the call synchronises `stream` before it returns.  More than 1024 states
+ * is rejected with ALS_E_INVALID. */
 int als_compute_flux_static(const als_grid* grid, int flux, int reconstruction, const double* in,
     double* out, int members, double* wave_speed, void* stream);
 

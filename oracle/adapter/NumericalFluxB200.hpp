@@ -76,8 +76,9 @@ public:
         const int s[3] = {start.x, start.y, start.z};
         const int e[3] = {end.x, end.y, end.z};
         double ws[3] = {0, 0, 0};
-        const int rc = als_compute_flux(&g, flux, reconstruction, in.data(), o.data(), s, e, ws,
-            nullptr);
+        // computeWaveSpeed == false: no wave speeds, so no synchronisation
+        const int rc = als_compute_flux(&g, flux, reconstruction, in.data(), o.data(), s, e,
+            computeWaveSpeed ? ws : nullptr, nullptr);
         if (rc != ALS_OK) {
             THROW("als_compute_flux: " << als_last_error());
         }
@@ -87,7 +88,9 @@ public:
                     plane * sizeof(double), cudaMemcpyDeviceToHost));
             }
         }
-        (void)computeWaveSpeed;
+        if (!computeWaveSpeed) {
+            return;
+        }
         waveSpeed.x = ws[0];
         if (dimension > 1) {
             waveSpeed.y = ws[1];

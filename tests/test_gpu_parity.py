@@ -110,6 +110,28 @@ def test_plugin_boundary_and_flux_match_reference(case):
     assert digest(out.cpu().numpy()) == case["net"]
 
 
+@pytest.mark.parametrize("dim,n", [(1, (40,)), (2, (33, 18)), (3, (12, 9, 10))])
+@pytest.mark.parametrize("flux,recon", [("hll3", "weno2"), ("hll", "eno3"), ("central", "none")])
+def test_plugin_flux_without_wave_speeds(dim, n, flux, recon):
+    """computeWaveSpeed == false (a null wave_speed in the C ABI): no wave
+    speeds come back, the call only enqueues, and the net flux is the same
+    bits as with them, also for a region inside the interior."""
+    g = ghost_cells(recon)
+    st = _dev(smooth_random_state(400 + dim, dim, n, g))
+    als.Boundary(dim, n, g, "periodic").applyBoundaryConditions(st)
+    nf = als.NumericalFlux(dim, n, flux, recon)
+    start = (1, 1, 1)[:dim] + (0,) * (3 - dim)
+    end = (-2, -1, -1)[:dim] + (0,) * (3 - dim)
+    for region in (((0, 0, 0), (0, 0, 0)), (start, end)):
+        ref = torch.full_like(st, 7.0)
+        ws = nf.computeFlux(st, ref, *region)
+        assert ws is not None and ws[0] > 0
+        out = torch.full_like(st, 7.0)
+        assert nf.computeFlux(st, out, *region, compute_wave_speed=False) is None
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+
+
 @pytest.mark.parametrize("dim,n", [(1, (20,)), (2, (11, 12)), (3, (8, 9, 10))])
 @pytest.mark.parametrize("recon", ["none", "weno2", "eno2", "eno3", "eno4", "mc", "mm", "wenof2", "weno3"])
 def test_plugin_reconstruction_matches_oracle(c_oracle, dim, n, recon):

@@ -103,3 +103,57 @@ def test_static_flux_rejects_more_states_than_its_array_holds():
                                      None)
     assert rc == -1
     assert b"1024" in lib.als_last_error()
+
+
+@pytest.mark.parametrize("entry", ["static", "allocating"])
+def test_flux_calls_from_concurrent_threads(entry):
+    """Four host threads, each on its own stream, call the flux entry point
+    40 times on their own states; every result equals the serial one.  The
+    static entry point shares one device array (calls on a device take
+    turns), the allocating one keeps accumulators per thread."""
+    import threading
+    dim, n, g, flux, recon = 2, (48, 40), 2, "hll3", "weno2"
+    states = [_states(900 + 10 * k, 2, dim, n, g) for k in range(4)]
+    serial = [_static(x, dim, n, g, flux, recon) if entry == "static"
+              else _allocating(x, dim, n, g, flux, recon) for x in states]
+    lib = _lib.load()
+    grid = _grid(dim, n, g)
+    errors = []
+
+    def worker(k):
+        stream = torch.cuda.Stream()
+        x = states[k]
+        try:
+            for _ in range(40):
+                with torch.cuda.stream(stream):
+                    out = torch.zeros_like(x)
+                ws = np.zeros((x.shape[0], 3))
+                handle = ctypes.c_void_p(stream.cuda_stream)
+                if entry == "static":
+                    rc = lib.als_compute_flux_static(
+                        ctypes.byref(grid), FLUX[flux], RECON[recon], ctypes.c_void_p(x.data_ptr()),
+                        ctypes.c_void_p(out.data_ptr()), x.shape[0], ws.ctypes.data_as(_D), handle)
+                    assert rc == 0, lib.als_last_error()
+                else:
+                    for m in range(x.shape[0]):
+                        w = np.zeros(3)
+                        rc = lib.als_compute_flux(
+                            ctypes.byref(grid), FLUX[flux], RECON[recon], _lib.plane_pointers(x[m]),
+                            _lib.plane_pointers(out[m]), None, None, w.ctypes.data_as(_D), handle)
+                        assert rc == 0, lib.als_last_error()
+                        ws[m] = w
+                stream.synchronize()
+                assert torch.equal(out, serial[k][0])
+                assert np.array_equal(ws, serial[k][1])
+        except Exception as exc:   # reported by the main thread
+            errors.append(exc)
+
+    # each thread zeroes its outputs on its own stream; the states are
+    # ready on every stream before the threads start
+    torch.cuda.synchronize()
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors[0]
