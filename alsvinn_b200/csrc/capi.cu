@@ -19,6 +19,7 @@
 
 #include "als_b200.h"
 #include "aux_kernels.cuh"
+#include "scratch.h"
 #include "stage_dispatch.cuh"
 
 namespace {
@@ -201,6 +202,58 @@ namespace als {
 // per host thread, read by als_last_error).
 int report_error(int code, const char* msg) {
     return fail(code, msg);
+}
+
+namespace {
+std::mutex g_scratch_mutex;
+cudaMemPool_t g_scratch_pools[256] = {};
+} // namespace
+
+// The library's pool on the current device, created on first use.
+static cudaError_t scratch_pool(cudaMemPool_t* pool) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    if (device < 0 || device >= 256) {
+        return cudaErrorInvalidDevice;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_pools[device]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        err = cudaMemPoolCreate(&p, &props);
+        if (err != cudaSuccess) {
+            return err;
+        }
+        unsigned long long keep = ~0ULL;   // the attribute is a 64-bit unsigned value
+        err = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (err != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return err;
+        }
+        g_scratch_pools[device] = p;
+    }
+    *pool = g_scratch_pools[device];
+    return cudaSuccess;
+}
+
+cudaError_t scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
+    cudaMemPool_t pool = nullptr;
+    const cudaError_t err = scratch_pool(&pool);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+}
+
+cudaError_t scratch_free(void* ptr, cudaStream_t stream) {
+    return cudaFreeAsync(ptr, stream);
 }
 } // namespace als
 
@@ -1462,7 +1515,7 @@ int als_solver_region_sums(als_solver* s, int first_member, int count, const int
         return rc;
     }
     double* dev = nullptr;
-    ALS_CUDA(cudaMallocAsync((void**)&dev, sizeof(double) * s->nv * count, s->stream));
+    ALS_CUDA(als::scratch_alloc((void**)&dev, sizeof(double) * s->nv * count, s->stream));
     for (int m = first_member; m < first_member + count; ++m) {
         const void* base = member_state_address(s, m);
         cudaError_t err;
@@ -1477,12 +1530,12 @@ int als_solver_region_sums(als_solver* s, int first_member, int count, const int
         }
         err = cudaGetLastError();
         if (err != cudaSuccess) {
-            cudaFreeAsync(dev, s->stream);
+            als::scratch_free(dev, s->stream);
             return fail(ALS_E_CUDA, std::string("region_sums: ") + cudaGetErrorString(err));
         }
     }
     ALS_CUDA(cudaMemcpyAsync(out, dev, sizeof(double) * s->nv * count, cudaMemcpyDeviceToHost, s->stream));
-    ALS_CUDA(cudaFreeAsync(dev, s->stream));
+    ALS_CUDA(als::scratch_free(dev, s->stream));
     ALS_CUDA(cudaStreamSynchronize(s->stream));
     return ALS_OK;
 }

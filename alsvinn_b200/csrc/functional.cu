@@ -31,6 +31,7 @@
 #include <string>
 
 #include "als_b200.h"
+#include "scratch.h"
 
 namespace als {
 int report_error(int code, const char* msg);
@@ -372,7 +373,7 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
             blocks /= 2;
         }
         double* partial = nullptr;
-        err = cudaMallocAsync((void**)&partial,
+        err = als::scratch_alloc((void**)&partial,
             sizeof(double) * size_t(members) * nsum * blocks, st);
         if (err == cudaSuccess) {
             dim3 grid3(blocks, members, nsum);
@@ -394,7 +395,7 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
                     out_member_stride, weight);
                 err = cudaGetLastError();
             }
-            const cudaError_t ferr = cudaFreeAsync(partial, st);
+            const cudaError_t ferr = als::scratch_free(partial, st);
             if (err == cudaSuccess) {
                 err = ferr;
             }

@@ -25,6 +25,7 @@
 #include <string>
 
 #include "als_b200.h"
+#include "scratch.h"
 
 namespace als {
 int report_error(int code, const char* msg);
@@ -331,7 +332,7 @@ extern "C" int als_structure_functions(const als_grid* grid, int boundary, int k
     const int chunk = int(std::max<long long>(1, std::min<long long>(
         std::min<long long>(members, 65535), (64LL << 20) / 8 / per_member)));
     double* partial = nullptr;
-    ST_CUDA(cudaMallocAsync((void**)&partial, sizeof(double) * per_member * chunk, s));
+    ST_CUDA(als::scratch_alloc((void**)&partial, sizeof(double) * per_member * chunk, s));
     const double cells = double(G.n[0]) * G.n[1] * G.n[2];
     cudaError_t err = cudaSuccess;
     for (int m0 = 0; m0 < members && err == cudaSuccess; m0 += chunk) {
@@ -353,7 +354,7 @@ extern "C" int als_structure_functions(const als_grid* grid, int boundary, int k
             err = cudaGetLastError();
         }
     }
-    cudaFreeAsync(partial, s);
+    als::scratch_free(partial, s);
     if (err != cudaSuccess) {
         return als::report_error(ALS_E_CUDA, cudaGetErrorString(err));
     }
