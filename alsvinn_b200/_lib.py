@@ -94,6 +94,7 @@ PROTOTYPES = {
     "als_stats_moments": (ctypes.c_int, [_VP, _LL, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     "als_stats_result": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "als_solver_destroy": (ctypes.c_int, [_VP]),
+    "als_solver_decompose": (ctypes.c_int, [_VP, _I]),
     "als_solver_geometry": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong), _I]),
     "als_solver_set_state": (ctypes.c_int, [_VP, _D, ctypes.c_int, ctypes.c_int]),
     "als_solver_set_state_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int]),

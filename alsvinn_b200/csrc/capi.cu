@@ -583,6 +583,8 @@ struct als_solver {
     int blocks_per_sm = 0;        // 0: one block per work item; > 0: persistent, blocks per SM
     unsigned long long* counter = nullptr;  // work counter of the persistent launches
     int members = 0;              // over all levels
+    int subdomains = 0;           // 1: the members are subdomains of one grid (als_solver_decompose)
+    int procs[3] = {1, 1, 1};     // subdomains per direction
     int cur = 0;                  // RK2 ping-pong: 1 when U^n of active members sits in B
     als::StepState* state = nullptr;
     als::StepState* host_state = nullptr;  // pinned mirror
@@ -653,6 +655,10 @@ als::LevelDesc solver_level(const als_solver* s, const SolverLevel& L, const voi
     D.state = s->state + L.first;
     D.members = L.cfg.members;
     D.tiles_per_member = L.grid.tiles[0] * L.grid.tiles[1] * L.grid.tiles[2];
+    D.subdomains = s->subdomains;
+    for (int d = 0; d < 3; ++d) {
+        D.procs[d] = s->procs[d];
+    }
     return D;
 }
 
@@ -798,6 +804,10 @@ int refresh_host_state(als_solver* s) {
     ALS_CUDA(cudaMemcpyAsync(s->host_state, s->state, sizeof(als::StepState) * s->members,
         cudaMemcpyDeviceToHost, s->stream));
     ALS_CUDA(cudaStreamSynchronize(s->stream));
+    // subdomains advance on member 0's state: every member reports it
+    for (int m = 1; s->subdomains && m < s->members; ++m) {
+        s->host_state[m] = s->host_state[0];
+    }
     return ALS_OK;
 }
 
@@ -934,6 +944,34 @@ int als_solver_create(const als_solver_config* cfg, int device, als_solver** out
     return als_solver_create_levels(cfg, 1, device, out);
 }
 
+int als_solver_decompose(als_solver* s, const int* procs) {
+    if (!s || !procs) {
+        return fail(ALS_E_INVALID, "null argument");
+    }
+    if (s->levels.size() != 1) {
+        return fail(ALS_E_INVALID, "a split grid is a solver of one level");
+    }
+    if (s->cfg.integrator != ALS_INT_RK2 && s->cfg.integrator != ALS_INT_RK3) {
+        return fail(ALS_E_UNSUPPORTED, "split grids advance with rungekutta2 or rungekutta3");
+    }
+    long long count = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (procs[d] < 1 || (d >= s->cfg.dimension && procs[d] != 1)) {
+            return fail(ALS_E_INVALID, "one or more subdomains per active direction, one per inactive");
+        }
+        count *= procs[d];
+    }
+    if (count != s->members) {
+        return fail(ALS_E_INVALID, "the solver needs one member per subdomain");
+    }
+    drop_graph(s);
+    s->subdomains = 1;
+    for (int d = 0; d < 3; ++d) {
+        s->procs[d] = procs[d];
+    }
+    return ALS_OK;
+}
+
 int als_solver_destroy(als_solver* s) {
     delete s;
     return ALS_OK;
@@ -983,7 +1021,8 @@ int als_solver_set_state(als_solver* s, const double* host, int first_member, in
     if (s->cfg.precision == ALS_FP64) {
         ALS_CUDA(cudaMemcpyAsync(static_cast<double*>(L.buf[0]) + (long long)local * L.member_elems,
             host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-        int rc = fill_member_ghosts<double>(s, L, L.buf[0], local, count);
+        // subdomains come with their ghosts (their blocks of the whole padded grid)
+        int rc = s->subdomains ? ALS_OK : fill_member_ghosts<double>(s, L, L.buf[0], local, count);
         if (rc != ALS_OK) {
             return rc;
         }
@@ -994,7 +1033,7 @@ int als_solver_set_state(als_solver* s, const double* host, int first_member, in
         }
         ALS_CUDA(cudaMemcpyAsync(static_cast<float*>(L.buf[0]) + (long long)local * L.member_elems,
             tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        int rc = fill_member_ghosts<float>(s, L, L.buf[0], local, count);
+        int rc = s->subdomains ? ALS_OK : fill_member_ghosts<float>(s, L, L.buf[0], local, count);
         if (rc != ALS_OK) {
             return rc;
         }
@@ -1015,8 +1054,9 @@ int als_solver_set_state_device(als_solver* s, const void* dev, int first_member
     const size_t bytes = size_t(L.member_elems) * count * s->elem;
     ALS_CUDA(cudaMemcpyAsync(static_cast<char*>(L.buf[0]) + size_t(local) * L.member_elems * s->elem,
         dev, bytes, cudaMemcpyDeviceToDevice, s->stream));
-    int rc = s->cfg.precision == ALS_FP64 ? fill_member_ghosts<double>(s, L, L.buf[0], local, count)
-                                          : fill_member_ghosts<float>(s, L, L.buf[0], local, count);
+    int rc = s->subdomains ? ALS_OK
+        : (s->cfg.precision == ALS_FP64 ? fill_member_ghosts<double>(s, L, L.buf[0], local, count)
+                                        : fill_member_ghosts<float>(s, L, L.buf[0], local, count));
     if (rc != ALS_OK) {
         return rc;
     }

@@ -172,6 +172,40 @@ __device__ __forceinline__ int boundary_images(int i, int n, int G, int bc, int*
     return c;
 }
 
+// The same for subdomain c (of p along the direction) of a split grid: a
+// side with a neighbouring subdomain sends the cell to that neighbour's
+// ghost layer (step -1 / +1: the member holding the image), a physical side
+// takes the boundary condition's image within the subdomain (step 0), as
+// CartesianCellExchanger.cpp:51-100 and the boundary do between them.
+__device__ __forceinline__ int subdomain_images(int i, int n, int G, int bc, int c, int p,
+    int* pos, int* step) {
+    int k = 0;
+    pos[k] = i + G;
+    step[k++] = 0;
+    const bool low_neighbour = p > 1 && (c > 0 || bc == BC_PERIODIC);
+    const bool high_neighbour = p > 1 && (c < p - 1 || bc == BC_PERIODIC);
+    if (i < G) {
+        if (low_neighbour || bc == BC_PERIODIC) {
+            // the low neighbour's (or, alone along this direction, our own) high ghosts
+            pos[k] = i + G + n;
+            step[k++] = low_neighbour ? -1 : 0;
+        } else {
+            pos[k] = G - 1 - i;
+            step[k++] = 0;
+        }
+    }
+    if (i >= n - G) {
+        if (high_neighbour || bc == BC_PERIODIC) {
+            pos[k] = i + G - n;
+            step[k++] = high_neighbour ? 1 : 0;
+        } else {
+            pos[k] = 2 * n + G - 1 - i;
+            step[k++] = 0;
+        }
+    }
+    return k;
+}
+
 // Simulator::checkConstraints (CPUCellComputer.cpp:80-128, Euler.hpp:269-277):
 // all conserved values and p, u finite, rho > 0, p > 0.
 template<class R, int NV>
@@ -399,7 +433,8 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
     const int tid = threadIdx.x;
     const GridDesc& gd = L.grid;
-    StepState* st = L.state ? L.state + member : nullptr;
+    // subdomains of one grid share member 0's state
+    StepState* st = L.state ? L.state + (L.subdomains ? 0 : member) : nullptr;
 
     R* box = reinterpret_cast<R*>(smem);
     R* rec = box + NV * Lay::BOX;
@@ -423,7 +458,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
         if (st) {
             const double dt = step_dt(st);
-            if (tile == 0 && tid == 0) {
+            if (tile == 0 && tid == 0 && (member == 0 || !L.subdomains)) {
                 st->dt = dt;
             }
             c = R(dt / st->dx[0]);
@@ -532,9 +567,30 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         }
         if (P.write_ghosts) {
             int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
-            const int nxi = boundary_images(gx, gd.n[0], gd.ghosts, P.bc, ix);
-            const int nyi = DIM > 1 ? boundary_images(gy, gd.n[1], gd.ghosts, P.bc, iy) : 1;
-            const int nzi = DIM > 2 ? boundary_images(gz, gd.n[2], gd.ghosts, P.bc, iz) : 1;
+            int sx[3] = {0, 0, 0}, sy[3] = {0, 0, 0}, sz[3] = {0, 0, 0};
+            int nxi, nyi = 1, nzi = 1;
+            // this member's subdomain coordinates (subdomains only)
+            int c0 = 0, c1 = 0, c2 = 0;
+            if (L.subdomains) {
+                c0 = member % L.procs[0];
+                c1 = (member / L.procs[0]) % L.procs[1];
+                c2 = member / (L.procs[0] * L.procs[1]);
+                nxi = subdomain_images(gx, gd.n[0], gd.ghosts, P.bc, c0, L.procs[0], ix, sx);
+                if (DIM > 1) {
+                    nyi = subdomain_images(gy, gd.n[1], gd.ghosts, P.bc, c1, L.procs[1], iy, sy);
+                }
+                if (DIM > 2) {
+                    nzi = subdomain_images(gz, gd.n[2], gd.ghosts, P.bc, c2, L.procs[2], iz, sz);
+                }
+            } else {
+                nxi = boundary_images(gx, gd.n[0], gd.ghosts, P.bc, ix);
+                if (DIM > 1) {
+                    nyi = boundary_images(gy, gd.n[1], gd.ghosts, P.bc, iy);
+                }
+                if (DIM > 2) {
+                    nzi = boundary_images(gz, gd.n[2], gd.ghosts, P.bc, iz);
+                }
+            }
             if (nxi * nyi * nzi > 1) {
                 for (int a = 0; a < nzi; ++a) {
                     for (int b = 0; b < nyi; ++b) {
@@ -543,9 +599,18 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
                                 continue;
                             }
                             const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
+                            // the member holding the image (steps wrap: periodic splits)
+                            long long target = base;
+                            if (L.subdomains) {
+                                const int t0 = (c0 + sx[e] + L.procs[0]) % L.procs[0];
+                                const int t1 = (c1 + sy[b] + L.procs[1]) % L.procs[1];
+                                const int t2 = (c2 + sz[a] + L.procs[2]) % L.procs[2];
+                                target = (long long)(t0 + L.procs[0] * (t1 + L.procs[1] * t2)) *
+                                    L.member_stride;
+                            }
 #pragma unroll
                             for (int v = 0; v < NV; ++v) {
-                                outp(v)[j] = val[v];
+                                static_cast<R*>(L.out[v])[target + j] = val[v];
                             }
                         }
                     }
@@ -554,7 +619,8 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         }
         if (LAST && st && !obeys_constraints<R, NV>(val, gamma)) {
             bad = true;
-            bad_idx = idx;
+            // subdomains: the member's padded plane offset first
+            bad_idx = L.subdomains ? (long long)member * gd.plane + idx : idx;
         }
     }
 
@@ -587,7 +653,10 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         if (tid == 0) {
             __threadfence();
             const unsigned int prev = atomicAdd(&st->arrive, 1u);
-            if (prev == unsigned(L.tiles_per_member) - 1) {
+            // subdomains: every tile of every member arrives at the shared state
+            const unsigned int tiles = unsigned(L.tiles_per_member) *
+                (L.subdomains ? unsigned(L.members) : 1u);
+            if (prev == tiles - 1) {
                 __threadfence();
                 finish_step(st);
             }
@@ -611,7 +680,7 @@ __device__ __forceinline__ void stage_item(const StageParams& P, long long w, un
     const int member = int(local / L.tiles_per_member);
     const int tile = int(local - (long long)member * L.tiles_per_member);
     if (L.state) {
-        const volatile StepState* st = L.state + member;
+        const volatile StepState* st = L.state + (L.subdomains ? 0 : member);
         if (st->done) {
             return;
         }

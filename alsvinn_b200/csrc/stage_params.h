@@ -61,6 +61,13 @@ struct LevelDesc {
     int members;
     int tiles_per_member;
     long long work_begin;       // first work item of this level in the launch
+    // Subdomains of one grid split over procs[0] x procs[1] x procs[2]
+    // members (member = x + procs[0] (y + procs[1] z)): they share state 0
+    // (one dt, one wave-speed maximum), and each updated cell also writes
+    // its images into the neighbouring members' ghost cells.  0: members
+    // are independent simulations.
+    int subdomains;
+    int procs[3];
 };
 
 // A launch walks a list of work items (level, member, tile): levels one

@@ -18,7 +18,14 @@ boundary slab -- full slabs, ghosts of the other axes included, so later
 axes carry the corners.  Interior results equal the undivided grid's bit for
 bit (the flux stencils are axis-aligned and read no corner ghosts).
 
-Two transports:
+`SplitSimulation` runs the same split in the fused solver instead
+(als_solver_decompose): the subdomains are the members of one solver, one
+launch per stage covers all of them, they share one time step, and each
+stage kernel writes every updated cell's images straight into the
+neighbouring subdomains' ghost layers, so no exchange step and no host
+round trip remain between the stages.
+
+Two transports for the plug-in path:
 
 * ``LocalExchange``: every subdomain lives in this process (one GPU); halo
   slabs are device-to-device copies.
@@ -276,3 +283,91 @@ class DecomposedSimulation:
                 sl[3 - d] = slice(sub.dec.start[d], sub.dec.start[d] + sub.dec.local_n[d])
             out[tuple(sl)] = sub.interior()
         return out
+
+
+class SplitSimulation:
+    """A grid of ``n`` cells split over ``procs`` subdomains that advance in
+    the fused solver (``Simulator.decompose``).  Subdomain r is member r
+    (x fastest, CartesianDecomposition.cpp:40-135).  The solver's corners are
+    subdomain 0's, as the reference computes them (origin, origin + dx *
+    local cells, CartesianDecomposition.cpp:69-72), moved by as many ulps as
+    it takes for (end - origin) / local cells to be the whole grid's cell
+    length to the bit: the reference's ranks each recompute the length from
+    their corners and can differ from the whole grid in the last bit; here
+    every subdomain takes the whole grid's time step."""
+
+    def __init__(self, dimension, n, procs, lower=None, upper=None, flux="hll3",
+                 reconstruction="weno2", integrator="rungekutta3", boundary="periodic",
+                 gamma=1.4, cfl=0.4, end_time=1.0, max_steps=0, precision="fp64", device=0):
+        from .simulator import Simulator
+        self.dimension = dimension
+        self.n = tuple(int(v) for v in n)[:dimension]
+        world = 1
+        for p in procs:
+            world *= int(p)
+        self.decs = [CartesianDecomposition(dimension, self.n, procs, r, boundary)
+                     for r in range(world)]
+        self.boundary = boundary
+        lower = list(lower or [0.0] * dimension)
+        upper = list(upper or [1.0] * dimension)
+        local_n = self.decs[0].local_n
+        dx = [(upper[d] - lower[d]) / self.n[d] for d in range(dimension)]
+        lo = [lower[d] for d in range(dimension)]
+        hi = [lo[d] + dx[d] * local_n[d] for d in range(dimension)]
+        for d in range(dimension):
+            for _ in range(64):
+                got = (hi[d] - lo[d]) / local_n[d]
+                if got == dx[d]:
+                    break
+                hi[d] = np.nextafter(hi[d], np.inf if got < dx[d] else -np.inf)
+            if (hi[d] - lo[d]) / local_n[d] != dx[d]:
+                raise ValueError("no subdomain corner gives the whole grid's cell length")
+        self.sim = Simulator(dimension, local_n, lo, hi, flux=flux, reconstruction=reconstruction,
+                             integrator=integrator, boundary=boundary, gamma=gamma, cfl=cfl,
+                             end_time=end_time, max_steps=max_steps, precision=precision,
+                             members=world, device=device)
+        self.sim.decompose(procs)
+        self.ghosts = self.sim.ghosts
+
+    def set_state(self, global_padded):
+        """Takes the whole grid's padded state (numpy, nvar x padded extents):
+        fills its ghosts with the boundary condition and hands every
+        subdomain its block."""
+        import torch
+        x = torch.from_numpy(np.ascontiguousarray(global_padded, dtype=np.float64)).cuda()
+        Boundary(self.dimension, self.n, self.ghosts, self.boundary).applyBoundaryConditions(x)
+        whole = x.cpu().numpy()
+        blocks = np.stack([whole[dec.local_slice(self.ghosts)] for dec in self.decs])
+        self.sim.set_state(blocks)
+
+    def gather(self):
+        """The whole grid's padded state (numpy) from the subdomains' blocks;
+        every cell, ghosts included, is taken from the subdomain whose block
+        holds it first (their blocks overlap in the ghost layers)."""
+        blocks = self.sim.get_state()
+        g = self.ghosts
+        shape = [blocks.shape[1]] + [1] * (3 - self.dimension) + \
+            [self.n[d] + 2 * g for d in reversed(range(self.dimension))]
+        out = np.zeros(shape)
+        for r in reversed(range(len(self.decs))):
+            out[self.decs[r].local_slice(g)] = blocks[r]
+        return out
+
+    def interior(self):
+        """The whole grid's interior cells (numpy)."""
+        full = self.gather()
+        g = self.ghosts
+        sl = [slice(None)] * 4
+        for d in range(self.dimension):
+            sl[3 - d] = slice(g, g + self.n[d])
+        return full[tuple(sl)]
+
+    def run(self):
+        self.sim.run()
+        return self.sim.info()
+
+    def advance(self, steps):
+        self.sim.advance(steps)
+
+    def close(self):
+        self.sim.close()

@@ -126,6 +126,14 @@ class Simulator:
                 return k
         raise ValueError("member %d out of range" % member)
 
+    def decompose(self, procs):
+        """Makes the members the subdomains of one grid split over ``procs``
+        ranks per direction (als_solver_decompose): one time step for all,
+        ghost layers written across subdomains by the stage kernels.  Call
+        before set_state, which then takes each block with its ghosts."""
+        p = list(procs) + [1] * (3 - len(procs))
+        _lib.check(self._lib.als_solver_decompose(self._h, (ctypes.c_int * 3)(*p[:3])))
+
     def set_state(self, states, first_member=0):
         """Uploads FP64 host states, shape (count, nvar, Nz, Ny, Nx) or (nvar, Nz, Ny, Nx)."""
         shape = self.levels[self._level_of(first_member)]["shape"]

@@ -199,6 +199,24 @@ int als_solver_create_levels(const als_solver_config* levels, int nlevels, int d
 int als_solver_level(const als_solver* s, int level, int* first_member, int* members,
     long long* plane);
 int als_solver_destroy(als_solver* s);
+/* Makes the members of a one-level RK2/RK3 solver the subdomains of one
+ * grid split over procs[0] x procs[1] x procs[2] ranks, as the reference's
+ * MPI path splits it (alsfvm/src/mpi/domain/CartesianDecomposition.cpp:40-135,
+ * rank = x + px (y + py z)); the level's n, lower and upper are one
+ * subdomain's, and inactive directions take 1.  The subdomains then advance
+ * as one simulation: one time step from the largest wave speed over all of
+ * them (CartesianCellExchanger.cpp:37-44), and each stage kernel writes
+ * every updated cell's images into the ghost layers of the neighbouring
+ * subdomains, in place of the reference's exchange of ghost slabs after
+ * each stage (CartesianCellExchanger.cpp:51-100); physical sides take the
+ * boundary condition.  Results equal the undivided grid's bit for bit.
+ * als_solver_set_state then takes each subdomain's padded block as given,
+ * ghosts included (its block of the whole grid with the whole grid's ghosts
+ * filled).  Every member reports the shared time, step and status;
+ * bad_index is member * padded plane + the cell's index in its block.
+ * ALS_E_UNSUPPORTED for forward Euler; ALS_E_INVALID unless the solver has
+ * one level of exactly procs[0] * procs[1] * procs[2] members. */
+int als_solver_decompose(als_solver* s, const int* procs);
 /* padded cells per plane (level 0) and the ghost width the solver uses */
 int als_solver_geometry(const als_solver* s, long long* plane, int* ghosts);
 /* Uploads member states (host, FP64, padded planes; ghost cells are filled

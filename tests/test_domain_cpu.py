@@ -97,6 +97,74 @@ def test_local_exchange_restores_the_global_ghosts(dim, n, procs, bc):
                     np.testing.assert_array_equal(got[tuple(sl)], want[tuple(sl)])
 
 
+def _subdomain_images(i, n, G, bc, c, p):
+    """(padded position, member step) pairs of interior cell i along one
+    direction of subdomain c of p: the integer logic of subdomain_images in
+    alsvinn_b200/csrc/stage_kernel.cuh, restated for a CPU check."""
+    out = [(i + G, 0)]
+    low = p > 1 and (c > 0 or bc == "periodic")
+    high = p > 1 and (c < p - 1 or bc == "periodic")
+    if i < G:
+        out.append((i + G + n, -1 if low else 0) if (low or bc == "periodic")
+                   else (G - 1 - i, 0))
+    if i >= n - G:
+        out.append((i + G - n, 1 if high else 0) if (high or bc == "periodic")
+                   else (2 * n + G - 1 - i, 0))
+    return out
+
+
+@pytest.mark.parametrize("dim,n,procs", [(1, (24,), (3,)), (1, (8,), (2,)), (2, (12, 10), (2, 2)),
+                                         (2, (16, 8), (4, 1)), (2, (8, 12), (1, 3)),
+                                         (3, (8, 8, 4), (2, 2, 1)), (3, (4, 8, 8), (1, 2, 2)),
+                                         (3, (8, 8, 8), (2, 2, 2))])
+@pytest.mark.parametrize("bc", ["periodic", "neumann"])
+def test_stage_kernel_images_rebuild_every_split_block(dim, n, procs, bc):
+    """The fused split solver's epilogue: every interior cell of every
+    subdomain writes its images (own boundary images and the neighbours'
+    ghost layers, corners as combined steps) into the members' blocks.
+    Starting from blocks whose ghosts are garbage, this must give each
+    block exactly its slice of the whole grid with the whole grid's ghosts,
+    and every write must land inside the member buffers."""
+    g = 2
+    U = _global_with_ghosts(dim, n, g, bc)
+    world = int(np.prod(procs))
+    decs = [domain.CartesianDecomposition(dim, n, procs, r, bc) for r in range(world)]
+    p3 = list(procs) + [1] * (3 - len(procs))
+    blocks = np.stack([U[d.local_slice(g)] for d in decs])
+    local = decs[0].local_n
+    inner = [slice(None)] * 4
+    for d in range(dim):
+        inner[3 - d] = slice(g, g + local[d])
+    work = np.full_like(blocks, -999.0)
+    for r in range(world):
+        work[r][tuple(inner)] = blocks[r][tuple(inner)]
+    ln = list(local) + [1] * (3 - dim)
+    for r, dec in enumerate(decs):
+        c = dec.coords
+        for gz in range(ln[2]):
+            for gy in range(ln[1]):
+                for gx in range(ln[0]):
+                    per_axis = []
+                    for d, i in enumerate((gx, gy, gz)):
+                        if d < dim:
+                            per_axis.append(_subdomain_images(i, ln[d], g, bc, c[d], p3[d]))
+                        else:
+                            per_axis.append([(0, 0)])
+                    src = work[r][:, per_axis[2][0][0], per_axis[1][0][0], per_axis[0][0][0]]
+                    for kz, (pz, sz) in enumerate(per_axis[2]):
+                        for ky, (py, sy) in enumerate(per_axis[1]):
+                            for kx, (px, sx) in enumerate(per_axis[0]):
+                                if kx == ky == kz == 0:
+                                    continue
+                                t = [(c[0] + sx) % p3[0], (c[1] + sy) % p3[1], (c[2] + sz) % p3[2]]
+                                m = t[0] + p3[0] * (t[1] + p3[1] * t[2])
+                                assert 0 <= m < world
+                                assert 0 <= pz < work.shape[2] and 0 <= py < work.shape[3] \
+                                    and 0 <= px < work.shape[4]
+                                work[m][:, pz, py, px] = src
+    np.testing.assert_array_equal(work, blocks)
+
+
 def _dist_worker(rank, world, port, out_dir, dim, n, procs, bc):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
