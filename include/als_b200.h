@@ -101,7 +101,8 @@ int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, i
  * flux is only enqueued on `stream`: no wave speeds, no synchronisation.
  * The wave-speed accumulators are three words of device memory that each
  * host thread allocates once per device and reuses (a call that reads them
- * back has finished with them when it returns). */
+ * back has finished with them when it returns); that first call on a thread
+ * and device allocates, so make it before any stream capture. */
 int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const double* const* in,
     double* const* out, const int* start, const int* end, double* wave_speed, void* stream);
 
