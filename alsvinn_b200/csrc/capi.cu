@@ -356,7 +356,8 @@ int als_fill_ghosts(const als_grid* grid, int boundary, double* const* planes, i
     }
     int lo[3] = {0, 0, 0};
     als::GridDesc gd = make_grid(grid->dimension, grid->n, grid->ghosts, lo, grid->n);
-    dim3 blocks(grid_blocks(gd.plane, 256), 1);
+    dim3 blocks(grid_blocks(als::ghost_shell_cells(grid->dimension, gd.n[0], gd.n[1], gd.n[2],
+        grid->ghosts), 256), 1);
     als::fill_ghosts<double><<<blocks, 256, 0, (cudaStream_t)stream>>>(
         planes_of<double>((void* const*)planes, nvar), nvar, gd.plane, 0, grid->dimension,
         gd.n[0], gd.n[1], gd.n[2], grid->ghosts, boundary);
@@ -770,7 +771,8 @@ int enqueue_step(als_solver* s, cudaEvent_t* ev = nullptr) {
 template<class R>
 int fill_member_ghosts(als_solver* s, const SolverLevel& L, void* base, int first_local,
     int count) {
-    dim3 blocks(grid_blocks(L.grid.plane, 256), count);
+    dim3 blocks(grid_blocks(als::ghost_shell_cells(s->cfg.dimension, L.grid.n[0], L.grid.n[1],
+        L.grid.n[2], s->g), 256), count);
     void* start = static_cast<char*>(base) + size_t(first_local) * L.member_elems * s->elem;
     als::fill_ghosts<R><<<blocks, 256, 0, s->stream>>>(contiguous_planes<R>(start, s->nv, L.grid.plane),
         s->nv, L.grid.plane, L.member_elems, s->cfg.dimension, L.grid.n[0], L.grid.n[1],
