@@ -13,6 +13,10 @@
 //  * MeanVariance compute/combine/finalize    alsuq/src/stats/MeanVariance.cpp:30-67,
 //                                             alsuq/src/stats/StatisticsHelper.cpp:35-79
 //  * STLMersenne sample draws                 alsuq/src/generator/STLMersenne.cpp:38-85
+//  * Statistics by name, combined, finalized and written as the UQ runner
+//    does it                                  alsuq/src/run/Runner.cpp:80-87
+//  * Functionals by name, output allocated as TimeIntegrationFunctional does
+//                                             alsfvm/src/functional/TimeIntegrationFunctional.cpp:64-72
 // All arithmetic is done by the reference's own classes; this file only wires
 // them together and copies planes in and out.
 #include "alsfvm/types.hpp"
@@ -56,9 +60,15 @@
 #include "alsfvm/DeviceConfiguration.hpp"
 #include "alsuq/generator/STLMersenne.hpp"
 #include "alsfvm/functional/structure_common.hpp"
+#include "alsfvm/functional/FunctionalFactory.hpp"
+#include "alsfvm/io/Writer.hpp"
+#include "alsuq/stats/StatisticsFactory.hpp"
+#include "alsuq/stats/StatisticsParameters.hpp"
+#include "alsuq/stats/stats_util.hpp"
 #ifdef ALSREF_WITH_B200
 #include "adapter/NumericalFluxB200.hpp"
 #include "adapter/B200Adapters.hpp"
+#include "adapter/StatisticsB200.hpp"
 #endif
 
 #include <algorithm>
@@ -337,7 +347,27 @@ void copyOut(const volume::Volume& v, double* planes) {
     }
 }
 
+// An io::Writer that copies the volume it is given (a statistic's result)
+// into caller memory.
+class CaptureWriter : public io::Writer {
+public:
+    explicit CaptureWriter(double* out) : out(out) {}
+    void write(const volume::Volume& conservedVariables, const grid::Grid&,
+        const simulator::TimestepInformation&) override {
+        copyOut(conservedVariables, out);
+        ++writes;
+    }
+    double* out;
+    int writes = 0;
+};
+
 } // namespace
+
+#ifdef ALSREF_WITH_B200
+// The B200 statistics registered by name, as a maintainer would in their
+// statistics source file.
+REGISTER_STATISTICS(b200, meanvar, alsuq::stats::MeanVarianceB200)
+#endif
 
 extern "C" {
 
@@ -640,6 +670,114 @@ int alsref_apply_diffusion(int dim, const int* n, const char* kind, const char* 
     } catch (std::exception& e) {
         g_diffusion = k0;
         g_diffusion_recon = r0;
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// The statistics `name` of `platform` from the reference's
+// StatisticsFactory ("cpu": the reference's own classes; "b200": the
+// adapters registered above, only in the B200 build) over `samples` padded
+// states at time `time` on one rank: each sample is written to it
+// (Statistics::write -> computeStatistics), then combineStatistics,
+// finalizeStatistics and writeStatistics run in the order of
+// Runner.cpp:80-87.  first_out / second_out receive the first two
+// statistics it names (mean and variance for meanvar), nvar padded planes
+// each.
+int alsref_statistics(const char* platform, const char* name, int dim, const int* n,
+    int ghosts, long samples, const double* states, double time, double* first_out,
+    double* second_out) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", "periodic", 1.4, 0.5);
+        auto o = build(s);
+        auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        boost::property_tree::ptree tree;
+        alsuq::stats::StatisticsParameters params(tree);
+        params.setNumberOfSamples(size_t(samples));
+        params.setMpiConfiguration(std::make_shared<alsutils::mpi::Configuration>(MPI_COMM_WORLD,
+                "cpu"));
+        params.setPlatform("cpu");
+        alsuq::stats::StatisticsFactory factory;
+        auto stats = factory.makeStatistics(platform, name, params);
+        auto names = stats->getStatisticsNames();
+        std::vector<std::shared_ptr<CaptureWriter>> captures;
+        double* outs[2] = {first_out, second_out};
+        for (size_t k = 0; k < names.size() && k < 2; ++k) {
+            captures.push_back(std::make_shared<CaptureWriter>(outs[k]));
+            std::shared_ptr<io::Writer> w = captures.back();
+            stats->addWriter(names[k], w);
+        }
+        const size_t stride = paddedCells(*u) * u->getNumberOfVariables();
+        const simulator::TimestepInformation info(time, 0);
+        for (long k = 0; k < samples; ++k) {
+            copyIn(*u, states + size_t(k) * stride);
+            stats->write(*u, *o.grid, info);
+        }
+        stats->combineStatistics();
+        stats->finalizeStatistics();
+        stats->writeStatistics(*o.grid);
+        for (auto& c : captures) {
+            if (c->writes != 1) {
+                THROW("statistic written " << c->writes << " times");
+            }
+        }
+        return 0;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// Number of doubles per variable of the functional `name`'s output for a
+// grid of n cells with `ghosts` ghost cells (functional size and ghost
+// widths as TimeIntegrationFunctional.cpp:64-72 allocates them).
+long alsref_functional_size(int dim, const int* n, int ghosts, const char* name, int degree,
+    double gamma) {
+    try {
+        double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", "periodic", gamma, 0.5);
+        auto o = build(s);
+        auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        functional::Functional::Parameters p(std::map<std::string, std::string>{});
+        p.addIntegerParameter("degree", degree);
+        p.addDoubleParameter("gamma", gamma);
+        auto f = functional::FunctionalFactory().makeFunctional("cpu", name, p);
+        const ivec3 size = f->getFunctionalSize(*o.grid);
+        const ivec3 g = f->getGhostCellSizes(*o.grid, *u);
+        auto out = o.volumeFactory->createConservedVolume(size.x, size.y, size.z, g.x);
+        return long(paddedCells(*out));
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// The functional `name` of the reference's FunctionalFactory ("cpu"), with
+// parameters degree and gamma, on the grid [lower, upper] of n cells:
+// out += weight * f(state) for one padded state.  `out` holds the output
+// volume's nvar planes (alsref_functional_size doubles each).
+int alsref_functional(int dim, const int* n, const double* lower, const double* upper,
+    int ghosts, const char* name, int degree, double gamma, double weight,
+    const double* planes, double* out) {
+    try {
+        auto s = makeSetup(dim, n, lower, upper, "hll", "none", "forwardeuler", "periodic",
+            gamma, 0.5);
+        auto o = build(s);
+        auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
+        copyIn(*u, planes);
+        functional::Functional::Parameters p(std::map<std::string, std::string>{});
+        p.addIntegerParameter("degree", degree);
+        p.addDoubleParameter("gamma", gamma);
+        auto f = functional::FunctionalFactory().makeFunctional("cpu", name, p);
+        const ivec3 size = f->getFunctionalSize(*o.grid);
+        const ivec3 g = f->getGhostCellSizes(*o.grid, *u);
+        auto res = o.volumeFactory->createConservedVolume(size.x, size.y, size.z, g.x);
+        copyIn(*res, out);
+        (*f)(*res, *u, weight, *o.grid);
+        copyOut(*res, out);
+        return 0;
+    } catch (std::exception& e) {
         g_last_error = e.what();
         return -1;
     }

@@ -226,6 +226,45 @@ def write_rk4_fixtures(ref):
         print(name, "steps=%d t=%r" % (steps, t))
 
 
+# Functionals of the reference's FunctionalFactory (Identity, Moment,
+# LogEntropy, BoundedVariation), on seeded states: (dim, n, kind, degree)
+FUNCTIONAL_CASES = [(dim, n, kind, degree)
+                    for dim, n in ((1, (37,)), (2, (13, 11)), (3, (7, 6, 5)))
+                    for kind, degrees in (("identity", (1,)), ("moment", (2, 3)),
+                                          ("log_entropy", (1,)), ("bv", (1, 2)))
+                    for degree in degrees
+                    if not (kind == "bv" and dim > 2)]
+FUNCTIONAL_MEMBERS = 2
+FUNCTIONAL_WEIGHT = 0.75
+FUNCTIONAL_BOX = ((0.0, -1.0, 0.0), (2.0, 1.0, 1.0))
+
+
+def functional_case_name(dim, kind, degree):
+    return "d%d-%s-p%d" % (dim, kind, degree)
+
+
+def write_functional_fixtures(ref):
+    """tests/golden/functionals_ref.npz: for every case and member k, the
+    state smooth_random_state(600 + 7 k + dim) (ghost width 2), an output
+    that starts at 0.5 + k, and the reference's out + 0.75 f(state)."""
+    out = {}
+    for dim, n, kind, degree in FUNCTIONAL_CASES:
+        name = functional_case_name(dim, kind, degree)
+        results, starts = [], []
+        for k in range(FUNCTIONAL_MEMBERS):
+            st = smooth_random_state(600 + 7 * k + dim, dim, n, 2)
+            size = ref.functional(dim, n, 2, kind, st, weight=0.0, degree=degree).shape[1]
+            start = np.full((dim + 2, size), 0.5 + k)
+            starts.append(start)
+            results.append(ref.functional(dim, n, 2, kind, st, weight=FUNCTIONAL_WEIGHT,
+                                          out=start, degree=degree, gamma=1.4,
+                                          lower=FUNCTIONAL_BOX[0], upper=FUNCTIONAL_BOX[1]))
+        out[name + "/start"] = np.stack(starts)
+        out[name + "/result"] = np.stack(results)
+    np.savez_compressed(os.path.join(HERE, "functionals_ref.npz"), **out)
+    print("functionals_ref.npz: %d cases" % len(FUNCTIONAL_CASES))
+
+
 def main():
     ref = RefOracle()
     out = {}
@@ -284,8 +323,10 @@ def main():
         f.write("# dim n bc H p seed sha256(out, nvar x H) max\n")
         for r in rows:
             f.write("%d %s %s %d %.17g %d %s %.17g\n" % r)
+    write_functional_fixtures(ref)
+    # alsuq's MeanVariance made by name through its StatisticsFactory
     states = np.stack([smooth_random_state(77 + k, 2, (6, 5), 2) for k in range(7)])
-    mean, var = ref.meanvar(2, (6, 5), 2, states)
+    mean, var = ref.statistics(2, (6, 5), 2, states, platform="cpu", name="meanvar")
     np.savez_compressed(os.path.join(HERE, "meanvar_7.npz"), mean=mean, var=var,
                         seeds=np.arange(77, 84))
     for k, v in out.items():
@@ -293,4 +334,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["functionals"]:
+        write_functional_fixtures(RefOracle())
+    else:
+        main()

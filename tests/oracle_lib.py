@@ -267,6 +267,13 @@ class RefOracle:
         L.alsref_apply_diffusion.argtypes = [ctypes.c_int, _I, ctypes.c_char_p, ctypes.c_char_p,
                                              ctypes.c_double, ctypes.c_int, _D, _D,
                                              ctypes.POINTER(ctypes.c_int)]
+        L.alsref_statistics.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, _I,
+                                        ctypes.c_int, ctypes.c_long, _D, ctypes.c_double, _D, _D]
+        L.alsref_functional_size.argtypes = [ctypes.c_int, _I, ctypes.c_int, ctypes.c_char_p,
+                                             ctypes.c_int, ctypes.c_double]
+        L.alsref_functional_size.restype = ctypes.c_long
+        L.alsref_functional.argtypes = [ctypes.c_int, _I, _D, _D, ctypes.c_int, ctypes.c_char_p,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _D]
 
     def set_diffusion(self, kind, recon="none"):
         """Diffusion operator of the following simulations (none by default)."""
@@ -347,6 +354,36 @@ class RefOracle:
                                                    bc.encode(), H, float(p), _dptr(st),
                                                    _dptr(out)))
         return out
+
+    def statistics(self, dim, n, ghosts, states, platform="cpu", name="meanvar", time=1.0):
+        """The statistics `name` of `platform` made by the reference's
+        StatisticsFactory over the padded states (samples first), combined,
+        finalized and written like alsuq's Runner; returns its first two
+        statistics (mean and variance for meanvar)."""
+        st = np.ascontiguousarray(states, dtype=np.float64)
+        first = np.zeros(st.shape[1:])
+        second = np.zeros(st.shape[1:])
+        self._check(self.lib.alsref_statistics(platform.encode(), name.encode(), dim,
+                                               self._vec(n, ctypes.c_int, 1), ghosts,
+                                               st.shape[0], _dptr(st), float(time),
+                                               _dptr(first), _dptr(second)))
+        return first, second
+
+    def functional(self, dim, n, ghosts, kind, planes, weight=1.0, out=None, degree=1,
+                   gamma=1.4, lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0)):
+        """out (nvar, size) += weight * f(planes) by the reference's
+        FunctionalFactory ("cpu") functional `kind`, for one padded state."""
+        nn = self._vec(n, ctypes.c_int, 1)
+        size = self.lib.alsref_functional_size(dim, nn, ghosts, kind.encode(), int(degree),
+                                               float(gamma))
+        self._check(size)
+        res = np.zeros((dim + 2, size)) if out is None else np.array(out, dtype=np.float64)
+        inp = np.ascontiguousarray(planes, dtype=np.float64)
+        self._check(self.lib.alsref_functional(dim, nn, self._vec(lower, ctypes.c_double, 0.0),
+                                               self._vec(upper, ctypes.c_double, 0.0), ghosts,
+                                               kind.encode(), int(degree), float(gamma),
+                                               float(weight), _dptr(inp), _dptr(res)))
+        return res
 
     def stlmersenne(self, dimension, first, count):
         out = np.zeros(dimension * count)

@@ -1,17 +1,27 @@
 """The functionals of alsfvm/src/functional/ in the oracle (CPU).
 
-The reference's functional sources need Boost (property trees for their
-parameters, boost::math::legendre_p), which this image lacks, so the
-restatement is pinned to the reference's own unit tests for these classes
-(test/library_tests/src/fvm/functional/EntropyTest.cpp, LegendreTest.cpp),
-ported here with their inputs and tolerances, to SciPy's Legendre
-polynomials, and to direct NumPy evaluations of the stated formulas.
+Identity, Moment, LogEntropy and BoundedVariation are pinned bit for bit
+to the reference's own classes: their sources are compiled into the
+reference build (oracle/_ref, with a property-tree stand-in for their
+parameters) and made by name through its FunctionalFactory; the committed
+fixture tests/golden/functionals_ref.npz carries their outputs where that
+build is absent.  Legendre and LegendrePointWise call boost::math::legendre_p
+(not available here), so the restatement of those is pinned to the
+reference's own unit tests (test/library_tests/src/fvm/functional/
+EntropyTest.cpp, LegendreTest.cpp), ported with their inputs and
+tolerances, and to SciPy's Legendre polynomials.  The alsuq statistics
+bv_direction and structure_2pt are checked against direct NumPy evaluations
+of their stated formulas.
 """
+import os
+
 import numpy as np
 import pytest
 import scipy.special
 
 from oracle_lib import padded_shape, smooth_random_state
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 GAMMA = 1.4
 
@@ -177,3 +187,62 @@ def test_structure_two_points(c_oracle):
                 i2 = np.minimum(np.arange(n[0]) + h2, n[0] - 1)
                 ref[h2, h1] = np.sum((u[:, i1] - u) ** 2 * (u[:, i2] - u)) / (n[0] * n[1])
         np.testing.assert_allclose(out[v].reshape(H, H), ref, rtol=1e-12, atol=1e-16)
+
+
+def _fixture_cases():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden",
+                                                  os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+MG = _fixture_cases()
+
+
+@pytest.mark.parametrize("dim,n,kind,degree", MG.FUNCTIONAL_CASES,
+                         ids=[MG.functional_case_name(c[0], c[2], c[3])
+                              for c in MG.FUNCTIONAL_CASES])
+def test_functionals_equal_reference_fixture(c_oracle, dim, n, kind, degree):
+    """The restatement gives the reference classes' bits (fixture made by
+    the reference build's FunctionalFactory)."""
+    z = np.load(os.path.join(GOLDEN, "functionals_ref.npz"))
+    name = MG.functional_case_name(dim, kind, degree)
+    for k in range(MG.FUNCTIONAL_MEMBERS):
+        st = smooth_random_state(600 + 7 * k + dim, dim, n, 2)
+        got = c_oracle.functional(dim, n, 2, kind, st, weight=MG.FUNCTIONAL_WEIGHT,
+                                  out=z[name + "/start"][k], degree=degree, gamma=GAMMA,
+                                  lower=MG.FUNCTIONAL_BOX[0], upper=MG.FUNCTIONAL_BOX[1])
+        np.testing.assert_array_equal(got, z[name + "/result"][k])
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("kind", ["identity", "moment", "log_entropy", "bv"])
+def test_functionals_equal_reference_build(c_oracle, ref_oracle, kind, seed):
+    """Fresh random cases against the reference build itself (skipped where
+    it is not built): grids, degrees, weights and boxes vary with the seed."""
+    rng = np.random.default_rng(seed)
+    dim = int(rng.integers(1, 3 if kind == "bv" else 4))
+    n = tuple(int(v) for v in rng.integers(4, 12, dim))
+    g = int(rng.integers(1, 4))
+    degree = int(rng.integers(1, 4))
+    lo = tuple(rng.uniform(-1, 0, 3))
+    hi = tuple(rng.uniform(1, 2, 3))
+    st = smooth_random_state(700 + seed, dim, n, g)
+    w = float(rng.uniform(-2, 2))
+    ref = ref_oracle.functional(dim, n, g, kind, st, weight=w, degree=degree, gamma=GAMMA,
+                                lower=lo, upper=hi)
+    got = c_oracle.functional(dim, n, g, kind, st, weight=w, degree=degree, gamma=GAMMA,
+                              lower=lo, upper=hi)
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_meanvar_statistics_by_name_equal_fixture(ref_oracle):
+    """alsuq's MeanVariance made by name through its StatisticsFactory and
+    run like the UQ runner (combine, finalize, write) gives the fixture's bits."""
+    z = np.load(os.path.join(GOLDEN, "meanvar_7.npz"))
+    states = np.stack([smooth_random_state(int(s), 2, (6, 5), 2) for s in z["seeds"]])
+    mean, var = ref_oracle.statistics(2, (6, 5), 2, states, platform="cpu", name="meanvar")
+    np.testing.assert_array_equal(mean, z["mean"])
+    np.testing.assert_array_equal(var, z["var"])
