@@ -60,6 +60,7 @@ class MemberInfo(ctypes.Structure):
 
 # name -> (restype, argtypes) for every function the header declares
 PROTOTYPES = {
+    "als_scratch_trim": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong]),
     "als_last_error": (ctypes.c_char_p, []),
     "als_version": (ctypes.c_int, []),
     "als_ghost_cells": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
@@ -84,7 +85,9 @@ PROTOTYPES = {
     "als_solver_level": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _LL]),
     "als_solver_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, _I]),
     "als_solver_get_schedule": (ctypes.c_int, [_VP, _I, _I]),
-    "als_solver_tune": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D]),
+    "als_solver_tune": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _I, _D]),
+    "als_solver_set_tiles": (ctypes.c_int, [_VP, _I]),
+    "als_solver_get_tiles": (ctypes.c_int, [_VP, _I, _I]),
     "als_solver_region_sums": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _I, _I, _D]),
     "als_stats_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(_VP)]),
     "als_stats_destroy": (ctypes.c_int, [_VP]),

@@ -33,7 +33,7 @@ FAST32 = ["-fmad=true"]
 # approximate, 3 blocks 5.9e9 (6.3e9 with the reciprocal forms that
 # euler_math.cuh uses for FP32); 16x16 tiles / 288 threads / 4 blocks 5.3e9;
 # 32x8 / 320 / 4 3.9e9.
-STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-DALS_STAGE2_BLOCKS=3"]
+STAGE32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-DALS_STAGE2_BLOCKS=3", "-DALS_STAGE2S_BLOCKS=4"]
 
 
 def nvcc_path():

@@ -66,46 +66,49 @@ int check_supported(int flux, int recon) {
 }
 
 cudaError_t launch_stage(int precision, int dim, int recon, int flux, int kind,
-    const als::StageParams& P, int blocks_per_sm, cudaStream_t s) {
+    const als::StageParams& P, int blocks_per_sm, cudaStream_t s, int shape = 0) {
     if (precision == ALS_FP64) {
         switch (dim) {
-        case 1: return als::launch_stage_f64_1d(recon, flux, kind, P, blocks_per_sm, s);
-        case 2: return als::launch_stage_f64_2d(recon, flux, kind, P, blocks_per_sm, s);
-        default: return als::launch_stage_f64_3d(recon, flux, kind, P, blocks_per_sm, s);
+        case 1: return als::launch_stage_f64_1d(recon, flux, kind, shape, P, blocks_per_sm, s);
+        case 2: return als::launch_stage_f64_2d(recon, flux, kind, shape, P, blocks_per_sm, s);
+        default: return als::launch_stage_f64_3d(recon, flux, kind, shape, P, blocks_per_sm, s);
         }
     }
     switch (dim) {
-    case 1: return als::launch_stage_f32_1d(recon, flux, kind, P, blocks_per_sm, s);
-    case 2: return als::launch_stage_f32_2d(recon, flux, kind, P, blocks_per_sm, s);
-    default: return als::launch_stage_f32_3d(recon, flux, kind, P, blocks_per_sm, s);
+    case 1: return als::launch_stage_f32_1d(recon, flux, kind, shape, P, blocks_per_sm, s);
+    case 2: return als::launch_stage_f32_2d(recon, flux, kind, shape, P, blocks_per_sm, s);
+    default: return als::launch_stage_f32_3d(recon, flux, kind, shape, P, blocks_per_sm, s);
     }
 }
 
-// Tile extent along d of the kernels built for (precision, dim), as reported
-// by the unit that holds them.
-int tile_extent(int precision, int dim, int d) {
+// Tile extent along d of tile shape `shape` of the kernels built for
+// (precision, dim), as reported by the unit that holds them.
+int tile_extent(int precision, int dim, int d, int shape = 0) {
     if (d >= dim) {
         return 1;
     }
     int tile[3] = {1, 1, 1};
     if (precision == ALS_FP64) {
-        dim == 1 ? als::stage_tile_f64_1d(tile) : (dim == 2 ? als::stage_tile_f64_2d(tile) : als::stage_tile_f64_3d(tile));
+        dim == 1 ? als::stage_tile_f64_1d(shape, tile)
+                 : (dim == 2 ? als::stage_tile_f64_2d(shape, tile) : als::stage_tile_f64_3d(shape, tile));
     } else {
-        dim == 1 ? als::stage_tile_f32_1d(tile) : (dim == 2 ? als::stage_tile_f32_2d(tile) : als::stage_tile_f32_3d(tile));
+        dim == 1 ? als::stage_tile_f32_1d(shape, tile)
+                 : (dim == 2 ? als::stage_tile_f32_2d(shape, tile) : als::stage_tile_f32_3d(shape, tile));
     }
     return tile[d];
 }
 
-// Geometry of a padded grid and the tiles covering the region [lo, hi).
+// Geometry of a padded grid and the tiles (of shape `shape`) covering the
+// region [lo, hi).
 als::GridDesc make_grid(int dim, const int* n, int g, const int* lo, const int* hi,
-    int precision = ALS_FP64) {
+    int precision = ALS_FP64, int shape = 0) {
     als::GridDesc gd;
     for (int d = 0; d < 3; ++d) {
         gd.n[d] = d < dim ? n[d] : 1;
         gd.N[d] = gd.n[d] + (d < dim ? 2 * g : 0);
         gd.lo[d] = d < dim ? lo[d] : 0;
         gd.hi[d] = d < dim ? hi[d] : 1;
-        const int t = tile_extent(precision, dim, d);
+        const int t = tile_extent(precision, dim, d, shape);
         gd.tiles[d] = std::max(1, (gd.hi[d] - gd.lo[d] + t - 1) / t);
     }
     gd.plane = (long long)gd.N[0] * gd.N[1] * gd.N[2];
@@ -204,10 +207,11 @@ int report_error(int code, const char* msg) {
     return fail(code, msg);
 }
 
-namespace {
+// One retaining pool per device: the release threshold is unlimited, so
+// the scratch of repeated calls is not unmapped and re-mapped at every
+// synchronisation; als_scratch_trim hands the unused part back.
 std::mutex g_scratch_mutex;
 cudaMemPool_t g_scratch_pools[256] = {};
-} // namespace
 
 // The library's pool on the current device, created on first use.
 static cudaError_t scratch_pool(cudaMemPool_t* pool) {
@@ -261,6 +265,23 @@ extern "C" {
 
 const char* als_last_error(void) {
     return g_error.c_str();
+}
+
+int als_scratch_trim(int device, unsigned long long keep_bytes) {
+    if (device < 0 || device >= 256) {
+        return fail(ALS_E_INVALID, "invalid device");
+    }
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(als::g_scratch_mutex);
+        pool = als::g_scratch_pools[device];
+    }
+    if (!pool) {
+        return ALS_OK;
+    }
+    DeviceGuard guard(device);
+    ALS_CUDA(cudaMemPoolTrimTo(pool, size_t(keep_bytes)));
+    return ALS_OK;
 }
 
 int als_version(void) {
@@ -564,7 +585,8 @@ namespace {
 // One grid level of a solver: its geometry, its members and its buffers.
 struct SolverLevel {
     als_solver_config cfg;        // this level's n, lower, upper, members
-    als::GridDesc grid;
+    als::GridDesc grid;           // tiles of this level's tile shape
+    int shape = 0;                // tile shape of its stage kernels (stage_kernel.cuh)
     int first = 0;                // global index of its first member
     long long member_elems = 0;   // nvar * plane
     double dx[3];
@@ -586,6 +608,7 @@ struct als_solver {
     int members = 0;              // over all levels
     int subdomains = 0;           // 1: the members are subdomains of one grid (als_solver_decompose)
     int procs[3] = {1, 1, 1};     // subdomains per direction
+    bool needs_state = false;     // split after its state was set: advancing waits for a new one
     int cur = 0;                  // RK2 ping-pong: 1 when U^n of active members sits in B
     als::StepState* state = nullptr;
     als::StepState* host_state = nullptr;  // pinned mirror
@@ -663,20 +686,23 @@ als::LevelDesc solver_level(const als_solver* s, const SolverLevel& L, const voi
     return D;
 }
 
-// Parameters of one stage over every level; `pick` chooses (in, un, out)
-// per level.
+// Parameters of one stage over the levels of tile shape `shape`, in the
+// solver's level order; `pick` chooses (in, un, out) per level.
 template<class Pick>
-als::StageParams solver_params(const als_solver* s, Pick pick) {
+als::StageParams solver_params(const als_solver* s, Pick pick, int shape = 0) {
     als::StageParams P;
     std::memset(&P, 0, sizeof(P));
-    P.nlevels = int(s->levels.size());
-    for (int k = 0; k < P.nlevels; ++k) {
+    P.nlevels = 0;
+    for (size_t k = 0; k < s->levels.size(); ++k) {
         const SolverLevel& L = s->levels[s->order[k]];
+        if (L.shape != shape) {
+            continue;
+        }
         const void* in;
         const void* un;
         void* out;
         pick(L, in, un, out);
-        P.level[k] = solver_level(s, L, in, un, out);
+        P.level[P.nlevels++] = solver_level(s, L, in, un, out);
     }
     P.bc = s->cfg.boundary;
     P.write_ghosts = 1;
@@ -696,26 +722,39 @@ cudaError_t launch_fe_update(als_solver* s, const SolverLevel& L) {
 }
 
 // Enqueues one time step of every level, each stage as one launch over all
-// levels.  FE: FLUX0 + fe_update.  RK2: FLUX0 + RK2_1 into the other buffer
-// (ping-pong).  RK3: FLUX0 + RK3_1 + RK3_2 in place.  With `ev`
-// (launches+1 events), records ev[0] before the first kernel and ev[k]
-// after kernel k.
+// levels of one tile shape (levels of different shapes take one launch per
+// shape, in shape order).  FE: FLUX0 + fe_update.  RK2: FLUX0 + RK2_1 into
+// the other buffer (ping-pong).  RK3: FLUX0 + RK3_1 + RK3_2 in place.  With
+// `ev` (stages+1 events), records ev[0] before the first kernel and ev[k]
+// after the launches of stage k.
+template<class Pick>
+cudaError_t launch_stage_all(const als_solver* s, int kind, Pick pick) {
+    for (int shape = 0; shape < als::kMaxShapes; ++shape) {
+        als::StageParams P = solver_params(s, pick, shape);
+        if (P.nlevels == 0) {
+            continue;
+        }
+        cudaError_t err = launch_stage(s->cfg.precision, s->cfg.dimension, s->cfg.reconstruction,
+            s->cfg.flux, kind, P, s->blocks_per_sm, s->stream, shape);
+        if (err != cudaSuccess) {
+            return err;
+        }
+    }
+    return cudaSuccess;
+}
+
 int enqueue_step(als_solver* s, cudaEvent_t* ev = nullptr) {
     const int prec = s->cfg.precision;
     const int dim = s->cfg.dimension;
-    const int recon = s->cfg.reconstruction;
-    const int flux = s->cfg.flux;
-    const int bps = s->blocks_per_sm;
     if (ev) {
         ALS_CUDA(cudaEventRecord(ev[0], s->stream));
     }
-    als::StageParams P = solver_params(s, [s](const SolverLevel& L, const void*& in,
-                                              const void*& un, void*& out) {
+    ALS_CUDA(launch_stage_all(s, als::KIND_FLUX0, [s](const SolverLevel& L, const void*& in,
+                                                      const void*& un, void*& out) {
         in = s->current(L);
         un = in;
         out = L.buf[1];
-    });
-    ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_FLUX0, P, bps, s->stream));
+    }));
     if (ev) {
         ALS_CUDA(cudaEventRecord(ev[1], s->stream));
     }
@@ -735,32 +774,32 @@ int enqueue_step(als_solver* s, cudaEvent_t* ev = nullptr) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
     } else if (s->cfg.integrator == ALS_INT_RK2) {
-        P = solver_params(s, [s](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+        ALS_CUDA(launch_stage_all(s, als::KIND_RK2_1, [s](const SolverLevel& L, const void*& in,
+                                                          const void*& un, void*& out) {
             in = L.buf[1];
             un = s->current(L);
             out = s->other(L);
-        });
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK2_1, P, bps, s->stream));
+        }));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
         s->cur ^= 1;
     } else {
-        P = solver_params(s, [](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+        ALS_CUDA(launch_stage_all(s, als::KIND_RK3_1, [](const SolverLevel& L, const void*& in,
+                                                         const void*& un, void*& out) {
             in = L.buf[1];
             un = L.buf[0];
             out = L.buf[2];
-        });
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_1, P, bps, s->stream));
+        }));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[2], s->stream));
         }
-        P = solver_params(s, [](const SolverLevel& L, const void*& in, const void*& un, void*& out) {
+        ALS_CUDA(launch_stage_all(s, als::KIND_RK3_2, [](const SolverLevel& L, const void*& in,
+                                                         const void*& un, void*& out) {
             in = L.buf[2];
             un = L.buf[0];
             out = L.buf[0];
-        });
-        ALS_CUDA(launch_stage(prec, dim, recon, flux, als::KIND_RK3_2, P, bps, s->stream));
+        }));
         if (ev) {
             ALS_CUDA(cudaEventRecord(ev[3], s->stream));
         }
@@ -818,6 +857,26 @@ void drop_graph(als_solver* s) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
     }
+}
+
+// Whether the stage kernels of this solver's configuration are built with
+// tile shape `shape`.
+bool shape_available(const als_solver* s, int shape) {
+    return shape >= 0 && shape < als::kMaxShapes &&
+        als::shape_built(s->cfg.dimension, s->cfg.reconstruction, s->cfg.flux, shape);
+}
+
+// Gives level l tile shape shapes[l] (available shapes only) and recovers
+// its tiles; the captured step graph no longer matches.
+void set_level_shapes(als_solver* s, const int* shapes) {
+    for (size_t l = 0; l < s->levels.size(); ++l) {
+        SolverLevel& L = s->levels[l];
+        L.shape = shapes[l];
+        int lo[3] = {0, 0, 0};
+        L.grid = make_grid(s->cfg.dimension, L.grid.n, s->g, lo, L.grid.n, s->cfg.precision,
+            L.shape);
+    }
+    drop_graph(s);
 }
 
 // members [first, first+count) must lie in one level; returns it or -1
@@ -971,6 +1030,9 @@ int als_solver_decompose(als_solver* s, const int* procs) {
     for (int d = 0; d < 3; ++d) {
         s->procs[d] = procs[d];
     }
+    // a state set before the split has its ghosts filled by the boundary
+    // condition, not from the neighbouring subdomains: a new state is due
+    s->needs_state = true;
     return ALS_OK;
 }
 
@@ -1010,10 +1072,23 @@ int als_solver_level(const als_solver* s, int level, int* first_member, int* mem
     return ALS_OK;
 }
 
+// A split grid's subdomains share member 0's clock and read each other's
+// cells as ghosts, so its state is set whole, in one call.
+static int check_split_state(const als_solver* s, int first_member, int count) {
+    if (s->subdomains && (first_member != 0 || count != s->members)) {
+        return fail(ALS_E_INVALID, "a split grid takes the state of all its subdomains in one call");
+    }
+    return ALS_OK;
+}
+
 int als_solver_set_state(als_solver* s, const double* host, int first_member, int count) {
     const int l = s ? range_level(s, first_member, count) : -1;
     if (!s || !host || l < 0) {
         return fail(ALS_E_INVALID, "invalid set_state arguments (members must lie in one level)");
+    }
+    int split_rc = check_split_state(s, first_member, count);
+    if (split_rc != ALS_OK) {
+        return split_rc;
     }
     DeviceGuard guard(s->device);
     const SolverLevel& L = s->levels[l];
@@ -1041,6 +1116,7 @@ int als_solver_set_state(als_solver* s, const double* host, int first_member, in
         }
         ALS_CUDA(cudaStreamSynchronize(s->stream));
     }
+    s->needs_state = false;
     return reset_members(s, first_member, count);
 }
 
@@ -1048,6 +1124,10 @@ int als_solver_set_state_device(als_solver* s, const void* dev, int first_member
     const int l = s ? range_level(s, first_member, count) : -1;
     if (!s || !dev || l < 0) {
         return fail(ALS_E_INVALID, "invalid set_state_device arguments (members must lie in one level)");
+    }
+    int split_rc = check_split_state(s, first_member, count);
+    if (split_rc != ALS_OK) {
+        return split_rc;
     }
     DeviceGuard guard(s->device);
     const SolverLevel& L = s->levels[l];
@@ -1062,6 +1142,7 @@ int als_solver_set_state_device(als_solver* s, const void* dev, int first_member
     if (rc != ALS_OK) {
         return rc;
     }
+    s->needs_state = false;
     return reset_members(s, first_member, count);
 }
 
@@ -1170,6 +1251,9 @@ int als_solver_state_pointer(als_solver* s, void** dev) {
 int als_solver_advance(als_solver* s, long long steps) {
     if (!s || steps < 0) {
         return fail(ALS_E_INVALID, "invalid advance arguments");
+    }
+    if (s->needs_state) {
+        return fail(ALS_E_INVALID, "set the state of the split grid after als_solver_decompose");
     }
     DeviceGuard guard(s->device);
     // whole time steps are captured once into a CUDA graph and replayed; the
@@ -1390,55 +1474,94 @@ int als_solver_get_schedule(const als_solver* s, int* blocks_per_sm, int* level_
     return ALS_OK;
 }
 
-// The schedule autotuner: times `steps` time steps under every candidate
-// (persistent blocks per SM x level order) from the same saved state, keeps
-// the fastest, and restores the state and member clocks, so tuning changes
-// no result.
+int als_solver_set_tiles(als_solver* s, const int* tile_shapes) {
+    if (!s || !tile_shapes) {
+        return fail(ALS_E_INVALID, "null argument");
+    }
+    for (size_t l = 0; l < s->levels.size(); ++l) {
+        if (!shape_available(s, tile_shapes[l])) {
+            return fail(ALS_E_UNSUPPORTED, "tile shape " + std::to_string(tile_shapes[l]) +
+                " is not built for this dimension, reconstruction and flux");
+        }
+    }
+    DeviceGuard guard(s->device);
+    ALS_CUDA(cudaStreamSynchronize(s->stream));
+    set_level_shapes(s, tile_shapes);
+    return ALS_OK;
+}
+
+int als_solver_get_tiles(const als_solver* s, int* tile_shapes, int* tile_extents) {
+    if (!s) {
+        return fail(ALS_E_INVALID, "null solver");
+    }
+    for (size_t l = 0; l < s->levels.size(); ++l) {
+        const SolverLevel& L = s->levels[l];
+        if (tile_shapes) {
+            tile_shapes[l] = L.shape;
+        }
+        if (tile_extents) {
+            for (int d = 0; d < 3; ++d) {
+                tile_extents[3 * l + d] = tile_extent(s->cfg.precision, s->cfg.dimension, d, L.shape);
+            }
+        }
+    }
+    return ALS_OK;
+}
+
+// The schedule autotuner: times `steps` time steps per candidate from the
+// same saved state, keeps the fastest, and restores the state and member
+// clocks, so tuning changes no result.  First the tile shape of each level
+// (coordinate search: one level's shape varied at a time, the others at
+// their best so far), then persistent blocks per SM x level order.
 int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_order,
-    double* best_ms_per_step) {
+    int* tile_shapes, double* best_ms_per_step) {
     if (!s || steps < 1) {
         return fail(ALS_E_INVALID, "invalid tune arguments");
     }
     DeviceGuard guard(s->device);
     ALS_CUDA(cudaStreamSynchronize(s->stream));
-    // save every buffer that holds state, and the member clocks
-    std::vector<void*> saved;
-    size_t total = 0;
+    // save the state buffer of every level (the flux and stage buffers are
+    // rewritten before they are read in every step) and the member clocks;
+    // the copies are freed on every return path
+    struct Saved {
+        std::vector<void*> p;
+        ~Saved() {
+            for (void* q : p) {
+                cudaFree(q);
+            }
+        }
+    } saved;
     for (SolverLevel& L : s->levels) {
         const size_t bytes = size_t(L.member_elems) * L.cfg.members * s->elem;
-        for (int b = 0; b < 3; ++b) {
-            if (!L.buf[b]) {
-                continue;
-            }
-            void* p = nullptr;
-            ALS_CUDA(cudaMalloc(&p, bytes));
-            ALS_CUDA(cudaMemcpyAsync(p, L.buf[b], bytes, cudaMemcpyDeviceToDevice, s->stream));
-            saved.push_back(p);
-            total += bytes;
-        }
+        void* p = nullptr;
+        ALS_CUDA(cudaMalloc(&p, bytes));
+        saved.p.push_back(p);
+        ALS_CUDA(cudaMemcpyAsync(p, s->current(L), bytes, cudaMemcpyDeviceToDevice, s->stream));
     }
-    als::StepState* saved_state = nullptr;
-    ALS_CUDA(cudaMalloc((void**)&saved_state, sizeof(als::StepState) * s->members));
+    void* state_copy = nullptr;
+    ALS_CUDA(cudaMalloc(&state_copy, sizeof(als::StepState) * s->members));
+    saved.p.push_back(state_copy);
+    als::StepState* saved_state = static_cast<als::StepState*>(state_copy);
     ALS_CUDA(cudaMemcpyAsync(saved_state, s->state, sizeof(als::StepState) * s->members,
         cudaMemcpyDeviceToDevice, s->stream));
     const int cur0 = s->cur;
     const int bps0 = s->blocks_per_sm;
     const std::vector<int> order0 = s->order;
+    std::vector<int> shapes0;
+    for (const SolverLevel& L : s->levels) {
+        shapes0.push_back(L.shape);
+    }
 
     auto restore = [&]() -> int {
+        s->cur = cur0;
         size_t k = 0;
         for (SolverLevel& L : s->levels) {
             const size_t bytes = size_t(L.member_elems) * L.cfg.members * s->elem;
-            for (int b = 0; b < 3; ++b) {
-                if (!L.buf[b]) {
-                    continue;
-                }
-                ALS_CUDA(cudaMemcpyAsync(L.buf[b], saved[k++], bytes, cudaMemcpyDeviceToDevice, s->stream));
-            }
+            ALS_CUDA(cudaMemcpyAsync(s->current(L), saved.p[k++], bytes, cudaMemcpyDeviceToDevice,
+                s->stream));
         }
         ALS_CUDA(cudaMemcpyAsync(s->state, saved_state, sizeof(als::StepState) * s->members,
             cudaMemcpyDeviceToDevice, s->stream));
-        s->cur = cur0;
         return ALS_OK;
     };
 
@@ -1461,37 +1584,67 @@ int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_ord
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ALS_CUDA(cudaEventCreate(&e0));
     ALS_CUDA(cudaEventCreate(&e1));
-    double best = 1e300;
+    int rc = ALS_OK;
+    // ms per step of the current shapes, order and blocks per SM (1e300 after an error)
+    auto time_steps = [&]() -> double {
+        if (rc != ALS_OK) {
+            return 1e300;
+        }
+        rc = restore();
+        // one untimed step, then the timed ones
+        for (int k = 0; k < 1 + steps && rc == ALS_OK; ++k) {
+            if (k == 1 && cudaEventRecord(e0, s->stream) != cudaSuccess) {
+                rc = fail(ALS_E_CUDA, "cudaEventRecord failed");
+            }
+            if (rc == ALS_OK) {
+                rc = enqueue_step(s);
+            }
+        }
+        if (rc == ALS_OK && (cudaEventRecord(e1, s->stream) != cudaSuccess ||
+                                cudaEventSynchronize(e1) != cudaSuccess)) {
+            rc = fail(ALS_E_CUDA, "timing failed");
+        }
+        float ms = 0;
+        if (rc == ALS_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = fail(ALS_E_CUDA, "cudaEventElapsedTime failed");
+        }
+        return rc == ALS_OK ? double(ms) / steps : 1e300;
+    };
+    std::vector<int> best_shapes = shapes0;
+    s->order = order0;
+    s->blocks_per_sm = bps0;
+    double best = time_steps();
+    for (size_t l = 0; l < s->levels.size() && rc == ALS_OK; ++l) {
+        for (int shape = 0; shape < als::kMaxShapes && rc == ALS_OK; ++shape) {
+            if (shape == best_shapes[l] || !shape_available(s, shape)) {
+                continue;
+            }
+            std::vector<int> trial = best_shapes;
+            trial[l] = shape;
+            set_level_shapes(s, trial.data());
+            const double ms = time_steps();
+            if (ms < best) {
+                best = ms;
+                best_shapes = trial;
+            }
+        }
+    }
+    set_level_shapes(s, best_shapes.data());
     int best_bps = bps0;
     std::vector<int> best_order = order0;
-    int rc = ALS_OK;
     for (const std::vector<int>& ord : orders) {
         for (int bps : bps_candidates) {
             if (rc != ALS_OK) {
                 break;
             }
+            if (ord == order0 && bps == bps0) {
+                continue;
+            }
             s->order = ord;
             s->blocks_per_sm = bps;
-            rc = restore();
-            // one untimed step, then the timed ones
-            for (int k = 0; k < 1 + steps && rc == ALS_OK; ++k) {
-                if (k == 1 && cudaEventRecord(e0, s->stream) != cudaSuccess) {
-                    rc = fail(ALS_E_CUDA, "cudaEventRecord failed");
-                }
-                if (rc == ALS_OK) {
-                    rc = enqueue_step(s);
-                }
-            }
-            if (rc == ALS_OK && (cudaEventRecord(e1, s->stream) != cudaSuccess ||
-                                    cudaEventSynchronize(e1) != cudaSuccess)) {
-                rc = fail(ALS_E_CUDA, "timing failed");
-            }
-            float ms = 0;
-            if (rc == ALS_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-                rc = fail(ALS_E_CUDA, "cudaEventElapsedTime failed");
-            }
-            if (rc == ALS_OK && ms / steps < best) {
-                best = ms / steps;
+            const double ms = time_steps();
+            if (ms < best) {
+                best = ms;
                 best_bps = bps;
                 best_order = ord;
             }
@@ -1499,14 +1652,10 @@ int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_ord
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    s->order = best_order;
+    s->blocks_per_sm = best_bps;
     int rc2 = restore();
     cudaStreamSynchronize(s->stream);
-    for (void* p : saved) {
-        cudaFree(p);
-    }
-    cudaFree(saved_state);
-    s->blocks_per_sm = best_bps;
-    s->order = best_order;
     drop_graph(s);
     if (rc != ALS_OK) {
         return rc;
@@ -1522,10 +1671,14 @@ int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_ord
             level_order[k] = best_order[k];
         }
     }
+    if (tile_shapes) {
+        for (size_t k = 0; k < best_shapes.size(); ++k) {
+            tile_shapes[k] = best_shapes[k];
+        }
+    }
     if (best_ms_per_step) {
         *best_ms_per_step = best;
     }
-    (void)total;
     return ALS_OK;
 }
 

@@ -204,9 +204,12 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
     } else if (sR < R(0)) {
         point_flux<R, NSD, D>(Rt, F);
     } else {
-        R FL[NV], FR[NV];
-        point_flux<R, NSD, D>(L, FL);
-        point_flux<R, NSD, D>(Rt, FR);
+        // Of the two point fluxes only the transverse momentum components
+        // (c[1+k] * ud, k != D: Euler.hpp:172-181 adds p along D only) enter
+        // before the star side is chosen; the chosen side's full point flux
+        // is formed after the choice.  Each value is the same product the
+        // reference forms, so the result is unchanged, and the two flux
+        // vectors are never live together.
         const R udl = L.ud - sL;
         const R udr = Rt.ud - sR;
         const R aa = udr * Rt.c[0] - udl * L.c[0];
@@ -220,14 +223,17 @@ __device__ __forceinline__ R flux_hll3(const FaceState<R, NSD>& L, const FaceSta
             if (k == D) {
                 us[k] = sm;
             } else {
-                us[k] = over_aa(FR[1 + k] - FL[1 + k] - sR * Rt.c[1 + k] + sL * L.c[1 + k]);
+                const R fr = Rt.c[1 + k] * Rt.ud;
+                const R fl = L.c[1 + k] * L.ud;
+                us[k] = over_aa(fr - fl - sR * Rt.c[1 + k] + sL * L.c[1 + k]);
             }
         }
         const bool left = sm >= R(0);
         const FaceState<R, NSD>& S = left ? L : Rt;
         const R sK = left ? sL : sR;
         const R udk = left ? udl : udr;
-        const R* FK = left ? FL : FR;
+        R FK[NV];
+        point_flux<R, NSD, D>(S, FK);
         const R den = sm - sK;
         const R iden = fast_recip<R>() ? R(1) / den : R(0);
         auto over_den = [&](R x) { return fast_recip<R>() ? x * iden : x / den; };

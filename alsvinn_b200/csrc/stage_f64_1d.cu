@@ -2,12 +2,12 @@
 #include "stage_dispatch.cuh"
 
 namespace als {
-cudaError_t launch_stage_f64_1d(int recon, int flux, int kind, const StageParams& P,
-    int blocks_per_sm, cudaStream_t s) {
-    return launch_stage_dim<double, 1>(recon, flux, kind, P, blocks_per_sm, s);
+cudaError_t launch_stage_f64_1d(int recon, int flux, int kind, int shape,
+    const StageParams& P, int blocks_per_sm, cudaStream_t s) {
+    return launch_stage_dim<double, 1>(recon, flux, kind, shape, P, blocks_per_sm, s);
 }
 
-void stage_tile_f64_1d(int* tile) {
-    stage_tile_dim<1>(tile);
+void stage_tile_f64_1d(int shape, int* tile) {
+    stage_tile_dim<1>(shape, tile);
 }
 } // namespace als

@@ -61,13 +61,25 @@ namespace als {
 #ifndef ALS_STAGE2_BLOCKS
 #define ALS_STAGE2_BLOCKS 2
 #endif
-template<int DIM> struct TileShape;
-template<> struct TileShape<1> {
+// SHAPE 0 is each dimension's default tile.  2-D also builds SHAPE 1, a
+// 16 x 16 tile of 288 threads: more halo work per cell than 32 x 16, but
+// more resident blocks per SM and finer work items, which can pay on small
+// grids or many members; the schedule tuner chooses per grid level
+// (als_solver_tune).  Measured alone on KH 1024^2 (FP64, ms per RK3 step):
+// 32 x 16 0.407, 16 x 16 0.438.
+#ifndef ALS_STAGE2S_BLOCKS
+#define ALS_STAGE2S_BLOCKS 3
+#endif
+template<int DIM, int SHAPE = 0> struct TileShape;
+template<> struct TileShape<1, 0> {
     static constexpr int X = 256, Y = 1, Z = 1, T = 256, B = 4;
 };
-template<> struct TileShape<2> {
+template<> struct TileShape<2, 0> {
     static constexpr int X = ALS_TILE2_X, Y = ALS_TILE2_Y, Z = 1, T = ALS_STAGE2_THREADS,
         B = ALS_STAGE2_BLOCKS;
+};
+template<> struct TileShape<2, 1> {
+    static constexpr int X = 16, Y = 16, Z = 1, T = 288, B = ALS_STAGE2S_BLOCKS;
 };
 #ifndef ALS_TILE3_X
 #define ALS_TILE3_X 8
@@ -93,25 +105,35 @@ template<> struct TileShape<2> {
 #ifndef ALS_STAGE3_BLOCKS
 #define ALS_STAGE3_BLOCKS 2
 #endif
-template<> struct TileShape<3> {
+template<> struct TileShape<3, 0> {
     static constexpr int X = ALS_TILE3_X, Y = ALS_TILE3_Y, Z = ALS_TILE3_Z, T = ALS_STAGE3_THREADS,
         B = ALS_STAGE3_BLOCKS;
 };
 
-template<class R, int DIM, int RECON, int FLUX>
+
+// Shapes built per (dimension, reconstruction, flux): the default for every
+// combination, the 2-D alternative for WENO2 with HLL, HLL3 and Central
+// (the ensemble and benchmark configurations).
+__host__ __device__ constexpr bool shape_built(int dim, int recon, int flux, int shape) {
+    return shape == 0 || (shape == 1 && dim == 2 && recon == RECON_WENO2 &&
+        (flux == FLUX_HLL || flux == FLUX_HLL3 || flux == FLUX_CENTRAL));
+}
+constexpr int kMaxShapes = 2;
+
+template<class R, int DIM, int RECON, int FLUX, int SHAPE = 0>
 struct StageLayout {
     static constexpr int NV = DIM + 2;
     static constexpr int G = stage_ghosts(RECON, FLUX);
     static constexpr bool STENCIL = stencil_flux(FLUX);
-    static constexpr int TX = TileShape<DIM>::X;
-    static constexpr int TY = TileShape<DIM>::Y;
-    static constexpr int TZ = TileShape<DIM>::Z;
+    static constexpr int TX = TileShape<DIM, SHAPE>::X;
+    static constexpr int TY = TileShape<DIM, SHAPE>::Y;
+    static constexpr int TZ = TileShape<DIM, SHAPE>::Z;
     static constexpr int BX = TX + 2 * G;
     static constexpr int BY = DIM > 1 ? TY + 2 * G : 1;
     static constexpr int BZ = DIM > 2 ? TZ + 2 * G : 1;
     static constexpr int BOX = BX * BY * BZ;
     static constexpr int CELLS = TX * TY * TZ;
-    static constexpr int THREADS = TileShape<DIM>::T;
+    static constexpr int THREADS = TileShape<DIM, SHAPE>::T;
     static constexpr int CPT = (CELLS + THREADS - 1) / THREADS;  // cells per thread
     // reconstructed cells / faces per direction: the tile extent grows by 2 / 1 along it
     static constexpr int REC0 = (TX + 2) * TY * TZ;
@@ -129,7 +151,8 @@ struct StageLayout {
     // resident blocks per SM the shared memory allows (228 KB per SM, 1 KB
     // reserved per block), capped; the register budget is sized to match
     static constexpr int BY_SMEM = int((228 * 1024) / (SMEM + 1024));
-    static constexpr int BLOCKS = BY_SMEM < 1 ? 1 : (BY_SMEM > TileShape<DIM>::B ? TileShape<DIM>::B : BY_SMEM);
+    static constexpr int BLOCKS = BY_SMEM < 1 ? 1
+        : (BY_SMEM > TileShape<DIM, SHAPE>::B ? TileShape<DIM, SHAPE>::B : BY_SMEM);
 };
 
 // dt of the step (Integrator.cpp:20-46) followed by the end-time clamp
@@ -292,10 +315,11 @@ __device__ __forceinline__ R warp_max(R v) {
     return v;
 }
 
-template<class R, int DIM, int RECON, int FLUX, int KIND, int D>
+template<class R, int DIM, int RECON, int FLUX, int SHAPE, int KIND, int D>
 __device__ __forceinline__ void stage_direction(const GridDesc& gd, R gamma, const R* box, R* rec,
-    R* flx, R (&acc)[StageLayout<R, DIM, RECON, FLUX>::CPT][DIM + 2], R& wmax, int x0, int y0, int z0) {
-    typedef StageLayout<R, DIM, RECON, FLUX> Lay;
+    R* flx, R (&acc)[StageLayout<R, DIM, RECON, FLUX, SHAPE>::CPT][DIM + 2], R& wmax, int x0, int y0,
+    int z0) {
+    typedef StageLayout<R, DIM, RECON, FLUX, SHAPE> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
     // extents of the reconstructed-cell index space (x fastest), offset -1 along D
@@ -424,10 +448,10 @@ __device__ __forceinline__ void finish_step(StepState* st) {
 }
 
 // One work item: tile `tile` of member `member` of level L.
-template<class R, int DIM, int RECON, int FLUX, int KIND>
+template<class R, int DIM, int RECON, int FLUX, int SHAPE, int KIND>
 __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc& L, int tile,
     int member, unsigned char* smem) {
-    typedef StageLayout<R, DIM, RECON, FLUX> Lay;
+    typedef StageLayout<R, DIM, RECON, FLUX, SHAPE> Lay;
     constexpr int NV = Lay::NV;
     constexpr int G = Lay::G;
     constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
@@ -506,12 +530,15 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         }
     }
     R wmax[3] = {R(0), R(0), R(0)};
-    stage_direction<R, DIM, RECON, FLUX, KIND, 0>(gd, gamma, box, rec, flx, acc, wmax[0], x0, y0, z0);
+    stage_direction<R, DIM, RECON, FLUX, SHAPE, KIND, 0>(gd, gamma, box, rec, flx, acc, wmax[0], x0,
+        y0, z0);
     if (DIM > 1) {
-        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 1 ? 1 : 0)>(gd, gamma, box, rec, flx, acc, wmax[1], x0, y0, z0);
+        stage_direction<R, DIM, RECON, FLUX, SHAPE, KIND, (DIM > 1 ? 1 : 0)>(gd, gamma, box, rec, flx,
+            acc, wmax[1], x0, y0, z0);
     }
     if (DIM > 2) {
-        stage_direction<R, DIM, RECON, FLUX, KIND, (DIM > 2 ? 2 : 0)>(gd, gamma, box, rec, flx, acc, wmax[2], x0, y0, z0);
+        stage_direction<R, DIM, RECON, FLUX, SHAPE, KIND, (DIM > 2 ? 2 : 0)>(gd, gamma, box, rec, flx,
+            acc, wmax[2], x0, y0, z0);
     }
 
     bool bad = false;
@@ -565,7 +592,13 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         for (int v = 0; v < NV; ++v) {
             outp(v)[idx] = val[v];
         }
-        if (P.write_ghosts) {
+        // a cell at least G' = gd.ghosts cells from every side of its grid
+        // has no boundary image (only the cells of the outer shell do)
+        const int gw = gd.ghosts;
+        const bool shell = gx < gw || gx >= gd.n[0] - gw ||
+            (DIM > 1 && (gy < gw || gy >= gd.n[1] - gw)) ||
+            (DIM > 2 && (gz < gw || gz >= gd.n[2] - gw));
+        if (P.write_ghosts && shell) {
             int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
             int sx[3] = {0, 0, 0}, sy[3] = {0, 0, 0}, sz[3] = {0, 0, 0};
             int nxi, nyi = 1, nzi = 1;
@@ -666,7 +699,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
 
 // Work item w of the launch: its level, member and tile, skipping members
 // that are done.
-template<class R, int DIM, int RECON, int FLUX, int KIND>
+template<class R, int DIM, int RECON, int FLUX, int SHAPE, int KIND>
 __device__ __forceinline__ void stage_item(const StageParams& P, long long w, unsigned char* smem) {
     int l = 0;
 #pragma unroll
@@ -685,7 +718,7 @@ __device__ __forceinline__ void stage_item(const StageParams& P, long long w, un
             return;
         }
     }
-    stage_tile<R, DIM, RECON, FLUX, KIND>(P, L, tile, member, smem);
+    stage_tile<R, DIM, RECON, FLUX, SHAPE, KIND>(P, L, tile, member, smem);
 }
 
 // Two launch modes.  Without a work counter every block takes the work item
@@ -693,8 +726,9 @@ __device__ __forceinline__ void stage_item(const StageParams& P, long long w, un
 // the launch is persistent: a fixed number of resident blocks take items
 // from the counter until the list is exhausted, and the last block to
 // leave resets the counter for the next launch.
-template<class R, int DIM, int RECON, int FLUX, int KIND>
-__global__ void __launch_bounds__((StageLayout<R, DIM, RECON, FLUX>::THREADS), (StageLayout<R, DIM, RECON, FLUX>::BLOCKS))
+template<class R, int DIM, int RECON, int FLUX, int KIND, int SHAPE = 0>
+__global__ void __launch_bounds__((StageLayout<R, DIM, RECON, FLUX, SHAPE>::THREADS),
+    (StageLayout<R, DIM, RECON, FLUX, SHAPE>::BLOCKS))
 stage_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ long long item;
@@ -704,7 +738,7 @@ stage_kernel(const StageParams P) {
     __syncthreads();
     // one call site, so the tile code is inlined once
     for (long long w = item; w < P.total_work;) {
-        stage_item<R, DIM, RECON, FLUX, KIND>(P, w, smem);
+        stage_item<R, DIM, RECON, FLUX, SHAPE, KIND>(P, w, smem);
         if (!P.counter) {
             break;
         }

@@ -6,8 +6,8 @@ Samples are independent, so the only exchange is the statistics at the end:
   reference's SimpleLoadBalancer (alsuq/src/mpi/SimpleLoadBalancer.cpp:35-97),
   including its requirement that the world size divides the sample count;
 * ``gather_moments``: every rank's Welford (n, mean, M2) gathered on every
-  rank with one all_gather per array (NCCL over NVLink for device tensors,
-  gloo for host tensors);
+  rank with one all_gather per array (NCCL over NVLink straight from device
+  memory; with a gloo group the arrays are staged through host memory);
 * ``merge_statistics``: a fresh FP64 accumulator into which all ranks'
   moments are Chan-merged in rank order on the device, so every rank holds
   the same bits.  The reference instead MPI_Reduces raw sums S1, S2 to rank 0
@@ -73,21 +73,40 @@ def samples_for_rank(total, world, rank):
     return rank * per, per
 
 
-def gather_moments(n, mean, m2, group=None):
-    """All ranks' (n, mean, M2), in rank order, on every rank.
+def _exchange_device(group=None):
+    """Where the collectives of `group` take their tensors: the current CUDA
+    device for NCCL, the host for gloo."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
 
-    ``mean`` and ``m2`` are FP64 tensors of the same length on every rank
-    (device tensors with NCCL, host tensors with gloo)."""
+
+def all_gather_tensor(x, group=None):
+    """All ranks' copies of tensor `x` (same shape on every rank), in rank
+    order, on x's device; staged through the host for gloo."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
+    via = _exchange_device(group)
+    xs = x.contiguous().to(via)
+    parts = [torch.empty_like(xs) for _ in range(world)]
+    dist.all_gather(parts, xs, group=group)
+    return [p.to(x.device) for p in parts]
+
+
+def gather_moments(n, mean, m2, group=None):
+    """All ranks' (n, mean, M2), in rank order, on every rank.
+
+    ``mean`` and ``m2`` are FP64 tensors of the same length on every rank;
+    the gathered arrays are returned on their device (NCCL exchanges device
+    memory directly, gloo through host copies)."""
+    import torch
     ns = torch.tensor([int(n)], dtype=torch.int64, device=mean.device)
-    n_all = [torch.zeros_like(ns) for _ in range(world)]
-    dist.all_gather(n_all, ns, group=group)
-    mean_all = [torch.empty_like(mean) for _ in range(world)]
-    dist.all_gather(mean_all, mean.contiguous(), group=group)
-    m2_all = [torch.empty_like(m2) for _ in range(world)]
-    dist.all_gather(m2_all, m2.contiguous(), group=group)
+    n_all = all_gather_tensor(ns, group)
+    mean_all = all_gather_tensor(mean, group)
+    m2_all = all_gather_tensor(m2, group)
     return [int(v.item()) for v in n_all], mean_all, m2_all
 
 
@@ -161,12 +180,8 @@ def kh_observable_ensemble(n, total_samples, precision="fp64", end_time=2.0, gro
     var = torch.zeros_like(mean)
     merged.result(mean, var)
     merged.close()
-    yt = torch.as_tensor(y, dtype=torch.float64, device="cuda")
-    ys = [torch.empty_like(yt) for _ in range(world)]
-    dist.all_gather(ys, yt, group=group)
-    pt = torch.as_tensor(params, dtype=torch.float64, device="cuda")
-    ps = [torch.empty_like(pt) for _ in range(world)]
-    dist.all_gather(ps, pt, group=group)
+    ys = all_gather_tensor(torch.as_tensor(y, dtype=torch.float64, device="cuda"), group)
+    ps = all_gather_tensor(torch.as_tensor(params, dtype=torch.float64, device="cuda"), group)
     shape = info["shape"]
     info["field_mean"] = mean.cpu().numpy().reshape(shape)
     info["field_var"] = var.cpu().numpy().reshape(shape)

@@ -205,14 +205,32 @@ class Simulator:
         _lib.check(self._lib.als_solver_get_schedule(self._h, ctypes.byref(bps), order))
         return {"blocks_per_sm": bps.value, "level_order": list(order)}
 
+    def set_tiles(self, shapes):
+        """Tile shape per level (0: the default; 1: 16x16 cells, 2-D WENO2 only)."""
+        arr = (ctypes.c_int * len(self.levels))(*[int(v) for v in shapes])
+        _lib.check(self._lib.als_solver_set_tiles(self._h, arr))
+
+    def tiles(self):
+        """{"shapes": [shape per level], "extents": [(x, y, z) tile cells per level]}."""
+        nl = len(self.levels)
+        shapes = (ctypes.c_int * nl)()
+        ext = (ctypes.c_int * (3 * nl))()
+        _lib.check(self._lib.als_solver_get_tiles(self._h, shapes, ext))
+        return {"shapes": list(shapes),
+                "extents": [tuple(ext[3 * k:3 * k + 3]) for k in range(nl)]}
+
     def tune(self, steps=3):
-        """Runs the schedule autotuner (state and clocks are restored)."""
+        """Runs the schedule autotuner (tile shape per level, blocks per SM,
+        level order); state and clocks are restored."""
+        nl = len(self.levels)
         bps = ctypes.c_int()
-        order = (ctypes.c_int * len(self.levels))()
+        order = (ctypes.c_int * nl)()
+        shapes = (ctypes.c_int * nl)()
         ms = ctypes.c_double()
-        _lib.check(self._lib.als_solver_tune(self._h, int(steps), ctypes.byref(bps), order,
+        _lib.check(self._lib.als_solver_tune(self._h, int(steps), ctypes.byref(bps), order, shapes,
                                              ctypes.byref(ms)))
-        return {"blocks_per_sm": bps.value, "level_order": list(order), "ms_per_step": ms.value}
+        return {"blocks_per_sm": bps.value, "level_order": list(order),
+                "tile_shapes": list(shapes), "ms_per_step": ms.value}
 
     def write_netcdf(self, basename, snapshot=0, member=0):
         """Writes member's state to <basename>_<snapshot>.nc (NetCDFWriter layout)."""

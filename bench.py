@@ -124,6 +124,44 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def fp64_issue_peak():
+    """(FP64 thread instructions/s, source): 148 SMs x 64 FP64 lanes per
+    clock (half the 128 FP32 lanes; B200's 37 TFLOP/s FP64 = 2 flops per
+    FMA lane) at the measured maximum SM clock."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    mhz, src = 1965.0, "nominal clock"
+    if os.path.exists(path):
+        with open(path) as f:
+            mhz = json.load(f).get("sm_max_mhz", mhz)
+        src = "sm_max_mhz of MEASURED_PEAKS.json"
+    return 148 * 64 * mhz * 1e6, "148 SMs x 64 FP64 lanes/clock x %.0f MHz (%s)" % (mhz, src)
+
+
+def fp64_roofline(dom, cells, hbm_peak, peak_kind, traffic, per_kernel):
+    """The binding ceiling of the plain FP64 method: FP64 instruction issue.
+    achieved = FP64 thread instructions per cell and stage (ncu
+    sm__sass_thread_inst_executed_op_fp64_pred_on over a launch, divided by
+    its cells; profiles/traffic_kh1024.json) x cells / the stage kernel's
+    event duration.  The HBM fraction of the same launch stands beside it."""
+    tpath = os.path.join(ROOT, "profiles", "traffic_kh1024.json")
+    per_cell = None
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            per_cell = json.load(f).get("fp64_inst_per_cell", {}).get(dom["kernel"])
+    peak, src = fp64_issue_peak()
+    out = {"bound": "fp64", "unit": "FP64 thread-inst/s", "peak": peak, "peak_source": src,
+           "kernel": "stage kernel '%s' (%.4f ms)" % (dom["kernel"], dom["ms"])}
+    if per_cell:
+        out["achieved"] = per_cell * cells / (dom["ms"] * 1e-3)
+        out["frac"] = out["achieved"] / peak
+        out["fp64_inst_per_cell"] = per_cell
+    out["hbm"] = {"achieved": dom["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                  "frac": dom["achieved_gbs"] / hbm_peak, "traffic": traffic,
+                  "peak_source": peak_kind}
+    out["per_kernel"] = per_kernel
+    return out
+
+
 def kh_state(sample):
     import alsvinn_b200 as als
     params = als.uniform_draws(40, sample, 1)[0]
@@ -177,7 +215,6 @@ def cpu_baseline(state, target_seconds=12.0):
 def run_reference_arm(args, rank):
     if rank != 0:
         return
-    state = kh_state(0)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_lib import RefOracle, ref_library_path
     if not os.path.exists(ref_library_path()):
@@ -187,6 +224,11 @@ def run_reference_arm(args, rank):
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     ref = RefOracle()
+    # the sample's parameters from the reference's own generator
+    # (STLMersenne.cpp:38-85); the initial-data formula is plain NumPy, so
+    # this arm loads none of the B200 library
+    import alsvinn_b200.initial_data as init
+    state = init.kelvin_helmholtz(N, ref.stlmersenne(40, 0, 1)[0], GHOSTS)
     # each bench step: one full KH 1024^2 time step by the reference's CPU code
     ref.simulate(DIM, (N, N), (0, 0), (1, 1), FLUX, RECON, INTEG, BC, 1.4, CFL, 2.0, state,
                  max_steps=args.warmup)
@@ -416,6 +458,7 @@ def run_uq(args, rank, world, local):
     t_cv = info_cv["solve_seconds"] + t_train + t_moments + t_eval
     per_sample = t_plain / M
     t_cv_with_data = t_cv + 1024 * per_sample
+    curve = uq_error_curve(y_or, fj, m1, m2, per_sample, t_train + t_moments)
     result = {
         "metric": "UQ time-to-error, plain batched MC / surrogate control variate "
                   "(KH %d^2, T=%g, mean and variance of mean rho over [0.25,0.75]^2)" % (n, T),
@@ -442,6 +485,7 @@ def run_uq(args, rank, world, local):
                    "seconds_moments": t_moments, "seconds_eval": t_eval},
             "ratio_including_training_data": t_plain / t_cv_with_data,
             "per_sample_seconds": per_sample,
+            "time_to_error_curve": curve,
         },
         # stage launches of both solves, plus the surrogate's (about 20 per
         # training step, 6 per inference chunk of 32768 rows)
@@ -450,6 +494,41 @@ def run_uq(args, rank, world, local):
         "clocks": clock_info,
     }
     print(json.dumps(result, default=float))
+
+
+def uq_error_curve(y_or, f_held, f_mean, f2_mean, per_sample, cv_fixed_seconds,
+                   counts=(128, 256, 512, 1024)):
+    """Errors of both estimators against the 4096-sample FP64 oracle at
+    several sample counts, over disjoint repetitions drawn from the held-out
+    samples 2048..4095 (their FP64 observables and surrogate values; no
+    training sample is reused).  Each point: sample count, RMS error of the
+    mean and of the variance over the repetitions for plain MC and for the
+    control variate, and the GPU wall-clock each arm needs for that count
+    (per-sample solve time of this run; the control variate adds its
+    training and E[f], E[f^2] passes)."""
+    from alsvinn_b200 import uq
+    mu, var = uq.plain_mc(y_or)
+    held = y_or[2048:]
+    out = []
+    for M in counts:
+        reps = held.size // M
+        ep, ev, cp, cv = [], [], [], []
+        for r in range(reps):
+            y = held[r * M:(r + 1) * M]
+            f = f_held[r * M:(r + 1) * M]
+            m_pl, v_pl = uq.plain_mc(y)
+            m_cv, v_cv, _, _ = uq.control_variate(y, f, f_mean, f2_mean)
+            ep.append(m_pl - mu)
+            ev.append(v_pl - var)
+            cp.append(m_cv - mu)
+            cv.append(v_cv - var)
+        rms = lambda e: float(np.sqrt(np.mean(np.square(e))))  # noqa: E731
+        out.append({"samples": M, "repetitions": reps,
+                    "plain": {"rms_err_mean": rms(ep), "rms_err_var": rms(ev),
+                              "seconds": M * per_sample},
+                    "cv": {"rms_err_mean": rms(cp), "rms_err_var": rms(cv),
+                           "seconds": M * per_sample + cv_fixed_seconds}})
+    return out
 
 
 def run_surrogate(args, rank, world, local):
@@ -685,6 +764,23 @@ def main():
         clock_info = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(step_ms)
+    merge_ms = None
+    if world > 1:
+        # the ensemble's end: FP64 Welford statistics of the members, merged
+        # across the ranks in rank order (NCCL all_gather + Chan merge)
+        from alsvinn_b200 import distributed
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record()
+        mv = als.MeanVariance(NVAR * sim.plane, device=local)
+        mv.add_solver(sim, 0)
+        merged = distributed.merge_statistics(mv)
+        merged.close()
+        mv.close()
+        m1.record()
+        torch.cuda.synchronize()
+        merge_ms = m0.elapsed_time(m1)
+        total_ms += merge_ms
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -739,13 +835,10 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Kelvin-Helmholtz initial data, sample index = rank)",
-        "config": dict(WORKLOAD, parallelism="independent ensemble members per GPU (replicas)"),
-        "roofline": {"bound": "hbm", "achieved": roof[dom]["achieved_gbs"],
-                     "peak": hbm_peak, "unit": "GB/s",
-                     "frac": roof[dom]["achieved_gbs"] / hbm_peak, "traffic": traffic,
-                     "kernel": "stage kernel '%s' (%.4f ms)" % (roof[dom]["kernel"], roof[dom]["ms"]),
-                     "peak_source": peak_kind, "per_kernel": roof,
-                     "note": "FP64 divide/sqrt-bound; HBM fraction is of measured copy bandwidth"},
+        "config": WORKLOAD,
+        "sharding": "one ensemble member per GPU (sample index = rank); with N > 1 the "
+                    "timed region ends with the FP64 statistics merge across ranks",
+        "roofline": fp64_roofline(roof[dom], cells, hbm_peak, peak_kind, traffic, roof),
         "e2e": {"value": world * cells * e2e_steps / e2e_secs, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": state_bytes / e2e_steps,
                 "d2h_bytes_per_step": state_bytes / e2e_steps,
@@ -755,6 +848,8 @@ def main():
         "schedule": schedule,
         "clocks": clock_info,
     }
+    if merge_ms is not None:
+        result["statistics_merge_ms"] = merge_ms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the CPU baseline is timed at N = 1 only
         result["cpu_baseline"] = cpu_baseline(state)

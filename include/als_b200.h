@@ -60,6 +60,13 @@ extern "C" {
 
 const char* als_last_error(void);
 int als_version(void);
+/* Scratch memory of the entry points that need temporary device memory
+ * (functionals, structure functions, region sums) comes from one retaining
+ * pool per device: it keeps the largest amount any call needed until the
+ * process exits, hidden from other allocators.  This hands the unused part
+ * of `device`'s pool back until at most `keep_bytes` stay reserved.  It has
+ * no counterpart in the reference (its volumes allocate per object). */
+int als_scratch_trim(int device, unsigned long long keep_bytes);
 
 /* Ghost width of a flux/reconstruction pair: max(stencil-1, reconstruction
  * ghosts).  Replaces NumericalFlux::getNumberOfGhostCells,
@@ -117,8 +124,10 @@ int als_compute_flux(const als_grid* grid, int flux, int reconstruction, const d
  * wave-speed accumulators live in a fixed 24 KiB device array inside the
  * library that every GPU loading it keeps until the process exits; no
  * cudaMalloc, cudaFree or allocating routine is called.  The first call on a
- * device looks the array's address up (cudaGetSymbolAddress): make that first
- * call before any stream capture.  Calls share the array and the call
+ * device looks the array's address up (cudaGetSymbolAddress) in the
+ * runtime's primary context of that device, which later calls on that
+ * device use: make that first call before any stream capture, and call it
+ * only with the primary context current.  Calls share the array and the call
  * clears what it uses; calls on one device from several threads take
  * turns (a lock held from the clearing of the array to the read-back), and
  * the call synchronises `stream` before it returns.  More than 1024 states
@@ -255,13 +264,25 @@ int als_solver_profile_step(als_solver* s, float* kernel_ms, int capacity);
  * work list (a permutation, NULL = as created). */
 int als_solver_set_schedule(als_solver* s, int blocks_per_sm, const int* level_order);
 int als_solver_get_schedule(const als_solver* s, int* blocks_per_sm, int* level_order);
-/* Autotuner: times `steps` steps under every candidate schedule (blocks per
- * SM in {0 (one per item), 1, 2, 3, 4} x level order in {as created, finest
- * first, coarsest first}) from the same saved state, keeps the fastest and
- * restores the state and member clocks, so results are unchanged.  Returns
- * the choice and its ms per step. */
+/* Tile shape of each level's stage kernels: 0 is every dimension's default
+ * (1-D 256, 2-D 32x16, 3-D 8x8x4 cells); 2-D WENO2 with HLL, HLL3 or
+ * Central also has shape 1 (16x16 cells, 288 threads).  Levels of
+ * different shapes take one launch per shape and stage.  The shape changes
+ * no result.  set returns ALS_E_UNSUPPORTED for a shape not built for the
+ * configuration; get fills tile_shapes[level] and tile_extents[3*level + d]
+ * (either may be NULL). */
+int als_solver_set_tiles(als_solver* s, const int* tile_shapes);
+int als_solver_get_tiles(const als_solver* s, int* tile_shapes, int* tile_extents);
+/* Autotuner: times `steps` steps per candidate from the same saved state,
+ * keeps the fastest and restores the state and member clocks, so results
+ * are unchanged.  It searches the tile shape of each level first (one level
+ * varied at a time, the others at their best so far), then blocks per SM in
+ * {0 (one per item), 1, 2, 3, 4} x level order in {as created, finest
+ * first, coarsest first}.  Returns the choice (any out pointer may be NULL)
+ * and its ms per step.  This replaces the reference's serial sample loop
+ * (alsuq/src/run/Runner.cpp:42-78), which has no schedule to choose. */
 int als_solver_tune(als_solver* s, int steps, int* blocks_per_sm, int* level_order,
-    double* best_ms_per_step);
+    int* tile_shapes, double* best_ms_per_step);
 /* FP64 sums of every conserved variable over the interior box [lo, hi)
  * (interior cell coordinates; NULL = whole interior) of members
  * [first_member, first_member+count) of one level: out[k*nvar + v].  The

@@ -1,0 +1,77 @@
+"""Generates tests/golden/final_time_*.npz: final-time results of the
+reference's own CPU time loop on the Kelvin-Helmholtz configurations.
+
+TEST INFRASTRUCTURE ONLY.  Run where the reference tree is available:
+
+    make -C oracle ref && python tests/golden/make_final_time.py [uq256] [kh1024]
+
+The reference build (oracle/_ref/libalsref.so: NumericalFluxCPU with
+HLL3, ReconstructionCPU with WENO2, RungeKutta3, BoundaryCPU periodic,
+driven like Simulator::incrementSolution, alsfvm/src/simulator/
+Simulator.cpp:191-214, with the end-time clamp of
+alsfvm/src/io/FixedIntervalWriter.cpp:45-53) runs each case to T = 2:
+
+* kh1024: KH 1024^2, parameters = alsuq STLMersenne sample 0, CFL 0.4
+  (about 23k steps; about half an hour on eight host cores);
+* uq256_<s>: KH 256^2 members s = 7 and 4095 of the 4096-sample UQ
+  oracle ensemble (parameters = STLMersenne sample s), CFL 0.4.
+
+What is stored, and why it is enough, is described in tests/final_time.py.
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import final_time as ft  # noqa: E402
+from oracle_lib import RefOracle  # noqa: E402
+
+CFL = 0.4
+END_TIME = 2.0
+
+
+def run_case(ref, name, n, sample):
+    import alsvinn_b200.initial_data as init
+    params = np.asarray(ref.stlmersenne(40, sample, 1)[0])
+    U_gen = init.kelvin_helmholtz(n, params, ft.GHOSTS, ft.GAMMA)
+    lo, hi = ft.band_limits_of(U_gen, n)
+    U0 = ft.kh_state_from_bands(n, lo, hi)
+    assert np.array_equal(U0, U_gen), "band reconstruction differs from the generator"
+    t0 = time.perf_counter()
+    rc, U, dts, steps, t = ref.simulate(2, (n, n), (0.0, 0.0), (1.0, 1.0), "hll3", "weno2",
+                                        "rungekutta3", "periodic", ft.GAMMA, CFL, END_TIME, U0,
+                                        dts_capacity=200000)
+    seconds = time.perf_counter() - t0
+    assert rc == 0, name
+    assert len(dts) == steps
+    s = ft.summary(U, n)
+    out = dict(n=n, sample=sample, params=params, band_lo=lo, band_hi=hi, ghosts=ft.GHOSTS,
+               gamma=ft.GAMMA, cfl=CFL, end_time=END_TIME, flux="hll3", recon="weno2",
+               integrator="rungekutta3", bc="periodic", steps=steps, t=t,
+               dts_sha256=ft.dts_digest(dts), dts_head=dts[:64], dts_tail=dts[-64:],
+               dts_min=dts.min(), dts_max=dts.max(), l1=s["l1"], sums=s["sums"],
+               block_sums=s["block_sums"], interior_sha256=s["interior_sha256"],
+               block=ft.BLOCK, observable=ft.observable(U, n), ref_loop_seconds=seconds,
+               ref_threads=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())))
+    np.savez_compressed(ft.fixture_path(name), **out)
+    print("%s: %d steps, t=%r, %.1f s, observable %.17g, sha %s"
+          % (name, steps, t, seconds, out["observable"], s["interior_sha256"][:16]))
+
+
+def main(which):
+    ref = RefOracle()
+    if "uq256" in which:
+        for s in (7, 4095):
+            run_case(ref, "uq256_%d" % s, 256, s)
+    if "kh1024" in which:
+        run_case(ref, "kh1024", 1024, 0)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["uq256", "kh1024"])

@@ -116,3 +116,22 @@ def test_split_solver_rejects_what_it_cannot_run():
             sim.decompose((2, 2))
         with pytest.raises(_lib.AlsError):
             sim.decompose((1, 1, 3))
+
+
+def test_split_solver_wants_its_whole_state_after_the_split():
+    """A state set before the split has ghosts from the boundary condition,
+    not from the neighbouring subdomains: advancing is refused until the
+    whole split state is set again, and a split state is set in one call."""
+    st = np.stack([smooth_random_state(5 + r, 2, (16, 16), 2) for r in range(4)])
+    with als.Simulator(2, (16, 16), members=4, end_time=0.01) as sim:
+        sim.set_state(st)
+        sim.decompose((2, 2))
+        with pytest.raises(_lib.AlsError):
+            sim.advance(1)
+        with pytest.raises(_lib.AlsError):
+            sim.set_state(st[1:], first_member=1)
+        with pytest.raises(_lib.AlsError):
+            sim.set_state(st[:2])
+        sim.set_state(st)
+        sim.advance(1)
+        assert sim.info(0)["steps"] == 1

@@ -142,3 +142,28 @@ def test_reference_time_loop_with_b200_rk4(ref_b200, dim, n, recon, flux, bc):
     assert a[0] == b[0] and a[3] == b[3] >= 1 and a[4] == b[4]
     np.testing.assert_array_equal(a[2], b[2])
     np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("dim,n,samples", [(1, (33,), 5), (2, (14, 12), 9), (3, (7, 6, 8), 4)])
+def test_meanvar_statistics_adapter_against_reference_class(ref_b200, dim, n, samples):
+    """MeanVarianceB200 (oracle/adapter/StatisticsB200.hpp, registered as
+    REGISTER_STATISTICS(b200, meanvar, ...)) and the reference's own
+    MeanVariance, both made by name through the reference's
+    StatisticsFactory and run like alsuq's Runner (write per sample,
+    combine, finalize, write): the FP64 Welford mean equals the raw-sum mean
+    to 1e-14 of the samples' magnitude mean(|U|) (a mean near zero, e.g. of
+    a momentum, has no relative scale of its own), and the Welford variance
+    M2/M equals S2/M - (S1/M)^2 to 1e-14 of the second moment's scale (the
+    raw-moment difference cancels; its own rounding error is of that size)."""
+    g = 2
+    states = np.stack([smooth_random_state(4000 + 13 * k + dim, dim, n, g)
+                       for k in range(samples)])
+    mean_ref, var_ref = ref_b200.statistics(dim, n, g, states, platform="cpu", name="meanvar")
+    mean, var = ref_b200.statistics(dim, n, g, states, platform="b200", name="meanvar")
+    scale = np.mean(np.abs(states), axis=0)
+    assert np.all(np.abs(mean - mean_ref) <= 1e-14 * scale)
+    second = np.mean(states * states, axis=0)
+    assert np.all(np.abs(var - var_ref) <= 1e-14 * np.maximum(second, 1e-300))
+    # and the Welford variance against an exactly rounded two-pass variance
+    exact = np.var(states.astype(np.longdouble), axis=0).astype(np.float64)
+    assert np.all(np.abs(var - exact) <= 1e-13 * np.maximum(exact, 1e-300) + 1e-300)

@@ -9,6 +9,7 @@ import pytest
 import torch
 
 import alsvinn_b200 as als
+from alsvinn_b200 import _lib
 from conftest import load_golden
 from oracle_lib import ghost_cells, padded_shape, smooth_random_state
 
@@ -26,9 +27,12 @@ def _level_states(levels, g, seed0):
     return states
 
 
-def _run_levels(levels, states, order=None, tune=False, **kw):
+def _run_levels(levels, states, order=None, tune=False, shapes=None, **kw):
     with als.Simulator(2, levels=levels, flux="hll3", reconstruction="weno2", cfl=0.4,
                        end_time=0.03, **kw) as sim:
+        if shapes is not None:
+            sim.set_tiles(shapes)
+            assert sim.tiles()["shapes"] == list(shapes)
         for k, lev in enumerate(sim.levels):
             sim.set_state(states[k], first_member=lev["first"])
         if tune:
@@ -39,6 +43,7 @@ def _run_levels(levels, states, order=None, tune=False, **kw):
                 np.testing.assert_array_equal(a, b)
             assert all(sim.info(m)["steps"] == 0 for m in range(sim.members))
             assert sim.schedule()["blocks_per_sm"] == choice["blocks_per_sm"]
+            assert sim.tiles()["shapes"] == choice["tile_shapes"]
         if order is not None:
             sim.set_schedule(0, order)
         sim.run()
@@ -76,6 +81,39 @@ def test_level_order_and_tuning_do_not_change_results():
     out, info = _run_levels(LEVELS, states, tune=True)
     for a, b in zip(base, out):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("integ", ["rungekutta3", "rungekutta2", "forwardeuler"])
+def test_tile_shape_per_level_does_not_change_results(precision, integ):
+    """Levels on the 16x16 tile, the 32x16 tile or a mix (one launch per
+    shape and stage), and persistent launches over them, give the same bits."""
+    g = ghost_cells("weno2")
+    states = _level_states(LEVELS, g, 800)
+    base, base_info = _run_levels(LEVELS, states, precision=precision, integrator=integ)
+    for shapes in ([1, 1, 1], [0, 1, 0], [1, 0, 1]):
+        out, info = _run_levels(LEVELS, states, shapes=shapes, precision=precision,
+                                integrator=integ)
+        for a, b in zip(base, out):
+            np.testing.assert_array_equal(a, b)
+        assert [i["steps"] for i in info] == [i["steps"] for i in base_info]
+
+
+def test_tile_shapes_report_extents_and_reject_unbuilt():
+    with als.Simulator(2, levels=LEVELS, flux="hll3", reconstruction="weno2", cfl=0.4,
+                       end_time=0.03) as sim:
+        t = sim.tiles()
+        assert t["shapes"] == [0, 0, 0] and t["extents"][0] == (32, 16, 1)
+        sim.set_tiles([1, 0, 1])
+        assert sim.tiles()["extents"] == [(16, 16, 1), (32, 16, 1), (16, 16, 1)]
+    with als.Simulator(2, levels=LEVELS, flux="hll3", reconstruction="eno3", cfl=0.4,
+                       end_time=0.03) as sim:
+        with pytest.raises(_lib.AlsError):
+            sim.set_tiles([1, 0, 0])
+    with als.Simulator(3, (8, 8, 8), (0, 0, 0), (1, 1, 1), flux="hll3",
+                       reconstruction="weno2") as sim:
+        with pytest.raises(_lib.AlsError):
+            sim.set_tiles([1])
 
 
 def test_fp32_multilevel_against_fp64():

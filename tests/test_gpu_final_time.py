@@ -1,0 +1,108 @@
+"""Final-time parity with the reference's CPU time loop (Simulator.cpp:191-214).
+
+The plain FP64 method must match the reference on the same inputs with
+identical step counts and a relative L1 difference of at most 1e-10 per
+conserved variable at the final time.  The fixtures hold the reference
+build's results at T = 2 (tests/golden/make_final_time.py):
+
+* KH 1024^2, WENO2 + HLL3, RK3, CFL 0.4, periodic (about 23k steps): the
+  benchmark configuration itself;
+* KH 256^2 members 7 and 4095 of the 4096-sample FP64 UQ oracle ensemble.
+
+Kelvin-Helmholtz at T = 2 is chaotic, so a single differing bit in any of
+the steps would show at the end: the tests assert the dt sequence digest
+and the sha256 of the final interior (bit equality), and the L1 bar.
+"""
+import numpy as np
+import pytest
+
+import alsvinn_b200 as als
+import final_time as ft
+
+pytestmark = pytest.mark.gpu
+
+L1_TOL = 1e-10
+
+
+def _solver(z, members=1, **kw):
+    n = z["n"]
+    return als.Simulator(2, (n, n), (0.0, 0.0), (1.0, 1.0), flux=z["flux"],
+                         reconstruction=z["recon"], integrator=z["integrator"], boundary=z["bc"],
+                         gamma=z["gamma"], cfl=z["cfl"], end_time=z["end_time"], members=members,
+                         **kw)
+
+
+def _check_final(z, U, steps, t):
+    n = z["n"]
+    assert steps == z["steps"], (steps, z["steps"])
+    assert t == z["t"], (t, z["t"])
+    s = ft.summary(U, n)
+    # relative L1 difference per conserved variable, bounded through the
+    # 16 x 16 block sums (sum_b |A_b - B_b| <= sum_cells |a - b|) and the norms
+    diff = np.abs(s["block_sums"] - z["block_sums"]).sum(axis=(1, 2))
+    rel = diff / z["l1"]
+    assert np.all(rel <= L1_TOL), rel
+    assert np.all(np.abs(s["l1"] - z["l1"]) <= L1_TOL * z["l1"]), (s["l1"], z["l1"])
+    # and bit equality of the whole interior
+    assert s["interior_sha256"] == z["interior_sha256"]
+
+
+def _step_by_step(sim):
+    dts = []
+    while not sim.info()["done"]:
+        sim.advance(1)
+        dts.append(sim.info()["dt"])
+    return np.array(dts)
+
+
+def test_kh1024_to_final_time_matches_reference():
+    """The headline configuration to T = 2 one step at a time: every dt of
+    the ~23k steps and the final state equal to the reference build's."""
+    z = ft.load("kh1024")
+    n = z["n"]
+    U0 = ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"])
+    with _solver(z) as sim:
+        sim.set_state(U0)
+        dts = _step_by_step(sim)
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["status"] == 0
+    assert len(dts) == z["steps"]
+    np.testing.assert_array_equal(dts[:64], z["dts_head"])
+    np.testing.assert_array_equal(dts[-64:], z["dts_tail"])
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    _check_final(z, U, info["steps"], info["t"])
+
+
+def test_uq_oracle_members_to_final_time_match_reference():
+    """Members 7 and 4095 of the UQ oracle ensemble, advanced together as
+    one batched FP64 ensemble (the path that generated the 4096-sample
+    oracle) by the graph-captured run: final states equal to the
+    reference's, and their observables equal to the ensemble fixture's."""
+    zs = [ft.load(name) for name in ("uq256_7", "uq256_4095")]
+    n = zs[0]["n"]
+    states = np.stack([ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"]) for z in zs])
+    with _solver(zs[0], members=len(zs)) as sim:
+        sim.set_state(states)
+        sim.run()
+        infos = [sim.info(m) for m in range(len(zs))]
+        U = sim.get_state()
+    oracle = np.load(ft.GOLDEN + "/uq_kh256_fp64_4096.npz")
+    for m, z in enumerate(zs):
+        assert infos[m]["status"] == 0
+        _check_final(z, U[m], infos[m]["steps"], infos[m]["t"])
+        assert ft.observable(U[m], n) == z["observable"]
+        assert int(oracle["steps"][z["sample"]]) == z["steps"]
+
+
+def test_uq_member_dt_sequence_matches_reference():
+    """Member 4095 alone, one step at a time: every dt equal to the reference's."""
+    z = ft.load("uq256_4095")
+    n = z["n"]
+    with _solver(z) as sim:
+        sim.set_state(ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"]))
+        dts = _step_by_step(sim)
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    _check_final(z, U, info["steps"], info["t"])

@@ -7,12 +7,20 @@ than the reference's sequential loop and log_entropy calls log, so those
 match to a relative 1e-12 (moment: 1e-14).  FP32 members are converted to
 FP64 on load, so the oracle runs on the same values widened.
 """
+import importlib.util
+import os
+
 import numpy as np
 import pytest
 import torch
 
 from alsvinn_b200 import functionals as fn
 from oracle_lib import smooth_random_state
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+MG = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(MG)
 
 pytestmark = pytest.mark.gpu
 
@@ -78,3 +86,43 @@ def test_time_integrated_functional(c_oracle):
                                          degree=1)
         last = t
     np.testing.assert_allclose(tif.value.cpu().numpy(), ref, rtol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("dim,n,kind,degree", MG.FUNCTIONAL_CASES,
+                         ids=[MG.functional_case_name(c[0], c[2], c[3])
+                              for c in MG.FUNCTIONAL_CASES])
+def test_functional_matches_reference_classes(dim, n, kind, degree, precision):
+    """Against the outputs of the reference's own Identity, Moment,
+    LogEntropy and BoundedVariation (made by name through its
+    FunctionalFactory in the reference build, tests/golden/make_golden.py):
+    identity exact, moment to 1e-14 (pow), sums to 1e-12 (fixed-order device
+    reduction, device log).  FP32 members: the reference ran on the FP64
+    states, so they are compared through their own widened values only for
+    identity (exact conversion) and skipped otherwise."""
+    z = np.load(os.path.join(GOLDEN, "functionals_ref.npz"))
+    name = MG.functional_case_name(dim, kind, degree)
+    states = np.stack([smooth_random_state(600 + 7 * k + dim, dim, n, 2)
+                       for k in range(MG.FUNCTIONAL_MEMBERS)])
+    dtype = torch.float64 if precision == "fp64" else torch.float32
+    if precision == "fp32" and kind != "identity":
+        pytest.skip("reference outputs are of the FP64 states")
+    x = torch.from_numpy(states).to(dtype).cuda().contiguous()
+    start = torch.from_numpy(z[name + "/start"]).cuda()
+    out = fn.functional(x, dim, n, 2, kind, weight=MG.FUNCTIONAL_WEIGHT, out=start.clone(),
+                        degree=degree, gamma=1.4, lower=MG.FUNCTIONAL_BOX[0],
+                        upper=MG.FUNCTIONAL_BOX[1]).cpu().numpy()
+    ref = z[name + "/result"]
+    if kind == "identity":
+        if precision == "fp64":
+            np.testing.assert_array_equal(out, ref)
+        else:
+            widened = x.double().cpu().numpy()
+            sl = [slice(None), slice(None)] + [slice(2, -2) if 3 - a <= dim else slice(None)
+                                               for a in range(3)]
+            expect = z[name + "/start"] + MG.FUNCTIONAL_WEIGHT * widened[tuple(sl)].reshape(
+                ref.shape)
+            np.testing.assert_array_equal(out, expect)
+    else:
+        rtol = 1e-14 if kind == "moment" else 1e-12
+        np.testing.assert_allclose(out, ref, rtol=rtol, atol=1e-14)
