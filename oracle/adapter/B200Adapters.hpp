@@ -1,7 +1,7 @@
 // boundary::Boundary, reconstruction::Reconstruction, integrator::Integrator
-// and diffusion::DiffusionOperator backed by the B200 library — the other adapter classes a maintainer adds
-// beside numflux::NumericalFluxB200, compiled
-// against the reference's headers:
+// and diffusion::DiffusionOperator backed by the B200 library: the other
+// adapter classes a maintainer adds to alsfvm's factories beside
+// numflux::NumericalFluxB200, compiled against the reference's headers:
 //   alsfvm/include/alsfvm/boundary/Boundary.hpp:25-35
 //   alsfvm/include/alsfvm/reconstruction/Reconstruction.hpp:40-58
 //   alsfvm/include/alsfvm/integrator/Integrator.hpp:52-100

@@ -1,6 +1,6 @@
 // numflux::NumericalFlux backed by the B200 library: the class a maintainer
-// adds to alsfvm to select this path as a platform,
-// compiled here against the reference's own headers
+// adds to alsfvm's flux factory to select this path as a platform, compiled
+// here against the reference's own headers
 // (alsfvm/include/alsfvm/numflux/NumericalFlux.hpp:25-52).
 //
 // TEST INFRASTRUCTURE in this repository: it is built only into

@@ -1,7 +1,7 @@
 """The drop-in boundary end to end: the reference's own time loop
 (Simulator::incrementSolution's substep loop over ConservedSystem, the
-end-time adjuster, the constraint check) with the adapter classes of
-INTEGRATION.md — compiled against the reference's headers
+end-time adjuster, the constraint check) with the adapter classes a
+maintainer adds to alsvinn — compiled against the reference's headers
 (oracle/adapter/) — in place of the reference's NumericalFluxCPU,
 Reconstruction, BoundaryCPU and integrators.  Every whole simulation must
 equal the reference's own, bit for bit.
