@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "stage_kernel.cuh"
+#include "stage_zmarch.cuh"
 
 namespace als {
 
@@ -14,10 +15,31 @@ namespace als {
 // persistent launch of as many blocks as can be resident at once (or
 // `blocks_per_sm` per SM when > 0, capped by what fits), never more than
 // there are work items.
+// The kernel, block size and shared memory of one (shape, kind): the tiled
+// stage_kernel, or for 3-D shape 1 the z-marching kernel.
+template<class R, int DIM, int RECON, int FLUX, int KIND, int SHAPE>
+struct StageLaunch {
+    typedef StageLayout<R, DIM, RECON, FLUX, SHAPE> Lay;
+    static constexpr int THREADS = Lay::THREADS;
+    static constexpr size_t SMEM = Lay::SMEM;
+    static decltype(&stage_kernel<R, DIM, RECON, FLUX, KIND, SHAPE>) kernel() {
+        return stage_kernel<R, DIM, RECON, FLUX, KIND, SHAPE>;
+    }
+};
+template<class R, int RECON, int FLUX, int KIND>
+struct StageLaunch<R, 3, RECON, FLUX, KIND, 1> {
+    typedef ZLayout<R, RECON, FLUX> Lay;
+    static constexpr int THREADS = Lay::THREADS;
+    static constexpr size_t SMEM = Lay::SMEM;
+    static decltype(&zmarch_kernel<R, RECON, FLUX, KIND>) kernel() {
+        return zmarch_kernel<R, RECON, FLUX, KIND>;
+    }
+};
+
 template<class R, int DIM, int RECON, int FLUX, int KIND, int SHAPE>
 cudaError_t launch_stage_one(const StageParams& P, int blocks_per_sm, cudaStream_t stream) {
-    typedef StageLayout<R, DIM, RECON, FLUX, SHAPE> Lay;
-    auto kernel = stage_kernel<R, DIM, RECON, FLUX, KIND, SHAPE>;
+    typedef StageLaunch<R, DIM, RECON, FLUX, KIND, SHAPE> Lay;
+    auto kernel = Lay::kernel();
     // raising the dynamic shared-memory limit is idempotent and cheap; it is
     // done on every launch so that every device the process uses is covered
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -130,11 +152,11 @@ void stage_tile_dim(int shape, int* tile) {
         tile[1] = TileShape<DIM, 0>::Y;
         tile[2] = TileShape<DIM, 0>::Z;
     }
-    if constexpr (DIM == 2) {
+    if constexpr (DIM >= 2) {
         if (shape == 1) {
-            tile[0] = TileShape<2, 1>::X;
-            tile[1] = TileShape<2, 1>::Y;
-            tile[2] = TileShape<2, 1>::Z;
+            tile[0] = TileShape<DIM, 1>::X;
+            tile[1] = TileShape<DIM, 1>::Y;
+            tile[2] = TileShape<DIM, 1>::Z;
         }
     }
 }

@@ -109,14 +109,32 @@ template<> struct TileShape<3, 0> {
     static constexpr int X = ALS_TILE3_X, Y = ALS_TILE3_Y, Z = ALS_TILE3_Z, T = ALS_STAGE3_THREADS,
         B = ALS_STAGE3_BLOCKS;
 };
-
+// 3-D shape 1: 16 x 16 columns marching along z over segments of
+// ALS_ZMARCH_SEG cells (stage_zmarch.cuh), 288 threads.
+#ifndef ALS_ZMARCH_SEG
+#define ALS_ZMARCH_SEG 32
+#endif
+#ifndef ALS_ZMARCH_BLOCKS
+#define ALS_ZMARCH_BLOCKS 2
+#endif
+#ifndef ALS_ZMARCH_THREADS
+#define ALS_ZMARCH_THREADS 288
+#endif
+template<> struct TileShape<3, 1> {
+    static constexpr int X = 16, Y = 16, Z = ALS_ZMARCH_SEG, T = ALS_ZMARCH_THREADS,
+        B = ALS_ZMARCH_BLOCKS;
+};
 
 // Shapes built per (dimension, reconstruction, flux): the default for every
-// combination, the 2-D alternative for WENO2 with HLL, HLL3 and Central
-// (the ensemble and benchmark configurations).
+// combination; in 2-D the 16 x 16 alternative for WENO2 with HLL, HLL3 and
+// Central (the ensemble and benchmark configurations); in 3-D the z-marching
+// columns for reconstructions that reach one cell each way (WENO2, ENO2, MC,
+// MM, WENOF2, none) with the two-point fluxes.
 __host__ __device__ constexpr bool shape_built(int dim, int recon, int flux, int shape) {
-    return shape == 0 || (shape == 1 && dim == 2 && recon == RECON_WENO2 &&
-        (flux == FLUX_HLL || flux == FLUX_HLL3 || flux == FLUX_CENTRAL));
+    return shape == 0 ||
+        (shape == 1 && dim == 2 && recon == RECON_WENO2 &&
+            (flux == FLUX_HLL || flux == FLUX_HLL3 || flux == FLUX_CENTRAL)) ||
+        (shape == 1 && dim == 3 && recon_ghosts(recon) <= 2 && !stencil_flux(flux));
 }
 constexpr int kMaxShapes = 2;
 
@@ -447,6 +465,120 @@ __device__ __forceinline__ void finish_step(StepState* st) {
     }
 }
 
+// The stage combination of one updated cell (interior coordinates gx, gy,
+// gz; its net flux `acc`; `ub`, its value of the stage's input state as
+// staged) and its writes: the cell, its boundary images (or, for a split
+// grid, the neighbouring subdomains' ghost cells), and, after the last
+// stage, the constraint check.
+template<class R, int DIM, int NV, int KIND>
+__device__ __forceinline__ void update_cell(const StageParams& P, const LevelDesc& L, int member,
+    long long base, R c, R gamma, const R* acc, const R* ub, int gx, int gy, int gz, bool& bad,
+    long long& bad_idx) {
+    constexpr bool LAST = KIND == KIND_RK3_2 || KIND == KIND_RK2_1;
+    const GridDesc& gd = L.grid;
+    const StepState* st = L.state ? L.state + (L.subdomains ? 0 : member) : nullptr;
+    auto unp = [&](int v) { return static_cast<const R*>(L.un[v]) + base; };
+    auto outp = [&](int v) { return static_cast<R*>(L.out[v]) + base; };
+    const int px = gx + gd.ghosts;
+    const int py = DIM > 1 ? gy + gd.ghosts : 0;
+    const int pz = DIM > 2 ? gz + gd.ghosts : 0;
+    const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
+    R val[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        R x = acc[v];
+        if (KIND == KIND_RK2_1) {
+            // RungeKutta2.cpp:57-63
+            x = x * c;
+            x = x + ub[v];
+            x = x + unp(v)[idx];
+            x = x * R(0.5);
+        } else if (KIND == KIND_RK3_1) {
+            // RungeKutta3.cpp:65-78
+            x = x * c;
+            x = x + ub[v];
+            x = x * R(1. / 3.);
+            x = x + unp(v)[idx];
+            x = x * R(3. / 4.);
+        } else if (KIND == KIND_RK3_2) {
+            // RungeKutta3.cpp:65-83
+            x = x * c;
+            x = x + ub[v];
+            x = x * R(2);
+            x = x + unp(v)[idx];
+            x = x * R(1. / 3.);
+        }
+        val[v] = x;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        outp(v)[idx] = val[v];
+    }
+    // a cell at least G' = gd.ghosts cells from every side of its grid
+    // has no boundary image (only the cells of the outer shell do)
+    const int gw = gd.ghosts;
+    const bool shell = gx < gw || gx >= gd.n[0] - gw ||
+        (DIM > 1 && (gy < gw || gy >= gd.n[1] - gw)) ||
+        (DIM > 2 && (gz < gw || gz >= gd.n[2] - gw));
+    if (P.write_ghosts && shell) {
+        int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
+        int sx[3] = {0, 0, 0}, sy[3] = {0, 0, 0}, sz[3] = {0, 0, 0};
+        int nxi, nyi = 1, nzi = 1;
+        // this member's subdomain coordinates (subdomains only)
+        int c0 = 0, c1 = 0, c2 = 0;
+        if (L.subdomains) {
+            c0 = member % L.procs[0];
+            c1 = (member / L.procs[0]) % L.procs[1];
+            c2 = member / (L.procs[0] * L.procs[1]);
+            nxi = subdomain_images(gx, gd.n[0], gd.ghosts, P.bc, c0, L.procs[0], ix, sx);
+            if (DIM > 1) {
+                nyi = subdomain_images(gy, gd.n[1], gd.ghosts, P.bc, c1, L.procs[1], iy, sy);
+            }
+            if (DIM > 2) {
+                nzi = subdomain_images(gz, gd.n[2], gd.ghosts, P.bc, c2, L.procs[2], iz, sz);
+            }
+        } else {
+            nxi = boundary_images(gx, gd.n[0], gd.ghosts, P.bc, ix);
+            if (DIM > 1) {
+                nyi = boundary_images(gy, gd.n[1], gd.ghosts, P.bc, iy);
+            }
+            if (DIM > 2) {
+                nzi = boundary_images(gz, gd.n[2], gd.ghosts, P.bc, iz);
+            }
+        }
+        if (nxi * nyi * nzi > 1) {
+            for (int a = 0; a < nzi; ++a) {
+                for (int b = 0; b < nyi; ++b) {
+                    for (int e = 0; e < nxi; ++e) {
+                        if (a == 0 && b == 0 && e == 0) {
+                            continue;
+                        }
+                        const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
+                        // the member holding the image (steps wrap: periodic splits)
+                        long long target = base;
+                        if (L.subdomains) {
+                            const int t0 = (c0 + sx[e] + L.procs[0]) % L.procs[0];
+                            const int t1 = (c1 + sy[b] + L.procs[1]) % L.procs[1];
+                            const int t2 = (c2 + sz[a] + L.procs[2]) % L.procs[2];
+                            target = (long long)(t0 + L.procs[0] * (t1 + L.procs[1] * t2)) *
+                                L.member_stride;
+                        }
+#pragma unroll
+                        for (int v = 0; v < NV; ++v) {
+                            static_cast<R*>(L.out[v])[target + j] = val[v];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (LAST && st && !obeys_constraints<R, NV>(val, gamma)) {
+        bad = true;
+        // subdomains: the member's padded plane offset first
+        bad_idx = L.subdomains ? (long long)member * gd.plane + idx : idx;
+    }
+}
+
 // One work item: tile `tile` of member `member` of level L.
 template<class R, int DIM, int RECON, int FLUX, int SHAPE, int KIND>
 __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc& L, int tile,
@@ -475,7 +607,6 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     // used; arrays of them would be held (and spilled) across the kernel
     auto inp = [&](int v) { return static_cast<const R*>(L.in[v]) + base; };
     auto unp = [&](int v) { return static_cast<const R*>(L.un[v]) + base; };
-    auto outp = [&](int v) { return static_cast<R*>(L.out[v]) + base; };
     const R gamma = R(P.gamma);
 
     R c = R(0);
@@ -497,27 +628,30 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
     // second stage (RungeKutta{2,3}.cpp: output *= dt/dx; output += U).
     // Planes may carry more ghost cells than the stencil needs (a diffusion
     // operator with a wider stencil sets the width): `sh` skips the extra ones.
+    // A box position is decoded once and serves every variable's plane.
     const int sh = gd.ghosts - G;
-    for (int i = tid; i < NV * Lay::BOX; i += Lay::THREADS) {
-        const int v = i / Lay::BOX;
-        const int b = i - v * Lay::BOX;
+    for (int b = tid; b < Lay::BOX; b += Lay::THREADS) {
         const int bx = b % Lay::BX;
         const int by = (b / Lay::BX) % Lay::BY;
         const int bz = b / (Lay::BX * Lay::BY);
         const int px = x0 + bx + sh;
         const int py = DIM > 1 ? y0 + by + sh : 0;
         const int pz = DIM > 2 ? z0 + bz + sh : 0;
-        R val = R(0);
-        if (px < gd.N[0] && py < gd.N[1] && pz < gd.N[2]) {
-            const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
-            if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
-                val = inp(v)[idx] * c;
-                val = val + unp(v)[idx];
-            } else {
-                val = inp(v)[idx];
+        const bool inside = px < gd.N[0] && py < gd.N[1] && pz < gd.N[2];
+        const long long idx = inside ? ((long long)pz * gd.N[1] + py) * gd.N[0] + px : 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R val = R(0);
+            if (inside) {
+                if (KIND == KIND_RK2_1 || KIND == KIND_RK3_1) {
+                    val = inp(v)[idx] * c;
+                    val = val + unp(v)[idx];
+                } else {
+                    val = inp(v)[idx];
+                }
             }
+            box[v * Lay::BOX + b] = val;
         }
-        box[i] = val;
     }
     __syncthreads();
 
@@ -556,105 +690,14 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const LevelDesc
         if (gx >= gd.hi[0] || (DIM > 1 && gy >= gd.hi[1]) || (DIM > 2 && gz >= gd.hi[2])) {
             continue;
         }
-        const int px = gx + gd.ghosts;
-        const int py = DIM > 1 ? gy + gd.ghosts : 0;
-        const int pz = DIM > 2 ? gz + gd.ghosts : 0;
-        const long long idx = ((long long)pz * gd.N[1] + py) * gd.N[0] + px;
         const int bidx = ((DIM > 2 ? cz + G : 0) * Lay::BY + (DIM > 1 ? cy + G : 0)) * Lay::BX + cx + G;
-        R val[NV];
+        R ub[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            R x = acc[k][v];
-            if (KIND == KIND_RK2_1) {
-                // RungeKutta2.cpp:57-63
-                x = x * c;
-                x = x + box[v * Lay::BOX + bidx];
-                x = x + unp(v)[idx];
-                x = x * R(0.5);
-            } else if (KIND == KIND_RK3_1) {
-                // RungeKutta3.cpp:65-78
-                x = x * c;
-                x = x + box[v * Lay::BOX + bidx];
-                x = x * R(1. / 3.);
-                x = x + unp(v)[idx];
-                x = x * R(3. / 4.);
-            } else if (KIND == KIND_RK3_2) {
-                // RungeKutta3.cpp:65-83
-                x = x * c;
-                x = x + box[v * Lay::BOX + bidx];
-                x = x * R(2);
-                x = x + unp(v)[idx];
-                x = x * R(1. / 3.);
-            }
-            val[v] = x;
+            ub[v] = box[v * Lay::BOX + bidx];
         }
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            outp(v)[idx] = val[v];
-        }
-        // a cell at least G' = gd.ghosts cells from every side of its grid
-        // has no boundary image (only the cells of the outer shell do)
-        const int gw = gd.ghosts;
-        const bool shell = gx < gw || gx >= gd.n[0] - gw ||
-            (DIM > 1 && (gy < gw || gy >= gd.n[1] - gw)) ||
-            (DIM > 2 && (gz < gw || gz >= gd.n[2] - gw));
-        if (P.write_ghosts && shell) {
-            int ix[3], iy[3] = {0, 0, 0}, iz[3] = {0, 0, 0};
-            int sx[3] = {0, 0, 0}, sy[3] = {0, 0, 0}, sz[3] = {0, 0, 0};
-            int nxi, nyi = 1, nzi = 1;
-            // this member's subdomain coordinates (subdomains only)
-            int c0 = 0, c1 = 0, c2 = 0;
-            if (L.subdomains) {
-                c0 = member % L.procs[0];
-                c1 = (member / L.procs[0]) % L.procs[1];
-                c2 = member / (L.procs[0] * L.procs[1]);
-                nxi = subdomain_images(gx, gd.n[0], gd.ghosts, P.bc, c0, L.procs[0], ix, sx);
-                if (DIM > 1) {
-                    nyi = subdomain_images(gy, gd.n[1], gd.ghosts, P.bc, c1, L.procs[1], iy, sy);
-                }
-                if (DIM > 2) {
-                    nzi = subdomain_images(gz, gd.n[2], gd.ghosts, P.bc, c2, L.procs[2], iz, sz);
-                }
-            } else {
-                nxi = boundary_images(gx, gd.n[0], gd.ghosts, P.bc, ix);
-                if (DIM > 1) {
-                    nyi = boundary_images(gy, gd.n[1], gd.ghosts, P.bc, iy);
-                }
-                if (DIM > 2) {
-                    nzi = boundary_images(gz, gd.n[2], gd.ghosts, P.bc, iz);
-                }
-            }
-            if (nxi * nyi * nzi > 1) {
-                for (int a = 0; a < nzi; ++a) {
-                    for (int b = 0; b < nyi; ++b) {
-                        for (int e = 0; e < nxi; ++e) {
-                            if (a == 0 && b == 0 && e == 0) {
-                                continue;
-                            }
-                            const long long j = ((long long)iz[a] * gd.N[1] + iy[b]) * gd.N[0] + ix[e];
-                            // the member holding the image (steps wrap: periodic splits)
-                            long long target = base;
-                            if (L.subdomains) {
-                                const int t0 = (c0 + sx[e] + L.procs[0]) % L.procs[0];
-                                const int t1 = (c1 + sy[b] + L.procs[1]) % L.procs[1];
-                                const int t2 = (c2 + sz[a] + L.procs[2]) % L.procs[2];
-                                target = (long long)(t0 + L.procs[0] * (t1 + L.procs[1] * t2)) *
-                                    L.member_stride;
-                            }
-#pragma unroll
-                            for (int v = 0; v < NV; ++v) {
-                                static_cast<R*>(L.out[v])[target + j] = val[v];
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        if (LAST && st && !obeys_constraints<R, NV>(val, gamma)) {
-            bad = true;
-            // subdomains: the member's padded plane offset first
-            bad_idx = L.subdomains ? (long long)member * gd.plane + idx : idx;
-        }
+        update_cell<R, DIM, NV, KIND>(P, L, member, base, c, gamma, acc[k], ub, gx, gy, gz, bad,
+            bad_idx);
     }
 
     if (KIND == KIND_FLUX0) {

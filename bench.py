@@ -297,6 +297,28 @@ def run_batch(args, rank, world, local):
         sim.close()
         return
     schedule = sim.tune(steps=2)
+    # the tuned choice against every level on one fixed tile shape (each
+    # timed over the same number of steps from the current state)
+    shape_ms = {}
+    for shape in (0, 1):
+        try:
+            sim.set_tiles([shape] * len(sim.levels))
+        except Exception:
+            continue
+        sim.advance(2)
+        sim.synchronize()
+        t0 = time.perf_counter()
+        sim.advance(4)
+        sim.synchronize()
+        shape_ms["all levels shape %d" % shape] = (time.perf_counter() - t0) * 1e3 / 4
+    sim.set_tiles(schedule["tile_shapes"])
+    sim.advance(2)
+    sim.synchronize()
+    t0 = time.perf_counter()
+    sim.advance(4)
+    sim.synchronize()
+    shape_ms["tuned %s" % schedule["tile_shapes"]] = (time.perf_counter() - t0) * 1e3 / 4
+    schedule["ms_per_step_by_tiles"] = shape_ms
     # the warm-up also captures the solver's 8-step CUDA graph, which the
     # first advance of 8 or more steps builds: at least 8 steps, so that the
     # capture is not part of the timed region

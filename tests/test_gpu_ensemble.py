@@ -111,9 +111,13 @@ def test_tile_shapes_report_extents_and_reject_unbuilt():
         with pytest.raises(_lib.AlsError):
             sim.set_tiles([1, 0, 0])
     with als.Simulator(3, (8, 8, 8), (0, 0, 0), (1, 1, 1), flux="hll3",
-                       reconstruction="weno2") as sim:
+                       reconstruction="eno3") as sim:
         with pytest.raises(_lib.AlsError):
             sim.set_tiles([1])
+    with als.Simulator(3, (8, 8, 8), (0, 0, 0), (1, 1, 1), flux="hll3",
+                       reconstruction="weno2") as sim:
+        sim.set_tiles([1])
+        assert sim.tiles()["extents"] == [(16, 16, 32)]
 
 
 def test_fp32_multilevel_against_fp64():
@@ -199,3 +203,56 @@ def test_uq_oracle_members_equal_single_runs_at_full_size(sample):
                                                     end_time=2.0)
     assert info["steps"][0] == z["steps"][sample]
     assert y[0] == z["y"][sample]
+
+
+Z_CASES = [((20, 18, 40), "weno2", "hll3", "rungekutta3", "periodic", 2),
+           ((17, 16, 33), "eno2", "hll", "rungekutta2", "neumann", 1),
+           ((16, 21, 18), "mc", "central", "forwardeuler", "periodic", 3),
+           ((18, 17, 35), "wenof2", "hll3", "rungekutta3", "neumann", 1),
+           ((16, 16, 16), "none", "hll", "rungekutta3", "periodic", 2),
+           ((19, 16, 20), "mm", "hll3", "rungekutta2", "periodic", 1)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("n,recon,flux,integ,bc,members", Z_CASES,
+                         ids=["%s-%s-%s-%s" % (c[1], c[2], c[3], c[4]) for c in Z_CASES])
+def test_z_marching_3d_tiles_equal_the_box_tiles(n, recon, flux, integ, bc, members, precision):
+    """3-D shape 1 (16x16 columns marching along z in segments) gives the
+    bits of shape 0 (8x8x4 boxes): every member, ghosts included, with
+    partial columns and segments, both boundaries, every integrator."""
+    g = ghost_cells(recon)
+    states = np.stack([smooth_random_state(300 + k, 3, n, g) for k in range(members)])
+    out = {}
+    for shape in (0, 1):
+        with als.Simulator(3, n, (0, 0, 0), (1, 1, 1), flux=flux, reconstruction=recon,
+                           integrator=integ, boundary=bc, cfl=0.4, end_time=0.02,
+                           precision=precision, members=members) as sim:
+            sim.set_tiles([shape])
+            sim.set_state(states)
+            sim.run()
+            out[shape] = (sim.get_state(), [sim.info(m) for m in range(members)])
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert [(i["steps"], i["t"], i["dt"]) for i in out[0][1]] == \
+        [(i["steps"], i["t"], i["dt"]) for i in out[1][1]]
+    assert out[0][1][0]["steps"] >= 2
+
+
+def test_z_marching_3d_against_the_oracle(c_oracle):
+    """Shape 1 on KH-like 3-D data against the C oracle directly (WENO2 +
+    HLL3, RK3, periodic), a grid of two z segments plus a partial one."""
+    n, g = (17, 16, 70), 2
+    st = smooth_random_state(41, 3, n, g)
+    cfg = c_oracle.config(3, n, (0, 0, 0), (1, 1, 1), "hll3", "weno2", "rungekutta3", "periodic",
+                          1.4)
+    rc, U_ref, dts, steps, t = c_oracle.simulate(cfg, st, 0.4, 10.0, max_steps=3)
+    with als.Simulator(3, n, (0, 0, 0), (1, 1, 1), flux="hll3", reconstruction="weno2",
+                       integrator="rungekutta3", boundary="periodic", cfl=0.4, end_time=10.0,
+                       max_steps=3) as sim:
+        sim.set_tiles([1])
+        assert sim.tiles()["extents"][0][:2] == (16, 16)
+        sim.set_state(st)
+        sim.run()
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert rc == 0 and info["steps"] == steps == 3 and info["t"] == t
+    np.testing.assert_array_equal(U, U_ref)
