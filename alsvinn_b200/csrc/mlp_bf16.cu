@@ -22,7 +22,10 @@ using namespace mlpk;
 
 namespace {
 
-constexpr long long kInferChunk = 65536;   // rows per inference chunk (multiple of 128)
+#ifndef ALS_MLP_INFER_CHUNK
+#define ALS_MLP_INFER_CHUNK 65536
+#endif
+constexpr long long kInferChunk = ALS_MLP_INFER_CHUNK;   // rows per inference chunk (multiple of 128)
 constexpr int kMaxSplits = 16;             // K splits of a weight gradient, row splits of a column sum
 
 int mlp_fail(int code, const std::string& msg) {

@@ -45,10 +45,14 @@ namespace als {
 //   48x12 / 576 threads / 2 blocks             0.579
 // (the first row is 0.433 since the barrier at the end of each direction
 // went, 0.430 since the constraint check skips its velocity divisions when
-// rho >= 1).  Keeping the tile's U^n in shared memory from the load phase
-// for the epilogue, instead of reading it there, ran slower (0.434 vs 0.430;
-// FP32 members 3 % slower).  All of these are build-time knobs; the FP32
-// units build with three blocks per SM.
+// rho >= 1, 0.407 since the HLL3 star branch forms only the chosen side's
+// point flux and interior cells skip the boundary-image code, 0.381 since
+// the staging decodes each box position once for all variables).  Keeping
+// the tile's U^n in shared memory from the load phase for the epilogue,
+// instead of reading it there, ran slower (0.434 vs 0.430; FP32 members 3 %
+// slower); so did the per-cell net-flux sums in shared memory (0.390 vs
+// 0.381) and a 32x14 tile of 512 threads at 64 registers (0.394).  All of
+// these are build-time knobs; the FP32 units build with three blocks per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
 #endif
@@ -93,7 +97,7 @@ template<> struct TileShape<2, 1> {
 // 3-D: an 8x8x4 tile needs 320/320/384 reconstructions and 288/288/320
 // face fluxes along x/y/z; its FP64 shared memory (90 KB) allows two blocks
 // per SM.  Measured on KH 128^3 x 8 members (FP64, ms per RK3 step):
-//   8x8x4 / 320 threads / 2 blocks (96 regs)   15.9
+//   8x8x4 / 320 threads / 2 blocks (96 regs)   15.9  (12.4 with the current flux and staging)
 //   8x4x4 / 192 threads / 4 blocks             17.2
 //   8x8x4 / 384 threads / 2 blocks (80 regs)   17.2
 //   8x8x2 / 256 threads / 3 blocks             19.8
@@ -110,7 +114,10 @@ template<> struct TileShape<3, 0> {
         B = ALS_STAGE3_BLOCKS;
 };
 // 3-D shape 1: 16 x 16 columns marching along z over segments of
-// ALS_ZMARCH_SEG cells (stage_zmarch.cuh), 288 threads.
+// ALS_ZMARCH_SEG cells (stage_zmarch.cuh), 288 threads (96 registers at two
+// blocks per SM).  KH 128^3 x 8, FP64, ms per RK3 step: 10.59 (segments of
+// 16: 10.66; 320 threads: 10.60; 256 threads, 128 registers but two rounds
+// per x-y phase: 12.17), against 12.40 for the 8x8x4 boxes.
 #ifndef ALS_ZMARCH_SEG
 #define ALS_ZMARCH_SEG 32
 #endif
