@@ -51,7 +51,9 @@ namespace als {
 // the tile's U^n in shared memory from the load phase for the epilogue,
 // instead of reading it there, ran slower (0.434 vs 0.430; FP32 members 3 %
 // slower); so did the per-cell net-flux sums in shared memory (0.390 vs
-// 0.381) and a 32x14 tile of 512 threads at 64 registers (0.394).  All of
+// 0.381), a 32x14 tile of 512 threads at 64 registers (0.394) and the x
+// direction done per warp on a row of a 30x17 tile with warp shuffles
+// instead of shared memory and barriers (0.423).  All of
 // these are build-time knobs; the FP32 units build with three blocks per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
