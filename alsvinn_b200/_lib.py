@@ -138,6 +138,7 @@ PROTOTYPES = {
     "als_mlp_set_params": (ctypes.c_int, [_VP, _VP]),
     "als_mlp_get_params": (ctypes.c_int, [_VP, _VP]),
     "als_mlp_forward": (ctypes.c_int, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
+    "als_mlp_forward_layers": (ctypes.c_int, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
     "als_mlp_gradients": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _VP,
                                          ctypes.POINTER(ctypes.c_float), _VP]),
     "als_mlp_train": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_float,

@@ -90,6 +90,10 @@ struct als_mlp {
     // two activation buffers, every hidden weight matrix
     bool tma = false;
     CUtensorMap tm_x, tm_h[2], tm_w[6];
+    // the whole-network inference kernel's maps (the packed inputs and the
+    // hidden weights); `fused` when it applies (width 256, biases aligned)
+    bool fused = false;
+    FusedMaps fmaps;
     std::vector<void*> allocations;
 };
 
@@ -189,6 +193,52 @@ int setup_tma(als_mlp* s) {
         MLP_TRY(encode_bf16_map(&s->tm_w[l], s->layers[l].wb, 256, s->layers[l].kpad, 256));
     }
     s->tma = true;
+    // the fused kernel reads biases and head weights as float4
+    bool aligned = (s->layers[s->cfg.hidden].w_off & 3) == 0;
+    s->fmaps.x = s->tm_x;
+    for (int l = 0; l < s->cfg.hidden; ++l) {
+        s->fmaps.w[l] = s->tm_w[l];
+        aligned = aligned && (s->layers[l].b_off & 3) == 0;
+    }
+    s->fused = aligned && kInferChunk % (2 * kTileM) == 0;
+    return ALS_OK;
+}
+
+int sm_count(int* sms) {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0;
+        MLP_CUDA(cudaGetDevice(&dev));
+        MLP_CUDA(cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev));
+    }
+    *sms = cached;
+    return ALS_OK;
+}
+
+// The whole network over `rows_pad` packed rows (a multiple of 256) of
+// s->xi in one launch; y[r] for r < rows_valid.
+int launch_fused_forward(als_mlp* s, long long rows_pad, long long rows_valid, float* y,
+                         cudaStream_t st) {
+    FusedArgs f = {};
+    for (int l = 0; l < s->cfg.hidden; ++l) {
+        f.bias[l] = s->p + s->layers[l].b_off;
+        f.nk[l] = s->layers[l].kpad / kChunkK;
+    }
+    const Layer& head = s->layers[s->cfg.hidden];
+    f.layers = s->cfg.hidden;
+    f.head_w = s->p + head.w_off;
+    f.head_b = s->p + head.b_off;
+    f.y = y;
+    f.rows_valid = rows_valid;
+    f.pairs = int(rows_pad / (2 * kTileM));
+    f.error = s->error;
+    f.wait_limit = s->wait_limit;
+    f.withhold_commit = s->withhold_commit;
+    int sms = 0;
+    MLP_TRY(sm_count(&sms));
+    mlp_forward_fused<<<f.pairs < sms ? f.pairs : sms, kTmaThreads, fused_smem_bytes(), st>>>(
+        s->fmaps, f);
+    MLP_CUDA(cudaGetLastError());
     return ALS_OK;
 }
 
@@ -420,6 +470,8 @@ int configure_kernels() {
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
     MLP_CUDA(cudaFuncSetAttribute(gemm_tma_forward<4, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tma_smem_bytes()));
+    MLP_CUDA(cudaFuncSetAttribute(mlp_forward_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  fused_smem_bytes()));
     MLP_TRY((configure_one<64, EPI_FORWARD>()));
     MLP_TRY((configure_one<128, EPI_FORWARD>()));
     MLP_TRY((configure_one<256, EPI_FORWARD>()));
@@ -433,6 +485,42 @@ int reset_adam(als_mlp* s, cudaStream_t st) {
     MLP_CUDA(cudaMemsetAsync(s->v, 0, sizeof(float) * s->nparams, st));
     MLP_CUDA(cudaMemsetAsync(s->step, 0, sizeof(long long), st));
     return ALS_OK;
+}
+
+// Inference in chunks of kInferChunk rows: the whole-network kernel when it
+// applies and `fused` is set, else one launch per layer (and the head).
+int forward_rows(als_mlp* s, const float* x_dev, long long rows, float* y_dev, void* stream,
+                 bool fused) {
+    if (!s || rows < 0 || (rows > 0 && (!x_dev || !y_dev))) {
+        return mlp_fail(ALS_E_INVALID, "invalid argument");
+    }
+    MLP_CUDA(cudaSetDevice(s->device));
+    MLP_TRY(join_caller(s, stream));
+    const cudaStream_t st = s->stream;
+    const Layer& L0 = s->layers[0];
+    const Layer& head = s->layers[s->cfg.hidden];
+    for (long long r0 = 0; r0 < rows; r0 += kInferChunk) {
+        const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
+        const bool whole = fused && s->fused;
+        const long long tile = whole ? 2 * kTileM : kTileM;
+        const long long rp = (n + tile - 1) / tile * tile;
+        pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, st>>>(
+            x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, s->xi, rp, L0.kpad);
+        MLP_CUDA(cudaGetLastError());
+        if (whole) {
+            MLP_TRY(launch_fused_forward(s, rp, n, y_dev + r0, st));
+            continue;
+        }
+        const __nv_bfloat16* last = nullptr;
+        MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st,
+                               s->tma ? y_dev + r0 : nullptr, n));
+        if (!s->tma) {
+            head_forward<<<grid_for(n * 32, 256), 256, 0, st>>>(last, s->cfg.width,
+                s->p + head.w_off, s->p + head.b_off, n, y_dev + r0);
+            MLP_CUDA(cudaGetLastError());
+        }
+    }
+    return check_error_flag(s);
 }
 
 } // namespace
@@ -589,30 +677,12 @@ int als_mlp_get_params(const als_mlp* s, float* params) {
 }
 
 int als_mlp_forward(als_mlp* s, const float* x_dev, long long rows, float* y_dev, void* stream) {
-    if (!s || rows < 0 || (rows > 0 && (!x_dev || !y_dev))) {
-        return mlp_fail(ALS_E_INVALID, "invalid argument");
-    }
-    MLP_CUDA(cudaSetDevice(s->device));
-    MLP_TRY(join_caller(s, stream));
-    const cudaStream_t st = s->stream;
-    const Layer& L0 = s->layers[0];
-    const Layer& head = s->layers[s->cfg.hidden];
-    for (long long r0 = 0; r0 < rows; r0 += kInferChunk) {
-        const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
-        const long long rp = (n + kTileM - 1) / kTileM * kTileM;
-        pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, st>>>(
-            x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, s->xi, rp, L0.kpad);
-        MLP_CUDA(cudaGetLastError());
-        const __nv_bfloat16* last = nullptr;
-        MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st,
-                               s->tma ? y_dev + r0 : nullptr, n));
-        if (!s->tma) {
-            head_forward<<<grid_for(n * 32, 256), 256, 0, st>>>(last, s->cfg.width,
-                s->p + head.w_off, s->p + head.b_off, n, y_dev + r0);
-            MLP_CUDA(cudaGetLastError());
-        }
-    }
-    return check_error_flag(s);
+    return forward_rows(s, x_dev, rows, y_dev, stream, true);
+}
+
+int als_mlp_forward_layers(als_mlp* s, const float* x_dev, long long rows, float* y_dev,
+                           void* stream) {
+    return forward_rows(s, x_dev, rows, y_dev, stream, false);
 }
 
 int als_mlp_gradients(als_mlp* s, const float* x_dev, const float* t_dev, int rows,

@@ -382,6 +382,309 @@ __global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_con
     }
 }
 
+// Inference of the whole network in one persistent kernel: every layer of a
+// pair of 128-row tiles runs with the activations kept in shared memory.
+//   warp 0  TMA producer: the two tiles' packed inputs (128 x 64 each) into
+//           the first K chunk of their activation buffers, then every
+//           layer's weight matrix, 64-wide K chunk by chunk (256 x 64,
+//           32 KB), through a ring of kFusedRing stages;
+//   warp 1  MMA issuer: per layer and K chunk, the chunk's MMAs for both
+//           tiles (so each weight chunk crosses from L2 once per pair) into
+//           the tiles' TMEM accumulators (2 x 256 columns);
+//   warps 4..19  epilogue: bias + GELU of both accumulators, BF16, written
+//           straight into the tiles' activation buffers in the 128-byte
+//           swizzled K-major layout the next layer's MMAs read (the layout a
+//           SWIZZLE_128B TMA load produces); after the last layer the
+//           256 -> 1 head instead, as gemm_tma_forward<NK, true> folds it.
+// Each layer's MMAs are issued chunk by chunk, K step by K step, as
+// gemm_tma_forward issues them, and the epilogue rounds at the same points,
+// so the results equal the per-layer kernels' bit for bit.  The activations
+// never leave the SM: per pair only the inputs (32 KB) come from HBM and the
+// weights (32 KB + 128 KB per hidden layer) from L2.  Every wait is bounded;
+// a timeout sets the error flag and the roles drain and return.
+constexpr int kFusedRing = 2;
+constexpr int kMaxFusedLayers = 6;
+constexpr uint32_t kActBytes = kTileM * 256 * 2;         // one tile's activations (64 KB)
+constexpr uint32_t kChunkBytes = kTileM * kChunkK * 2;   // one 64-wide K chunk of a tile (16 KB)
+constexpr uint32_t kWChunkBytes = 256 * kChunkK * 2;     // one weight K chunk (32 KB)
+
+constexpr int fused_smem_bytes() {
+    return int(2 * kActBytes + kFusedRing * kWChunkBytes) + 1024;
+}
+
+struct FusedMaps {
+    CUtensorMap x;                       // packed inputs (rows x 64), box 64 x 128
+    CUtensorMap w[kMaxFusedLayers];      // layer weights (256 x kpad), box 64 x 256
+};
+
+struct FusedArgs {
+    const float* bias[kMaxFusedLayers];  // 16-byte aligned
+    int nk[kMaxFusedLayers];             // 64-wide K chunks of each layer
+    int layers;
+    const float* head_w;                 // 16-byte aligned
+    const float* head_b;
+    float* y;
+    long long rows_valid;
+    int pairs;                           // tile pairs (rows_pad / 256)
+    int* error;                          // set to 1 when a wait gave up
+    unsigned wait_limit;                 // polls per wait; 0: kWaitLimit
+    int withhold_commit;                 // failure-detection test: the layer
+                                         // completions are never committed
+};
+
+__global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_constant__ FusedMaps maps,
+                                                                 const __grid_constant__ FusedArgs g) {
+    constexpr int BN = 256;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t x_full[2];
+    __shared__ uint64_t a_free[2];
+    __shared__ uint64_t a_ready;
+    __shared__ uint64_t b_full[kFusedRing];
+    __shared__ uint64_t b_empty[kFusedRing];
+    __shared__ uint64_t t_full;
+    __shared__ uint64_t drain;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    __shared__ float head_part[2][4][kTileM];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = base;                       // 2 tiles x 64 KB of activations
+    unsigned char* sB = base + 2 * kActBytes;       // kFusedRing x 32 KB of weights
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int L = g.layers;
+    const unsigned limit = g.wait_limit ? g.wait_limit : kWaitLimit;
+    if (warp == 0) {
+        tmem_alloc(&tmem_base, 2 * BN);
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&x_full[s], 1);
+            mbar_init(&a_free[s], 1);
+        }
+        mbar_init(&a_ready, 16);             // one arrival per epilogue warp
+        for (int r = 0; r < kFusedRing; ++r) {
+            mbar_init(&b_full[r], 1);
+            mbar_init(&b_empty[r], 1);
+        }
+        mbar_init(&t_full, 1);
+        mbar_init(&drain, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    volatile int* abort_v = &abort_flag;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;            // weight chunks issued
+            int nx = 0;            // pairs whose inputs were issued
+            for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x) {
+                // the previous pair's last MMAs no longer read the buffers
+                if (nx > 0 && !(mbar_wait(&a_free[0], unsigned((nx - 1) & 1), limit) &&
+                                mbar_wait(&a_free[1], unsigned((nx - 1) & 1), limit))) {
+                    *abort_v = 1;
+                    break;
+                }
+                for (int s = 0; s < 2; ++s) {
+                    mbar_expect_tx(&x_full[s], kChunkBytes);
+                    tma_load_2d(sA + s * kActBytes, &maps.x, 0, (2 * q + s) * kTileM, &x_full[s]);
+                }
+                ++nx;
+                for (int l = 0; l < L && !*abort_v; ++l) {
+                    for (int c = 0; c < g.nk[l]; ++c, ++it) {
+                        const int slot = it % kFusedRing;
+                        if (it >= kFusedRing &&
+                            !mbar_wait(&b_empty[slot], unsigned((it / kFusedRing - 1) & 1), limit)) {
+                            *abort_v = 1;
+                            break;
+                        }
+                        mbar_expect_tx(&b_full[slot], kWChunkBytes);
+                        tma_load_2d(sB + slot * kWChunkBytes, &maps.w[l], c * kChunkK, 0,
+                                    &b_full[slot]);
+                    }
+                }
+            }
+            // copies still in flight (an aborted run) land before the block exits
+            for (int r = 0; r < kFusedRing; ++r) {
+                const int n = it > r ? (it - r + kFusedRing - 1) / kFusedRing : 0;
+                if (n > 0) {
+                    mbar_wait(&b_full[r], unsigned((n - 1) & 1));
+                }
+            }
+            if (nx > 0) {
+                mbar_wait(&x_full[0], unsigned((nx - 1) & 1));
+                mbar_wait(&x_full[1], unsigned((nx - 1) & 1));
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc_bf16(kTileM, BN);
+            bool ok = true;
+            int it = 0;
+            int k = 0;             // layer passes of this block
+            int pi = 0;
+            for (int q = blockIdx.x; ok && q < g.pairs && !*abort_v; q += gridDim.x, ++pi) {
+                for (int l = 0; ok && l < L; ++l, ++k) {
+                    if (l == 0) {
+                        ok = mbar_wait(&x_full[0], unsigned(pi & 1), limit) &&
+                            mbar_wait(&x_full[1], unsigned(pi & 1), limit);
+                    }
+                    // the epilogue has read the accumulators and written this
+                    // layer's input activations
+                    if (ok && k > 0) {
+                        ok = mbar_wait(&a_ready, unsigned((k - 1) & 1), limit);
+                    }
+                    if (!ok) {
+                        break;
+                    }
+                    tc_fence_after();
+                    for (int c = 0; c < g.nk[l]; ++c, ++it) {
+                        const int slot = it % kFusedRing;
+                        if (!mbar_wait(&b_full[slot], unsigned((it / kFusedRing) & 1), limit)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t b0 = smem_u32(sB + slot * kWChunkBytes);
+#pragma unroll
+                        for (int s = 0; s < 2; ++s) {
+                            const uint32_t a0 = smem_u32(sA + s * kActBytes + c * kChunkBytes);
+#pragma unroll
+                            for (int j = 0; j < kChunkK / 16; ++j) {
+                                mma_bf16(tmem + uint32_t(s * BN), smem_desc_sw128(a0 + j * 32),
+                                         smem_desc_sw128(b0 + j * 32), idesc,
+                                         (c > 0 || j > 0) ? 1u : 0u);
+                            }
+                        }
+                        mma_commit(&b_empty[slot]);
+                    }
+                    if (!ok) {
+                        break;
+                    }
+                    if (!g.withhold_commit) {
+                        mma_commit(&t_full);
+                    }
+                    if (l == L - 1) {
+                        mma_commit(&a_free[0]);
+                        mma_commit(&a_free[1]);
+                    }
+                }
+            }
+            if (!ok) {
+                *abort_v = 1;
+            }
+            // every MMA this thread issued is complete before TMEM is freed
+            mma_commit(&drain);
+            mbar_wait(&drain, 0);
+        }
+    } else if (warp >= kEpiWarp0) {
+        const int ew = warp - kEpiWarp0;          // 0..15
+        const int quarter = warp & 3;             // TMEM lanes 32 quarter .. + 31
+        const int cg = ew >> 2;                   // columns 64 cg .. + 63
+        const int row = quarter * 32 + lane;
+        const float* head_w = g.head_w;
+        int k = 0;
+        for (int q = blockIdx.x; q < g.pairs; q += gridDim.x) {
+            for (int l = 0; l < L; ++l, ++k) {
+                const bool last = l == L - 1;
+                const float* bias = g.bias[l];
+                bool ok = !*abort_v && mbar_wait(&t_full, unsigned(k & 1), limit);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) {
+                    *abort_v = 1;
+                } else {
+                    tc_fence_after();
+#pragma unroll 1
+                    for (int s = 0; s < 2; ++s) {
+                        const uint32_t lane_base =
+                            tmem + uint32_t(s * BN) + (uint32_t(quarter * 32) << 16);
+                        // this row of every K chunk: 8-row atoms of 1024 bytes
+                        unsigned char* arow = sA + s * kActBytes + (row >> 3) * 1024 + (row & 7) * 128;
+                        float hsum = 0.0f;
+#pragma unroll 1
+                        for (int c0 = cg * 64; c0 < cg * 64 + 64; c0 += 16) {
+                            float v[16];
+                            tmem_load16(lane_base + uint32_t(c0), v);
+                            __align__(16) float b[16];
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) {
+                                reinterpret_cast<float4*>(b)[i] =
+                                    reinterpret_cast<const float4*>(bias + c0)[i];
+                            }
+                            if (!last) {
+                                __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+                                for (int i = 0; i < 16; ++i) {
+                                    hb[i] = __float2bfloat16_rn(gelu(v[i] + b[i]));
+                                }
+                                // next layer's K chunk c0 / 64, 16-byte units u0 and
+                                // u0 + 1, swizzled by the row within its atom
+                                unsigned char* chunk = arow + (c0 >> 6) * kChunkBytes;
+                                const int u0 = (c0 & 63) >> 3;
+                                *reinterpret_cast<uint4*>(chunk + ((u0 ^ (row & 7)) << 4)) =
+                                    reinterpret_cast<const uint4*>(hb)[0];
+                                *reinterpret_cast<uint4*>(chunk + (((u0 + 1) ^ (row & 7)) << 4)) =
+                                    reinterpret_cast<const uint4*>(hb)[1];
+                            } else {
+                                __align__(16) float w[16];
+#pragma unroll
+                                for (int i = 0; i < 4; ++i) {
+                                    reinterpret_cast<float4*>(w)[i] =
+                                        reinterpret_cast<const float4*>(head_w + c0)[i];
+                                }
+#pragma unroll
+                                for (int i = 0; i < 16; ++i) {
+                                    const float h = __bfloat162float(
+                                        __float2bfloat16_rn(gelu(v[i] + b[i])));
+                                    hsum += h * w[i];
+                                }
+                            }
+                        }
+                        if (last) {
+                            head_part[s][cg][row] = hsum;
+                        }
+                    }
+                }
+                if (last) {
+                    // every epilogue warp passes this barrier once per pair, aborted or not
+                    named_barrier_sync(1, 16 * 32);
+                    const int et = ew * 32 + lane;       // 0..511
+                    if (!*abort_v && et < 2 * kTileM) {
+                        const int s = et / kTileM;
+                        const int r = et - s * kTileM;
+                        const long long m = (long long)(2 * q + s) * kTileM + r;
+                        if (m < g.rows_valid) {
+                            g.y[m] = ((head_part[s][0][r] + head_part[s][1][r]) +
+                                      (head_part[s][2][r] + head_part[s][3][r])) + g.head_b[0];
+                        }
+                    }
+                }
+                // the accumulators are read, and this layer's outputs visible to
+                // the tensor core, before the next layer's MMAs are issued
+                tc_fence_before();
+                fence_async_shared();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&a_ready);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_v) {
+        atomicExch(g.error, 1);
+    }
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_free(tmem, 2 * BN);
+    }
+}
+
 // x (rows x nin, FP32) -> xb (rows_pad x kpad, BF16), zero padded; one
 // 16-byte store of 8 values per work item.
 __global__ void pack_inputs(const float* __restrict__ x, long long rows, int nin,

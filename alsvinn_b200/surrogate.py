@@ -74,13 +74,16 @@ class Surrogate:
             t = t.reshape(shape)
         return t
 
-    def forward_raw(self, x):
-        """Network output for rows of x (no target scaling)."""
+    def forward_raw(self, x, per_layer=False):
+        """Network output for rows of x (no target scaling); `per_layer`
+        runs one kernel per layer instead of the whole-network kernel (the
+        same results)."""
         x = self._dev(x)
         rows = x.shape[0]
         y = self._torch.empty(rows, dtype=self._torch.float32, device=self.device)
         stream = self._torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(self._lib.als_mlp_forward(self._h, x.data_ptr(), rows, y.data_ptr(), stream))
+        fn = self._lib.als_mlp_forward_layers if per_layer else self._lib.als_mlp_forward
+        _lib.check(fn(self._h, x.data_ptr(), rows, y.data_ptr(), stream))
         return y
 
     def __call__(self, x):

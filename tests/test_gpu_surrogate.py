@@ -114,6 +114,58 @@ def test_inference_in_chunks_is_row_independent():
     np.testing.assert_array_equal(full[65500:65700], part)
 
 
+@pytest.mark.parametrize("inputs,hidden", [(40, 4), (64, 1), (7, 2), (33, 6)])
+def test_whole_network_kernel_equals_the_per_layer_kernels(inputs, hidden):
+    """The 256-wide network's inference runs as one kernel (activations kept
+    on the SM); its outputs equal those of one kernel per layer bit for bit,
+    for ragged row counts, a row count that crosses the 262,144-row chunk,
+    and every depth.  The per-layer path is itself checked against the
+    oracle above."""
+    rng = np.random.default_rng(inputs * 10 + hidden)
+    with als.Surrogate(inputs, 256, hidden, max_batch=1024, seed=hidden) as s:
+        for rows in (1, 127, 255, 256, 257, 5000, 262144 + 300):
+            x = torch.tensor(rng.uniform(0, 1, (rows, inputs)).astype(np.float32), device="cuda:0")
+            fused = s.forward_raw(x).cpu().numpy()
+            layered = s.forward_raw(x, per_layer=True).cpu().numpy()
+            np.testing.assert_array_equal(fused, layered, err_msg="rows %d" % rows)
+
+
+@pytest.mark.parametrize("hidden", [1, 6])
+def test_whole_network_kernel_matches_oracle(hidden):
+    inputs, rows = 40, 700
+    rng = np.random.default_rng(hidden)
+    x = rng.uniform(0, 1, (rows, inputs)).astype(np.float32)
+    with als.Surrogate(inputs, 256, hidden, max_batch=1024, seed=13) as s:
+        y = s.forward_raw(x).cpu().numpy().astype(np.float64)
+        p = s.params()
+    ref, _ = mo.forward(p, x, inputs, 256, hidden, bf16_path=True)
+    scale = np.abs(ref).max() + 1e-3
+    # the tolerances of test_forward_matches_oracle
+    assert np.abs(y - ref).max() <= 1e-2 * scale, np.abs(y - ref).max()
+    assert np.abs(y - ref).mean() <= 1e-3 * scale
+
+
+def test_whole_network_kernel_wait_timeout_is_reported_and_the_handle_recovers():
+    """Failure detection without a fault: with the layer completions of the
+    whole-network kernel withheld, the epilogue's bounded waits run out, the
+    roles drain their MMAs and copies, free tensor memory and return, and the
+    call reports ALS_E_CUDA.  Afterwards the same handle gives the same
+    outputs as before, bit for bit."""
+    rng = np.random.default_rng(12)
+    x = torch.tensor(rng.random((3000, 40), dtype=np.float32), device="cuda:0")
+    with als.Surrogate(seed=5) as s:
+        y0 = s.forward_raw(x).cpu().numpy()
+        lib = als._lib.load()
+        als._lib.check(lib.als_mlp_test_wait_timeout(s._h, 1024, 1))
+        with pytest.raises(als._lib.AlsError) as err:
+            s.forward_raw(x)
+        assert err.value.code == -2 and "timed out" in str(err.value)
+        als._lib.check(lib.als_mlp_test_wait_timeout(s._h, 0, 0))
+        torch.cuda.synchronize()
+        y1 = s.forward_raw(x).cpu().numpy()
+    np.testing.assert_array_equal(y0, y1)
+
+
 def test_device_uniform_draws_and_moments():
     with als.Surrogate(seed=3) as s:
         x = torch.empty(40 * 4096, dtype=torch.float32, device="cuda")
