@@ -193,14 +193,11 @@ int setup_tma(als_mlp* s) {
         MLP_TRY(encode_bf16_map(&s->tm_w[l], s->layers[l].wb, 256, s->layers[l].kpad, 256));
     }
     s->tma = true;
-    // the fused kernel reads biases and head weights as float4
-    bool aligned = (s->layers[s->cfg.hidden].w_off & 3) == 0;
     s->fmaps.x = s->tm_x;
     for (int l = 0; l < s->cfg.hidden; ++l) {
         s->fmaps.w[l] = s->tm_w[l];
-        aligned = aligned && (s->layers[l].b_off & 3) == 0;
     }
-    s->fused = aligned && kInferChunk % (2 * kTileM) == 0;
+    s->fused = kInferChunk % (2 * kTileM) == 0;
     return ALS_OK;
 }
 
@@ -487,8 +484,9 @@ int reset_adam(als_mlp* s, cudaStream_t st) {
     return ALS_OK;
 }
 
-// Inference in chunks of kInferChunk rows: the whole-network kernel when it
-// applies and `fused` is set, else one launch per layer (and the head).
+// Inference in chunks of kInferChunk rows: the input packing, then the
+// whole-network kernel when it applies and `fused` is set, else one launch
+// per layer (and the head).
 int forward_rows(als_mlp* s, const float* x_dev, long long rows, float* y_dev, void* stream,
                  bool fused) {
     if (!s || rows < 0 || (rows > 0 && (!x_dev || !y_dev))) {

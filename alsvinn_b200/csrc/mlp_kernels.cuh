@@ -418,10 +418,10 @@ struct FusedMaps {
 };
 
 struct FusedArgs {
-    const float* bias[kMaxFusedLayers];  // 16-byte aligned
+    const float* bias[kMaxFusedLayers];
     int nk[kMaxFusedLayers];             // 64-wide K chunks of each layer
     int layers;
-    const float* head_w;                 // 16-byte aligned
+    const float* head_w;
     const float* head_b;
     float* y;
     long long rows_valid;
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
     constexpr int BN = 256;
     extern __shared__ unsigned char smem_raw[];
     __shared__ uint64_t x_full[2];
-    __shared__ uint64_t a_free[2];
+    __shared__ uint64_t a_free;
     __shared__ uint64_t a_ready;
     __shared__ uint64_t b_full[kFusedRing];
     __shared__ uint64_t b_empty[kFusedRing];
@@ -446,6 +446,8 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     __shared__ float head_part[2][4][kTileM];
+    // the layers' biases, then the head's weights (read by every row)
+    __shared__ __align__(16) float s_par[kMaxFusedLayers + 1][256];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* sA = base;                       // 2 tiles x 64 KB of activations
@@ -458,10 +460,9 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         tmem_alloc(&tmem_base, 2 * BN);
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < 2; ++s) {
-            mbar_init(&x_full[s], 1);
-            mbar_init(&a_free[s], 1);
-        }
+        mbar_init(&x_full[0], 1);
+        mbar_init(&x_full[1], 1);
+        mbar_init(&a_free, 1);
         mbar_init(&a_ready, 16);             // one arrival per epilogue warp
         for (int r = 0; r < kFusedRing; ++r) {
             mbar_init(&b_full[r], 1);
@@ -471,6 +472,10 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         mbar_init(&drain, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < (L + 1) * 256; i += blockDim.x) {
+        const int l = i >> 8;
+        s_par[l][i & 255] = l < L ? g.bias[l][i & 255] : g.head_w[i & 255];
     }
     tc_fence_before();
     __syncthreads();
@@ -484,8 +489,7 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
             int nx = 0;            // pairs whose inputs were issued
             for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x) {
                 // the previous pair's last MMAs no longer read the buffers
-                if (nx > 0 && !(mbar_wait(&a_free[0], unsigned((nx - 1) & 1), limit) &&
-                                mbar_wait(&a_free[1], unsigned((nx - 1) & 1), limit))) {
+                if (nx > 0 && !mbar_wait(&a_free, unsigned((nx - 1) & 1), limit)) {
                     *abort_v = 1;
                     break;
                 }
@@ -569,8 +573,7 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                         mma_commit(&t_full);
                     }
                     if (l == L - 1) {
-                        mma_commit(&a_free[0]);
-                        mma_commit(&a_free[1]);
+                        mma_commit(&a_free);
                     }
                 }
             }
@@ -586,12 +589,12 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         const int quarter = warp & 3;             // TMEM lanes 32 quarter .. + 31
         const int cg = ew >> 2;                   // columns 64 cg .. + 63
         const int row = quarter * 32 + lane;
-        const float* head_w = g.head_w;
+        const float* head_w = s_par[L];
         int k = 0;
         for (int q = blockIdx.x; q < g.pairs; q += gridDim.x) {
             for (int l = 0; l < L; ++l, ++k) {
                 const bool last = l == L - 1;
-                const float* bias = g.bias[l];
+                const float* bias = s_par[l];
                 bool ok = !*abort_v && mbar_wait(&t_full, unsigned(k & 1), limit);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) {
@@ -605,22 +608,34 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                         // this row of every K chunk: 8-row atoms of 1024 bytes
                         unsigned char* arow = sA + s * kActBytes + (row >> 3) * 1024 + (row & 7) * 128;
                         float hsum = 0.0f;
-#pragma unroll 1
-                        for (int c0 = cg * 64; c0 < cg * 64 + 64; c0 += 16) {
-                            float v[16];
-                            tmem_load16(lane_base + uint32_t(c0), v);
+                        // 16 columns at a time; the next 16 are read from TMEM
+                        // while these are computed
+                        uint32_t r[2][16];
+                        tmem_load16_start(lane_base + uint32_t(cg * 64), r[0]);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            tmem_load_wait(r[j & 1]);
+                            if (j < 3) {
+                                tmem_load16_start(lane_base + uint32_t(cg * 64 + 16 * (j + 1)),
+                                                  r[(j + 1) & 1]);
+                            }
+                            const int c0 = cg * 64 + 16 * j;
                             __align__(16) float b[16];
 #pragma unroll
                             for (int i = 0; i < 4; ++i) {
                                 reinterpret_cast<float4*>(b)[i] =
                                     reinterpret_cast<const float4*>(bias + c0)[i];
                             }
-                            if (!last) {
-                                __align__(16) __nv_bfloat16 hb[16];
+                            // BF16 rounding of pairs (each element rounded to
+                            // nearest even, as the scalar conversion does)
+                            __nv_bfloat162 hb[8];
 #pragma unroll
-                                for (int i = 0; i < 16; ++i) {
-                                    hb[i] = __float2bfloat16_rn(gelu(v[i] + b[i]));
-                                }
+                            for (int i = 0; i < 8; ++i) {
+                                hb[i] = __floats2bfloat162_rn(
+                                    gelu(__uint_as_float(r[j & 1][2 * i]) + b[2 * i]),
+                                    gelu(__uint_as_float(r[j & 1][2 * i + 1]) + b[2 * i + 1]));
+                            }
+                            if (!last) {
                                 // next layer's K chunk c0 / 64, 16-byte units u0 and
                                 // u0 + 1, swizzled by the row within its atom
                                 unsigned char* chunk = arow + (c0 >> 6) * kChunkBytes;
@@ -637,10 +652,9 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                                         reinterpret_cast<const float4*>(head_w + c0)[i];
                                 }
 #pragma unroll
-                                for (int i = 0; i < 16; ++i) {
-                                    const float h = __bfloat162float(
-                                        __float2bfloat16_rn(gelu(v[i] + b[i])));
-                                    hsum += h * w[i];
+                                for (int i = 0; i < 8; ++i) {
+                                    hsum += __low2float(hb[i]) * w[2 * i];
+                                    hsum += __high2float(hb[i]) * w[2 * i + 1];
                                 }
                             }
                         }

@@ -66,15 +66,20 @@ __device__ __forceinline__ float tanh_hw(float x) {
     return y;
 }
 
+// The argument as z (k + k a z^2) and the value as z/2 + z/2 tanh(u): three
+// and two operations around the tanh.
+__device__ __forceinline__ float gelu_arg(float z) {
+    return z * fmaf(0.035677408136300125f, z * z, 0.79788456080286536f);
+}
+
 __device__ __forceinline__ float gelu(float z) {
-    const float u = 0.79788456080286536f * (z + 0.044715f * z * z * z);
-    return 0.5f * z * (1.0f + tanh_hw(u));
+    const float hz = 0.5f * z;
+    return fmaf(hz, tanh_hw(gelu_arg(z)), hz);
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
     // d/dz: (1 + t)/2 + z/2 (1 - t^2) k (1 + 3 a z^2), t = tanh(u)
-    const float u = 0.79788456080286536f * (z + 0.044715f * z * z * z);
-    const float t = tanh_hw(u);
+    const float t = tanh_hw(gelu_arg(z));
     return 0.5f * (1.0f + t) +
         0.5f * z * (1.0f - t * t) * 0.79788456080286536f * (1.0f + 0.134145f * z * z);
 }
@@ -160,6 +165,29 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 32 lanes x 32 bits, 16 consecutive columns per thread, without waiting:
+// the registers are valid after tmem_load_wait on them.
+__device__ __forceinline__ void tmem_load16_start(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// Waits for every TMEM load of this thread; the registers of `r` pass
+// through the wait, so no use of them is scheduled before it.
+__device__ __forceinline__ void tmem_load_wait(uint32_t* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
 }
 
 // 32 lanes x 32 bits, 16 consecutive columns per thread.

@@ -54,9 +54,10 @@ int als_mlp_set_params(als_mlp* h, const float* params);
 int als_mlp_get_params(const als_mlp* h, float* params);
 
 /* Inference: y_dev[r] = f(x_dev[r, :]) for `rows` rows of `inputs` FP32
- * features (row-major).  Any number of rows.  A 256-wide network runs as one
- * kernel per 262,144 rows (every layer and the head, activations kept on the
- * SM); other widths run one kernel per layer. */
+ * features (row-major).  Any number of rows.  Per 262,144 rows a 256-wide
+ * network runs as two kernels: the inputs' BF16 rounding, then every layer
+ * and the head in one kernel with the activations kept on the SM; other
+ * widths run one kernel per layer. */
 int als_mlp_forward(als_mlp* h, const float* x_dev, long long rows, float* y_dev, void* stream);
 
 /* The same inference with one kernel per layer (activations through device
