@@ -384,24 +384,26 @@ __global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_con
 
 // Inference of the whole network in one persistent kernel: every layer of a
 // pair of 128-row tiles runs with the activations kept in shared memory.
-//   warp 0  TMA producer: the two tiles' packed inputs (128 x 64 each) into
-//           the first K chunk of their activation buffers, then every
-//           layer's weight matrix, 64-wide K chunk by chunk (256 x 64,
+//   warp 0  TMA producer, in the MMA warp's order: each tile's packed inputs
+//           (128 x 64) into the first K chunk of its activation buffer, and
+//           every layer's weight matrix, 64-wide K chunk by chunk (256 x 64,
 //           32 KB), through a ring of kFusedRing stages;
-//   warp 1  MMA issuer: per layer and K chunk, the chunk's MMAs for both
-//           tiles (so each weight chunk crosses from L2 once per pair) into
-//           the tiles' TMEM accumulators (2 x 256 columns);
-//   warps 4..19  epilogue: bias + GELU of both accumulators, BF16, written
-//           straight into the tiles' activation buffers in the 128-byte
-//           swizzled K-major layout the next layer's MMAs read (the layout a
-//           SWIZZLE_128B TMA load produces); after the last layer the
-//           256 -> 1 head instead, as gemm_tma_forward<NK, true> folds it.
+//   warp 1  MMA issuer: the tiles alternate layer by layer (tile 0 layer l,
+//           tile 1 layer l, tile 0 layer l + 1, ...), each into its own TMEM
+//           accumulator (2 x 256 columns), so one tile's MMAs run while the
+//           epilogue works on the other; the weights stream from L2 once
+//           per tile;
+//   warps 4..19  epilogue: bias + GELU of one tile's accumulator, BF16,
+//           written straight into the tile's activation buffer in the
+//           128-byte swizzled K-major layout the next layer's MMAs read (the
+//           layout a SWIZZLE_128B TMA load produces); after the last layer
+//           the 256 -> 1 head instead, as gemm_tma_forward<NK, true> folds it.
 // Each layer's MMAs are issued chunk by chunk, K step by K step, as
 // gemm_tma_forward issues them, and the epilogue rounds at the same points,
 // so the results equal the per-layer kernels' bit for bit.  The activations
-// never leave the SM: per pair only the inputs (32 KB) come from HBM and the
-// weights (32 KB + 128 KB per hidden layer) from L2.  Every wait is bounded;
-// a timeout sets the error flag and the roles drain and return.
+// never leave the SM: per tile only the packed inputs (16 KB) come from HBM
+// and the weights (32 KB + 128 KB per hidden layer) from L2.  Every wait is
+// bounded; a timeout sets the error flag and the roles drain and return.
 constexpr int kFusedRing = 2;
 constexpr int kMaxFusedLayers = 6;
 constexpr uint32_t kActBytes = kTileM * 256 * 2;         // one tile's activations (64 KB)
@@ -437,11 +439,11 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
     constexpr int BN = 256;
     extern __shared__ unsigned char smem_raw[];
     __shared__ uint64_t x_full[2];
-    __shared__ uint64_t a_free;
-    __shared__ uint64_t a_ready;
+    __shared__ uint64_t a_free[2];
+    __shared__ uint64_t a_ready[2];
     __shared__ uint64_t b_full[kFusedRing];
     __shared__ uint64_t b_empty[kFusedRing];
-    __shared__ uint64_t t_full;
+    __shared__ uint64_t t_full[2];
     __shared__ uint64_t drain;
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
@@ -460,15 +462,16 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         tmem_alloc(&tmem_base, 2 * BN);
     }
     if (threadIdx.x == 0) {
-        mbar_init(&x_full[0], 1);
-        mbar_init(&x_full[1], 1);
-        mbar_init(&a_free, 1);
-        mbar_init(&a_ready, 16);             // one arrival per epilogue warp
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&x_full[s], 1);
+            mbar_init(&a_free[s], 1);
+            mbar_init(&a_ready[s], 16);      // one arrival per epilogue warp
+            mbar_init(&t_full[s], 1);
+        }
         for (int r = 0; r < kFusedRing; ++r) {
             mbar_init(&b_full[r], 1);
             mbar_init(&b_empty[r], 1);
         }
-        mbar_init(&t_full, 1);
         mbar_init(&drain, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -485,30 +488,35 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
 
     if (warp == 0) {
         if (lane == 0) {
+            // in the MMA warp's order: per pair, layer and tile, the tile's
+            // inputs (first layer) and the layer's weight chunks
             int it = 0;            // weight chunks issued
             int nx = 0;            // pairs whose inputs were issued
-            for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x) {
-                // the previous pair's last MMAs no longer read the buffers
-                if (nx > 0 && !mbar_wait(&a_free, unsigned((nx - 1) & 1), limit)) {
-                    *abort_v = 1;
-                    break;
-                }
-                for (int s = 0; s < 2; ++s) {
-                    mbar_expect_tx(&x_full[s], kChunkBytes);
-                    tma_load_2d(sA + s * kActBytes, &maps.x, 0, (2 * q + s) * kTileM, &x_full[s]);
-                }
-                ++nx;
+            for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x, ++nx) {
                 for (int l = 0; l < L && !*abort_v; ++l) {
-                    for (int c = 0; c < g.nk[l]; ++c, ++it) {
-                        const int slot = it % kFusedRing;
-                        if (it >= kFusedRing &&
-                            !mbar_wait(&b_empty[slot], unsigned((it / kFusedRing - 1) & 1), limit)) {
-                            *abort_v = 1;
-                            break;
+                    for (int s = 0; s < 2 && !*abort_v; ++s) {
+                        if (l == 0) {
+                            // the previous pair's last MMAs of this tile are done
+                            if (nx > 0 && !mbar_wait(&a_free[s], unsigned((nx - 1) & 1), limit)) {
+                                *abort_v = 1;
+                                break;
+                            }
+                            mbar_expect_tx(&x_full[s], kChunkBytes);
+                            tma_load_2d(sA + s * kActBytes, &maps.x, 0, (2 * q + s) * kTileM,
+                                        &x_full[s]);
                         }
-                        mbar_expect_tx(&b_full[slot], kWChunkBytes);
-                        tma_load_2d(sB + slot * kWChunkBytes, &maps.w[l], c * kChunkK, 0,
-                                    &b_full[slot]);
+                        for (int c = 0; c < g.nk[l]; ++c, ++it) {
+                            const int slot = it % kFusedRing;
+                            if (it >= kFusedRing &&
+                                !mbar_wait(&b_empty[slot], unsigned((it / kFusedRing - 1) & 1),
+                                           limit)) {
+                                *abort_v = 1;
+                                break;
+                            }
+                            mbar_expect_tx(&b_full[slot], kWChunkBytes);
+                            tma_load_2d(sB + slot * kWChunkBytes, &maps.w[l], c * kChunkK, 0,
+                                        &b_full[slot]);
+                        }
                     }
                 }
             }
@@ -526,54 +534,54 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         }
     } else if (warp == 1) {
         if (lane == 0) {
+            // tiles alternate: while the epilogue works on one tile, the
+            // other tile's next layer runs on the tensor core
             const uint32_t idesc = instr_desc_bf16(kTileM, BN);
             bool ok = true;
             int it = 0;
-            int k = 0;             // layer passes of this block
             int pi = 0;
             for (int q = blockIdx.x; ok && q < g.pairs && !*abort_v; q += gridDim.x, ++pi) {
-                for (int l = 0; ok && l < L; ++l, ++k) {
-                    if (l == 0) {
-                        ok = mbar_wait(&x_full[0], unsigned(pi & 1), limit) &&
-                            mbar_wait(&x_full[1], unsigned(pi & 1), limit);
-                    }
-                    // the epilogue has read the accumulators and written this
-                    // layer's input activations
-                    if (ok && k > 0) {
-                        ok = mbar_wait(&a_ready, unsigned((k - 1) & 1), limit);
-                    }
-                    if (!ok) {
-                        break;
-                    }
-                    tc_fence_after();
-                    for (int c = 0; c < g.nk[l]; ++c, ++it) {
-                        const int slot = it % kFusedRing;
-                        if (!mbar_wait(&b_full[slot], unsigned((it / kFusedRing) & 1), limit)) {
-                            ok = false;
+                for (int l = 0; ok && l < L; ++l) {
+                    const int k = pi * L + l;          // layer passes of each tile
+                    for (int s = 0; ok && s < 2; ++s) {
+                        if (l == 0) {
+                            ok = mbar_wait(&x_full[s], unsigned(pi & 1), limit);
+                        }
+                        // the epilogue has read this tile's accumulator and
+                        // written the layer's input activations
+                        if (ok && k > 0) {
+                            ok = mbar_wait(&a_ready[s], unsigned((k - 1) & 1), limit);
+                        }
+                        if (!ok) {
                             break;
                         }
                         tc_fence_after();
-                        const uint32_t b0 = smem_u32(sB + slot * kWChunkBytes);
-#pragma unroll
-                        for (int s = 0; s < 2; ++s) {
+                        const uint32_t d = tmem + uint32_t(s * BN);
+                        for (int c = 0; c < g.nk[l]; ++c, ++it) {
+                            const int slot = it % kFusedRing;
+                            if (!mbar_wait(&b_full[slot], unsigned((it / kFusedRing) & 1), limit)) {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint32_t b0 = smem_u32(sB + slot * kWChunkBytes);
                             const uint32_t a0 = smem_u32(sA + s * kActBytes + c * kChunkBytes);
 #pragma unroll
                             for (int j = 0; j < kChunkK / 16; ++j) {
-                                mma_bf16(tmem + uint32_t(s * BN), smem_desc_sw128(a0 + j * 32),
-                                         smem_desc_sw128(b0 + j * 32), idesc,
-                                         (c > 0 || j > 0) ? 1u : 0u);
+                                mma_bf16(d, smem_desc_sw128(a0 + j * 32), smem_desc_sw128(b0 + j * 32),
+                                         idesc, (c > 0 || j > 0) ? 1u : 0u);
                             }
+                            mma_commit(&b_empty[slot]);
                         }
-                        mma_commit(&b_empty[slot]);
-                    }
-                    if (!ok) {
-                        break;
-                    }
-                    if (!g.withhold_commit) {
-                        mma_commit(&t_full);
-                    }
-                    if (l == L - 1) {
-                        mma_commit(&a_free);
+                        if (!ok) {
+                            break;
+                        }
+                        if (!g.withhold_commit) {
+                            mma_commit(&t_full[s]);
+                        }
+                        if (l == L - 1) {
+                            mma_commit(&a_free[s]);
+                        }
                     }
                 }
             }
@@ -590,19 +598,20 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         const int cg = ew >> 2;                   // columns 64 cg .. + 63
         const int row = quarter * 32 + lane;
         const float* head_w = s_par[L];
-        int k = 0;
-        for (int q = blockIdx.x; q < g.pairs; q += gridDim.x) {
-            for (int l = 0; l < L; ++l, ++k) {
+        int pi = 0;
+        for (int q = blockIdx.x; q < g.pairs; q += gridDim.x, ++pi) {
+            for (int l = 0; l < L; ++l) {
+                const int k = pi * L + l;
                 const bool last = l == L - 1;
                 const float* bias = s_par[l];
-                bool ok = !*abort_v && mbar_wait(&t_full, unsigned(k & 1), limit);
-                ok = __all_sync(0xffffffffu, ok);
-                if (!ok) {
-                    *abort_v = 1;
-                } else {
-                    tc_fence_after();
 #pragma unroll 1
-                    for (int s = 0; s < 2; ++s) {
+                for (int s = 0; s < 2; ++s) {
+                    bool ok = !*abort_v && mbar_wait(&t_full[s], unsigned(k & 1), limit);
+                    ok = __all_sync(0xffffffffu, ok);
+                    if (!ok) {
+                        *abort_v = 1;
+                    } else {
+                        tc_fence_after();
                         const uint32_t lane_base =
                             tmem + uint32_t(s * BN) + (uint32_t(quarter * 32) << 16);
                         // this row of every K chunk: 8-row atoms of 1024 bytes
@@ -662,28 +671,26 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                             head_part[s][cg][row] = hsum;
                         }
                     }
-                }
-                if (last) {
-                    // every epilogue warp passes this barrier once per pair, aborted or not
-                    named_barrier_sync(1, 16 * 32);
-                    const int et = ew * 32 + lane;       // 0..511
-                    if (!*abort_v && et < 2 * kTileM) {
-                        const int s = et / kTileM;
-                        const int r = et - s * kTileM;
-                        const long long m = (long long)(2 * q + s) * kTileM + r;
-                        if (m < g.rows_valid) {
-                            g.y[m] = ((head_part[s][0][r] + head_part[s][1][r]) +
-                                      (head_part[s][2][r] + head_part[s][3][r])) + g.head_b[0];
+                    if (last) {
+                        // every epilogue warp passes this barrier once per tile, aborted or not
+                        named_barrier_sync(1, 16 * 32);
+                        const int et = ew * 32 + lane;       // 0..511
+                        if (!*abort_v && et < kTileM) {
+                            const long long m = (long long)(2 * q + s) * kTileM + et;
+                            if (m < g.rows_valid) {
+                                g.y[m] = ((head_part[s][0][et] + head_part[s][1][et]) +
+                                          (head_part[s][2][et] + head_part[s][3][et])) + g.head_b[0];
+                            }
                         }
                     }
-                }
-                // the accumulators are read, and this layer's outputs visible to
-                // the tensor core, before the next layer's MMAs are issued
-                tc_fence_before();
-                fence_async_shared();
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&a_ready);
+                    // the accumulator is read, and this layer's outputs visible to
+                    // the tensor core, before the tile's next layer is issued
+                    tc_fence_before();
+                    fence_async_shared();
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(&a_ready[s]);
+                    }
                 }
             }
         }
