@@ -90,10 +90,16 @@ struct als_mlp {
     // two activation buffers, every hidden weight matrix
     bool tma = false;
     CUtensorMap tm_x, tm_h[2], tm_w[6];
-    // the whole-network inference kernel's maps (the packed inputs and the
-    // hidden weights); `fused` when it applies (width 256, biases aligned)
+    // the whole-network inference kernel: its maps over either packed-input
+    // buffer (xi, xi2) and the hidden weights; the side stream packs the
+    // next chunk's inputs while the network runs on the current one
     bool fused = false;
-    FusedMaps fmaps;
+    FusedMaps fmaps[2];
+    CUtensorMap tm_x2;
+    __nv_bfloat16* xi2 = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t packed[2] = {nullptr, nullptr};
+    cudaEvent_t xi_free[2] = {nullptr, nullptr};
     std::vector<void*> allocations;
 };
 
@@ -193,9 +199,12 @@ int setup_tma(als_mlp* s) {
         MLP_TRY(encode_bf16_map(&s->tm_w[l], s->layers[l].wb, 256, s->layers[l].kpad, 256));
     }
     s->tma = true;
-    s->fmaps.x = s->tm_x;
+    MLP_TRY(encode_bf16_map(&s->tm_x2, s->xi2, kInferChunk, 64, kTileM));
+    s->fmaps[0].x = s->tm_x;
+    s->fmaps[1].x = s->tm_x2;
     for (int l = 0; l < s->cfg.hidden; ++l) {
-        s->fmaps.w[l] = s->tm_w[l];
+        s->fmaps[0].w[l] = s->tm_w[l];
+        s->fmaps[1].w[l] = s->tm_w[l];
     }
     s->fused = kInferChunk % (2 * kTileM) == 0;
     return ALS_OK;
@@ -213,8 +222,9 @@ int sm_count(int* sms) {
 }
 
 // The whole network over `rows_pad` packed rows (a multiple of 256) of
-// s->xi in one launch; y[r] for r < rows_valid.
-int launch_fused_forward(als_mlp* s, long long rows_pad, long long rows_valid, float* y,
+// packed-input buffer `b` (s->xi, s->xi2) in one launch; y[r] for
+// r < rows_valid.
+int launch_fused_forward(als_mlp* s, int b, long long rows_pad, long long rows_valid, float* y,
                          cudaStream_t st) {
     FusedArgs f = {};
     for (int l = 0; l < s->cfg.hidden; ++l) {
@@ -234,7 +244,7 @@ int launch_fused_forward(als_mlp* s, long long rows_pad, long long rows_valid, f
     int sms = 0;
     MLP_TRY(sm_count(&sms));
     mlp_forward_fused<<<f.pairs < sms ? f.pairs : sms, kTmaThreads, fused_smem_bytes(), st>>>(
-        s->fmaps, f);
+        s->fmaps[b], f);
     MLP_CUDA(cudaGetLastError());
     return ALS_OK;
 }
@@ -485,8 +495,9 @@ int reset_adam(als_mlp* s, cudaStream_t st) {
 }
 
 // Inference in chunks of kInferChunk rows: the input packing, then the
-// whole-network kernel when it applies and `fused` is set, else one launch
-// per layer (and the head).
+// whole-network kernel when it applies and `fused` is set (the packing of
+// the next chunk overlapping the current one), else one launch per layer
+// (and the head).
 int forward_rows(als_mlp* s, const float* x_dev, long long rows, float* y_dev, void* stream,
                  bool fused) {
     if (!s || rows < 0 || (rows > 0 && (!x_dev || !y_dev))) {
@@ -497,18 +508,34 @@ int forward_rows(als_mlp* s, const float* x_dev, long long rows, float* y_dev, v
     const cudaStream_t st = s->stream;
     const Layer& L0 = s->layers[0];
     const Layer& head = s->layers[s->cfg.hidden];
+    if (fused && s->fused) {
+        // chunk i is packed on the side stream into buffer i & 1 while chunk
+        // i - 1 runs through the network on the main stream
+        MLP_CUDA(cudaStreamWaitEvent(s->side, s->ev, 0));   // the caller's prior work
+        int i = 0;
+        for (long long r0 = 0; r0 < rows; r0 += kInferChunk, ++i) {
+            const int b = i & 1;
+            const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
+            const long long rp = (n + 2 * kTileM - 1) / (2 * kTileM) * (2 * kTileM);
+            if (i >= 2) {
+                MLP_CUDA(cudaStreamWaitEvent(s->side, s->xi_free[b], 0));
+            }
+            pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, s->side>>>(
+                x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, b ? s->xi2 : s->xi, rp, L0.kpad);
+            MLP_CUDA(cudaGetLastError());
+            MLP_CUDA(cudaEventRecord(s->packed[b], s->side));
+            MLP_CUDA(cudaStreamWaitEvent(st, s->packed[b], 0));
+            MLP_TRY(launch_fused_forward(s, b, rp, n, y_dev + r0, st));
+            MLP_CUDA(cudaEventRecord(s->xi_free[b], st));
+        }
+        return check_error_flag(s);
+    }
     for (long long r0 = 0; r0 < rows; r0 += kInferChunk) {
         const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
-        const bool whole = fused && s->fused;
-        const long long tile = whole ? 2 * kTileM : kTileM;
-        const long long rp = (n + tile - 1) / tile * tile;
+        const long long rp = (n + kTileM - 1) / kTileM * kTileM;
         pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, st>>>(
             x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, s->xi, rp, L0.kpad);
         MLP_CUDA(cudaGetLastError());
-        if (whole) {
-            MLP_TRY(launch_fused_forward(s, rp, n, y_dev + r0, st));
-            continue;
-        }
         const __nv_bfloat16* last = nullptr;
         MLP_TRY(forward_hidden(s, s->xi, rp, nullptr, nullptr, s->hi, &last, st,
                                s->tma ? y_dev + r0 : nullptr, n));
@@ -557,8 +584,14 @@ int als_mlp_create(const als_mlp_config* cfg, int device, als_mlp** out) {
         s->layers.push_back(L);
     }
     s->nparams = off;
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming) != cudaSuccess) {
+    bool made = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int b = 0; b < 2 && made; ++b) {
+        made = cudaEventCreateWithFlags(&s->packed[b], cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&s->xi_free[b], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!made) {
         return cleanup(mlp_fail(ALS_E_CUDA, "stream/event creation failed"));
     }
     int rc = ALS_OK;
@@ -588,6 +621,9 @@ int als_mlp_create(const als_mlp_config* cfg, int device, als_mlp** out) {
     rc = rc ? rc : dev_alloc(s, &s->col_scratch, size_t(kMaxSplits) * Wd);
     rc = rc ? rc : dev_alloc(s, &s->dy, B);
     rc = rc ? rc : dev_alloc(s, &s->xi, size_t(kInferChunk) * s->layers[0].kpad);
+    if (c.width == 256) {
+        rc = rc ? rc : dev_alloc(s, &s->xi2, size_t(kInferChunk) * s->layers[0].kpad);
+    }
     rc = rc ? rc : dev_alloc(s, &s->hi[0], size_t(kInferChunk) * Wd);
     rc = rc ? rc : dev_alloc(s, &s->hi[1], size_t(kInferChunk) * Wd);
     if (rc) {
@@ -610,14 +646,21 @@ int als_mlp_destroy(als_mlp* s) {
     if (s->stream) {
         cudaStreamSynchronize(s->stream);
     }
+    if (s->side) {
+        cudaStreamSynchronize(s->side);
+    }
     for (void* p : s->allocations) {
         cudaFree(p);
     }
-    if (s->ev) {
-        cudaEventDestroy(s->ev);
+    for (cudaEvent_t e : {s->ev, s->packed[0], s->packed[1], s->xi_free[0], s->xi_free[1]}) {
+        if (e) {
+            cudaEventDestroy(e);
+        }
     }
-    if (s->stream) {
-        cudaStreamDestroy(s->stream);
+    for (cudaStream_t t : {s->stream, s->side}) {
+        if (t) {
+            cudaStreamDestroy(t);
+        }
     }
     delete s;
     return ALS_OK;

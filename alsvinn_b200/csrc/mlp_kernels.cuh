@@ -18,19 +18,22 @@ template <int BN, int EPI>
 __device__ __forceinline__ void epilogue16(const GemmArgs& g, long long m, int n, const float* v,
                                            int n_valid) {
     if (EPI == EPI_FORWARD) {
-        __align__(16) __nv_bfloat16 hb[16];
-        __align__(16) float z[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            z[i] = v[i] + g.bias[n + i];
-            hb[i] = __float2bfloat16_rn(gelu(z[i]));
-        }
         if (g.z) {
+            __align__(16) float z[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                z[i] = v[i] + g.bias[n + i];
+            }
             float4* dz = reinterpret_cast<float4*>(g.z + m * g.ldz + n);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 dz[i] = reinterpret_cast<const float4*>(z)[i];
             }
+        }
+        __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            hb[i] = __float2bfloat16_rn(gelu_half(fmaf(0.5f, v[i], 0.5f * g.bias[n + i])));
         }
         uint4* dh = reinterpret_cast<uint4*>(g.h + m * g.ldh + n);
         dh[0] = reinterpret_cast<const uint4*>(hb)[0];
@@ -204,7 +207,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 
 template <int NK, bool HEAD>
-__global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_forward(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB,
                                                                 GemmArgs g, const float* head_w,
                                                                 const float* head_b, float* y,
@@ -338,8 +341,8 @@ __global__ void __launch_bounds__(kTmaThreads) gemm_tma_forward(const __grid_con
                     if (HEAD) {
 #pragma unroll
                         for (int i = 0; i < 16; ++i) {
-                            const float h =
-                                __bfloat162float(__float2bfloat16_rn(gelu(v[i] + g.bias[c0 + i])));
+                            const float h = __bfloat162float(__float2bfloat16_rn(
+                                gelu_half(fmaf(0.5f, v[i], 0.5f * g.bias[c0 + i]))));
                             hsum += h * head_w[c0 + i];
                         }
                     } else {
@@ -448,7 +451,7 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     __shared__ float head_part[2][4][kTileM];
-    // the layers' biases, then the head's weights (read by every row)
+    // the layers' half biases, then the head's weights (read by every row)
     __shared__ __align__(16) float s_par[kMaxFusedLayers + 1][256];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -478,7 +481,7 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
     }
     for (int i = threadIdx.x; i < (L + 1) * 256; i += blockDim.x) {
         const int l = i >> 8;
-        s_par[l][i & 255] = l < L ? g.bias[l][i & 255] : g.head_w[i & 255];
+        s_par[l][i & 255] = l < L ? 0.5f * g.bias[l][i & 255] : g.head_w[i & 255];
     }
     tc_fence_before();
     __syncthreads();
@@ -641,8 +644,9 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
 #pragma unroll
                             for (int i = 0; i < 8; ++i) {
                                 hb[i] = __floats2bfloat162_rn(
-                                    gelu(__uint_as_float(r[j & 1][2 * i]) + b[2 * i]),
-                                    gelu(__uint_as_float(r[j & 1][2 * i + 1]) + b[2 * i + 1]));
+                                    gelu_half(fmaf(0.5f, __uint_as_float(r[j & 1][2 * i]), b[2 * i])),
+                                    gelu_half(fmaf(0.5f, __uint_as_float(r[j & 1][2 * i + 1]),
+                                                   b[2 * i + 1])));
                             }
                             if (!last) {
                                 // next layer's K chunk c0 / 64, 16-byte units u0 and

@@ -66,15 +66,22 @@ __device__ __forceinline__ float tanh_hw(float x) {
     return y;
 }
 
-// The argument as z (k + k a z^2) and the value as z/2 + z/2 tanh(u): three
-// and two operations around the tanh.
+// The argument as z (k + k a z^2) and the value as z/2 + z/2 tanh(u).
 __device__ __forceinline__ float gelu_arg(float z) {
     return z * fmaf(0.035677408136300125f, z * z, 0.79788456080286536f);
 }
 
+// The GELU of z from hz = z/2: u = hz (2k + 8 k a hz^2) is z (k + k a z^2)
+// to the bit (every factor scaled by a power of two), and the value is
+// hz + hz tanh(u): four operations around the tanh.  The epilogues form hz
+// as fma(1/2, acc, bias/2), which is half of acc + bias exactly.
+__device__ __forceinline__ float gelu_half(float hz) {
+    const float c = fmaf(8.0f * 0.035677408136300125f, hz * hz, 2.0f * 0.79788456080286536f);
+    return fmaf(hz, tanh_hw(hz * c), hz);
+}
+
 __device__ __forceinline__ float gelu(float z) {
-    const float hz = 0.5f * z;
-    return fmaf(hz, tanh_hw(gelu_arg(z)), hz);
+    return gelu_half(0.5f * z);
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
