@@ -23,8 +23,13 @@
 // (per block: strided per-thread sums, then a shared-memory tree; the block
 // partials in block order), so they are deterministic and equal the
 // reference's sequential sums to rounding.  Legendre polynomials use the
-// three-term recurrence (Bonnet) P_{l+1} = ((2l+1) x P_l - l P_{l-1})/(l+1),
-// the recurrence of the boost::math::legendre_p the reference's CPU path calls.
+// three-term recurrence (Bonnet) P_{l+1} = ((2l+1) x P_l - l P_{l-1})/(l+1) of
+// the boost::math::legendre_p the reference's CPU path calls, with its
+// reflection of negative degrees (l -> -l - 1), in FP64: Boost's default
+// policy runs the recurrence in long double, so values differ from the
+// reference's by a few units of 2^-52 (about 2.5 per degree at most; |P| <= 1).
+// An argument outside [-1, 1] is Boost's domain error (an exception in the
+// reference); this stream-ordered entry point evaluates the polynomial there.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -72,6 +77,9 @@ __device__ __forceinline__ long long padded_index(const Geometry& G, long long c
 }
 
 __device__ __forceinline__ double legendre_p(int l, double x) {
+    if (l < 0) {
+        l = -l - 1;
+    }
     double p0 = 1, p1 = x;
     if (l == 0) {
         return p0;
@@ -321,12 +329,9 @@ int als_functional(const als_grid* grid, int kind, const als_functional_params* 
     if (members > 1 && (member_stride < nvar * G.plane || out_member_stride < nvar * per_var)) {
         return als::report_error(ALS_E_INVALID, "member strides smaller than one member");
     }
-    if ((kind == ALS_FUNCTIONAL_MOMENT || kind == ALS_FUNCTIONAL_LEGENDRE_POINTWISE ||
-         kind == ALS_FUNCTIONAL_BV || kind == ALS_FUNCTIONAL_BV_DIRECTION) && params->degree < 0) {
-        return als::report_error(ALS_E_INVALID, "negative degree");
-    }
-    if (kind == ALS_FUNCTIONAL_LEGENDRE && (params->degree_k < 0 || params->degree_n < 0 ||
-        params->degree_m < 0)) {
+    // (the Legendre degrees may be negative: P_{-l-1} = P_l, as in Boost)
+    if ((kind == ALS_FUNCTIONAL_MOMENT || kind == ALS_FUNCTIONAL_BV ||
+         kind == ALS_FUNCTIONAL_BV_DIRECTION) && params->degree < 0) {
         return als::report_error(ALS_E_INVALID, "negative degree");
     }
     // Legendre.cpp:54-58 / LegendrePointWise.cpp:49-53 accept 2-D grids only;

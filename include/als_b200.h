@@ -375,6 +375,10 @@ int als_structure_functions(const als_grid* grid, int boundary, int kind, int di
  * Cell midpoints and volumes follow Grid.cpp:24-41 (a direction with one
  * cell has length 1).  Sums over cells are reduced in a fixed order
  * (deterministic; equal to the reference's sequential sums to rounding).
+ * The Legendre polynomials are boost::math::legendre_p's recurrence in FP64
+ * (the reference's Boost evaluates it in long double: values agree to a few
+ * units of 2^-52), a negative degree l taken as -l - 1; an argument outside
+ * [-1, 1], Boost's domain error in the reference, is evaluated here.
  * Stream-ordered. */
 #define ALS_FUNCTIONAL_IDENTITY 0            /* "identity" */
 #define ALS_FUNCTIONAL_MOMENT 1              /* "moment" */

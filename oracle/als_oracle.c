@@ -1480,20 +1480,33 @@ int orc_set_diffusion(orc_config* cfg, int kind, int recon) {
 
 /* ------------------------------------------------------------ functionals */
 
-/* boost::math::legendre_p's recurrence (Bonnet):
- * P_{l+1} = ((2l+1) x P_l - l P_{l-1}) / (l+1), from P_0 = 1, P_1 = x. */
-static double legendre_p(int l, double x) {
-    double p0 = 1, p1 = x;
-    int m;
-    if (l == 0) {
-        return p0;
+/* boost::math::legendre_p(int l, double x), which Legendre.cpp:79-81 and
+ * LegendrePointWise.cpp:74 call (Boost.Math special_functions/legendre.hpp,
+ * not in /root/reference), as that library documents it under its default
+ * policy: the double argument evaluated in long double (promote_double) and
+ * rounded to double once at the end, a negative degree l taken as -l - 1,
+ * P_0 = 1, P_1 = x and Bonnet's recurrence
+ * P_{n+1} = ((2n+1) x P_n - n P_{n-1}) / (n+1), terms formed left to right.
+ * |x| > 1 is Boost's domain error (an exception in the reference): here the
+ * caller's flag is set and 0 returned. */
+static double legendre_p(int l, double x, int* domain_error) {
+    const unsigned degree = l < 0 ? (unsigned)(-l - 1) : (unsigned)l;
+    const long double xl = x;
+    long double p0 = 1, p1 = xl;
+    unsigned m;
+    if (xl < -1 || xl > 1) {
+        *domain_error = 1;
+        return 0;
     }
-    for (m = 1; m < l; ++m) {
-        const double next = ((2 * m + 1) * x * p1 - m * p0) / (m + 1);
+    if (degree == 0) {
+        return (double)p0;
+    }
+    for (m = 1; m < degree; ++m) {
+        const long double next = ((2 * m + 1) * xl * p1 - m * p0) / (m + 1);
         p0 = p1;
         p1 = next;
     }
-    return p1;
+    return (double)p1;
 }
 
 long orc_functional_size(int dim, const int* n, int g, int kind, int number_of_h) {
@@ -1518,6 +1531,7 @@ int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_
     double len[3], sides[3], dV;
     const int nvar = dim + 2;
     long per_var;
+    int domain_error = 0;
     for (d = 0; d < 3; ++d) {
         nn[d] = d < dim ? n[d] : 1;
         N[d] = nn[d] + (d < dim ? 2 * g : 0);
@@ -1647,7 +1661,7 @@ int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_
                     } else if (kind == ORC_FUNCTIONAL_LEGENDRE_POINTWISE) {
                         /* LegendrePointWise.cpp:58-76 */
                         const double value = (u - p->min_value) / (p->max_value - p->min_value);
-                        out[v * per_var + c] += legendre_p(p->degree, value) * weight;
+                        out[v * per_var + c] += legendre_p(p->degree, value, &domain_error) * weight;
                     } else if (kind == ORC_FUNCTIONAL_LEGENDRE) {
                         /* Legendre.cpp:62-90, midpoints Grid.cpp:148-171 */
                         const double x = (p->lower[0] + len[0] * i) + len[0] / 2.0;
@@ -1655,8 +1669,9 @@ int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_
                         const double xs = 2 * (x - p->lower[0]) / sides[0] - 1;
                         const double ys = 2 * (y - p->lower[1]) / sides[1] - 1;
                         const double value = (u - p->min_value) / (p->max_value - p->min_value);
-                        integral += legendre_p(p->degree_k, xs) * legendre_p(p->degree_n, ys) *
-                            legendre_p(p->degree_m, value) * dV;
+                        integral += legendre_p(p->degree_k, xs, &domain_error) *
+                            legendre_p(p->degree_n, ys, &domain_error) *
+                            legendre_p(p->degree_m, value, &domain_error) * dV;
                     } else {
                         /* HostMemory::getTotalVariation (HostMemory.cpp:325-362):
                          * cells after the first along x and, in 2-D, y */
@@ -1677,5 +1692,5 @@ int orc_functional(int dim, const int* n, int g, int kind, const orc_functional_
             out[v * per_var] += weight * integral;
         }
     }
-    return 0;
+    return domain_error ? -2 : 0;
 }

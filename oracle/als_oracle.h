@@ -92,7 +92,10 @@ int orc_obeys_constraints(const orc_config* cfg, const double* planes);
 
 /* Functionals (alsfvm/src/functional/): out += weight * f(U) for one state,
  * sums in the reference's sequential order.  Output per variable:
- * orc_functional_size elements (interior cells, padded cells or 1). */
+ * orc_functional_size elements (interior cells, padded cells or 1).
+ * Returns 0, -1 for a functional the reference does not define on the grid,
+ * -2 when a Legendre argument left [-1, 1] (boost::math::legendre_p's
+ * domain error, an exception in the reference). */
 enum { ORC_FUNCTIONAL_IDENTITY = 0, ORC_FUNCTIONAL_MOMENT = 1, ORC_FUNCTIONAL_LOG_ENTROPY = 2,
        ORC_FUNCTIONAL_LEGENDRE = 3, ORC_FUNCTIONAL_LEGENDRE_POINTWISE = 4, ORC_FUNCTIONAL_BV = 5,
        ORC_FUNCTIONAL_BV_DIRECTION = 6, ORC_FUNCTIONAL_STRUCTURE_2PT = 7 };

@@ -732,6 +732,23 @@ int alsref_statistics(const char* platform, const char* name, int dim, const int
 // Number of doubles per variable of the functional `name`'s output for a
 // grid of n cells with `ghosts` ghost cells (functional size and ghost
 // widths as TimeIntegrationFunctional.cpp:64-72 allocates them).
+// The parameters every functional of the factory reads (Moment and
+// BoundedVariation "degree", LogEntropy "gamma", Legendre "minValue",
+// "maxValue", "degree_k", "degree_n", "degree_m", LegendrePointWise
+// "minValue", "maxValue", "degree").
+functional::Functional::Parameters functionalParameters(int degree, double gamma,
+    const int* legendre_degrees, double min_value, double max_value) {
+    functional::Functional::Parameters p(std::map<std::string, std::string>{});
+    p.addIntegerParameter("degree", degree);
+    p.addDoubleParameter("gamma", gamma);
+    p.addIntegerParameter("degree_k", legendre_degrees ? legendre_degrees[0] : 0);
+    p.addIntegerParameter("degree_n", legendre_degrees ? legendre_degrees[1] : 0);
+    p.addIntegerParameter("degree_m", legendre_degrees ? legendre_degrees[2] : 0);
+    p.addDoubleParameter("minValue", min_value);
+    p.addDoubleParameter("maxValue", max_value);
+    return p;
+}
+
 long alsref_functional_size(int dim, const int* n, int ghosts, const char* name, int degree,
     double gamma) {
     try {
@@ -739,9 +756,7 @@ long alsref_functional_size(int dim, const int* n, int ghosts, const char* name,
         auto s = makeSetup(dim, n, lo, hi, "hll", "none", "forwardeuler", "periodic", gamma, 0.5);
         auto o = build(s);
         auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
-        functional::Functional::Parameters p(std::map<std::string, std::string>{});
-        p.addIntegerParameter("degree", degree);
-        p.addDoubleParameter("gamma", gamma);
+        auto p = functionalParameters(degree, gamma, nullptr, 0.0, 1.0);
         auto f = functional::FunctionalFactory().makeFunctional("cpu", name, p);
         const ivec3 size = f->getFunctionalSize(*o.grid);
         const ivec3 g = f->getGhostCellSizes(*o.grid, *u);
@@ -754,21 +769,20 @@ long alsref_functional_size(int dim, const int* n, int ghosts, const char* name,
 }
 
 // The functional `name` of the reference's FunctionalFactory ("cpu"), with
-// parameters degree and gamma, on the grid [lower, upper] of n cells:
+// parameters degree, gamma, the Legendre degrees (k, n, m) and the value
+// range [min_value, max_value], on the grid [lower, upper] of n cells:
 // out += weight * f(state) for one padded state.  `out` holds the output
 // volume's nvar planes (alsref_functional_size doubles each).
 int alsref_functional(int dim, const int* n, const double* lower, const double* upper,
-    int ghosts, const char* name, int degree, double gamma, double weight,
-    const double* planes, double* out) {
+    int ghosts, const char* name, int degree, double gamma, const int* legendre_degrees,
+    double min_value, double max_value, double weight, const double* planes, double* out) {
     try {
         auto s = makeSetup(dim, n, lower, upper, "hll", "none", "forwardeuler", "periodic",
             gamma, 0.5);
         auto o = build(s);
         auto u = o.volumeFactory->createConservedVolume(s.n.x, s.n.y, s.n.z, ghosts);
         copyIn(*u, planes);
-        functional::Functional::Parameters p(std::map<std::string, std::string>{});
-        p.addIntegerParameter("degree", degree);
-        p.addDoubleParameter("gamma", gamma);
+        auto p = functionalParameters(degree, gamma, legendre_degrees, min_value, max_value);
         auto f = functional::FunctionalFactory().makeFunctional("cpu", name, p);
         const ivec3 size = f->getFunctionalSize(*o.grid);
         const ivec3 g = f->getGhostCellSizes(*o.grid, *u);

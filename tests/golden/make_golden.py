@@ -243,6 +243,26 @@ def functional_case_name(dim, kind, degree):
     return "d%d-%s-p%d" % (dim, kind, degree)
 
 
+# Legendre and LegendrePointWise (2-D only) with their value range
+# [min, max] = LEGENDRE_RANGE, which maps every variable of the seeded
+# states into [0, 1]; degree -3 is evaluated as degree 2 by Boost.
+LEGENDRE_N = (13, 11)
+LEGENDRE_RANGE = (-3.0, 3.0)
+LEGENDRE_CASES = [("legendre", dict(degree_k=1, degree_n=2, degree_m=3)),
+                  ("legendre", dict(degree_k=0, degree_n=0, degree_m=6)),
+                  ("legendre", dict(degree_k=4, degree_n=1, degree_m=2)),
+                  ("legendre_pointwise", dict(degree=2)),
+                  ("legendre_pointwise", dict(degree=7)),
+                  ("legendre_pointwise", dict(degree=-3))]
+
+
+def legendre_case_name(kind, params):
+    if kind == "legendre":
+        return "d2-legendre-k%dn%dm%d" % (params["degree_k"], params["degree_n"],
+                                          params["degree_m"])
+    return "d2-legendre_pointwise-p%d" % params["degree"]
+
+
 def write_functional_fixtures(ref):
     """tests/golden/functionals_ref.npz: for every case and member k, the
     state smooth_random_state(600 + 7 k + dim) (ghost width 2), an output
@@ -261,8 +281,24 @@ def write_functional_fixtures(ref):
                                           lower=FUNCTIONAL_BOX[0], upper=FUNCTIONAL_BOX[1]))
         out[name + "/start"] = np.stack(starts)
         out[name + "/result"] = np.stack(results)
+    lo, hi = LEGENDRE_RANGE
+    for kind, params in LEGENDRE_CASES:
+        name = legendre_case_name(kind, params)
+        results, starts = [], []
+        for k in range(FUNCTIONAL_MEMBERS):
+            st = smooth_random_state(600 + 7 * k + 2, 2, LEGENDRE_N, 2)
+            size = ref.functional(2, LEGENDRE_N, 2, kind, st, weight=0.0, min_value=lo,
+                                  max_value=hi, **params).shape[1]
+            start = np.full((4, size), 0.5 + k)
+            starts.append(start)
+            results.append(ref.functional(2, LEGENDRE_N, 2, kind, st, weight=FUNCTIONAL_WEIGHT,
+                                          out=start, min_value=lo, max_value=hi,
+                                          lower=FUNCTIONAL_BOX[0], upper=FUNCTIONAL_BOX[1],
+                                          **params))
+        out[name + "/start"] = np.stack(starts)
+        out[name + "/result"] = np.stack(results)
     np.savez_compressed(os.path.join(HERE, "functionals_ref.npz"), **out)
-    print("functionals_ref.npz: %d cases" % len(FUNCTIONAL_CASES))
+    print("functionals_ref.npz: %d cases" % (len(FUNCTIONAL_CASES) + len(LEGENDRE_CASES)))
 
 
 def main():

@@ -187,6 +187,8 @@ class COracle:
         inp = np.ascontiguousarray(planes, dtype=np.float64)
         rc = self.lib.orc_functional(dim, nn, g, FUNCTIONAL[kind], ctypes.byref(p), _dptr(inp),
                                      _dptr(res), float(weight))
+        if rc == -2:
+            raise ValueError("functional %s: a Legendre argument outside [-1, 1]" % kind)
         if rc != 0:
             raise ValueError("functional %s not defined in %d-D" % (kind, dim))
         return res
@@ -273,7 +275,8 @@ class RefOracle:
                                              ctypes.c_int, ctypes.c_double]
         L.alsref_functional_size.restype = ctypes.c_long
         L.alsref_functional.argtypes = [ctypes.c_int, _I, _D, _D, ctypes.c_int, ctypes.c_char_p,
-                                        ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _D]
+                                        ctypes.c_int, ctypes.c_double, _I, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, _D, _D]
 
     def set_diffusion(self, kind, recon="none"):
         """Diffusion operator of the following simulations (none by default)."""
@@ -370,7 +373,8 @@ class RefOracle:
         return first, second
 
     def functional(self, dim, n, ghosts, kind, planes, weight=1.0, out=None, degree=1,
-                   gamma=1.4, lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0)):
+                   gamma=1.4, lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0), degree_k=0,
+                   degree_n=0, degree_m=0, min_value=0.0, max_value=1.0):
         """out (nvar, size) += weight * f(planes) by the reference's
         FunctionalFactory ("cpu") functional `kind`, for one padded state."""
         nn = self._vec(n, ctypes.c_int, 1)
@@ -379,9 +383,11 @@ class RefOracle:
         self._check(size)
         res = np.zeros((dim + 2, size)) if out is None else np.array(out, dtype=np.float64)
         inp = np.ascontiguousarray(planes, dtype=np.float64)
+        degrees = (ctypes.c_int * 3)(int(degree_k), int(degree_n), int(degree_m))
         self._check(self.lib.alsref_functional(dim, nn, self._vec(lower, ctypes.c_double, 0.0),
                                                self._vec(upper, ctypes.c_double, 0.0), ghosts,
-                                               kind.encode(), int(degree), float(gamma),
+                                               kind.encode(), int(degree), float(gamma), degrees,
+                                               float(min_value), float(max_value),
                                                float(weight), _dptr(inp), _dptr(res)))
         return res
 

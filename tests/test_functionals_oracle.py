@@ -1,17 +1,22 @@
 """The functionals of alsfvm/src/functional/ in the oracle (CPU).
 
-Identity, Moment, LogEntropy and BoundedVariation are pinned bit for bit
-to the reference's own classes: their sources are compiled into the
-reference build (oracle/_ref, with a property-tree stand-in for their
-parameters) and made by name through its FunctionalFactory; the committed
-fixture tests/golden/functionals_ref.npz carries their outputs where that
-build is absent.  Legendre and LegendrePointWise call boost::math::legendre_p
-(not available here), so the restatement of those is pinned to the
-reference's own unit tests (test/library_tests/src/fvm/functional/
-EntropyTest.cpp, LegendreTest.cpp), ported with their inputs and
-tolerances, and to SciPy's Legendre polynomials.  The alsuq statistics
-bv_direction and structure_2pt are checked against direct NumPy evaluations
-of their stated formulas.
+Identity, Moment, LogEntropy, BoundedVariation, Legendre and
+LegendrePointWise are pinned bit for bit to the reference's own classes:
+their sources are compiled into the reference build (oracle/_ref, with a
+property-tree stand-in for their parameters) and made by name through its
+FunctionalFactory; the committed fixture tests/golden/functionals_ref.npz
+carries their outputs where that build is absent.  The Legendre classes
+call boost::math::legendre_p, which is not in this image: the build gets a
+restatement of it (oracle/ref_shims/boost/math/special_functions/
+legendre.hpp: long double evaluation, negative degrees reflected, a domain
+error outside [-1, 1], as Boost's default policy has it), so what these
+fixtures pin is the reference's use of it (scaling, midpoints, sums,
+weights).  The restatement is also checked against the reference's own
+unit tests (test/library_tests/src/fvm/functional/EntropyTest.cpp,
+LegendreTest.cpp), ported with their inputs and tolerances, and against
+SciPy's Legendre polynomials.  The alsuq statistics bv_direction and
+structure_2pt are checked against direct NumPy evaluations of their stated
+formulas.
 """
 import os
 
@@ -67,10 +72,14 @@ def test_log_entropy_result_is_one(c_oracle):
 
 
 def test_legendre_constant(c_oracle):
-    """LegendreTest.ConstantTest: degrees 0, weight 0.5 -> 0.5 per variable
+    """LegendreTest.ConstantTest: every variable sin(2 pi x y) at the
+    midpoints, degrees 0, range [-1, 1], weight 0.5 -> 0.5 per variable
     (ASSERT_DOUBLE_EQ: within 4 ulps)."""
     n, g = (3, 2), 2
-    U = _euler2_state(n, g, lambda rho, m: np.sin(2 * np.pi * m))
+    U = np.zeros(padded_shape(2, n, g))
+    x, y = _midpoints(n)
+    X, Y = np.meshgrid(x, y)
+    U[:, 0, g:-g, g:-g] = np.sin(2 * np.pi * X * Y)[None]
     out = c_oracle.functional(2, n, g, "legendre", U, weight=0.5, degree_k=0, degree_n=0,
                               degree_m=0, min_value=-1, max_value=1)
     assert np.all(np.abs(out[:, 0] - 0.5) <= 4 * np.spacing(0.5))
@@ -97,11 +106,11 @@ def test_legendre_integral_formula(c_oracle):
     n, g = (9, 7), 2
     st = smooth_random_state(21, 2, n, g)
     out = c_oracle.functional(2, n, g, "legendre", st, weight=1.5, degree_k=2, degree_n=3,
-                              degree_m=1, min_value=0.5, max_value=1.5)
+                              degree_m=1, min_value=-3.0, max_value=3.0)
     x, y = _midpoints(n)
     X, Y = np.meshgrid(2 * x - 1, 2 * y - 1)
     for v in range(4):
-        val = (st[v, 0, g:-g, g:-g] - 0.5) / 1.0
+        val = (st[v, 0, g:-g, g:-g] + 3.0) / 6.0
         ref = np.sum(scipy.special.eval_legendre(2, X) * scipy.special.eval_legendre(3, Y) *
                      val) * (1 / 9) * (1 / 7)
         assert abs(out[v, 0] - 1.5 * ref) < 1e-13
@@ -215,6 +224,61 @@ def test_functionals_equal_reference_fixture(c_oracle, dim, n, kind, degree):
                                   out=z[name + "/start"][k], degree=degree, gamma=GAMMA,
                                   lower=MG.FUNCTIONAL_BOX[0], upper=MG.FUNCTIONAL_BOX[1])
         np.testing.assert_array_equal(got, z[name + "/result"][k])
+
+
+@pytest.mark.parametrize("kind,params", MG.LEGENDRE_CASES,
+                         ids=[MG.legendre_case_name(*c) for c in MG.LEGENDRE_CASES])
+def test_legendre_equal_reference_fixture(c_oracle, kind, params):
+    """Legendre and LegendrePointWise of the reference build (with Boost's
+    legendre_p restated) give the same bits as the oracle."""
+    z = np.load(os.path.join(GOLDEN, "functionals_ref.npz"))
+    name = MG.legendre_case_name(kind, params)
+    lo, hi = MG.LEGENDRE_RANGE
+    for k in range(MG.FUNCTIONAL_MEMBERS):
+        st = smooth_random_state(600 + 7 * k + 2, 2, MG.LEGENDRE_N, 2)
+        got = c_oracle.functional(2, MG.LEGENDRE_N, 2, kind, st, weight=MG.FUNCTIONAL_WEIGHT,
+                                  out=z[name + "/start"][k], min_value=lo, max_value=hi,
+                                  lower=MG.FUNCTIONAL_BOX[0], upper=MG.FUNCTIONAL_BOX[1],
+                                  **params)
+        np.testing.assert_array_equal(got, z[name + "/result"][k])
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_legendre_equal_reference_build(c_oracle, ref_oracle, seed):
+    """Fresh random Legendre cases against the reference build itself
+    (skipped where it is not built), negative degrees included."""
+    rng = np.random.default_rng(40 + seed)
+    n = tuple(int(v) for v in rng.integers(4, 12, 2))
+    g = int(rng.integers(1, 4))
+    st = smooth_random_state(740 + seed, 2, n, g)
+    lo, hi = tuple(rng.uniform(-1, 0, 3)), tuple(rng.uniform(1, 2, 3))
+    w = float(rng.uniform(-2, 2))
+    vrange = dict(min_value=-4.0 + seed, max_value=4.0 + seed)
+    for kind, params in (("legendre", dict(degree_k=int(rng.integers(0, 6)),
+                                           degree_n=int(rng.integers(-4, 6)),
+                                           degree_m=int(rng.integers(0, 9)))),
+                         ("legendre_pointwise", dict(degree=int(rng.integers(-6, 12))))):
+        ref = ref_oracle.functional(2, n, g, kind, st, weight=w, lower=lo, upper=hi,
+                                    **vrange, **params)
+        got = c_oracle.functional(2, n, g, kind, st, weight=w, lower=lo, upper=hi,
+                                  **vrange, **params)
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_legendre_domain_and_negative_degrees(c_oracle):
+    """Boost's legendre_p, as the reference calls it: an argument outside
+    [-1, 1] is a domain error, and degree -l - 1 is degree l."""
+    n, g = (6, 5), 2
+    st = smooth_random_state(3, 2, n, g)
+    with pytest.raises(ValueError, match="outside"):
+        c_oracle.functional(2, n, g, "legendre_pointwise", st, degree=2, min_value=0.9,
+                            max_value=1.1)
+    for l in range(6):
+        a = c_oracle.functional(2, n, g, "legendre_pointwise", st, degree=l, min_value=-3,
+                                max_value=3)
+        b = c_oracle.functional(2, n, g, "legendre_pointwise", st, degree=-l - 1, min_value=-3,
+                                max_value=3)
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("seed", range(4))

@@ -1,11 +1,14 @@
 """The functionals (als_functional) on the GPU against the oracle.
 
-Pointwise functionals (identity, legendre_pointwise) evaluate the same
-operations in the same order and match exactly; moment calls pow, and the
-sums (log_entropy, legendre, bv) are reduced in a different (fixed) order
-than the reference's sequential loop and log_entropy calls log, so those
-match to a relative 1e-12 (moment: 1e-14).  FP32 members are converted to
-FP64 on load, so the oracle runs on the same values widened.
+Identity evaluates the same operations in the same order and matches
+exactly; moment calls pow, and the sums (log_entropy, legendre, bv) are
+reduced in a different (fixed) order than the reference's sequential loop
+and log_entropy calls log, so those match to a relative 1e-12 (moment:
+1e-14).  The Legendre polynomials run in FP64 where the reference's Boost
+(and the oracle) run them in long double: legendre_pointwise matches to
+1e-13 absolute per value (|P| <= 1, degrees up to 7 here).  FP32 members
+are converted to FP64 on load, so the oracle runs on the same values
+widened.
 """
 import importlib.util
 import os
@@ -34,7 +37,9 @@ for _dim, _n in ((1, (37,)), (2, (23, 19)), (3, (9, 8, 7))):
             continue
         CASES.append((_dim, _n, _kind))
 
-PARAMS = dict(degree=2, degree_k=1, degree_n=2, degree_m=3, min_value=0.8, max_value=1.2,
+# [min_value, max_value] maps the seeded states into [0, 1], the domain of
+# the Legendre polynomials
+PARAMS = dict(degree=2, degree_k=1, degree_n=2, degree_m=3, min_value=-3.0, max_value=3.0,
               gamma=1.4, lower=(0.0, -1.0, 0.0), upper=(2.0, 1.0, 1.0))
 
 
@@ -55,8 +60,10 @@ def test_functional_matches_oracle(c_oracle, dim, n, kind, precision):
     for m in range(members):
         ref = c_oracle.functional(dim, n, g, kind, widened[m], weight=0.75,
                                   out=start[m].cpu().numpy(), **params)
-        if kind in ("identity", "legendre_pointwise"):
+        if kind == "identity":
             np.testing.assert_array_equal(got[m], ref)
+        elif kind == "legendre_pointwise":
+            np.testing.assert_allclose(got[m], ref, rtol=0, atol=1e-13)
         else:
             rtol = 1e-14 if kind == "moment" else 1e-12
             np.testing.assert_allclose(got[m], ref, rtol=rtol, atol=1e-14)
@@ -126,3 +133,28 @@ def test_functional_matches_reference_classes(dim, n, kind, degree, precision):
     else:
         rtol = 1e-14 if kind == "moment" else 1e-12
         np.testing.assert_allclose(out, ref, rtol=rtol, atol=1e-14)
+
+
+@pytest.mark.parametrize("kind,params", MG.LEGENDRE_CASES,
+                         ids=[MG.legendre_case_name(*c) for c in MG.LEGENDRE_CASES])
+def test_legendre_matches_reference_classes(kind, params):
+    """Against the reference's own Legendre and LegendrePointWise (with
+    Boost's legendre_p restated: long double, negative degrees reflected):
+    FP64 polynomials, 1e-13 absolute per value; the integral also reduced in
+    another order, 1e-12 relative."""
+    z = np.load(os.path.join(GOLDEN, "functionals_ref.npz"))
+    name = MG.legendre_case_name(kind, params)
+    states = np.stack([smooth_random_state(600 + 7 * k + 2, 2, MG.LEGENDRE_N, 2)
+                       for k in range(MG.FUNCTIONAL_MEMBERS)])
+    x = torch.from_numpy(states).cuda().contiguous()
+    lo, hi = MG.LEGENDRE_RANGE
+    start = torch.from_numpy(z[name + "/start"]).cuda()
+    out = fn.functional(x, 2, MG.LEGENDRE_N, 2, kind, weight=MG.FUNCTIONAL_WEIGHT,
+                        out=start.clone(), min_value=lo, max_value=hi,
+                        lower=MG.FUNCTIONAL_BOX[0], upper=MG.FUNCTIONAL_BOX[1],
+                        **params).cpu().numpy()
+    ref = z[name + "/result"]
+    if kind == "legendre_pointwise":
+        np.testing.assert_allclose(out, ref, rtol=0, atol=1e-13)
+    else:
+        np.testing.assert_allclose(out, ref, rtol=1e-12, atol=1e-14)
