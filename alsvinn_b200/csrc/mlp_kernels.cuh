@@ -329,7 +329,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_forward(const __grid_
             if (!ok) {
                 *abort_v = 1;
             }
-            float hsum = 0.0f;
+            // even and odd columns summed apart, then added
+            float2 hsum2 = make_float2(0.0f, 0.0f);
             if (ok) {
                 tc_fence_after();
                 const long long m = (long long)t * kTileM + row;
@@ -340,10 +341,13 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_forward(const __grid_
                     tmem_load16(lane_base + uint32_t(c0), v);
                     if (HEAD) {
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const float h = __bfloat162float(__float2bfloat16_rn(
+                        for (int i = 0; i < 16; i += 2) {
+                            const float h0 = __bfloat162float(__float2bfloat16_rn(
                                 gelu_half(fmaf(0.5f, v[i], 0.5f * g.bias[c0 + i]))));
-                            hsum += h * head_w[c0 + i];
+                            const float h1 = __bfloat162float(__float2bfloat16_rn(
+                                gelu_half(fmaf(0.5f, v[i + 1], 0.5f * g.bias[c0 + i + 1]))));
+                            hsum2 = __ffma2_rn(make_float2(h0, h1),
+                                               make_float2(head_w[c0 + i], head_w[c0 + i + 1]), hsum2);
                         }
                     } else {
                         epilogue16<BN, EPI_FORWARD>(g, m, c0, v, BN);
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_forward(const __grid_
                 }
             }
             if (HEAD) {
-                head_part[acc][cg][row] = hsum;
+                head_part[acc][cg][row] = hsum2.x + hsum2.y;
                 named_barrier_sync(1, 16 * 32);
                 const int et = ew * 32 + lane;       // 0..511
                 if (ok && et < kTileM) {
@@ -619,7 +623,8 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                             tmem + uint32_t(s * BN) + (uint32_t(quarter * 32) << 16);
                         // this row of every K chunk: 8-row atoms of 1024 bytes
                         unsigned char* arow = sA + s * kActBytes + (row >> 3) * 1024 + (row & 7) * 128;
-                        float hsum = 0.0f;
+                        // head: even and odd columns summed apart, then added
+                        float2 hsum2 = make_float2(0.0f, 0.0f);
                         // 16 columns at a time; the next 16 are read from TMEM
                         // while these are computed
                         uint32_t r[2][16];
@@ -638,15 +643,18 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                                 reinterpret_cast<float4*>(b)[i] =
                                     reinterpret_cast<const float4*>(bias + c0)[i];
                             }
-                            // BF16 rounding of pairs (each element rounded to
-                            // nearest even, as the scalar conversion does)
+                            // pairs of columns: half pre-activation, GELU and BF16
+                            // rounding (each element as the scalar operations
+                            // round it)
                             __nv_bfloat162 hb[8];
 #pragma unroll
                             for (int i = 0; i < 8; ++i) {
-                                hb[i] = __floats2bfloat162_rn(
-                                    gelu_half(fmaf(0.5f, __uint_as_float(r[j & 1][2 * i]), b[2 * i])),
-                                    gelu_half(fmaf(0.5f, __uint_as_float(r[j & 1][2 * i + 1]),
-                                                   b[2 * i + 1])));
+                                const float2 acc = make_float2(__uint_as_float(r[j & 1][2 * i]),
+                                                               __uint_as_float(r[j & 1][2 * i + 1]));
+                                const float2 hz = __ffma2_rn(make_float2(0.5f, 0.5f), acc,
+                                                             reinterpret_cast<const float2*>(b)[i]);
+                                const float2 h = gelu_half2(hz);
+                                hb[i] = __floats2bfloat162_rn(h.x, h.y);
                             }
                             if (!last) {
                                 // next layer's K chunk c0 / 64, 16-byte units u0 and
@@ -666,13 +674,13 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                                 }
 #pragma unroll
                                 for (int i = 0; i < 8; ++i) {
-                                    hsum += __low2float(hb[i]) * w[2 * i];
-                                    hsum += __high2float(hb[i]) * w[2 * i + 1];
+                                    hsum2 = __ffma2_rn(__bfloat1622float2(hb[i]),
+                                                       reinterpret_cast<const float2*>(w)[i], hsum2);
                                 }
                             }
                         }
                         if (last) {
-                            head_part[s][cg][row] = hsum;
+                            head_part[s][cg][row] = hsum2.x + hsum2.y;
                         }
                     }
                     if (last) {

@@ -84,6 +84,16 @@ __device__ __forceinline__ float gelu(float z) {
     return gelu_half(0.5f * z);
 }
 
+// gelu_half of two values with the paired FP32 instructions (each component
+// rounded as the scalar operation rounds it, so the results are gelu_half's).
+__device__ __forceinline__ float2 gelu_half2(float2 hz) {
+    const float2 c = __ffma2_rn(make_float2(8.0f * 0.035677408136300125f, 8.0f * 0.035677408136300125f),
+                                __fmul2_rn(hz, hz),
+                                make_float2(2.0f * 0.79788456080286536f, 2.0f * 0.79788456080286536f));
+    const float2 u = __fmul2_rn(hz, c);
+    return __ffma2_rn(hz, make_float2(tanh_hw(u.x), tanh_hw(u.y)), hz);
+}
+
 __device__ __forceinline__ float gelu_grad(float z) {
     // d/dz: (1 + t)/2 + z/2 (1 - t^2) k (1 + 3 a z^2), t = tanh(u)
     const float t = tanh_hw(gelu_arg(z));
