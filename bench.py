@@ -142,12 +142,18 @@ def fp64_roofline(dom, cells, hbm_peak, peak_kind, traffic, per_kernel):
     achieved = FP64 thread instructions per cell and stage (ncu
     sm__sass_thread_inst_executed_op_fp64_pred_on over a launch, divided by
     its cells; profiles/traffic_kh1024.json) x cells / the stage kernel's
-    event duration.  The HBM fraction of the same launch stands beside it."""
+    event duration.  Beside it: the issue of all instructions (ncu
+    smsp__thread_inst_executed per cell against 148 SMs x 4 schedulers x 32
+    lanes per clock; predicated-off lanes are not counted, so this fraction
+    is a lower bound of the issue slots used) and the HBM fraction of the
+    same launch."""
     tpath = os.path.join(ROOT, "profiles", "traffic_kh1024.json")
-    per_cell = None
+    per_cell = all_per_cell = None
     if os.path.exists(tpath):
         with open(tpath) as f:
-            per_cell = json.load(f).get("fp64_inst_per_cell", {}).get(dom["kernel"])
+            t = json.load(f)
+        per_cell = t.get("fp64_inst_per_cell", {}).get(dom["kernel"])
+        all_per_cell = t.get("inst_per_cell", {}).get(dom["kernel"])
     peak, src = fp64_issue_peak()
     out = {"bound": "fp64", "unit": "FP64 thread-inst/s", "peak": peak, "peak_source": src,
            "kernel": "stage kernel '%s' (%.4f ms)" % (dom["kernel"], dom["ms"])}
@@ -155,6 +161,12 @@ def fp64_roofline(dom, cells, hbm_peak, peak_kind, traffic, per_kernel):
         out["achieved"] = per_cell * cells / (dom["ms"] * 1e-3)
         out["frac"] = out["achieved"] / peak
         out["fp64_inst_per_cell"] = per_cell
+    if all_per_cell:
+        issue_peak = peak * 2          # 128 thread-instructions per SM and clock
+        achieved = all_per_cell * cells / (dom["ms"] * 1e-3)
+        out["issue"] = {"achieved": achieved, "peak": issue_peak, "unit": "thread-inst/s",
+                        "frac": achieved / issue_peak, "inst_per_cell": all_per_cell,
+                        "peak_source": "148 SMs x 4 schedulers x 32 lanes per clock"}
     out["hbm"] = {"achieved": dom["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
                   "frac": dom["achieved_gbs"] / hbm_peak, "traffic": traffic,
                   "peak_source": peak_kind}
