@@ -206,7 +206,11 @@ class Simulator:
         return {"blocks_per_sm": bps.value, "level_order": list(order)}
 
     def set_tiles(self, shapes):
-        """Tile shape per level (0: the default; 1: 16x16 cells, 2-D WENO2 only)."""
+        """Tile shape per level: 0 the dimension's box tile (2-D 32x16, 3-D
+        8x8x4 cells); 1 the alternative where it is built (2-D 16x16 cells
+        for WENO2 with HLL, HLL3 or Central; 3-D 16x16 columns marching along
+        z, the 3-D default, for reconstructions reaching one cell with the
+        two-point fluxes)."""
         arr = (ctypes.c_int * len(self.levels))(*[int(v) for v in shapes])
         _lib.check(self._lib.als_solver_set_tiles(self._h, arr))
 

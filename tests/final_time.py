@@ -18,7 +18,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GAMMA = 1.4
 GHOSTS = 2
 BLOCK = 16
-CASES = ("uq256_7", "uq256_4095", "kh1024")
+CASES = ("uq256_7", "uq256_4095", "kh1024")    # 2-D, initial data as band limits
+CASES3 = ("kh3d48",)                           # 3-D, initial data by the generator
 
 
 def fixture_path(name):
@@ -31,9 +32,12 @@ def load(name):
     for k in ("n", "sample", "ghosts", "steps", "block"):
         out[k] = int(out[k])
     for k in ("gamma", "cfl", "end_time", "t", "observable", "dts_min", "dts_max"):
-        out[k] = float(out[k])
-    for k in ("flux", "recon", "integrator", "bc", "dts_sha256", "interior_sha256"):
-        out[k] = str(out[k])
+        if k in out:
+            out[k] = float(out[k])
+    for k in ("flux", "recon", "integrator", "bc", "dts_sha256", "interior_sha256",
+              "initial_sha256"):
+        if k in out:
+            out[k] = str(out[k])
     return out
 
 
@@ -85,6 +89,29 @@ def summary(U, n, ghosts=GHOSTS):
     blocks = I.reshape(I.shape[0], b, BLOCK, b, BLOCK).sum(axis=(2, 4))
     return {"l1": l1, "sums": sums, "block_sums": blocks,
             "interior_sha256": hashlib.sha256(I.tobytes()).hexdigest()}
+
+
+BLOCK3 = 8
+
+
+def interior3(U, n, ghosts=GHOSTS):
+    return np.ascontiguousarray(U[:, ghosts:ghosts + n, ghosts:ghosts + n, ghosts:ghosts + n])
+
+
+def summary3(U, n, ghosts=GHOSTS):
+    """summary() of a 3-D state: per-variable L1 norms and sums, 8 x 8 x 8
+    block sums and the sha256 of the final interior."""
+    I = interior3(U, n, ghosts)
+    l1 = np.array([math.fsum(np.abs(I[v]).ravel()) for v in range(I.shape[0])])
+    sums = np.array([math.fsum(I[v].ravel()) for v in range(I.shape[0])])
+    b = n // BLOCK3
+    blocks = I.reshape(I.shape[0], b, BLOCK3, b, BLOCK3, b, BLOCK3).sum(axis=(2, 4, 6))
+    return {"l1": l1, "sums": sums, "block_sums": blocks,
+            "interior_sha256": hashlib.sha256(I.tobytes()).hexdigest()}
+
+
+def state_digest(U):
+    return hashlib.sha256(np.ascontiguousarray(U, dtype=np.float64).tobytes()).hexdigest()
 
 
 def observable(U, n, ghosts=GHOSTS):

@@ -14,7 +14,10 @@ alsfvm/src/io/FixedIntervalWriter.cpp:45-53) runs each case to T = 2:
 * kh1024: KH 1024^2, parameters = alsuq STLMersenne sample 0, CFL 0.4
   (about 23k steps; about half an hour on eight host cores);
 * uq256_<s>: KH 256^2 members s = 7 and 4095 of the 4096-sample UQ
-  oracle ensemble (parameters = STLMersenne sample s), CFL 0.4.
+  oracle ensemble (parameters = STLMersenne sample s), CFL 0.4;
+* kh3d48: KH on the unit cube, 48^3, parameters = STLMersenne sample 0,
+  CFL 0.4 (the 3-D path, whose z-marching tiles cover 48 = 32 + 16 cells
+  in two segments).
 
 What is stored, and why it is enough, is described in tests/final_time.py.
 """
@@ -64,6 +67,34 @@ def run_case(ref, name, n, sample):
           % (name, steps, t, seconds, out["observable"], s["interior_sha256"][:16]))
 
 
+def run_case_3d(ref, name, n, sample):
+    """KH on the periodic unit cube (interfaces perturbed along x + z),
+    n^3 cells, the same scheme to T = 2; the initial state is the
+    generator's (its digest stored), the final one summarised per 8^3 block."""
+    import alsvinn_b200.initial_data as init
+    params = np.asarray(ref.stlmersenne(40, sample, 1)[0])
+    U0 = init.kelvin_helmholtz(n, params, ft.GHOSTS, ft.GAMMA, dimension=3)
+    t0 = time.perf_counter()
+    rc, U, dts, steps, t = ref.simulate(3, (n, n, n), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), "hll3",
+                                        "weno2", "rungekutta3", "periodic", ft.GAMMA, CFL,
+                                        END_TIME, U0, dts_capacity=200000)
+    seconds = time.perf_counter() - t0
+    assert rc == 0, name
+    assert len(dts) == steps
+    s = ft.summary3(U, n)
+    out = dict(n=n, sample=sample, params=params, initial_sha256=ft.state_digest(U0),
+               ghosts=ft.GHOSTS, gamma=ft.GAMMA, cfl=CFL, end_time=END_TIME, flux="hll3",
+               recon="weno2", integrator="rungekutta3", bc="periodic", steps=steps, t=t,
+               dts_sha256=ft.dts_digest(dts), dts_head=dts[:64], dts_tail=dts[-64:],
+               dts_min=dts.min(), dts_max=dts.max(), l1=s["l1"], sums=s["sums"],
+               block_sums=s["block_sums"], interior_sha256=s["interior_sha256"],
+               block=ft.BLOCK3, ref_loop_seconds=seconds,
+               ref_threads=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())))
+    np.savez_compressed(ft.fixture_path(name), **out)
+    print("%s: %d steps, t=%r, %.1f s, sha %s" % (name, steps, t, seconds,
+                                                  s["interior_sha256"][:16]))
+
+
 def main(which):
     ref = RefOracle()
     if "uq256" in which:
@@ -71,7 +102,9 @@ def main(which):
             run_case(ref, "uq256_%d" % s, 256, s)
     if "kh1024" in which:
         run_case(ref, "kh1024", 1024, 0)
+    if "kh3d48" in which:
+        run_case_3d(ref, "kh3d48", 48, 0)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["uq256", "kh1024"])
+    main(sys.argv[1:] or ["uq256", "kh1024", "kh3d48"])

@@ -26,6 +26,14 @@ def test_band_limits_rebuild_the_generator_state(name):
     assert z["t"] == z["end_time"]
 
 
+@pytest.mark.parametrize("name", ft.CASES3)
+def test_3d_generator_state_is_the_fixture_initial_state(name):
+    z = ft.load(name)
+    U = init.kelvin_helmholtz(z["n"], z["params"], z["ghosts"], z["gamma"], dimension=3)
+    assert ft.state_digest(U) == z["initial_sha256"]
+    assert z["t"] == z["end_time"] and z["steps"] > 64
+
+
 @pytest.mark.parametrize("name", ("uq256_7", "uq256_4095"))
 def test_uq_oracle_ensemble_pinned_to_reference_members(name):
     z = ft.load(name)
@@ -44,12 +52,12 @@ def test_parameters_are_the_reference_draws(ref_oracle):
     import json
     import subprocess
     import sys
-    zs = sorted((ft.load(name) for name in ft.CASES), key=lambda z: z["sample"])
-    samples = [z["sample"] for z in zs]
+    zs = sorted((ft.load(name) for name in ft.CASES + ft.CASES3), key=lambda z: z["sample"])
+    samples = sorted(set(z["sample"] for z in zs))
     code = ("import json, sys; sys.path.insert(0, %r); from oracle_lib import RefOracle; "
             "r = RefOracle(); print(json.dumps([r.stlmersenne(40, s, 1)[0].tolist() for s in %r]))"
             % (os.path.dirname(os.path.abspath(__file__)), samples))
     out = subprocess.run([sys.executable, "-c", code], check=True, capture_output=True, text=True)
-    draws = json.loads(out.stdout.strip().splitlines()[-1])
-    for z, d in zip(zs, draws):
-        np.testing.assert_array_equal(np.array(d), z["params"])
+    draws = dict(zip(samples, json.loads(out.stdout.strip().splitlines()[-1])))
+    for z in zs:
+        np.testing.assert_array_equal(np.array(draws[z["sample"]]), z["params"])

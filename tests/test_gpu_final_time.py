@@ -7,7 +7,8 @@ build's results at T = 2 (tests/golden/make_final_time.py):
 
 * KH 1024^2, WENO2 + HLL3, RK3, CFL 0.4, periodic (about 23k steps): the
   benchmark configuration itself;
-* KH 256^2 members 7 and 4095 of the 4096-sample FP64 UQ oracle ensemble.
+* KH 256^2 members 7 and 4095 of the 4096-sample FP64 UQ oracle ensemble;
+* KH on the unit cube, 48^3 (1,475 steps), through both 3-D tile shapes.
 
 Kelvin-Helmholtz at T = 2 is chaotic, so a single differing bit in any of
 the steps would show at the end: the tests assert the dt sequence digest
@@ -17,6 +18,7 @@ import numpy as np
 import pytest
 
 import alsvinn_b200 as als
+import alsvinn_b200.initial_data as init
 import final_time as ft
 
 pytestmark = pytest.mark.gpu
@@ -106,3 +108,34 @@ def test_uq_member_dt_sequence_matches_reference():
         U = sim.get_state()[0]
     assert ft.dts_digest(dts) == z["dts_sha256"]
     _check_final(z, U, info["steps"], info["t"])
+
+
+@pytest.mark.parametrize("shape", [1, 0], ids=["z-marching columns", "8x8x4 boxes"])
+def test_kh3d_to_final_time_matches_reference(shape):
+    """3-D KH 48^3 to T = 2 one step at a time with each 3-D tile shape:
+    every dt and the final interior equal to the reference build's (48
+    cells along z are two z-marching segments, 32 + 16)."""
+    z = ft.load("kh3d48")
+    n = z["n"]
+    U0 = init.kelvin_helmholtz(n, z["params"], ft.GHOSTS, ft.GAMMA, dimension=3)
+    assert ft.state_digest(U0) == z["initial_sha256"]
+    with als.Simulator(3, (n, n, n), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), flux=z["flux"],
+                       reconstruction=z["recon"], integrator=z["integrator"], boundary=z["bc"],
+                       gamma=z["gamma"], cfl=z["cfl"], end_time=z["end_time"]) as sim:
+        sim.set_tiles([shape])
+        assert sim.tiles()["shapes"] == [shape]
+        sim.set_state(U0)
+        dts = _step_by_step(sim)
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["status"] == 0
+    assert info["steps"] == z["steps"] and info["t"] == z["t"]
+    np.testing.assert_array_equal(dts[:64], z["dts_head"])
+    np.testing.assert_array_equal(dts[-64:], z["dts_tail"])
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    s = ft.summary3(U, n)
+    # (the z momentum stays zero: its L1 norm is 0 in both, so its block
+    # differences must be 0)
+    diff = np.abs(s["block_sums"] - z["block_sums"]).sum(axis=(1, 2, 3))
+    assert np.all(diff <= L1_TOL * z["l1"]), (diff, z["l1"])
+    assert s["interior_sha256"] == z["interior_sha256"]
