@@ -18,7 +18,9 @@
  * Pointers named *_dev are device pointers; all other arrays are host
  * memory.  Every function returns ALS_OK or a negative ALS_E* code, with
  * als_last_error() describing the failure.  Functions taking a stream
- * enqueue on it and return after the work has completed.
+ * enqueue on it and return after the work has completed.  A handle's calls
+ * share its device workspace: use a handle from one host thread at a time
+ * (separate handles are independent).
  */
 #ifndef ALS_SURROGATE_H
 #define ALS_SURROGATE_H
