@@ -145,6 +145,26 @@ def test_whole_network_kernel_matches_oracle(hidden):
     assert np.abs(y - ref).mean() <= 1e-3 * scale
 
 
+def test_whole_network_inference_waits_for_the_callers_stream():
+    """The inputs are written on the caller's stream after a bounded GPU
+    sleep; the call (two chunks, the second one's inputs packed on the
+    library's side stream) still sees them, on every chunk."""
+    rows = 262144 + 4000
+    gen = torch.Generator(device="cuda:0").manual_seed(5)
+    src = torch.rand((rows, 40), device="cuda:0", generator=gen)
+    with als.Surrogate(seed=9) as s:
+        expect = s.forward_raw(src).cpu().numpy()
+        x = torch.zeros_like(src)
+        side = torch.cuda.Stream(device="cuda:0")
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            torch.cuda._sleep(50_000_000)      # about 25 ms of spinning on the GPU
+            x.copy_(src)
+            y = s.forward_raw(x)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(y.cpu().numpy(), expect)
+
+
 def test_whole_network_kernel_wait_timeout_is_reported_and_the_handle_recovers():
     """Failure detection without a fault: with the layer completions of the
     whole-network kernel withheld, the epilogue's bounded waits run out, the
