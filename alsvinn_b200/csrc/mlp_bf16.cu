@@ -22,10 +22,13 @@ using namespace mlpk;
 
 namespace {
 
-// Rows per inference chunk (a multiple of 128).  Measured on the 2^20-row
-// forward call (the E[f], E[f^2] pass): 65,536 rows 1.84 ms, 262,144 1.39 ms,
-// 1,048,576 1.30 ms; larger chunks amortise each launch's set-up and tail
-// but hold 0.6 KB of BF16 workspace per row on the device.
+// Rows per inference chunk (a multiple of 256).  The per-layer path keeps
+// 0.6 KB of BF16 workspace per chunk row (packed inputs and two activation
+// buffers), the whole-network kernel 0.25 KB (two packed-input buffers).
+// Measured on the 2^20-row forward call through the per-layer path:
+// 65,536 rows 1.84 ms, 262,144 1.39 ms, 1,048,576 1.30 ms; the whole-network
+// kernel takes 0.58 ms with 262,144-row chunks, the packing of each chunk
+// after the first hidden behind the previous one.
 #ifndef ALS_MLP_INFER_CHUNK
 #define ALS_MLP_INFER_CHUNK 262144
 #endif
