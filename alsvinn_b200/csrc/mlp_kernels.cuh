@@ -497,20 +497,22 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
         if (lane == 0) {
             // in the MMA warp's order: per pair, layer and tile, the tile's
             // inputs (first layer) and the layer's weight chunks
-            int it = 0;            // weight chunks issued
-            int nx = 0;            // pairs whose inputs were issued
-            for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x, ++nx) {
+            int it = 0;                // weight chunks issued
+            int nx[2] = {0, 0};        // input tiles issued, per tile of the pair
+            for (int q = blockIdx.x; q < g.pairs && !*abort_v; q += gridDim.x) {
                 for (int l = 0; l < L && !*abort_v; ++l) {
                     for (int s = 0; s < 2 && !*abort_v; ++s) {
                         if (l == 0) {
                             // the previous pair's last MMAs of this tile are done
-                            if (nx > 0 && !mbar_wait(&a_free[s], unsigned((nx - 1) & 1), limit)) {
+                            if (nx[s] > 0 &&
+                                !mbar_wait(&a_free[s], unsigned((nx[s] - 1) & 1), limit)) {
                                 *abort_v = 1;
                                 break;
                             }
                             mbar_expect_tx(&x_full[s], kChunkBytes);
                             tma_load_2d(sA + s * kActBytes, &maps.x, 0, (2 * q + s) * kTileM,
                                         &x_full[s]);
+                            ++nx[s];
                         }
                         for (int c = 0; c < g.nk[l]; ++c, ++it) {
                             const int slot = it % kFusedRing;
@@ -534,9 +536,10 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                     mbar_wait(&b_full[r], unsigned((n - 1) & 1));
                 }
             }
-            if (nx > 0) {
-                mbar_wait(&x_full[0], unsigned((nx - 1) & 1));
-                mbar_wait(&x_full[1], unsigned((nx - 1) & 1));
+            for (int s = 0; s < 2; ++s) {
+                if (nx[s] > 0) {
+                    mbar_wait(&x_full[s], unsigned((nx[s] - 1) & 1));
+                }
             }
         }
     } else if (warp == 1) {
