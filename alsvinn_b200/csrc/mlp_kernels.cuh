@@ -274,6 +274,14 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_forward(const __grid_
                     tma_load_2d(sA + slot * kABytes, &tmA, c * kChunkK, t * kTileM, &a_full[slot]);
                 }
             }
+            // copies still in flight (an aborted run) land before the block exits
+            mbar_wait(&b_full, 0);
+            for (int r = 0; r < kRing; ++r) {
+                const long long n = it > r ? (it - r + kRing - 1) / kRing : 0;
+                if (n > 0) {
+                    mbar_wait(&a_full[r], unsigned((n - 1) & 1));
+                }
+            }
         }
     } else if (warp == 1) {
         if (lane == 0) {
