@@ -14,6 +14,10 @@ path (the plug-in Reconstruction, Boundary and Integrator classes).
   accumulated by the FP64 Welford MeanVariance on the device; the RMS
   errors of mean and variance over the 40 dimensions must fall at rate
   1/2 (at least 0.49).
+* test/library_tests/src/fvm/integrator/ForwardEulerTest.cpp and
+  RungeKutta2Test.cpp: the same system (below); every rate between
+  consecutive resolutions within 0.1 of -1 (N = 2^4 .. 2^14) and within
+  0.05 of -2 (N = 2^6 .. 2^14).
 * test/library_tests/src/fvm/integrator/IntegratorConvergenceTest.cpp:
   du/dt = u, u(0) = 1, integrated to t = 1 with N = 2^6 .. 2^9 constant
   steps through the integrator's stage combinations (the system returns
@@ -103,10 +107,10 @@ INTEGRATORS = [("forwardeuler", 0.9), ("rungekutta2", 1.9), ("rungekutta3", 2.9)
                ("rungekutta4", 3.9)]
 
 
-@pytest.mark.parametrize("name,expected", INTEGRATORS, ids=[i[0] for i in INTEGRATORS])
-def test_integrator_convergence(name, expected):
+def _ode_errors(name, ks):
+    """(log N, log |e - u(1)|) for N = 2 << k, k in ks."""
     errors, resolutions = [], []
-    for k in range(5, 9):
+    for k in ks:
         N = 2 << k
         dt = 1.0 / N
         integ = als.Integrator(name, _ODESystem(dt), cfl=1.0)
@@ -125,7 +129,22 @@ def test_integrator_convergence(name, expected):
         u = float(volumes[0].item())
         errors.append(math.log(abs(math.exp(1.0) - u)))
         resolutions.append(math.log(N))
+    return resolutions, errors
+
+
+@pytest.mark.parametrize("name,expected", INTEGRATORS, ids=[i[0] for i in INTEGRATORS])
+def test_integrator_convergence(name, expected):
+    resolutions, errors = _ode_errors(name, range(5, 9))
     assert _rate(resolutions, errors) >= expected, (name, _rate(resolutions, errors))
+
+
+@pytest.mark.parametrize("name,ks,rate,tol", [("forwardeuler", range(3, 14), -1.0, 0.1),
+                                              ("rungekutta2", range(5, 14), -2.0, 5e-2)],
+                         ids=["ForwardEulerTest", "RungeKutta2Test"])
+def test_integrator_rate_between_resolutions(name, ks, rate, tol):
+    resolutions, errors = _ode_errors(name, ks)
+    slopes = np.diff(errors) / np.diff(resolutions)
+    assert np.all(np.abs(slopes - rate) <= tol), slopes
 
 
 def test_monte_carlo_mean_and_variance_converge_at_rate_one_half():
