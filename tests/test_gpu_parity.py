@@ -172,6 +172,33 @@ def test_plugin_weno2_known_answer():
     assert abs(left[0, 0, 0, 2].item() - expect_l) < 1e-8
 
 
+@pytest.mark.parametrize("recon,value,tol", [("eno2", 0.0, 0.0), ("eno2", 1.0, 0.0),
+                                             ("eno3", 0.0, 0.0), ("eno3", 1.0, 2e-6)],
+                         ids=["ConstantZeroTestSecondOrder", "ConstantOneTestSecondOrder",
+                              "ConstantZeroTestThirdOrder", "ConstantOneTestThirdOrder"])
+def test_plugin_eno_constant_states(recon, value, tol):
+    """EnoTest.cpp:47-220 through the plug-in Reconstruction: a 10 x 10
+    state that is constant everywhere (0, or 1 with energy 10) reconstructs
+    to itself along x on the reference's range (cells g-1 .. N-g along x,
+    the interior rows), exactly for ENO2 and zero, within 2e-6 otherwise."""
+    n = (10, 10)
+    rec = als.Reconstruction(2, n, recon)
+    g = rec.getNumberOfGhostCells()
+    st = np.zeros(padded_shape(2, n, g))
+    if value:
+        st[:3] = value
+        st[3] = 10 * value
+    x = _dev(st)
+    left = torch.zeros_like(x)
+    right = torch.zeros_like(x)
+    rec.performReconstruction(x, 0, left, right)
+    N = n[0] + 2 * g
+    box = (slice(None), 0, slice(g, n[1] + g), slice(g - 1, N - (g - 1)))
+    expect = st[box]
+    assert np.all(np.abs(left.cpu().numpy()[box] - expect) <= tol)
+    assert np.all(np.abs(right.cpu().numpy()[box] - expect) <= tol)
+
+
 @pytest.mark.parametrize("integ", ["forwardeuler", "rungekutta2", "rungekutta3"])
 def test_plugin_time_loop_matches_oracle(c_oracle, integ):
     """Simulator::incrementSolution driven through the plug-in calls only."""
