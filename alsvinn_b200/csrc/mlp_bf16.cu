@@ -497,6 +497,32 @@ int reset_adam(als_mlp* s, cudaStream_t st) {
     return ALS_OK;
 }
 
+// The whole-network path over `rows` rows: chunk i is packed on the side
+// stream into buffer i & 1 while chunk i - 1 runs through the network on
+// the main stream.
+int forward_fused_chunks(als_mlp* s, const float* x_dev, long long rows, float* y_dev,
+                         cudaStream_t st) {
+    const Layer& L0 = s->layers[0];
+    MLP_CUDA(cudaStreamWaitEvent(s->side, s->ev, 0));   // the caller's prior work
+    int i = 0;
+    for (long long r0 = 0; r0 < rows; r0 += kInferChunk, ++i) {
+        const int b = i & 1;
+        const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
+        const long long rp = (n + 2 * kTileM - 1) / (2 * kTileM) * (2 * kTileM);
+        if (i >= 2) {
+            MLP_CUDA(cudaStreamWaitEvent(s->side, s->xi_free[b], 0));
+        }
+        pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, s->side>>>(
+            x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, b ? s->xi2 : s->xi, rp, L0.kpad);
+        MLP_CUDA(cudaGetLastError());
+        MLP_CUDA(cudaEventRecord(s->packed[b], s->side));
+        MLP_CUDA(cudaStreamWaitEvent(st, s->packed[b], 0));
+        MLP_TRY(launch_fused_forward(s, b, rp, n, y_dev + r0, st));
+        MLP_CUDA(cudaEventRecord(s->xi_free[b], st));
+    }
+    return ALS_OK;
+}
+
 // Inference in chunks of kInferChunk rows: the input packing, then the
 // whole-network kernel when it applies and `fused` is set (the packing of
 // the next chunk overlapping the current one), else one launch per layer
@@ -512,24 +538,11 @@ int forward_rows(als_mlp* s, const float* x_dev, long long rows, float* y_dev, v
     const Layer& L0 = s->layers[0];
     const Layer& head = s->layers[s->cfg.hidden];
     if (fused && s->fused) {
-        // chunk i is packed on the side stream into buffer i & 1 while chunk
-        // i - 1 runs through the network on the main stream
-        MLP_CUDA(cudaStreamWaitEvent(s->side, s->ev, 0));   // the caller's prior work
-        int i = 0;
-        for (long long r0 = 0; r0 < rows; r0 += kInferChunk, ++i) {
-            const int b = i & 1;
-            const long long n = rows - r0 < kInferChunk ? rows - r0 : kInferChunk;
-            const long long rp = (n + 2 * kTileM - 1) / (2 * kTileM) * (2 * kTileM);
-            if (i >= 2) {
-                MLP_CUDA(cudaStreamWaitEvent(s->side, s->xi_free[b], 0));
-            }
-            pack_inputs<<<grid_for(rp * (L0.kpad / 8), 256), 256, 0, s->side>>>(
-                x_dev + r0 * s->cfg.inputs, n, s->cfg.inputs, b ? s->xi2 : s->xi, rp, L0.kpad);
-            MLP_CUDA(cudaGetLastError());
-            MLP_CUDA(cudaEventRecord(s->packed[b], s->side));
-            MLP_CUDA(cudaStreamWaitEvent(st, s->packed[b], 0));
-            MLP_TRY(launch_fused_forward(s, b, rp, n, y_dev + r0, st));
-            MLP_CUDA(cudaEventRecord(s->xi_free[b], st));
+        const int rc = forward_fused_chunks(s, x_dev, rows, y_dev, st);
+        if (rc != ALS_OK) {
+            // no packing of the caller's inputs outlives a failed call
+            cudaStreamSynchronize(s->side);
+            return rc;
         }
         return check_error_flag(s);
     }
