@@ -53,7 +53,9 @@ namespace als {
 // slower); so did the per-cell net-flux sums in shared memory (0.390 vs
 // 0.381), a 32x14 tile of 512 threads at 64 registers (0.394) and the x
 // direction done per warp on a row of a 30x17 tile with warp shuffles
-// instead of shared memory and barriers (0.423).  All of
+// instead of shared memory and barriers (0.423); so did one block of 576
+// threads per SM, with registers to spare and no spills (0.384 vs 0.376).
+// All of
 // these are build-time knobs; the FP32 units build with three blocks per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
