@@ -55,8 +55,8 @@ namespace als {
 // direction done per warp on a row of a 30x17 tile with warp shuffles
 // instead of shared memory and barriers (0.423); so did one block of 576
 // threads per SM, with registers to spare and no spills (0.384 vs 0.376).
-// All of
-// these are build-time knobs; the FP32 units build with three blocks per SM.
+// All of these are build-time knobs; the FP32 units build with three blocks
+// per SM.
 #ifndef ALS_TILE2_X
 #define ALS_TILE2_X 32
 #endif
