@@ -1482,7 +1482,7 @@ int orc_set_diffusion(orc_config* cfg, int kind, int recon) {
 
 /* boost::math::legendre_p(int l, double x), which Legendre.cpp:79-81 and
  * LegendrePointWise.cpp:74 call (Boost.Math special_functions/legendre.hpp,
- * not in /root/reference), as that library documents it under its default
+ * not part of the reference's tree), as that library documents it under its default
  * policy: the double argument evaluated in long double (promote_double) and
  * rounded to double once at the end, a negative degree l taken as -l - 1,
  * P_0 = 1, P_1 = x and Bonnet's recurrence
