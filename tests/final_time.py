@@ -20,6 +20,12 @@ GHOSTS = 2
 BLOCK = 16
 CASES = ("uq256_7", "uq256_4095", "kh1024")    # 2-D, initial data as band limits
 CASES3 = ("kh3d48",)                           # 3-D, initial data by the generator
+# KH 256^2 to T = 2 with other schemes: (reconstruction, flux, integrator, ghosts)
+SCHEMES = {"kh256_eno3_hll_rk2": ("eno3", "hll", "rungekutta2", 3),
+           "kh256_mc_hll3_rk3": ("mc", "hll3", "rungekutta3", 2),
+           "kh256_weno3_hll3_rk3": ("weno3", "hll3", "rungekutta3", 3),
+           "kh256_wenof2_hll_rk3": ("wenof2", "hll", "rungekutta3", 2)}
+SCHEME_CASES = tuple(SCHEMES)
 
 
 def fixture_path(name):

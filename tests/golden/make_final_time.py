@@ -15,6 +15,10 @@ alsfvm/src/io/FixedIntervalWriter.cpp:45-53) runs each case to T = 2:
   (about 23k steps; about half an hour on eight host cores);
 * uq256_<s>: KH 256^2 members s = 7 and 4095 of the 4096-sample UQ
   oracle ensemble (parameters = STLMersenne sample s), CFL 0.4;
+* kh256_<scheme>: KH 256^2, parameters = STLMersenne samples 1, 2, 3, 4, CFL 0.4,
+  with the other reconstruction / flux / integrator combinations of
+  tests/final_time.py's SCHEMES (ENO3, MC, WENO3, WENOF2; HLL, HLL3; RK2,
+  RK3);
 * kh3d48: KH on the unit cube, 48^3, parameters = STLMersenne sample 0,
   CFL 0.4 (the 3-D path, whose z-marching tiles cover 48 = 32 + 16 cells
   in two segments).
@@ -39,28 +43,29 @@ CFL = 0.4
 END_TIME = 2.0
 
 
-def run_case(ref, name, n, sample):
+def run_case(ref, name, n, sample, recon="weno2", flux="hll3", integrator="rungekutta3",
+             ghosts=ft.GHOSTS):
     import alsvinn_b200.initial_data as init
     params = np.asarray(ref.stlmersenne(40, sample, 1)[0])
-    U_gen = init.kelvin_helmholtz(n, params, ft.GHOSTS, ft.GAMMA)
-    lo, hi = ft.band_limits_of(U_gen, n)
-    U0 = ft.kh_state_from_bands(n, lo, hi)
+    U_gen = init.kelvin_helmholtz(n, params, ghosts, ft.GAMMA)
+    lo, hi = ft.band_limits_of(U_gen, n, ghosts)
+    U0 = ft.kh_state_from_bands(n, lo, hi, ghosts)
     assert np.array_equal(U0, U_gen), "band reconstruction differs from the generator"
     t0 = time.perf_counter()
-    rc, U, dts, steps, t = ref.simulate(2, (n, n), (0.0, 0.0), (1.0, 1.0), "hll3", "weno2",
-                                        "rungekutta3", "periodic", ft.GAMMA, CFL, END_TIME, U0,
+    rc, U, dts, steps, t = ref.simulate(2, (n, n), (0.0, 0.0), (1.0, 1.0), flux, recon,
+                                        integrator, "periodic", ft.GAMMA, CFL, END_TIME, U0,
                                         dts_capacity=200000)
     seconds = time.perf_counter() - t0
     assert rc == 0, name
     assert len(dts) == steps
-    s = ft.summary(U, n)
-    out = dict(n=n, sample=sample, params=params, band_lo=lo, band_hi=hi, ghosts=ft.GHOSTS,
-               gamma=ft.GAMMA, cfl=CFL, end_time=END_TIME, flux="hll3", recon="weno2",
-               integrator="rungekutta3", bc="periodic", steps=steps, t=t,
+    s = ft.summary(U, n, ghosts)
+    out = dict(n=n, sample=sample, params=params, band_lo=lo, band_hi=hi, ghosts=ghosts,
+               gamma=ft.GAMMA, cfl=CFL, end_time=END_TIME, flux=flux, recon=recon,
+               integrator=integrator, bc="periodic", steps=steps, t=t,
                dts_sha256=ft.dts_digest(dts), dts_head=dts[:64], dts_tail=dts[-64:],
                dts_min=dts.min(), dts_max=dts.max(), l1=s["l1"], sums=s["sums"],
                block_sums=s["block_sums"], interior_sha256=s["interior_sha256"],
-               block=ft.BLOCK, observable=ft.observable(U, n), ref_loop_seconds=seconds,
+               block=ft.BLOCK, observable=ft.observable(U, n, ghosts), ref_loop_seconds=seconds,
                ref_threads=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())))
     np.savez_compressed(ft.fixture_path(name), **out)
     print("%s: %d steps, t=%r, %.1f s, observable %.17g, sha %s"
@@ -104,7 +109,13 @@ def main(which):
         run_case(ref, "kh1024", 1024, 0)
     if "kh3d48" in which:
         run_case_3d(ref, "kh3d48", 48, 0)
+    if "schemes" in which:
+        # samples 1, 2, ... in increasing order: the reference's generator is
+        # one engine per process that only moves forward
+        for i, name in enumerate(ft.SCHEME_CASES):
+            recon, flux, integrator, ghosts = ft.SCHEMES[name]
+            run_case(ref, name, 256, 1 + i, recon, flux, integrator, ghosts)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["uq256", "kh1024", "kh3d48"])
+    main(sys.argv[1:] or ["uq256", "kh1024", "kh3d48", "schemes"])

@@ -17,11 +17,16 @@ import alsvinn_b200.initial_data as init
 import final_time as ft
 
 
-@pytest.mark.parametrize("name", ft.CASES)
+@pytest.mark.parametrize("name", ft.CASES + ft.SCHEME_CASES)
 def test_band_limits_rebuild_the_generator_state(name):
     z = ft.load(name)
     U = init.kelvin_helmholtz(z["n"], z["params"], z["ghosts"], z["gamma"])
-    np.testing.assert_array_equal(ft.kh_state_from_bands(z["n"], z["band_lo"], z["band_hi"]), U)
+    np.testing.assert_array_equal(
+        ft.kh_state_from_bands(z["n"], z["band_lo"], z["band_hi"], z["ghosts"]), U)
+    if name in ft.SCHEMES:
+        recon, flux, integrator, ghosts = ft.SCHEMES[name]
+        assert (z["recon"], z["flux"], z["integrator"], z["ghosts"]) == \
+            (recon, flux, integrator, ghosts)
     assert z["steps"] == len(z["dts_head"]) or z["steps"] > 64
     assert z["t"] == z["end_time"]
 
@@ -52,7 +57,8 @@ def test_parameters_are_the_reference_draws(ref_oracle):
     import json
     import subprocess
     import sys
-    zs = sorted((ft.load(name) for name in ft.CASES + ft.CASES3), key=lambda z: z["sample"])
+    zs = sorted((ft.load(name) for name in ft.CASES + ft.CASES3 + ft.SCHEME_CASES),
+                key=lambda z: z["sample"])
     samples = sorted(set(z["sample"] for z in zs))
     code = ("import json, sys; sys.path.insert(0, %r); from oracle_lib import RefOracle; "
             "r = RefOracle(); print(json.dumps([r.stlmersenne(40, s, 1)[0].tolist() for s in %r]))"

@@ -8,7 +8,9 @@ build's results at T = 2 (tests/golden/make_final_time.py):
 * KH 1024^2, WENO2 + HLL3, RK3, CFL 0.4, periodic (about 23k steps): the
   benchmark configuration itself;
 * KH 256^2 members 7 and 4095 of the 4096-sample FP64 UQ oracle ensemble;
-* KH on the unit cube, 48^3 (1,475 steps), through both 3-D tile shapes.
+* KH on the unit cube, 48^3 (1,475 steps), through both 3-D tile shapes;
+* KH 256^2 with ENO3 + HLL + RK2, MC + HLL3 + RK3, WENO3 + HLL3 + RK3 and
+  WENOF2 + HLL + RK3 (6,166 to 6,765 steps each).
 
 Kelvin-Helmholtz at T = 2 is chaotic, so a single differing bit in any of
 the steps would show at the end: the tests assert the dt sequence digest
@@ -38,7 +40,7 @@ def _check_final(z, U, steps, t):
     n = z["n"]
     assert steps == z["steps"], (steps, z["steps"])
     assert t == z["t"], (t, z["t"])
-    s = ft.summary(U, n)
+    s = ft.summary(U, n, z["ghosts"])
     # relative L1 difference per conserved variable, bounded through the
     # 16 x 16 block sums (sum_b |A_b - B_b| <= sum_cells |a - b|) and the norms
     diff = np.abs(s["block_sums"] - z["block_sums"]).sum(axis=(1, 2))
@@ -106,6 +108,27 @@ def test_uq_member_dt_sequence_matches_reference():
         dts = _step_by_step(sim)
         info = sim.info()
         U = sim.get_state()[0]
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    _check_final(z, U, info["steps"], info["t"])
+
+
+@pytest.mark.parametrize("name", ft.SCHEME_CASES)
+def test_other_schemes_to_final_time_match_reference(name):
+    """KH 256^2 to T = 2 one step at a time with the other reconstruction,
+    flux and integrator combinations: every dt and the final interior
+    equal to the reference build's."""
+    z = ft.load(name)
+    n = z["n"]
+    U0 = ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"], z["ghosts"])
+    with _solver(z) as sim:
+        sim.set_state(U0)
+        dts = _step_by_step(sim)
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["status"] == 0
+    assert len(dts) == z["steps"]
+    np.testing.assert_array_equal(dts[:64], z["dts_head"])
+    np.testing.assert_array_equal(dts[-64:], z["dts_tail"])
     assert ft.dts_digest(dts) == z["dts_sha256"]
     _check_final(z, U, info["steps"], info["t"])
 
