@@ -116,6 +116,33 @@ def summary3(U, n, ghosts=GHOSTS):
             "interior_sha256": hashlib.sha256(I.tobytes()).hexdigest()}
 
 
+# Riemann problems with Neumann boundaries, run to their final time:
+# name: (dimension, n, reconstruction, flux, integrator, ghosts, end time)
+RIEMANN = {"sod2d256_neumann": (2, 256, "weno2", "hll3", "rungekutta3", 2, 0.25),
+           "sod3d32_neumann": (3, 32, "weno2", "hll3", "rungekutta3", 2, 0.2)}
+RIEMANN_CASES = tuple(RIEMANN)
+
+
+def riemann_state(dim, n, ghosts=GHOSTS, gamma=GAMMA):
+    """Sod across the diagonal of the unit square / cube: rho = 1, p = 1
+    where the cell midpoints' coordinates sum to less than dim / 2, else
+    rho = 0.125, p = 0.1; at rest; ghost cells zero (padded planes)."""
+    x = (np.arange(n) + 0.5) / n
+    grids = np.meshgrid(*([x] * dim), indexing="ij")      # axis order z, y, x reversed below
+    total = sum(grids)
+    inside = total < dim / 2.0
+    rho = np.where(inside, 1.0, 0.125)
+    p = np.where(inside, 1.0, 0.1)
+    E = p / (gamma - 1)
+    N = n + 2 * ghosts
+    shape = (dim + 2,) + (1,) * (3 - dim) + (N,) * dim
+    U = np.zeros(shape)
+    inner = (slice(ghosts, ghosts + n),) * dim
+    U[(0,) + (0,) * (3 - dim) + inner] = rho
+    U[(dim + 1,) + (0,) * (3 - dim) + inner] = E
+    return U
+
+
 def state_digest(U):
     return hashlib.sha256(np.ascontiguousarray(U, dtype=np.float64).tobytes()).hexdigest()
 

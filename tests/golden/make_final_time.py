@@ -19,6 +19,9 @@ alsfvm/src/io/FixedIntervalWriter.cpp:45-53) runs each case to T = 2:
   with the other reconstruction / flux / integrator combinations of
   tests/final_time.py's SCHEMES (ENO3, MC, WENO3, WENOF2; HLL, HLL3; RK2,
   RK3);
+* sod2d256_neumann, sod3d32_neumann: Sod across the diagonal of the unit
+  square (256^2, T = 0.25) and cube (32^3, T = 0.2) with Neumann
+  boundaries, WENO2 + HLL3, RK3;
 * kh3d48: KH on the unit cube, 48^3, parameters = STLMersenne sample 0,
   CFL 0.4 (the 3-D path, whose z-marching tiles cover 48 = 32 + 16 cells
   in two segments).
@@ -100,6 +103,32 @@ def run_case_3d(ref, name, n, sample):
                                                   s["interior_sha256"][:16]))
 
 
+def run_case_riemann(ref, name):
+    """A diagonal Sod problem with Neumann boundaries to its final time;
+    the initial state is rebuilt by tests/final_time.py (digest stored)."""
+    dim, n, recon, flux, integrator, ghosts, end_time = ft.RIEMANN[name]
+    U0 = ft.riemann_state(dim, n, ghosts)
+    t0 = time.perf_counter()
+    rc, U, dts, steps, t = ref.simulate(dim, (n,) * dim, (0.0,) * dim, (1.0,) * dim, flux, recon,
+                                        integrator, "neumann", ft.GAMMA, CFL, end_time, U0,
+                                        dts_capacity=200000)
+    seconds = time.perf_counter() - t0
+    assert rc == 0, name
+    assert len(dts) == steps
+    s = ft.summary(U, n, ghosts) if dim == 2 else ft.summary3(U, n, ghosts)
+    out = dict(n=n, dim=dim, sample=-1, initial_sha256=ft.state_digest(U0), ghosts=ghosts,
+               gamma=ft.GAMMA, cfl=CFL, end_time=end_time, flux=flux, recon=recon,
+               integrator=integrator, bc="neumann", steps=steps, t=t,
+               dts_sha256=ft.dts_digest(dts), dts_head=dts[:64], dts_tail=dts[-64:],
+               dts_min=dts.min(), dts_max=dts.max(), l1=s["l1"], sums=s["sums"],
+               block_sums=s["block_sums"], interior_sha256=s["interior_sha256"],
+               block=ft.BLOCK if dim == 2 else ft.BLOCK3, ref_loop_seconds=seconds,
+               ref_threads=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())))
+    np.savez_compressed(ft.fixture_path(name), **out)
+    print("%s: %d steps, t=%r, %.1f s, sha %s" % (name, steps, t, seconds,
+                                                  s["interior_sha256"][:16]))
+
+
 def main(which):
     ref = RefOracle()
     if "uq256" in which:
@@ -109,6 +138,9 @@ def main(which):
         run_case(ref, "kh1024", 1024, 0)
     if "kh3d48" in which:
         run_case_3d(ref, "kh3d48", 48, 0)
+    if "riemann" in which:
+        for name in ft.RIEMANN_CASES:
+            run_case_riemann(ref, name)
     if "schemes" in which:
         # samples 1, 2, ... in increasing order: the reference's generator is
         # one engine per process that only moves forward
@@ -118,4 +150,4 @@ def main(which):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["uq256", "kh1024", "kh3d48", "schemes"])
+    main(sys.argv[1:] or ["uq256", "kh1024", "kh3d48", "schemes", "riemann"])

@@ -31,6 +31,17 @@ def test_band_limits_rebuild_the_generator_state(name):
     assert z["t"] == z["end_time"]
 
 
+@pytest.mark.parametrize("name", ft.RIEMANN_CASES)
+def test_riemann_state_is_the_fixture_initial_state(name):
+    z = ft.load(name)
+    dim, n, recon, flux, integrator, ghosts, end_time = ft.RIEMANN[name]
+    assert (int(z["dim"]), z["n"], z["recon"], z["flux"], z["integrator"], z["ghosts"],
+            z["end_time"], z["bc"]) == (dim, n, recon, flux, integrator, ghosts, end_time,
+                                        "neumann")
+    assert ft.state_digest(ft.riemann_state(dim, n, ghosts)) == z["initial_sha256"]
+    assert z["t"] == z["end_time"]
+
+
 @pytest.mark.parametrize("name", ft.CASES3)
 def test_3d_generator_state_is_the_fixture_initial_state(name):
     z = ft.load(name)

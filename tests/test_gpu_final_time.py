@@ -10,7 +10,8 @@ build's results at T = 2 (tests/golden/make_final_time.py):
 * KH 256^2 members 7 and 4095 of the 4096-sample FP64 UQ oracle ensemble;
 * KH on the unit cube, 48^3 (1,475 steps), through both 3-D tile shapes;
 * KH 256^2 with ENO3 + HLL + RK2, MC + HLL3 + RK3, WENO3 + HLL3 + RK3 and
-  WENOF2 + HLL + RK3 (6,166 to 6,765 steps each).
+  WENOF2 + HLL + RK3 (6,166 to 6,765 steps each);
+* Sod across the diagonal with Neumann boundaries, 2-D 256^2 and 3-D 32^3.
 
 Kelvin-Helmholtz at T = 2 is chaotic, so a single differing bit in any of
 the steps would show at the end: the tests assert the dt sequence digest
@@ -131,6 +132,34 @@ def test_other_schemes_to_final_time_match_reference(name):
     np.testing.assert_array_equal(dts[-64:], z["dts_tail"])
     assert ft.dts_digest(dts) == z["dts_sha256"]
     _check_final(z, U, info["steps"], info["t"])
+
+
+@pytest.mark.parametrize("name", ft.RIEMANN_CASES)
+def test_neumann_riemann_to_final_time_matches_reference(name):
+    """Sod across the diagonal with Neumann boundaries (2-D 256^2 to
+    T = 0.25, 3-D 32^3 to T = 0.2), one step at a time: every dt and the
+    final interior equal to the reference build's."""
+    z = ft.load(name)
+    dim, n, g = int(z["dim"]), z["n"], z["ghosts"]
+    U0 = ft.riemann_state(dim, n, g)
+    assert ft.state_digest(U0) == z["initial_sha256"]
+    with als.Simulator(dim, (n,) * dim, (0.0,) * dim, (1.0,) * dim, flux=z["flux"],
+                       reconstruction=z["recon"], integrator=z["integrator"], boundary=z["bc"],
+                       gamma=z["gamma"], cfl=z["cfl"], end_time=z["end_time"]) as sim:
+        sim.set_state(U0)
+        dts = _step_by_step(sim)
+        info = sim.info()
+        U = sim.get_state()[0]
+    assert info["status"] == 0
+    assert info["steps"] == z["steps"] and info["t"] == z["t"]
+    np.testing.assert_array_equal(dts[:64], z["dts_head"])
+    np.testing.assert_array_equal(dts[-64:], z["dts_tail"])
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    s = ft.summary(U, n, g) if dim == 2 else ft.summary3(U, n, g)
+    axes = tuple(range(1, s["block_sums"].ndim))
+    diff = np.abs(s["block_sums"] - z["block_sums"]).sum(axis=axes)
+    assert np.all(diff <= L1_TOL * z["l1"]), (diff, z["l1"])
+    assert s["interior_sha256"] == z["interior_sha256"]
 
 
 @pytest.mark.parametrize("shape", [1, 0], ids=["z-marching columns", "8x8x4 boxes"])
