@@ -134,6 +134,40 @@ def test_other_schemes_to_final_time_match_reference(name):
     _check_final(z, U, info["steps"], info["t"])
 
 
+@pytest.mark.parametrize("name", ["uq256_7", "kh256_eno3_hll_rk2"])
+def test_plugin_path_to_final_time_matches_reference(name):
+    """The drop-in path itself to T = 2: the reference's time loop
+    (Simulator.cpp:191-214) over the plug-in NumericalFlux, Integrator and
+    Boundary calls, one host round trip per step for dt, as an alsvinn run
+    with this platform selected would drive them.  Every dt and the final
+    interior equal the reference build's."""
+    import torch
+    z = ft.load(name)
+    n, g = z["n"], z["ghosts"]
+    U0 = ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"], g)
+    nf = als.NumericalFlux(2, (n, n), z["flux"], z["recon"], gamma=z["gamma"])
+    bnd = als.Boundary(2, (n, n), nf.getNumberOfGhostCells(), z["bc"])
+    it = als.Integrator(z["integrator"], nf, z["cfl"])
+    first = torch.from_numpy(U0).cuda()
+    vols = [first] + [torch.zeros_like(first) for _ in range(it.getNumberOfSubsteps())]
+    bnd.applyBoundaryConditions(vols[0])
+    cell = [1.0 / n, 1.0 / n, 1.0]
+    t, dts = 0.0, []
+    while t < z["end_time"]:
+        dt = 0.0
+        for s in range(it.getNumberOfSubsteps()):
+            dt = it.performSubstep(vols, cell, dt, vols[s + 1], s, t, z["end_time"])
+            bnd.applyBoundaryConditions(vols[s + 1])
+        vols[0], vols[-1] = vols[-1], vols[0]
+        dts.append(dt)
+        t += dt
+    torch.cuda.synchronize()
+    dts = np.array(dts)
+    assert len(dts) == z["steps"] and t == z["t"]
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    _check_final(z, vols[0].cpu().numpy(), len(dts), t)
+
+
 @pytest.mark.parametrize("name", ft.RIEMANN_CASES)
 def test_neumann_riemann_to_final_time_matches_reference(name):
     """Sod across the diagonal with Neumann boundaries (2-D 256^2 to
