@@ -168,6 +168,31 @@ def test_plugin_path_to_final_time_matches_reference(name):
     _check_final(z, vols[0].cpu().numpy(), len(dts), t)
 
 
+@pytest.mark.parametrize("name,procs", [("uq256_7", (2, 2)), ("kh256_mc_hll3_rk3", (4, 1))])
+def test_split_domain_to_final_time_matches_reference(name, procs):
+    """The grid split into subdomains inside the fused solver (halos written
+    into the neighbours' ghost layers by the stage kernels, the reference's
+    Cartesian decomposition) to T = 2: the same step count and t, and the
+    gathered interior equal to the reference build's undivided run."""
+    import hashlib
+    from alsvinn_b200 import domain
+    z = ft.load(name)
+    n, g = z["n"], z["ghosts"]
+    U0 = ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"], g)
+    split = domain.SplitSimulation(2, (n, n), procs, flux=z["flux"], reconstruction=z["recon"],
+                                   integrator=z["integrator"], boundary=z["bc"],
+                                   gamma=z["gamma"], cfl=z["cfl"], end_time=z["end_time"])
+    try:
+        split.set_state(U0)
+        info = split.run()
+        inner = np.ascontiguousarray(split.interior()[:, 0])
+    finally:
+        split.close()
+    assert info["status"] == 0
+    assert info["steps"] == z["steps"] and info["t"] == z["t"]
+    assert hashlib.sha256(inner.tobytes()).hexdigest() == z["interior_sha256"]
+
+
 @pytest.mark.parametrize("name", ft.RIEMANN_CASES)
 def test_neumann_riemann_to_final_time_matches_reference(name):
     """Sod across the diagonal with Neumann boundaries (2-D 256^2 to
