@@ -193,6 +193,33 @@ def test_split_domain_to_final_time_matches_reference(name, procs):
     assert hashlib.sha256(inner.tobytes()).hexdigest() == z["interior_sha256"]
 
 
+def test_multilevel_batch_to_final_time_matches_reference():
+    """One batched solver over two grid levels (UQ members 7 and 4095 at
+    256^2, the headline KH at 1024^2), one launch per stage over all of
+    them, run to T = 2: every member takes its own reference step count and
+    ends on the reference build's exact bits."""
+    import hashlib
+    names = [["uq256_7", "uq256_4095"], ["kh1024"]]
+    zs = [[ft.load(nm) for nm in level] for level in names]
+    levels = [{"n": (z[0]["n"], z[0]["n"]), "members": len(z)} for z in zs]
+    z0 = zs[0][0]
+    with als.Simulator(2, levels=levels, flux=z0["flux"], reconstruction=z0["recon"],
+                       integrator=z0["integrator"], boundary=z0["bc"], gamma=z0["gamma"],
+                       cfl=z0["cfl"], end_time=z0["end_time"]) as sim:
+        for k, lev in enumerate(sim.levels):
+            sim.set_state(np.stack([ft.kh_state_from_bands(z["n"], z["band_lo"], z["band_hi"])
+                                    for z in zs[k]]), first_member=lev["first"])
+        sim.run()
+        for k, lev in enumerate(sim.levels):
+            out = sim.get_state(lev["first"])
+            for m, z in enumerate(zs[k]):
+                info = sim.info(lev["first"] + m)
+                assert info["status"] == 0
+                assert info["steps"] == z["steps"] and info["t"] == z["t"]
+                inner = ft.interior(out[m], z["n"])
+                assert hashlib.sha256(inner.tobytes()).hexdigest() == z["interior_sha256"]
+
+
 @pytest.mark.parametrize("name", ft.RIEMANN_CASES)
 def test_neumann_riemann_to_final_time_matches_reference(name):
     """Sod across the diagonal with Neumann boundaries (2-D 256^2 to
