@@ -62,6 +62,32 @@ TECNO_CASES = [(1, (32,), "tecno6", "rungekutta3", "periodic"),
                (3, (10, 11, 10), "tecno4", "forwardeuler", "periodic")]
 
 
+@pytest.mark.parametrize("platform", ["b200-all"])
+def test_reference_time_loop_with_b200_classes_to_final_time(ref_b200, platform):
+    """The reference's own loop with all the adapter classes (flux,
+    reconstruction, boundary, integrator) to T = 2 on the KH 256^2 UQ member
+    7 (WENO2 + HLL3 + RK3, 6,330 steps; about 90 s, the adapters exchange
+    host volumes with the device on every call): the dt sequence and the
+    final interior equal the reference's CPU classes' (the committed
+    final-time fixture)."""
+    import hashlib
+    import final_time as ft
+    z = ft.load("uq256_7")
+    n = z["n"]
+    U0 = ft.kh_state_from_bands(n, z["band_lo"], z["band_hi"])
+    ref_b200.set_flux_platform(platform)
+    try:
+        rc, U, dts, steps, t = ref_b200.simulate(2, (n, n), (0.0, 0.0), (1.0, 1.0), z["flux"],
+                                                 z["recon"], z["integrator"], z["bc"], z["gamma"],
+                                                 z["cfl"], z["end_time"], U0)
+    finally:
+        ref_b200.set_flux_platform("cpu")
+    assert rc == 0
+    assert steps == z["steps"] and t == z["t"]
+    assert ft.dts_digest(dts) == z["dts_sha256"]
+    assert hashlib.sha256(ft.interior(U, n).tobytes()).hexdigest() == z["interior_sha256"]
+
+
 @pytest.mark.parametrize("platform", ["b200", "b200-all"])
 @pytest.mark.parametrize("dim,n,flux,integ,bc", TECNO_CASES,
                          ids=["d%d-%s-%s-%s" % (c[0], c[2], c[3], c[4]) for c in TECNO_CASES])
