@@ -639,54 +639,53 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                         // 16 columns at a time; the next 16 are read from TMEM
                         // while these are computed
                         uint32_t r[2][16];
+                        const int sw = (row & 7) << 4;        // this row's 16-byte unit swizzle
+                        unsigned char* chunk = arow + cg * kChunkBytes;
                         tmem_load16_start(lane_base + uint32_t(cg * 64), r[0]);
+                        if (!last) {
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            tmem_load_wait(r[j & 1]);
-                            if (j < 3) {
-                                tmem_load16_start(lane_base + uint32_t(cg * 64 + 16 * (j + 1)),
-                                                  r[(j + 1) & 1]);
-                            }
-                            const int c0 = cg * 64 + 16 * j;
-                            __align__(16) float b[16];
-#pragma unroll
-                            for (int i = 0; i < 4; ++i) {
-                                reinterpret_cast<float4*>(b)[i] =
-                                    reinterpret_cast<const float4*>(bias + c0)[i];
-                            }
-                            // pairs of columns: half pre-activation, GELU and BF16
-                            // rounding (each element as the scalar operations
-                            // round it)
-                            __nv_bfloat162 hb[8];
-#pragma unroll
-                            for (int i = 0; i < 8; ++i) {
-                                const float2 acc = make_float2(__uint_as_float(r[j & 1][2 * i]),
-                                                               __uint_as_float(r[j & 1][2 * i + 1]));
-                                const float2 hz = __ffma2_rn(make_float2(0.5f, 0.5f), acc,
-                                                             reinterpret_cast<const float2*>(b)[i]);
-                                const float2 h = gelu_half2(hz);
-                                hb[i] = __floats2bfloat162_rn(h.x, h.y);
-                            }
-                            if (!last) {
-                                // next layer's K chunk c0 / 64, 16-byte units u0 and
-                                // u0 + 1, swizzled by the row within its atom
-                                unsigned char* chunk = arow + (c0 >> 6) * kChunkBytes;
-                                const int u0 = (c0 & 63) >> 3;
-                                *reinterpret_cast<uint4*>(chunk + ((u0 ^ (row & 7)) << 4)) =
-                                    reinterpret_cast<const uint4*>(hb)[0];
-                                *reinterpret_cast<uint4*>(chunk + (((u0 + 1) ^ (row & 7)) << 4)) =
-                                    reinterpret_cast<const uint4*>(hb)[1];
-                            } else {
-                                __align__(16) float w[16];
-#pragma unroll
-                                for (int i = 0; i < 4; ++i) {
-                                    reinterpret_cast<float4*>(w)[i] =
-                                        reinterpret_cast<const float4*>(head_w + c0)[i];
+                            for (int j = 0; j < 4; ++j) {
+                                tmem_load_wait(r[j & 1]);
+                                if (j < 3) {
+                                    tmem_load16_start(lane_base + uint32_t(cg * 64 + 16 * (j + 1)),
+                                                      r[(j + 1) & 1]);
                                 }
+                                const float* bj = bias + cg * 64 + 16 * j;
+                                __nv_bfloat162 hb[8];
 #pragma unroll
                                 for (int i = 0; i < 8; ++i) {
-                                    hsum2 = __ffma2_rn(__bfloat1622float2(hb[i]),
-                                                       reinterpret_cast<const float2*>(w)[i], hsum2);
+                                    const float2 acc = make_float2(__uint_as_float(r[j & 1][2 * i]),
+                                                                   __uint_as_float(r[j & 1][2 * i + 1]));
+                                    const float2 hz = __ffma2_rn(make_float2(0.5f, 0.5f), acc,
+                                                                 reinterpret_cast<const float2*>(bj)[i]);
+                                    const float2 h = gelu_half2(hz);
+                                    hb[i] = __floats2bfloat162_rn(h.x, h.y);
+                                }
+                                *reinterpret_cast<uint4*>(chunk + (((2 * j) << 4) ^ sw)) =
+                                    reinterpret_cast<const uint4*>(hb)[0];
+                                *reinterpret_cast<uint4*>(chunk + (((2 * j + 1) << 4) ^ sw)) =
+                                    reinterpret_cast<const uint4*>(hb)[1];
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                tmem_load_wait(r[j & 1]);
+                                if (j < 3) {
+                                    tmem_load16_start(lane_base + uint32_t(cg * 64 + 16 * (j + 1)),
+                                                      r[(j + 1) & 1]);
+                                }
+                                const float* bj = bias + cg * 64 + 16 * j;
+                                const float* wj = head_w + cg * 64 + 16 * j;
+#pragma unroll
+                                for (int i = 0; i < 8; ++i) {
+                                    const float2 acc = make_float2(__uint_as_float(r[j & 1][2 * i]),
+                                                                   __uint_as_float(r[j & 1][2 * i + 1]));
+                                    const float2 hz = __ffma2_rn(make_float2(0.5f, 0.5f), acc,
+                                                                 reinterpret_cast<const float2*>(bj)[i]);
+                                    const float2 h = gelu_half2(hz);
+                                    const __nv_bfloat162 hb = __floats2bfloat162_rn(h.x, h.y);
+                                    hsum2 = __ffma2_rn(__bfloat1622float2(hb),
+                                                       reinterpret_cast<const float2*>(wj)[i], hsum2);
                                 }
                             }
                         }
