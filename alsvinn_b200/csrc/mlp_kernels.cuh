@@ -642,7 +642,11 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                         const int sw = (row & 7) << 4;        // this row's 16-byte unit swizzle
                         unsigned char* chunk = arow + cg * kChunkBytes;
                         tmem_load16_start(lane_base + uint32_t(cg * 64), r[0]);
+                        // pairs of columns: half pre-activation, GELU and BF16
+                        // rounding (each element as the scalar operations round it)
                         if (!last) {
+                            // into the next layer's K chunk cg: 16-byte units 2j
+                            // and 2j + 1 of this row, swizzled within its 8-row atom
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 tmem_load_wait(r[j & 1]);
@@ -667,6 +671,8 @@ __global__ void __launch_bounds__(kTmaThreads) mlp_forward_fused(const __grid_co
                                     reinterpret_cast<const uint4*>(hb)[1];
                             }
                         } else {
+                            // the 256 -> 1 head: the rounded activations times the
+                            // head's weights, even and odd columns summed apart
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 tmem_load_wait(r[j & 1]);
